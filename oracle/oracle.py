@@ -1,0 +1,193 @@
+"""ORACLE — test infrastructure, not product code.
+
+Python access to the two checkers of the NISE propagation path:
+  * the reference programs compiled from their own sources (oracle/_ref/NISE_acc,
+    NISE_fast, 2DFFT; recipe in oracle/Makefile), run on keyword files, and
+  * the C restatement nise_oracle.c in FP32 (reference arithmetic) and FP64.
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+TECHNIQUES = {"Absorption": 0, "2DIR": 1, "GBIR": 2, "SEIR": 3, "EAIR": 4, "noEAIR": 5}
+ICM2IFS = np.float32(2.99792458e-5)
+TWOPI = np.float32(2 * 3.14159265359)
+
+
+class OracleParams(ctypes.Structure):
+    _fields_ = [
+        ("singles", ctypes.c_int), ("doubles", ctypes.c_int),
+        ("length", ctypes.c_int), ("sample", ctypes.c_int), ("begin", ctypes.c_int), ("end", ctypes.c_int),
+        ("tmax1", ctypes.c_int), ("tmax2", ctypes.c_int), ("tmax3", ctypes.c_int),
+        ("deltat", ctypes.c_float), ("ts", ctypes.c_int),
+        ("lifetime", ctypes.c_float), ("homogen", ctypes.c_float), ("inhomogen", ctypes.c_float),
+        ("window", ctypes.c_int), ("fft", ctypes.c_int),
+        ("thres", ctypes.c_float), ("couplingcut", ctypes.c_float), ("anharmonicity", ctypes.c_float),
+        ("min1", ctypes.c_float), ("max1", ctypes.c_float), ("min2", ctypes.c_float),
+        ("max2", ctypes.c_float), ("min3", ctypes.c_float), ("max3", ctypes.c_float),
+        ("ham_coupling", ctypes.c_int), ("propagation", ctypes.c_int), ("technique", ctypes.c_int),
+        ("energy", ctypes.c_char * 256), ("dipole", ctypes.c_char * 256), ("coupling", ctypes.c_char * 256),
+        ("anharm", ctypes.c_char * 256), ("overtone", ctypes.c_char * 256), ("shift", ctypes.c_char * 256),
+    ]
+
+
+def params(keywords, files):
+    """Oracle parameters from a keyword dict (readinput.c:24-289 semantics for
+    the keywords on the path) and the trajectory file dict."""
+    kw = {k: str(v) for k, v in keywords.items()}
+    p = OracleParams()
+    p.ts = 5
+    p.tmax1, p.tmax2, p.tmax3 = 256, 0, 256
+    p.singles = int(kw.get("Singles", 0))
+    p.doubles = int(kw.get("Doubles", 0))
+    p.length = int(kw["Length"])
+    p.sample = int(kw["Samplerate"])
+    p.begin = int(kw.get("BeginPoint", 0))
+    p.end = int(kw.get("EndPoint", 0))
+    if "RunTimes" in kw:
+        p.tmax1, p.tmax2, p.tmax3 = (int(x) for x in kw["RunTimes"].split()[:3])
+    p.deltat = float(kw["Timestep"])
+    p.ts = int(kw.get("Trotter", 5))
+    p.lifetime = float(kw.get("Lifetime", 0))
+    p.homogen = float(kw.get("Homogeneous", 0))
+    p.inhomogen = float(kw.get("Inhomogeneous", 0))
+    p.window = 1 if kw.get("Window", "") == "Hann" else 0
+    p.fft = int(kw.get("FFT", 0))
+    p.couplingcut = float(kw.get("Couplingcut", 0))
+    p.anharmonicity = float(kw.get("Anharmonicity", 0))
+    mins = [float(x) for x in kw.get("MinFrequencies", "0 0 0").split()[:3]]
+    maxs = [float(x) for x in kw.get("MaxFrequencies", "0 0 0").split()[:3]]
+    p.min1, p.min2, p.min3 = mins
+    p.max1, p.max2, p.max3 = maxs
+    p.ham_coupling = 1 if kw.get("HamiltonianType", "Full") == "Coupling" else 0
+    prop = kw.get("Propagation", "")
+    p.propagation = {"Coupling": 1, "Diagonal": 2, "RK4": 3}.get(prop, 0)
+    p.technique = TECHNIQUES[kw.get("Technique", "Absorption")]
+    if p.technique != 0:
+        p.tmax3 = p.tmax1  # readinput.c:212
+    thres = np.float32(float(kw.get("Threshold", 0)))
+    if p.propagation == 0:  # readinput.c:264-267, in float arithmetic
+        s = np.float32(np.float32(np.float32(p.deltat) * ICM2IFS) * TWOPI) / np.float32(p.ts)
+        thres = np.float32(thres * np.float32(s * s))
+    p.thres = float(thres)
+    for key in ("energy", "dipole", "coupling", "anharm", "overtone", "shift"):
+        setattr(p, key, (files.get(key) or "").encode())
+    return p
+
+
+_libs = {}
+
+
+def lib(prec="f64"):
+    if prec not in _libs:
+        path = os.path.join(REF_DIR, "liboracle_%s.so" % prec)
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        P = ctypes.POINTER(OracleParams)
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.oracle_absorption.argtypes = [P, dp, dp, ctypes.POINTER(ctypes.c_int)]
+        L.oracle_2dir.argtypes = [P, dp, ctypes.POINTER(ctypes.c_int)]
+        L.oracle_1dfft.argtypes = [P, dp, dp, ctypes.c_int, dp, dp, dp, ctypes.c_int]
+        L.oracle_print2d_normalize.argtypes = [P, dp, dp, ctypes.c_int]
+        fp = ctypes.POINTER(ctypes.c_float)
+        L.oracle_propagate_vector.argtypes = [P, fp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.oracle_propagate_doubles.argtypes = [P, fp, ctypes.c_void_p, ctypes.c_void_p, fp]
+        L.oracle_propagate_t2.argtypes = [P, fp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.oracle_dipole_double.argtypes = [P, fp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p, fp]
+        L.oracle_dipole_double_last.argtypes = L.oracle_dipole_double.argtypes
+        L.oracle_eigh.argtypes = [ctypes.c_int, dp, dp, dp]
+        _libs[prec] = L
+    return _libs[prec]
+
+
+def build(ref=True):
+    """Compile the restatement and, when the reference sources are present, the reference."""
+    targets = ["oracle"]
+    if ref and os.path.isdir("/root/reference/src"):
+        targets.append("ref")
+    subprocess.run(["make", "-s"] + targets, cwd=HERE, check=True)
+
+
+def _ptr(a, t=ctypes.c_double):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def absorption(p, prec="f64"):
+    """Raw response sums and the normaliser (absorption.c:92-192)."""
+    re = np.zeros(p.tmax1)
+    im = np.zeros(p.tmax1)
+    n = ctypes.c_int(0)
+    rc = lib(prec).oracle_absorption(ctypes.byref(p), _ptr(re), _ptr(im), ctypes.byref(n))
+    if rc != 0:
+        raise RuntimeError("oracle_absorption failed (%d)" % rc)
+    return re, im, n.value
+
+
+def spectrum(p, re, im, samples, prec="f64"):
+    fft = max(p.fft, p.tmax1)
+    w = np.zeros(fft)
+    sr = np.zeros(fft)
+    si = np.zeros(fft)
+    rows = lib(prec).oracle_1dfft(ctypes.byref(p), _ptr(np.ascontiguousarray(re, dtype=np.float64)),
+                                  _ptr(np.ascontiguousarray(im, dtype=np.float64)), samples, _ptr(w), _ptr(sr),
+                                  _ptr(si), fft)
+    return w[:rows], sr[:rows], si[:rows]
+
+
+def twodir(p, prec="f64"):
+    """Raw 12 x tmax3 x tmax1 response sums and the sample count."""
+    R = np.zeros((12, p.tmax3, p.tmax1))
+    n = ctypes.c_int(0)
+    rc = lib(prec).oracle_2dir(ctypes.byref(p), _ptr(R), ctypes.byref(n))
+    if rc != 0:
+        raise RuntimeError("oracle_2dir failed (%d)" % rc)
+    return R, n.value
+
+
+def normalize_2d(p, R, count, prec="f64"):
+    out = R.copy()
+    for k in range(0, 12, 2):
+        re = np.ascontiguousarray(out[k])
+        im = np.ascontiguousarray(out[k + 1])
+        lib(prec).oracle_print2d_normalize(ctypes.byref(p), _ptr(re), _ptr(im), count)
+        out[k], out[k + 1] = re, im
+    return out
+
+
+# ------------------------------------------------------------ reference binary
+def run_reference(input_path, workdir, binary="NISE_acc", threads=1, timeout=3600):
+    exe = os.path.join(REF_DIR, binary)
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    r = subprocess.run([exe, os.path.abspath(input_path)], cwd=workdir, env=env, stdout=subprocess.PIPE,
+                       stderr=subprocess.STDOUT, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError("reference failed (%d):\n%s" % (r.returncode, r.stdout[-2000:]))
+    return r.stdout
+
+
+def read_td_absorption(path):
+    a = np.loadtxt(path, ndmin=2)
+    return a[:, 0], a[:, 1], a[:, 2]
+
+
+def read_spectrum(path):
+    a = np.loadtxt(path, ndmin=2)
+    return a[:, 0], a[:, 1], a[:, 2]
+
+
+def read_2d(path, tmax1, tmax3):
+    a = np.loadtxt(path, ndmin=2)
+    re = a[:, 3].reshape(tmax1, tmax3).T
+    im = a[:, 4].reshape(tmax1, tmax3).T
+    return re, im
+
+
+R2D_FILES = ["RparI.dat", "RparII.dat", "RperI.dat", "RperII.dat", "RcroI.dat", "RcroII.dat"]
