@@ -1,0 +1,169 @@
+/*
+ * nise_b200 — C ABI of the B200 engine for the NISE wavefunction-propagation
+ * path (linear absorption and 2DIR).  Plain C types only; the caller owns
+ * every output buffer; every entry returns an int status (NISE_OK == 0) and
+ * never exits the process.  One context per host thread; all device work of a
+ * context runs on a stream the context owns.
+ *
+ * Reference interfaces replaced (GHlacour/NISE_2017, src/):
+ *   nise_params            <- t_non (types.h:37-90), the fields on this path
+ *   nise_params_default    <- defaults in readInput (readinput.c:24-44)
+ *   nise_read_input        <- readInput (readinput.c:13-289)
+ *   nise_load_files        <- open_files/read_coupling/read_shift and the
+ *                             fseek+fread frame readers (read_trajectory.c:15-457,
+ *                             hamshift.c:13-47), as one bulk load into HBM
+ *   nise_set_trajectory    <- the same, from record images already in host memory
+ *   nise_absorption        <- absorption() (absorption.c:18-202), the response part
+ *   nise_absorption_fft    <- do_1DFFT() (1DFFT.c:144-228)
+ *   nise_2dir              <- calc_2DIR() (calc_2DIR.c:22-629), one GPU instead of MPI ranks
+ *   nise_propagate         <- propagate_vector() (propagate.c:20-39), batched
+ *   nise_propagate_doubles <- propagate_vec_coupling_S_doubles / _RK4_doubles /
+ *                             propagate_double_sparce (propagate.c:376-1394)
+ *   nise_write_*           <- the output writers (absorption.c:181-189,
+ *                             1DFFT.c:208-228, print2D in MPI_subs.c:20-34)
+ */
+#ifndef NISE_B200_H
+#define NISE_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NISE_B200_ABI_VERSION 1
+
+/* Status codes. */
+#define NISE_OK 0
+#define NISE_ERR_ARG (-1)         /* invalid argument or keyword value */
+#define NISE_ERR_IO (-2)          /* file missing or trajectory too short */
+#define NISE_ERR_SHAPE (-3)       /* sizes inconsistent with the parameters */
+#define NISE_ERR_DEVICE (-4)      /* CUDA error (message in nise_last_error) */
+#define NISE_ERR_TIMEOUT (-5)     /* a bounded device wait gave up */
+#define NISE_ERR_UNSUPPORTED (-6) /* combination not implemented */
+#define NISE_ERR_NOMEM (-7)       /* host or device allocation failed */
+#define NISE_ERR_STATE (-8)       /* call order (e.g. no trajectory loaded) */
+
+/* Propagation keyword (readinput.c:236-254).  Any string other than
+ * Coupling/Diagonal/RK4 selects SPARSE, as in the reference. */
+enum { NISE_PROP_SPARSE = 0, NISE_PROP_COUPLING = 1, NISE_PROP_DIAGONAL = 2, NISE_PROP_RK4 = 3 };
+/* HamiltonianType keyword. */
+enum { NISE_HAM_FULL = 0, NISE_HAM_COUPLING = 1 };
+/* Technique keyword (techniques on this path). */
+enum {
+    NISE_TECH_ABSORPTION = 0,
+    NISE_TECH_2DIR = 1,
+    NISE_TECH_GBIR = 2,
+    NISE_TECH_SEIR = 3,
+    NISE_TECH_EAIR = 4,
+    NISE_TECH_NOEAIR = 5,
+    NISE_TECH_OTHER = 99
+};
+/* Arithmetic of the propagation.  FP32 reproduces the reference's single
+ * precision operations (same formulas and order, no fused multiply-add) and
+ * accumulates responses in FP64; FP64 propagates in double precision. */
+enum { NISE_FP32 = 0, NISE_FP64 = 1 };
+/* Launch mode: BATCHED runs every start point and polarisation of the job in
+ * one launch; PLAIN launches one start point (three polarisations) at a time,
+ * the structure of the reference's sample loop. */
+enum { NISE_BATCHED = 0, NISE_PLAIN = 1 };
+
+typedef struct {
+    /* t_non fields on the path (types.h:37-90), keyword names in comments */
+    int singles, doubles;          /* Singles, Doubles */
+    int length, sample;            /* Length, Samplerate */
+    int begin, end;                /* BeginPoint, EndPoint (0 = all samples) */
+    int tmax1, tmax2, tmax3;       /* RunTimes */
+    float deltat;                  /* Timestep (fs) */
+    int ts;                        /* Trotter */
+    float lifetime, homogen, inhomogen; /* Lifetime, Homogeneous, Inhomogeneous (fs) */
+    int window;                    /* Window: 0 none, 1 Hann */
+    int fft;                       /* FFT */
+    float thres;                   /* Threshold as written (scaled internally, readinput.c:264-267) */
+    float couplingcut;             /* Couplingcut (cm^-1) */
+    float anharmonicity;           /* Anharmonicity (0: read Anharmonicfile/Overtonedipolefile) */
+    float min1, max1, min2, max2, min3, max3; /* MinFrequencies, MaxFrequencies */
+    int hamiltonian;               /* HamiltonianType: NISE_HAM_* */
+    int propagation;               /* Propagation: NISE_PROP_* */
+    int technique;                 /* Technique: NISE_TECH_* */
+    char technique_name[64];       /* Technique string as written */
+    char energyFName[256];         /* Hamiltonianfile */
+    char dipoleFName[256];         /* Dipolefile */
+    char couplingFName[256];       /* Couplingfile */
+    char anharFName[256];          /* Anharmonicfile */
+    char overdipFName[256];        /* Overtonedipolefile */
+    char singleShiftFName[256];    /* SingleShiftfile */
+    /* engine controls (no reference counterpart) */
+    int precision;                 /* NISE_FP32 or NISE_FP64 */
+    int launch_mode;               /* NISE_BATCHED or NISE_PLAIN */
+    int device;                    /* CUDA device ordinal */
+} nise_params;
+
+typedef struct nise_ctx nise_ctx;
+
+/* Defaults of readInput (readinput.c:24-44) plus engine controls. */
+int nise_params_default(nise_params *p);
+/* Parse a NISE keyword file with readInput's matching rules (first token
+ * compared by strncmp over its own length; last occurrence wins; unknown
+ * lines ignored).  Applies the post-parse rules on this path: tmax3 = tmax1
+ * for 2D techniques, length checks.  Diagonal is accepted (the reference
+ * exits on it).  Returns NISE_ERR_IO if the file is missing. */
+int nise_read_input(const char *path, nise_params *p);
+
+int nise_create(const nise_params *p, nise_ctx **out);
+void nise_destroy(nise_ctx *ctx);
+/* Message of the last failed call on this context ("" if none). */
+const char *nise_last_error(const nise_ctx *ctx);
+/* Message of the last failed call that had no context (nise_create etc.). */
+const char *nise_global_error(void);
+
+/* Read the files named in the parameters (binary layouts of
+ * read_trajectory.c) and copy every record to device memory once. */
+int nise_load_files(nise_ctx *ctx);
+/* Same from caller memory: byte images of the files (records with their
+ * int32 tags).  coupling is required for HamiltonianType Coupling;
+ * anharm/overtone when Anharmonicity is 0 on a 2D technique; others NULL. */
+int nise_set_trajectory(nise_ctx *ctx, const void *energy, size_t energy_bytes, const void *dipole,
+                        size_t dipole_bytes, const void *coupling, size_t coupling_bytes, const void *anharm,
+                        size_t anharm_bytes, const void *overtone, size_t overtone_bytes);
+/* SingleShiftfile contents: H_ii <- H_ii * a + b (hamshift.c:59-66); n = 0 clears. */
+int nise_set_singleshift(nise_ctx *ctx, int n, const int *sites, const float *a, const float *b);
+
+/* Linear absorption response (absorption.c:92-154): raw sums over samples
+ * and polarisations, re_S/im_S of length tmax1, and the normaliser (end). */
+int nise_absorption(nise_ctx *ctx, double *re_S, double *im_S, int *samples);
+/* 1D spectrum of a response (1DFFT.c:144-228), FFT on the device.  Writes
+ * up to max_rows rows (frequency cm^-1, Re, Im) in the reference's order. */
+int nise_absorption_fft(nise_ctx *ctx, const double *re_S, const double *im_S, int samples, double *freq,
+                        double *spec_re, double *spec_im, int max_rows, int *rows);
+
+/* 2DIR family (calc_2DIR.c:22-629): raw sums of the 12 response arrays,
+ * R[12][tmax3][tmax1] in the order rrIpar riIpar rrIIpar riIIpar rrIper
+ * riIper rrIIper riIIper rrIcro riIcro rrIIcro riIIcro, and the sample
+ * count print2D divides by. */
+int nise_2dir(nise_ctx *ctx, double *R, int *sample_count);
+
+/* Batched propagate_vector: nvec vectors (rows of re/im, float for FP32 or
+ * double for FP64 contexts), vector v propagated one step with the packed,
+ * already shifted Hamiltonian H + v*N(N+1)/2, sign +1 or -1. */
+int nise_propagate(nise_ctx *ctx, const float *H, void *re, void *im, int nvec, int sign);
+/* Batched doubles propagation (propagate_double_2DIR_control's per-vector
+ * step) for vectors of length N(N+1)/2; anh is per-site (or NULL). */
+int nise_propagate_doubles(nise_ctx *ctx, const float *H, void *re, void *im, int nvec, const float *anh);
+
+/* Output files in the reference's text formats. */
+int nise_write_td_absorption(const char *path, const nise_params *p, const double *re_S, const double *im_S,
+                             int samples);
+int nise_write_spectrum(const char *path, const double *freq, const double *spec_re, const double *spec_im,
+                        int rows);
+/* print2D: divides by sample_count, halves the t3 = 0 row, writes t1 t2 t3 Re Im. */
+int nise_write_2d(const char *path, const nise_params *p, const double *re, const double *im, int sample_count);
+
+/* Device time of the kernels of the last compute call (ms), and how many of
+ * this library's kernels it launched. */
+int nise_last_timing(const nise_ctx *ctx, double *kernel_ms, long *launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

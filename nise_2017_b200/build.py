@@ -21,7 +21,9 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = [
-    "engine.cu",
+    "absorption.cu",
+    "fft.cu",
+    "twodir.cu",
 ]
 CPP_SOURCES = [
     "api.cpp",
@@ -72,8 +74,7 @@ def build_engine(force=False, verbose_ptxas=False):
     common = ["-O3", "-std=c++17", "-I" + INCLUDE, "-I" + CSRC, "-Xcompiler", "-fPIC"]
     for s in CU_SOURCES:
         o = os.path.join(objdir, s + ".o")
-        cmd = [NVCC] + ARCH + common + ["-lineinfo", "--use_fast_math" if False else "-DNISE_ACCURATE",
-                                        "-c", os.path.join(CSRC, s), "-o", o]
+        cmd = [NVCC] + ARCH + common + ["-lineinfo", "-c", os.path.join(CSRC, s), "-o", o]
         if verbose_ptxas:
             cmd.insert(1, "-Xptxas=-v")
         _run(cmd)

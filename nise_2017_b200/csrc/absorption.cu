@@ -1,0 +1,839 @@
+// Linear-absorption kernels: per-frame coefficient preparation, the three
+// singles propagation schemes applied to every start point and polarisation
+// of a job, and the deterministic response reduction.
+//
+// Work decomposition.  A job is the set of vectors v = 3*(s-begin)+x: start
+// point s (frame ti = s*Samplerate) and dipole component x.  Each vector runs
+// the sample loop of absorption.c:119-145: S[t1] += mu(ti+t1).psi, then psi
+// <- U(ti+t1) psi, for t1 < tmax (the step after the last response is not
+// taken; it cannot change any output).  The Trotter and RK4 schemes are
+// sequential inside a vector (each rotation/update reads the previous one),
+// so a thread owns a vector and keeps it in shared memory, interleaved by
+// lane ([site][lane]) so a warp's accesses to one site are conflict-free.
+// Per-frame coefficients (phases, rotation cos/sin, RK4 values) are computed
+// once per frame by a preparation kernel and read by every vector that
+// crosses the frame.  The sparse Taylor scheme is a sparse-matrix product per
+// Taylor order: a CTA owns G vectors and spreads the sites over its threads.
+#include <cstdio>
+
+#include "common.cuh"
+#include "engine.h"
+
+namespace {
+
+template <typename R> struct Cst;
+template <> struct Cst<float> {
+    static __device__ __forceinline__ float2 rot(float j, float fsub, float cut) {
+        // propagate.c:853 (list keeps |J| > cut), :880-882
+        if (!(fabsf(j) > cut)) return make_float2(1.0f, 0.0f);
+        float J = __fmul_rn(j, fsub);
+        float si = (float)(-sin((double)J));
+        float co = sqrtf(__fsub_rn(1.0f, __fmul_rn(si, si)));
+        return make_float2(co, si);
+    }
+};
+template <> struct Cst<double> {
+    static __device__ __forceinline__ double2 rot(float j, double fsub, float cut) {
+        if (!(fabsf(j) > cut)) return make_double2(1.0, 0.0);
+        double J = (double)j * fsub;
+        double si = -sin(J);
+        return make_double2(sqrt(1.0 - si * si), si);
+    }
+};
+
+// ------------------------------------------------------------ Trotter
+template <typename R>
+__global__ void k_prep_trotter(DevTraj T, TrotterPlan P, R fsub) {
+    typedef typename Vec2<R>::T R2;
+    long per = P.n + (P.rot_static ? 0 : P.k);
+    long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (tid >= P.nf * per) return;
+    long fi = tid / per;
+    int e = (int)(tid % per);
+    long t = P.f0 + fi;
+    if (e < P.n) {
+        float h = traj_diag(T, t, e, P.singleshift != 0);
+        double arg = 0.5 * (double)h * (double)fsub;  // cos(0.5 * H0[a] * f), propagate.c:864
+        R2 u;
+        u.x = (R)cos(arg);
+        u.y = (R)(-sin(arg));
+        ((R2 *)P.U)[fi * P.n + e] = u;
+    } else {
+        int k = e - P.n;
+        int2 ab = P.pairs[k];
+        ((R2 *)P.rot)[fi * P.k + k] = Cst<R>::rot(traj_coupling(T, t, ab.x, ab.y), fsub, T.cut);
+    }
+}
+
+template <typename R>
+__global__ void k_prep_trotter_static(DevTraj T, TrotterPlan P, R fsub) {
+    typedef typename Vec2<R>::T R2;
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= P.k) return;
+    int2 ab = P.pairs[k];
+    ((R2 *)P.rot)[k] = Cst<R>::rot(traj_coupling(T, 0, ab.x, ab.y), fsub, T.cut);
+}
+
+// One Trotter step (m sub-steps) of the vector held in column `lane` of S.
+template <typename R>
+__device__ __forceinline__ void trotter_step(typename Vec2<R>::T *S, int B, int lane, int n, int K,
+                                             const int2 *__restrict__ pairs,
+                                             const typename Vec2<R>::T *__restrict__ Uf,
+                                             const typename Vec2<R>::T *__restrict__ Rf, int m) {
+    typedef typename Vec2<R>::T R2;
+    typedef Ar<R> A;
+    for (int sub = 0; sub < m; sub++) {
+        for (int a = 0; a < n; a++) {  // propagate.c:870-873
+            R2 z = S[a * B + lane], u = Uf[a], o;
+            o.x = A::sub(A::mul(z.x, u.x), A::mul(z.y, u.y));
+            o.y = A::add(A::mul(z.y, u.x), A::mul(z.x, u.y));
+            S[a * B + lane] = o;
+        }
+        for (int k = 0; k < K; k++) {  // propagate.c:876-888
+            int2 ab = pairs[k];
+            R2 cs = Rf[k];
+            R2 xa = S[ab.x * B + lane], xb = S[ab.y * B + lane], ya, yb;
+            ya.x = A::sub(A::mul(cs.x, xa.x), A::mul(cs.y, xb.y));
+            ya.y = A::add(A::mul(cs.x, xa.y), A::mul(cs.y, xb.x));
+            yb.x = A::sub(A::mul(cs.x, xb.x), A::mul(cs.y, xa.y));
+            yb.y = A::add(A::mul(cs.x, xb.y), A::mul(cs.y, xa.x));
+            S[ab.x * B + lane] = ya;
+            S[ab.y * B + lane] = yb;
+        }
+        for (int a = 0; a < n; a++) {  // propagate.c:891-894
+            R2 z = S[a * B + lane], u = Uf[a], o;
+            o.x = A::sub(A::mul(z.x, u.x), A::mul(z.y, u.y));
+            o.y = A::add(A::mul(z.y, u.x), A::mul(z.x, u.y));
+            S[a * B + lane] = o;
+        }
+    }
+}
+
+// Response of one vector at one time: sum_i mu_i * psi_i.  In FP32 the
+// product is rounded to float before the FP64 sum, as calc_S1
+// (absorption.c:205-212) does with a double accumulator.
+template <typename R>
+__device__ __forceinline__ double2 dot_mu(const DevTraj &T, long t, int x, const typename Vec2<R>::T *S, int B,
+                                          int lane, int n) {
+    double re = 0, im = 0;
+    for (int i = 0; i < n; i++) {
+        R m = (R)traj_mu(T, t, x, i);
+        typename Vec2<R>::T z = S[i * B + lane];
+        re += (double)Ar<R>::mul(m, z.x);
+        im += (double)Ar<R>::mul(m, z.y);
+    }
+    return make_double2(re, im);
+}
+
+template <typename R>
+__global__ void k_abs_trotter(DevTraj T, TrotterPlan P, AbsJob J, double2 *resp, int nvec) {
+    typedef typename Vec2<R>::T R2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R2 *S = (R2 *)smem_raw;
+    const int B = blockDim.x, lane = threadIdx.x, n = P.n;
+    int v = blockIdx.x * B + lane;
+    if (v >= nvec) return;
+    int s = J.begin + v / 3, x = v % 3;
+    long ti = (long)s * J.sample;
+    for (int i = 0; i < n; i++) {
+        R2 z;
+        z.x = (R)traj_mu(T, ti, x, i);
+        z.y = 0;
+        S[i * B + lane] = z;
+    }
+    const R2 *U = (const R2 *)P.U, *rot = (const R2 *)P.rot;
+    for (int t1 = 0; t1 < J.tmax; t1++) {
+        long tj = ti + t1;
+        resp[(size_t)v * J.tmax + t1] = dot_mu<R>(T, tj, x, S, B, lane, n);
+        if (t1 == J.tmax - 1) break;
+        const R2 *Uf = U + (tj - P.f0) * n;
+        const R2 *Rf = P.rot_static ? rot : rot + (tj - P.f0) * P.k;
+        trotter_step<R>(S, B, lane, n, P.k, P.pairs, Uf, Rf, J.ts);
+    }
+}
+
+// ------------------------------------------------------------ RK4
+template <typename R>
+__global__ void k_prep_rk4(DevTraj T, Rk4Plan P, R fsub) {
+    long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (tid >= P.nf * P.k) return;
+    long fi = tid / P.k;
+    int k = (int)(tid % P.k);
+    long t = P.f0 + fi;
+    int2 ab = P.entries[k];
+    float h;
+    bool keep;
+    if (ab.x == ab.y) {
+        h = traj_diag(T, t, ab.x, P.singleshift != 0);
+        keep = true;
+    } else {
+        h = traj_coupling(T, t, ab.x, ab.y);
+        keep = fabsf(h) > T.cut;  // propagate.c:298
+    }
+    R v = keep ? Ar<R>::mul((R)fsub, (R)h) : (R)0;
+    ((R *)P.val)[fi * P.k + k] = v;
+}
+
+// k_q accumulation with the operand types of propagate.c:323-357: the first
+// and last stages are float, the two middle stages are evaluated in double
+// (the literal 0.5 promotes them) and rounded back to float.
+template <typename R> struct Rk4Ops;
+template <> struct Rk4Ops<float> {
+    static __device__ __forceinline__ float half(float acc, float h, float c, float k, bool minus) {
+        double y = __dmul_rn((double)h, __dadd_rn((double)c, __dmul_rn((double)k, 0.5)));
+        return (float)(minus ? __dsub_rn((double)acc, y) : __dadd_rn((double)acc, y));
+    }
+    static __device__ __forceinline__ float full(float acc, float h, float c, float k, bool minus) {
+        float y = __fmul_rn(h, __fadd_rn(c, k));
+        return minus ? __fsub_rn(acc, y) : __fadd_rn(acc, y);
+    }
+    static __device__ __forceinline__ float first(float acc, float h, float c, bool minus) {
+        float y = __fmul_rn(h, c);
+        return minus ? __fsub_rn(acc, y) : __fadd_rn(acc, y);
+    }
+    static __device__ __forceinline__ float update(float c, float k1, float k2, float k3, float k4) {
+        float sum = __fadd_rn(__fadd_rn(__fadd_rn(k1, __fmul_rn(2.0f, k2)), __fmul_rn(2.0f, k3)), k4);
+        return (float)__dadd_rn((double)c, __ddiv_rn((double)sum, 6.0));
+    }
+};
+template <> struct Rk4Ops<double> {
+    static __device__ __forceinline__ double half(double acc, double h, double c, double k, bool minus) {
+        double y = h * (c + k * 0.5);
+        return minus ? acc - y : acc + y;
+    }
+    static __device__ __forceinline__ double full(double acc, double h, double c, double k, bool minus) {
+        double y = h * (c + k);
+        return minus ? acc - y : acc + y;
+    }
+    static __device__ __forceinline__ double first(double acc, double h, double c, bool minus) {
+        double y = h * c;
+        return minus ? acc - y : acc + y;
+    }
+    static __device__ __forceinline__ double update(double c, double k1, double k2, double k3, double k4) {
+        return c + (k1 + 2.0 * k2 + 2.0 * k3 + k4) / 6.0;
+    }
+};
+
+template <typename R>
+__device__ __forceinline__ R norm_of(const typename Vec2<R>::T *C, int B, int lane, int n) {
+    R s = 0;
+    for (int a = 0; a < n; a++) {  // find_norm, NISE_subs.c:125-133
+        typename Vec2<R>::T z = C[a * B + lane];
+        s = Ar<R>::add(s, Ar<R>::add(Ar<R>::mul(z.x, z.x), Ar<R>::mul(z.y, z.y)));
+    }
+    return s;
+}
+
+// One RK4 step (m sub-steps), propagate.c:311-366.  S holds the state and
+// K1..K4 follow it in shared memory, all [site][lane].
+template <typename R>
+__device__ __forceinline__ void rk4_step(typename Vec2<R>::T *S, int B, int lane, int n, int K,
+                                         const int2 *__restrict__ ent, const R *__restrict__ val, int m) {
+    typedef typename Vec2<R>::T R2;
+    typedef Rk4Ops<R> O;
+    R2 *K1 = S + (size_t)n * B, *K2 = K1 + (size_t)n * B, *K3 = K2 + (size_t)n * B, *K4 = K3 + (size_t)n * B;
+    for (int sub = 0; sub < m; sub++) {
+        for (int a = 0; a < n; a++) {
+            R2 z;
+            z.x = 0;
+            z.y = 0;
+            K1[a * B + lane] = z; K2[a * B + lane] = z; K3[a * B + lane] = z; K4[a * B + lane] = z;
+        }
+        for (int k = 0; k < K; k++) {
+            int2 e = ent[k];
+            R h = val[k];
+            int c = e.x, r = e.y;
+            R2 sr = S[r * B + lane], kc = K1[c * B + lane];
+            kc.x = O::first(kc.x, h, sr.y, false);
+            kc.y = O::first(kc.y, h, sr.x, true);
+            K1[c * B + lane] = kc;
+            if (r != c) {
+                R2 sc = S[c * B + lane], kr = K1[r * B + lane];
+                kr.x = O::first(kr.x, h, sc.y, false);
+                kr.y = O::first(kr.y, h, sc.x, true);
+                K1[r * B + lane] = kr;
+            }
+        }
+        for (int stage = 1; stage < 4; stage++) {
+            R2 *Kp = stage == 1 ? K1 : (stage == 2 ? K2 : K3);
+            R2 *Kn = stage == 1 ? K2 : (stage == 2 ? K3 : K4);
+            for (int k = 0; k < K; k++) {
+                int2 e = ent[k];
+                R h = val[k];
+                int c = e.x, r = e.y;
+                R2 sr = S[r * B + lane], pr = Kp[r * B + lane], kc = Kn[c * B + lane];
+                if (stage < 3) {
+                    kc.x = O::half(kc.x, h, sr.y, pr.y, false);
+                    kc.y = O::half(kc.y, h, sr.x, pr.x, true);
+                } else {
+                    kc.x = O::full(kc.x, h, sr.y, pr.y, false);
+                    kc.y = O::full(kc.y, h, sr.x, pr.x, true);
+                }
+                Kn[c * B + lane] = kc;
+                if (r != c) {
+                    R2 sc = S[c * B + lane], pc = Kp[c * B + lane], kr = Kn[r * B + lane];
+                    if (stage < 3) {
+                        kr.x = O::half(kr.x, h, sc.y, pc.y, false);
+                        kr.y = O::half(kr.y, h, sc.x, pc.x, true);
+                    } else {
+                        kr.x = O::full(kr.x, h, sc.y, pc.y, false);
+                        kr.y = O::full(kr.y, h, sc.x, pc.x, true);
+                    }
+                    Kn[r * B + lane] = kr;
+                }
+            }
+        }
+        R norm = norm_of<R>(S, B, lane, n);
+        for (int a = 0; a < n; a++) {
+            R2 z = S[a * B + lane], k1 = K1[a * B + lane], k2 = K2[a * B + lane], k3 = K3[a * B + lane],
+               k4 = K4[a * B + lane];
+            z.x = O::update(z.x, k1.x, k2.x, k3.x, k4.x);
+            z.y = O::update(z.y, k1.y, k2.y, k3.y, k4.y);
+            S[a * B + lane] = z;
+        }
+        R nn = norm_of<R>(S, B, lane, n);  // re_normalize, NISE_subs.c:136-148
+        if (norm != nn) {
+            R factor = (R)sqrt((double)(norm / nn));
+            for (int a = 0; a < n; a++) {
+                R2 z = S[a * B + lane];
+                z.x = Ar<R>::mul(z.x, factor);
+                z.y = Ar<R>::mul(z.y, factor);
+                S[a * B + lane] = z;
+            }
+        }
+    }
+}
+
+template <typename R>
+__global__ void k_abs_rk4(DevTraj T, Rk4Plan P, AbsJob J, double2 *resp, int nvec) {
+    typedef typename Vec2<R>::T R2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R2 *S = (R2 *)smem_raw;
+    const int B = blockDim.x, lane = threadIdx.x, n = P.n;
+    int v = blockIdx.x * B + lane;
+    if (v >= nvec) return;
+    int s = J.begin + v / 3, x = v % 3;
+    long ti = (long)s * J.sample;
+    for (int i = 0; i < n; i++) {
+        R2 z;
+        z.x = (R)traj_mu(T, ti, x, i);
+        z.y = 0;
+        S[i * B + lane] = z;
+    }
+    for (int t1 = 0; t1 < J.tmax; t1++) {
+        long tj = ti + t1;
+        resp[(size_t)v * J.tmax + t1] = dot_mu<R>(T, tj, x, S, B, lane, n);
+        if (t1 == J.tmax - 1) break;
+        rk4_step<R>(S, B, lane, n, P.k, P.entries, (const R *)P.val + (tj - P.f0) * P.k, J.ts);
+    }
+}
+
+// ------------------------------------------------------------ sparse Taylor
+// Order of the Taylor series of exp(-i H f) per frame: the smallest K with
+// b^(K+1)/(K+1)! * e^b <= tol, b = |f| * (max|h_ii| + max row sum |J|) >= ||H f||.
+template <typename R>
+__global__ void k_prep_taylor(DevTraj T, TaylorPlan P, double rowabs, double f, double tol, int *order) {
+    long fi = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (fi >= P.nf) return;
+    long t = P.f0 + fi;
+    double dmax = 0;
+    for (int i = 0; i < P.n; i++) dmax = fmax(dmax, fabs((double)traj_diag(T, t, i, P.singleshift != 0)));
+    double b = fabs(f) * (dmax + rowabs), term = exp(b);
+    int K = 0;
+    for (K = 0; K < 60; K++) {
+        term *= b / (K + 1);
+        if (term <= tol) break;
+    }
+    order[fi] = K < 1 ? 1 : K;
+}
+
+template <typename R, int G, int RPT>
+__global__ void __launch_bounds__(512) k_abs_taylor(DevTraj T, TaylorPlan P, AbsJob J, double2 *resp, int nvec) {
+    typedef typename Vec2<R>::T R2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = P.n, tid = threadIdx.x, NT = blockDim.x;
+    R2 *cur = (R2 *)smem_raw, *nxt = cur + (size_t)n * G;
+    double *red = (double *)(nxt + (size_t)n * G);  // [NT/32][2G]
+    const int v0 = blockIdx.x * G;
+    int xg[G];
+    long tig[G];
+    bool valid[G];
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+        int v = v0 + g;
+        valid[g] = v < nvec;
+        int vv = valid[g] ? v : v0;
+        xg[g] = vv % 3;
+        tig[g] = (long)(J.begin + vv / 3) * J.sample;
+    }
+    R2 psi[RPT][G];
+    float dg[RPT][G];
+#pragma unroll
+    for (int r = 0; r < RPT; r++) {
+        int i = tid + r * NT;
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            psi[r][g].x = (i < n) ? (R)traj_mu(T, tig[g], xg[g], i) : (R)0;
+            psi[r][g].y = 0;
+        }
+    }
+    const R *jval = (const R *)P.val;
+    for (int t1 = 0; t1 < J.tmax; t1++) {
+        // response (absorption.c:128-130): block reduction of mu.psi per vector
+        double part[2 * G];
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            double re = 0, im = 0;
+#pragma unroll
+            for (int r = 0; r < RPT; r++) {
+                int i = tid + r * NT;
+                if (i < n) {
+                    R m = (R)traj_mu(T, tig[g] + t1, xg[g], i);
+                    re += (double)(m * psi[r][g].x);
+                    im += (double)(m * psi[r][g].y);
+                }
+            }
+            part[2 * g] = re;
+            part[2 * g + 1] = im;
+        }
+#pragma unroll
+        for (int q = 0; q < 2 * G; q++)
+            for (int o = 16; o > 0; o >>= 1) part[q] += __shfl_xor_sync(0xffffffffu, part[q], o);
+        if ((tid & 31) == 0)
+#pragma unroll
+            for (int q = 0; q < 2 * G; q++) red[(tid >> 5) * 2 * G + q] = part[q];
+        __syncthreads();
+        if (tid < G && valid[tid]) {
+            double re = 0, im = 0;
+            for (int w = 0; w < NT / 32; w++) { re += red[w * 2 * G + 2 * tid]; im += red[w * 2 * G + 2 * tid + 1]; }
+            resp[(size_t)(v0 + tid) * J.tmax + t1] = make_double2(re, im);
+        }
+        if (t1 == J.tmax - 1) break;
+        // per-frame diagonal and series order
+        int K = 1;
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            long tj = tig[g] + t1;
+            K = max(K, P.order[tj - P.f0]);
+#pragma unroll
+            for (int r = 0; r < RPT; r++) {
+                int i = tid + r * NT;
+                dg[r][g] = (i < n) ? traj_diag(T, tj, i, P.singleshift != 0) : 0.0f;
+            }
+        }
+        // psi <- sum_k (-i f H)^k / k! psi ; cur holds the current term
+#pragma unroll
+        for (int r = 0; r < RPT; r++) {
+            int i = tid + r * NT;
+            if (i < n)
+#pragma unroll
+                for (int g = 0; g < G; g++) cur[(size_t)i * G + g] = psi[r][g];
+        }
+        for (int k = 1; k <= K; k++) {
+            __syncthreads();
+            R c = (R)(J.f / k);
+#pragma unroll
+            for (int r = 0; r < RPT; r++) {
+                int i = tid + r * NT;
+                if (i >= n) continue;
+                R2 y[G];
+#pragma unroll
+                for (int g = 0; g < G; g++) {
+                    R2 z = cur[(size_t)i * G + g];
+                    y[g].x = (R)dg[r][g] * z.x;
+                    y[g].y = (R)dg[r][g] * z.y;
+                }
+                for (int e = P.row_ptr[i]; e < P.row_ptr[i + 1]; e++) {
+                    int j = P.col[e];
+                    R w = jval[e];
+                    const R2 *cj = cur + (size_t)j * G;
+#pragma unroll
+                    for (int g = 0; g < G; g++) {
+                        R2 z = cj[g];
+                        y[g].x += w * z.x;
+                        y[g].y += w * z.y;
+                    }
+                }
+#pragma unroll
+                for (int g = 0; g < G; g++) {
+                    R2 nz;
+                    nz.x = c * y[g].y;   // (-i)(c)(y) = c*y.im - i c*y.re
+                    nz.y = -c * y[g].x;
+                    nxt[(size_t)i * G + g] = nz;
+                    psi[r][g].x += nz.x;
+                    psi[r][g].y += nz.y;
+                }
+            }
+            __syncthreads();
+            R2 *tmp = cur;
+            cur = nxt;
+            nxt = tmp;
+        }
+        __syncthreads();
+    }
+}
+
+// Coupling pattern of HamiltonianType Full trajectories: flag[idx] = 1 for
+// packed off-diagonal idx when |J| > cut in any frame of [f0, f0+nf).
+__global__ void k_pattern_scan(DevTraj T, long f0, long nf, int *flag) {
+    long nn2 = (long)T.n * (T.n + 1) / 2;
+    long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (tid >= nn2) return;
+    int a = 0;
+    long rem = tid;
+    while (rem >= T.n - a) { rem -= T.n - a; a++; }
+    int b = a + (int)rem;
+    if (a == b) return;
+    int any = 0;
+    for (long t = f0; t < f0 + nf && !any; t++) any = fabsf(traj_coupling(T, t, a, b)) > T.cut;
+    flag[tid] = any;
+}
+
+__global__ void k_reduce_resp(const double2 *resp, int nvec, int tmax, double2 *out) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= tmax) return;
+    double re = 0, im = 0;
+    for (int v = 0; v < nvec; v++) {
+        double2 z = resp[(size_t)v * tmax + t];
+        re += z.x;
+        im += z.y;
+    }
+    out[t] = make_double2(re, im);
+}
+
+// ------------------------------------------------------------ single steps
+// nise_propagate: each thread propagates one vector with its own packed H.
+template <typename R>
+__global__ void k_step_coupling(int n, float cut, const float *H, R *re, R *im, int nvec, int ts, R fsub) {
+    typedef typename Vec2<R>::T R2;
+    typedef Ar<R> A;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R2 *S = (R2 *)smem_raw;
+    const int B = blockDim.x, lane = threadIdx.x;
+    int v = blockIdx.x * B + lane;
+    if (v >= nvec) return;
+    const float *h = H + (size_t)v * n * (n + 1) / 2;
+    for (int a = 0; a < n; a++) {
+        R2 z;
+        z.x = re[(size_t)v * n + a];
+        z.y = im[(size_t)v * n + a];
+        S[a * B + lane] = z;
+    }
+    for (int sub = 0; sub < ts; sub++) {
+        for (int pass = 0; pass < 2; pass++) {
+            if (pass == 1) {
+                for (int a = 0; a < n; a++)
+                    for (int b = a + 1; b < n; b++) {
+                        float j = h[sindex(a, b, n)];
+                        if (!(fabsf(j) > cut)) continue;
+                        R2 cs = Cst<R>::rot(j, fsub, cut);
+                        R2 xa = S[a * B + lane], xb = S[b * B + lane], ya, yb;
+                        ya.x = A::sub(A::mul(cs.x, xa.x), A::mul(cs.y, xb.y));
+                        ya.y = A::add(A::mul(cs.x, xa.y), A::mul(cs.y, xb.x));
+                        yb.x = A::sub(A::mul(cs.x, xb.x), A::mul(cs.y, xa.y));
+                        yb.y = A::add(A::mul(cs.x, xb.y), A::mul(cs.y, xa.x));
+                        S[a * B + lane] = ya;
+                        S[b * B + lane] = yb;
+                    }
+            }
+            for (int a = 0; a < n; a++) {
+                double arg = 0.5 * (double)h[sindex(a, a, n)] * (double)fsub;
+                R ur = (R)cos(arg), ui = (R)(-sin(arg));
+                R2 z = S[a * B + lane], o;
+                o.x = A::sub(A::mul(z.x, ur), A::mul(z.y, ui));
+                o.y = A::add(A::mul(z.y, ur), A::mul(z.x, ui));
+                S[a * B + lane] = o;
+            }
+        }
+    }
+    for (int a = 0; a < n; a++) {
+        R2 z = S[a * B + lane];
+        re[(size_t)v * n + a] = z.x;
+        im[(size_t)v * n + a] = z.y;
+    }
+}
+
+template <typename R>
+__global__ void k_step_rk4(int n, float cut, const float *H, R *re, R *im, int nvec, int ts, R fsub, int2 *ent_ws,
+                           R *val_ws, int kmax_all) {
+    typedef typename Vec2<R>::T R2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R2 *S = (R2 *)smem_raw;
+    const int B = blockDim.x, lane = threadIdx.x;
+    int v = blockIdx.x * B + lane;
+    if (v >= nvec) return;
+    const float *h = H + (size_t)v * n * (n + 1) / 2;
+    int2 *ent = ent_ws + (size_t)v * kmax_all;
+    R *val = val_ws + (size_t)v * kmax_all;
+    int K = 0;
+    for (int a = 0; a < n; a++)
+        for (int b = a; b < n; b++) {
+            float x = h[sindex(a, b, n)];
+            if (fabsf(x) > cut || a == b) {
+                ent[K] = make_int2(a, b);
+                val[K] = Ar<R>::mul((R)fsub, (R)x);
+                K++;
+            }
+        }
+    for (int a = 0; a < n; a++) {
+        R2 z;
+        z.x = re[(size_t)v * n + a];
+        z.y = im[(size_t)v * n + a];
+        S[a * B + lane] = z;
+    }
+    rk4_step<R>(S, B, lane, n, K, ent, val, ts);
+    for (int a = 0; a < n; a++) {
+        R2 z = S[a * B + lane];
+        re[(size_t)v * n + a] = z.x;
+        im[(size_t)v * n + a] = z.y;
+    }
+}
+
+// Exact step exp(-i H f) psi by a Taylor series on the dense packed H
+// (one thread per vector, for small n).
+template <typename R>
+__global__ void k_step_taylor(int n, const float *H, R *re, R *im, int nvec, double f) {
+    typedef typename Vec2<R>::T R2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int B = blockDim.x, lane = threadIdx.x;
+    R2 *cur = (R2 *)smem_raw, *nxt = cur + (size_t)n * B, *acc = nxt + (size_t)n * B;
+    int v = blockIdx.x * B + lane;
+    if (v >= nvec) return;
+    const float *h = H + (size_t)v * n * (n + 1) / 2;
+    double bound = 0;
+    for (int a = 0; a < n; a++) {
+        double rs = 0;
+        for (int b = 0; b < n; b++) rs += fabs((double)h[sindex(a, b, n)]);
+        bound = fmax(bound, rs);
+    }
+    double bnd = fabs(f) * bound, term = exp(bnd), tol = sizeof(R) == 4 ? 1e-12 : 1e-18;
+    int K;
+    for (K = 0; K < 80; K++) {
+        term *= bnd / (K + 1);
+        if (term <= tol) break;
+    }
+    for (int a = 0; a < n; a++) {
+        R2 z;
+        z.x = re[(size_t)v * n + a];
+        z.y = im[(size_t)v * n + a];
+        cur[a * B + lane] = z;
+        acc[a * B + lane] = z;
+    }
+    for (int k = 1; k <= K; k++) {
+        R c = (R)(f / k);
+        for (int a = 0; a < n; a++) {
+            R yr = 0, yi = 0;
+            for (int b = 0; b < n; b++) {
+                R w = (R)h[sindex(a, b, n)];
+                R2 z = cur[b * B + lane];
+                yr += w * z.x;
+                yi += w * z.y;
+            }
+            R2 nz;
+            nz.x = c * yi;
+            nz.y = -c * yr;
+            nxt[a * B + lane] = nz;
+            R2 s = acc[a * B + lane];
+            s.x += nz.x;
+            s.y += nz.y;
+            acc[a * B + lane] = s;
+        }
+        R2 *tmp = cur;
+        cur = nxt;
+        nxt = tmp;
+    }
+    for (int a = 0; a < n; a++) {
+        R2 z = acc[a * B + lane];
+        re[(size_t)v * n + a] = z.x;
+        im[(size_t)v * n + a] = z.y;
+    }
+}
+
+int lanes_for(size_t bytes_per_lane, int want) {
+    const size_t budget = 200 * 1024;
+    int b = want;
+    while (b > 1 && (size_t)b * bytes_per_lane > budget) b >>= 1;
+    return b;
+}
+
+template <typename K>
+int set_smem(K kernel, size_t bytes) {
+    if (bytes > 48 * 1024)
+        return (int)cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    return 0;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ launchers
+int launch_prep_trotter(int prec, const DevTraj &T, const TrotterPlan &P, double fsub, float fsub32,
+                        cudaStream_t s) {
+    long per = P.n + (P.rot_static ? 0 : P.k);
+    long tot = P.nf * per;
+    int bs = 256;
+    long grid = (tot + bs - 1) / bs;
+    if (prec == 0) {
+        if (tot) k_prep_trotter<float><<<grid, bs, 0, s>>>(T, P, fsub32);
+        if (P.rot_static && P.k) k_prep_trotter_static<float><<<(P.k + 255) / 256, 256, 0, s>>>(T, P, fsub32);
+    } else {
+        if (tot) k_prep_trotter<double><<<grid, bs, 0, s>>>(T, P, fsub);
+        if (P.rot_static && P.k) k_prep_trotter_static<double><<<(P.k + 255) / 256, 256, 0, s>>>(T, P, fsub);
+    }
+    return (int)cudaGetLastError();
+}
+
+int launch_abs_trotter(int prec, const DevTraj &T, const TrotterPlan &P, const AbsJob &J, double2 *resp,
+                       cudaStream_t s) {
+    int nvec = 3 * J.nsamp;
+    size_t per_lane = (size_t)P.n * (prec == 0 ? sizeof(float2) : sizeof(double2));
+    int B = lanes_for(per_lane, 64);
+    size_t smem = per_lane * B;
+    int grid = (nvec + B - 1) / B;
+    int e;
+    if (prec == 0) {
+        if ((e = set_smem(k_abs_trotter<float>, smem))) return e;
+        k_abs_trotter<float><<<grid, B, smem, s>>>(T, P, J, resp, nvec);
+    } else {
+        if ((e = set_smem(k_abs_trotter<double>, smem))) return e;
+        k_abs_trotter<double><<<grid, B, smem, s>>>(T, P, J, resp, nvec);
+    }
+    return (int)cudaGetLastError();
+}
+
+int launch_prep_rk4(int prec, const DevTraj &T, const Rk4Plan &P, double fsub, float fsub32, cudaStream_t s) {
+    long tot = P.nf * P.k;
+    if (!tot) return 0;
+    if (prec == 0) k_prep_rk4<float><<<(tot + 255) / 256, 256, 0, s>>>(T, P, fsub32);
+    else k_prep_rk4<double><<<(tot + 255) / 256, 256, 0, s>>>(T, P, fsub);
+    return (int)cudaGetLastError();
+}
+
+int launch_abs_rk4(int prec, const DevTraj &T, const Rk4Plan &P, const AbsJob &J, double2 *resp, cudaStream_t s) {
+    int nvec = 3 * J.nsamp;
+    size_t per_lane = 5 * (size_t)P.n * (prec == 0 ? sizeof(float2) : sizeof(double2));
+    int B = lanes_for(per_lane, 64);
+    size_t smem = per_lane * B;
+    int grid = (nvec + B - 1) / B;
+    int e;
+    if (prec == 0) {
+        if ((e = set_smem(k_abs_rk4<float>, smem))) return e;
+        k_abs_rk4<float><<<grid, B, smem, s>>>(T, P, J, resp, nvec);
+    } else {
+        if ((e = set_smem(k_abs_rk4<double>, smem))) return e;
+        k_abs_rk4<double><<<grid, B, smem, s>>>(T, P, J, resp, nvec);
+    }
+    return (int)cudaGetLastError();
+}
+
+int launch_prep_taylor(int prec, const DevTraj &T, TaylorPlan &P, double rowabs_max, double f, int *order,
+                       cudaStream_t s) {
+    double tol = prec == 0 ? 1e-10 : 1e-17;
+    if (P.nf) k_prep_taylor<float><<<(P.nf + 127) / 128, 128, 0, s>>>(T, P, rowabs_max, f, tol, order);
+    P.order = order;
+    return (int)cudaGetLastError();
+}
+
+template <typename R, int G, int RPT>
+static int run_taylor(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int nvec,
+                      cudaStream_t s) {
+    int NT = 512;
+    size_t smem = 2 * (size_t)P.n * G * sizeof(typename Vec2<R>::T) + (NT / 32) * 2 * G * sizeof(double);
+    int e;
+    if ((e = set_smem(k_abs_taylor<R, G, RPT>, smem))) return e;
+    int grid = (nvec + G - 1) / G;
+    k_abs_taylor<R, G, RPT><<<grid, NT, smem, s>>>(T, P, J, resp, nvec);
+    return (int)cudaGetLastError();
+}
+
+int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp,
+                      int vec_per_cta, cudaStream_t s) {
+    int nvec = 3 * J.nsamp;
+    int rpt = (P.n + 511) / 512;
+    if (rpt > 4 || !P.static_j) return (int)cudaErrorNotSupported;
+    rpt = rpt <= 1 ? 1 : (rpt <= 2 ? 2 : 4);
+#define TAY(R, G)                                                                                  \
+    do {                                                                                           \
+        if (rpt == 1) return run_taylor<R, G, 1>(T, P, J, resp, nvec, s);                          \
+        if (rpt == 2) return run_taylor<R, G, 2>(T, P, J, resp, nvec, s);                          \
+        return run_taylor<R, G, 4>(T, P, J, resp, nvec, s);                                        \
+    } while (0)
+    if (prec == 0) {
+        if (vec_per_cta <= 3) TAY(float, 3);
+        TAY(float, 8);
+    } else {
+        if (vec_per_cta <= 3) TAY(double, 3);
+        TAY(double, 4);
+    }
+#undef TAY
+}
+
+int launch_pattern_scan(const DevTraj &T, long f0, long nf, int *flag, cudaStream_t s) {
+    long nn2 = (long)T.n * (T.n + 1) / 2;
+    k_pattern_scan<<<(nn2 + 255) / 256, 256, 0, s>>>(T, f0, nf, flag);
+    return (int)cudaGetLastError();
+}
+
+int launch_reduce_resp(const double2 *resp, int nvec, int tmax, double2 *out, cudaStream_t s) {
+    k_reduce_resp<<<(tmax + 127) / 128, 128, 0, s>>>(resp, nvec, tmax, out);
+    return (int)cudaGetLastError();
+}
+
+int launch_step_coupling(int prec, int n, float cut, const float *H, void *re, void *im, int nvec, int ts,
+                         double fsub, float fsub32, cudaStream_t s) {
+    size_t per_lane = (size_t)n * (prec == 0 ? sizeof(float2) : sizeof(double2));
+    int B = lanes_for(per_lane, 64);
+    size_t smem = per_lane * B;
+    int e;
+    if (prec == 0) {
+        if ((e = set_smem(k_step_coupling<float>, smem))) return e;
+        k_step_coupling<float><<<(nvec + B - 1) / B, B, smem, s>>>(n, cut, H, (float *)re, (float *)im, nvec, ts,
+                                                                   fsub32);
+    } else {
+        if ((e = set_smem(k_step_coupling<double>, smem))) return e;
+        k_step_coupling<double><<<(nvec + B - 1) / B, B, smem, s>>>(n, cut, H, (double *)re, (double *)im, nvec,
+                                                                    ts, fsub);
+    }
+    return (int)cudaGetLastError();
+}
+
+int launch_step_rk4(int prec, int n, float cut, const float *H, void *re, void *im, int nvec, int ts, double fsub,
+                    float fsub32, cudaStream_t s) {
+    size_t rsz = prec == 0 ? sizeof(float) : sizeof(double);
+    size_t per_lane = 5 * (size_t)n * 2 * rsz;
+    int B = lanes_for(per_lane, 64);
+    size_t smem = per_lane * B;
+    int kmax = n * (n + 1) / 2;
+    int2 *ent = nullptr;
+    void *val = nullptr;
+    int e;
+    if ((e = (int)cudaMallocAsync((void **)&ent, sizeof(int2) * (size_t)kmax * nvec, s))) return e;
+    if ((e = (int)cudaMallocAsync(&val, rsz * (size_t)kmax * nvec, s))) return e;
+    if (prec == 0) {
+        if ((e = set_smem(k_step_rk4<float>, smem))) return e;
+        k_step_rk4<float><<<(nvec + B - 1) / B, B, smem, s>>>(n, cut, H, (float *)re, (float *)im, nvec, ts, fsub32,
+                                                              ent, (float *)val, kmax);
+    } else {
+        if ((e = set_smem(k_step_rk4<double>, smem))) return e;
+        k_step_rk4<double><<<(nvec + B - 1) / B, B, smem, s>>>(n, cut, H, (double *)re, (double *)im, nvec, ts,
+                                                               fsub, ent, (double *)val, kmax);
+    }
+    e = (int)cudaGetLastError();
+    cudaFreeAsync(ent, s);
+    cudaFreeAsync(val, s);
+    return e;
+}
+
+int launch_step_taylor(int prec, int n, const float *H, void *re, void *im, int nvec, double f, cudaStream_t s) {
+    size_t per_lane = 3 * (size_t)n * (prec == 0 ? sizeof(float2) : sizeof(double2));
+    int B = lanes_for(per_lane, 64);
+    size_t smem = per_lane * B;
+    int e;
+    if (prec == 0) {
+        if ((e = set_smem(k_step_taylor<float>, smem))) return e;
+        k_step_taylor<float><<<(nvec + B - 1) / B, B, smem, s>>>(n, H, (float *)re, (float *)im, nvec, f);
+    } else {
+        if ((e = set_smem(k_step_taylor<double>, smem))) return e;
+        k_step_taylor<double><<<(nvec + B - 1) / B, B, smem, s>>>(n, H, (double *)re, (double *)im, nvec, f);
+    }
+    return (int)cudaGetLastError();
+}

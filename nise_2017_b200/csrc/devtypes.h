@@ -1,0 +1,28 @@
+// Plain data types shared by host code (api.cpp) and device code.
+#pragma once
+
+// Trajectory records as the reference reads them (read_trajectory.c):
+// every record is an int32 tag followed by float32 data, addressed here in
+// 4-byte words so the tag is word 0.
+struct DevTraj {
+    const float *energy;     // energy record image
+    long e_words;            // words per energy record
+    long e_frames;
+    int full;                // 1: packed N(N+1)/2 (+doubles) frames; 0: N diagonal values
+    const float *dipole;     // dipole record image (per-frame dipoles)
+    long d_words;
+    long d_frames;
+    const float *mu_static;  // [3][N] for HamiltonianType Coupling (else nullptr)
+    const float *hc;         // packed coupling frame (HamiltonianType Coupling), cut applied
+    const float *anh;        // anharmonicity records (N per frame) or nullptr
+    long a_frames;
+    const float *over;       // overtone dipole records (3N per frame) or nullptr
+    long o_frames;
+    const int *shift_site;   // SingleShift sites
+    const float *shift_ab;   // (a, b) pairs
+    int nshift;
+    int n;                   // singles
+    float shifte;            // (min1 + max1) / 2
+    float cut;               // Couplingcut
+};
+

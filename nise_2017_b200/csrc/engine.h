@@ -1,0 +1,86 @@
+// Host-side launch interface of the engine's kernels (implemented in the
+// .cu files, called by api.cpp).  Every launcher returns a cudaError_t value
+// cast to int (0 = success) and only enqueues work on the given stream.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "devtypes.h"
+
+// Per-frame coefficients of the Trotter "Coupling" scheme
+// (propagate_vec_coupling_S, propagate.c:821-899) for frames [f0, f0+nf):
+//   U[t][a]   = (cos(h_a f/2), -sin(h_a f/2))     half-step diagonal phase
+//   rot[t][k] = (co, si), si = -sin(J_k f), co = sqrt(1 - si^2)
+// for the coupling pattern pairs[k] = (a, b), a < b, in lexicographic order.
+// With a static coupling frame, rot has one row shared by all frames.
+struct TrotterPlan {
+    int n, k;
+    const int2 *pairs;  // device [k]
+    long f0, nf;
+    void *U;            // R2 [nf][n]
+    void *rot;          // R2 [nf][k] or [k]
+    int rot_static;
+    int singleshift;    // apply SingleShift to the diagonal (absorption path)
+};
+
+// Per-frame sparse lists of the RK4 scheme (propagate_vec_RK4,
+// propagate.c:261-373): entries[k] = (a, b), a <= b, diagonal always kept,
+// val[t][k] = f * H_ab (0 where |H_ab| <= cut in that frame).
+struct Rk4Plan {
+    int n, k;
+    const int2 *entries;
+    long f0, nf;
+    void *val;          // R [nf][k]
+    int singleshift;
+};
+
+// Sparse exact propagator exp(-i H f) by a Taylor series on a static CSR
+// coupling matrix plus the per-frame diagonal.
+struct TaylorPlan {
+    int n, nnz;
+    const int *row_ptr, *col;
+    const void *val;       // R [nnz], static couplings (HamiltonianType Coupling)
+    const int *pidx;       // packed index of every CSR entry (per-frame couplings)
+    int static_j;
+    long f0, nf;
+    const int *order;      // [nf] Taylor order per frame
+    int singleshift;
+};
+
+// A batch of linear-absorption start points: vectors v = 3*(s-begin)+x for
+// samples s in [begin, begin+nsamp), polarisations x = 0..2.
+struct AbsJob {
+    int begin, nsamp, sample, tmax, ts;
+    double f;              // full-step phase factor deltat*icm2ifs*2pi (no /ts)
+    float f32_sub;         // same / ts in the reference's float arithmetic
+    double f64_sub;        // same / ts in double
+    float f32_full;        // deltat*icm2ifs*2pi in float arithmetic
+};
+
+int launch_prep_trotter(int prec, const DevTraj &T, const TrotterPlan &P, double fsub, float fsub32,
+                        cudaStream_t s);
+int launch_abs_trotter(int prec, const DevTraj &T, const TrotterPlan &P, const AbsJob &J, double2 *resp,
+                       cudaStream_t s);
+int launch_prep_rk4(int prec, const DevTraj &T, const Rk4Plan &P, double fsub, float fsub32, cudaStream_t s);
+int launch_abs_rk4(int prec, const DevTraj &T, const Rk4Plan &P, const AbsJob &J, double2 *resp, cudaStream_t s);
+int launch_prep_taylor(int prec, const DevTraj &T, TaylorPlan &P, double rowabs_max, double f, int *order,
+                       cudaStream_t s);
+int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp,
+                      int vec_per_cta, cudaStream_t s);
+// flag[idx] = 1 for packed off-diagonals with |J| > cut in any frame of [f0, f0+nf).
+int launch_pattern_scan(const DevTraj &T, long f0, long nf, int *flag, cudaStream_t s);
+// Sum resp[v][t] over v in order (deterministic) into out[t].
+int launch_reduce_resp(const double2 *resp, int nvec, int tmax, double2 *out, cudaStream_t s);
+// 1D spectrum (1DFFT.c:144-228) of the response on the device.
+struct FftJob {
+    int tmax, fft, samples, window, fp32;
+    double deltat, lifetime, homogen, inhomogen;
+};
+int launch_fft1d(const FftJob &J, const double2 *resp, double2 *spec, cudaStream_t s);
+
+// Batched single steps on caller Hamiltonians (nise_propagate): vector v
+// uses packed H + v*n(n+1)/2.
+int launch_step_coupling(int prec, int n, float cut, const float *H, void *re, void *im, int nvec, int ts,
+                         double fsub, float fsub32, cudaStream_t s);
+int launch_step_rk4(int prec, int n, float cut, const float *H, void *re, void *im, int nvec, int ts,
+                    double fsub, float fsub32, cudaStream_t s);
+int launch_step_taylor(int prec, int n, const float *H, void *re, void *im, int nvec, double f, cudaStream_t s);

@@ -1,0 +1,63 @@
+// Engine-internal host definitions shared by api.cpp and the 2D driver.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "devtypes.h"
+#include "nise_b200.h"
+
+struct nise_ctx {
+    nise_params p;
+    std::string err;
+    int n = 0;
+    long nn2 = 0;
+    float shifte = 0;
+    float thres = 0;  // Threshold after the reference's rescaling
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0;
+    long launches = 0;
+    bool loaded = false;
+    // trajectory in device memory (record images, 4-byte words)
+    float *d_energy = nullptr, *d_dipole = nullptr, *d_hc = nullptr, *d_mu_static = nullptr;
+    float *d_anh = nullptr, *d_over = nullptr, *d_shift_ab = nullptr;
+    int *d_shift_site = nullptr;
+    int nshift = 0;
+    long e_words = 0, e_frames = 0, d_words = 0, d_frames = 0, a_frames = 0, o_frames = 0;
+    std::vector<float> h_hc;        // coupling frame (HamiltonianType Coupling), shifted, cut
+    std::vector<float> h_mu_static; // dipoles of frame 0 (HamiltonianType Coupling)
+};
+
+int nise_fail(nise_ctx *c, int code, const char *fmt, ...);
+int nise_cuda(nise_ctx *c, int e, const char *what);
+float nise_f32(const nise_params &p, int sign, int m);
+double nise_f64(const nise_params &p, int sign, int m);
+DevTraj nise_devtraj(const nise_ctx *c);
+int nise_pattern(nise_ctx *c, long f0, long nf, std::vector<int2> &pairs);
+int nise_check_frames(nise_ctx *c, long last_frame);
+
+// Stream-ordered device buffer owned by one call.
+template <typename T> struct DevBuf {
+    T *p = nullptr;
+    cudaStream_t s = nullptr;
+    int alloc(nise_ctx *c, size_t count) {
+        s = c->stream;
+        if (count == 0) count = 1;
+        if (cudaMallocAsync((void **)&p, sizeof(T) * count, s) != cudaSuccess) {
+            p = nullptr;
+            return nise_fail(c, NISE_ERR_NOMEM, "device allocation of %zu bytes failed", sizeof(T) * count);
+        }
+        return NISE_OK;
+    }
+    int upload(nise_ctx *c, const std::vector<T> &h) {
+        int rc = alloc(c, h.size());
+        if (rc) return rc;
+        if (!h.empty()) cudaMemcpyAsync(p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s);
+        return NISE_OK;
+    }
+    ~DevBuf() {
+        if (p) cudaFreeAsync(p, s);
+    }
+};

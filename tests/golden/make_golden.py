@@ -1,0 +1,132 @@
+"""Generate the golden fixtures of the NISE propagation path.
+
+Each case is a seeded synthetic trajectory (nise_2017_b200.synth, regenerated
+by the tests from the spec stored in cases.json) run through the reference
+program compiled from its own sources (oracle/_ref/NISE_acc, recipe in
+oracle/Makefile).  The reference's output files are stored as arrays:
+  absorption cases: td = TD_Absorption.dat columns, spec = Absorption.dat columns
+  2D cases:         R  = [6 files][Re, Im][t3][t1] of RparI.dat ... RcroII.dat
+
+Run from the repository root:  python tests/golden/make_golden.py
+"""
+import json
+import os
+import shutil
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from nise_2017_b200 import synth  # noqa: E402
+import oracle  # noqa: E402
+
+L, C = synth.LATTICE, synth.CLUSTER
+CASES = {
+    # linear absorption
+    "abs_coupling_full": dict(
+        spec=dict(n_sites=16, frames=600, dt_fs=2.0, geometry=synth.CHAIN, seed=11),
+        keywords=synth.c0_keywords(Length=600, RunTimes="64 0 0", FFT=1024)),
+    "abs_coupling_static": dict(
+        spec=dict(n_sites=24, frames=400, dt_fs=1.0, geometry=L, spacing=8.0, eps0=15000.0, sigma=300.0,
+                  tau_fs=50.0, jcut=2.0, mu_jitter=0.0, ham_type=synth.COUPLING, dipole_frames=1, seed=12),
+        keywords=synth.c1_keywords(Singles=24, Length=400, RunTimes="48 0 0", Samplerate=40,
+                                   Propagation="Coupling", FFT=512)),
+    "abs_sparse_static": dict(
+        spec=dict(n_sites=32, frames=400, dt_fs=1.0, geometry=L, spacing=8.0, eps0=15000.0, sigma=300.0,
+                  tau_fs=50.0, jcut=2.0, mu_jitter=0.0, ham_type=synth.COUPLING, dipole_frames=1, seed=13),
+        keywords=synth.c1_keywords(Singles=32, Length=400, RunTimes="64 0 0", Samplerate=50, FFT=1000)),
+    "abs_rk4_full": dict(
+        spec=dict(n_sites=12, frames=500, dt_fs=2.0, geometry=synth.CHAIN, seed=14),
+        keywords=synth.c0_keywords(Singles=12, Length=500, RunTimes="64 0 0", Propagation="RK4", Trotter=3,
+                                   FFT=2048)),
+    "abs_shift_window": dict(
+        spec=dict(n_sites=10, frames=400, dt_fs=2.0, geometry=synth.CHAIN, seed=15),
+        keywords=synth.c0_keywords(Singles=10, Length=400, RunTimes="50 0 0", Samplerate=30, Window="Hann",
+                                   Homogeneous=800, Inhomogeneous=300, FFT=256, BeginPoint=1, EndPoint=9),
+        shift=[(2, 1.0, 5.0), (7, 1.02, -3.0)]),
+    # 2DIR family
+    "2d_coupling": dict(
+        spec=dict(n_sites=5, frames=300, dt_fs=2.0, geometry=C, spacing=6.0, sigma=12.0, tau_fs=200.0,
+                  mu_jitter=0.0, ham_type=synth.COUPLING, dipole_frames=1, seed=21),
+        keywords=synth.c2_keywords(Singles=5, Length=300, RunTimes="8 0 8", Samplerate=40)),
+    "2d_coupling_t2": dict(
+        spec=dict(n_sites=5, frames=300, dt_fs=2.0, geometry=C, spacing=6.0, sigma=12.0, tau_fs=200.0,
+                  mu_jitter=0.0, ham_type=synth.COUPLING, dipole_frames=1, seed=22),
+        keywords=synth.c2_keywords(Singles=5, Length=300, RunTimes="8 3 8", Samplerate=40)),
+    "2d_rk4": dict(
+        spec=dict(n_sites=5, frames=300, dt_fs=2.0, geometry=C, spacing=6.0, sigma=12.0, tau_fs=200.0,
+                  mu_jitter=0.0, ham_type=synth.COUPLING, dipole_frames=1, seed=23),
+        keywords=synth.c2_keywords(Singles=5, Length=300, RunTimes="8 0 8", Samplerate=40, Propagation="RK4")),
+    "2d_sparse": dict(
+        spec=dict(n_sites=5, frames=300, dt_fs=2.0, geometry=C, spacing=6.0, sigma=12.0, tau_fs=200.0,
+                  mu_jitter=0.0, ham_type=synth.COUPLING, dipole_frames=1, seed=24),
+        keywords=synth.c2_keywords(Singles=5, Length=300, RunTimes="8 0 8", Samplerate=40, Propagation="Sparse",
+                                   Threshold=0)),
+    "2d_full_anhfile": dict(
+        spec=dict(n_sites=4, frames=260, dt_fs=2.0, geometry=synth.CHAIN, j_nn=-6.0, j_sigma=1.5, seed=25),
+        keywords=synth.c2_keywords(Singles=4, Length=260, RunTimes="6 0 6", Samplerate=30, Anharmonicity=0,
+                                   HamiltonianType="Full"),
+        anharm=True),
+    "2d_gbir": dict(
+        spec=dict(n_sites=5, frames=300, dt_fs=2.0, geometry=C, spacing=6.0, seed=26, ham_type=synth.COUPLING,
+                  dipole_frames=1, mu_jitter=0.0),
+        keywords=synth.c2_keywords(Singles=5, Length=300, RunTimes="8 2 8", Samplerate=40, Technique="GBIR")),
+    "2d_seir": dict(
+        spec=dict(n_sites=5, frames=300, dt_fs=2.0, geometry=C, spacing=6.0, seed=26, ham_type=synth.COUPLING,
+                  dipole_frames=1, mu_jitter=0.0),
+        keywords=synth.c2_keywords(Singles=5, Length=300, RunTimes="8 2 8", Samplerate=40, Technique="SEIR")),
+    "2d_eair": dict(
+        spec=dict(n_sites=5, frames=300, dt_fs=2.0, geometry=C, spacing=6.0, seed=26, ham_type=synth.COUPLING,
+                  dipole_frames=1, mu_jitter=0.0),
+        keywords=synth.c2_keywords(Singles=5, Length=300, RunTimes="8 2 8", Samplerate=40, Technique="EAIR")),
+}
+
+
+def materialise(case, directory):
+    """Write the trajectory (and shift file) of a case; returns the file dict."""
+    s = synth.spec(**case["spec"])
+    files = synth.write(s, directory, anharm=case.get("anharm", False))
+    if case.get("shift"):
+        path = os.path.join(directory, "Shift.txt")
+        with open(path, "w") as f:
+            f.write("%d\n" % len(case["shift"]))
+            for site, a, b in case["shift"]:
+                f.write("%d %f %f\n" % (site, a, b))
+        files["shift"] = path
+    return files
+
+
+def main():
+    manifest = {}
+    for name, case in CASES.items():
+        work = tempfile.mkdtemp(prefix="golden_")
+        try:
+            files = materialise(case, work)
+            inp = synth.write_input(os.path.join(work, "input"), case["keywords"], files)
+            oracle.run_reference(inp, work)
+            out = {}
+            if case["keywords"]["Technique"] == "Absorption":
+                out["td"] = np.loadtxt(os.path.join(work, "TD_Absorption.dat"), ndmin=2)
+                out["spec"] = np.loadtxt(os.path.join(work, "Absorption.dat"), ndmin=2)
+            else:
+                p = oracle.params(case["keywords"], files)
+                R = np.zeros((6, 2, p.tmax3, p.tmax1))
+                for k, fn in enumerate(oracle.R2D_FILES):
+                    R[k, 0], R[k, 1] = oracle.read_2d(os.path.join(work, fn), p.tmax1, p.tmax3)
+                out["R"] = R
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+            manifest[name] = {k: v for k, v in case.items()}
+            print("golden", name, {k: v.shape for k, v in out.items()})
+        finally:
+            shutil.rmtree(work, ignore_errors=True)
+    with open(os.path.join(HERE, "cases.json"), "w") as f:
+        json.dump(manifest, f, indent=1, sort_keys=True)
+
+
+if __name__ == "__main__":
+    main()
