@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Benchmark of the NISE propagation engine on one node.
+
+Workload (default): batched linear absorption, Propagation Sparse (exact
+propagator, Threshold 0), N = 1024 sites on an 8x8x16 lattice (8 A spacing,
+static point-dipole couplings cut at 2 cm^-1), OU site energies (15000 cm^-1,
+sigma 300, tau 50 fs), 100000 frames x 1 fs, RunTimes 256, Samplerate 50:
+1995 start points x 3 polarisations = 1.57e9 site-steps per step.  Seeded
+synthetic trajectory (no dataset exists for this benchmark).
+
+A step is one whole job: every start point and polarisation propagated
+through its 256 frames, the response reduced and the 1D spectrum computed.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (under torch.distributed.run) every rank runs an independent
+replica of the job on its own GPU (replicas only: the path has no exchange
+step); value = site-steps of all ranks / max device time over ranks.
+
+--impl reference times the reference's own CPU propagator
+(propagate_vector, compiled from the reference sources into
+oracle/_ref/ref_bench) on the same workload's Hamiltonian: one vector step
+per host thread, all threads concurrently; rank 0 only.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "site-steps/s & time-to-spectrum: batched vs plain on 1 B200, <=1e-5 vs CPU"
+UNIT = "site-steps/s"
+WORKLOAD = "batched linear absorption, Propagation Sparse (exact exp(-iH dt), Threshold 0), N=1024 lattice"
+
+
+def parse():
+    a = argparse.ArgumentParser()
+    a.add_argument("--gpus", type=int, default=1)
+    a.add_argument("--steps", type=int, default=10)
+    a.add_argument("--warmup", type=int, default=3)
+    a.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    a.add_argument("--frames", type=int, default=100000, help="trajectory length (default: the full workload)")
+    a.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline (profiling runs)")
+    return a.parse_args()
+
+
+def config_dict(frames, extra=None):
+    d = {"workload": WORKLOAD, "sites": 1024, "frames": frames, "timestep_fs": 1.0, "tmax1": 256,
+         "samplerate": 50, "polarisations": 3, "propagation": "Sparse", "threshold": 0,
+         "hamiltonian": "Coupling (static point-dipole couplings, |J| >= 2 cm^-1)",
+         "l2": "inputs larger than L2 (410 MB trajectory streamed per step)", "parallelism": "replicas"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+def workload(frames):
+    from nise_2017_b200 import synth
+    s = synth.c1_spec(frames=frames)
+    kw = synth.c1_keywords(Length=frames)
+    return s, kw
+
+
+def site_steps(kw_len, n=1024, tmax=256, sample=50):
+    nsamp = (kw_len - tmax - 1) // sample + 1
+    return nsamp, 3 * nsamp * n * tmax
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": len(self.rows)}
+        try:
+            sm = [float(r[1]) for r in self.rows]
+            out["sm_mhz"] = statistics.median(sm) if sm else None
+            out["sm_max_mhz"] = float(self.rows[0][2]) if self.rows else None
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            reasons = set()
+            for r in self.rows:
+                for i, nm in enumerate(names):
+                    if r[5 + i].lower() == "active":
+                        reasons.add(nm)
+            out["reasons"] = sorted(reasons)
+        except (ValueError, IndexError):
+            pass
+        return out
+
+
+def read_traffic():
+    """DRAM bytes per launch (dram__bytes_read.sum + write) from the committed ncu summary."""
+    out = {}
+    try:
+        with open(os.path.join(ROOT, "profiles", "dram_traffic.txt")) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) == 2:
+                    out[parts[0]] = float(parts[1])
+    except (OSError, ValueError):
+        pass
+    return out
+
+
+def cpu_baseline(frames_dir, threads, steps=1):
+    """The reference's propagate_vector (oracle/_ref/ref_bench) on this workload's Hamiltonian."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
+    if not os.path.exists(exe):
+        return None, "oracle/_ref/ref_bench not built"
+    env = dict(os.environ, OPENBLAS_NUM_THREADS="1", OMP_NUM_THREADS=str(threads))
+    cmd = [exe, os.path.join(frames_dir, "Energy.bin"), os.path.join(frames_dir, "Coupling.bin"), "1024", "0", "2",
+           "1", "5", "0", "13500", "16500", str(threads), str(steps)]
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True, env=env)
+    if r.returncode != 0:
+        return None, r.stdout[-300:]
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    return d, None
+
+
+def write_small_trajectory(directory, frames=4):
+    from nise_2017_b200 import synth
+    s = synth.c1_spec(frames=frames)
+    synth.write(s, directory)
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import nise_2017_b200 as nise
+    from nise_2017_b200 import synth
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    spec, kw = workload(args.frames)
+    nsamp, per_step = site_steps(args.frames)
+    n = spec.n_sites
+    e_bytes = spec.frames * (4 + 4 * n)
+    d_bytes = 4 + 12 * n
+    c_bytes = 4 + 4 * n * (n + 1) // 2
+    E = torch.empty(e_bytes, dtype=torch.uint8, pin_memory=True)
+    D = torch.empty(d_bytes, dtype=torch.uint8, pin_memory=True)
+    C = torch.empty(c_bytes, dtype=torch.uint8, pin_memory=True)
+    rc = synth.lib().nise_synth_fill(ctypes.byref(spec), E.data_ptr(), D.data_ptr(), C.data_ptr(), None, None)
+    assert rc == 0
+    stream = torch.cuda.current_stream()
+
+    def ctx_for(mode, **extra):
+        p = nise.params_from_keywords(dict(kw, **extra), device=local, launch_mode=mode)
+        c = nise.Context(p)
+        c.set_stream(stream.cuda_stream)
+        return c
+
+    def trajectory(c):
+        lib = nise.lib()
+        rc = lib.nise_set_trajectory(c._h, E.data_ptr(), e_bytes, D.data_ptr(), d_bytes, C.data_ptr(), c_bytes,
+                                     None, 0, None, 0)
+        c._check(rc)
+
+    def one_step(c):
+        re, im, ns = c.absorption()
+        tot, main, launches = c.timing()
+        fl, hb = c.work()
+        w, sr, si = c.absorption_fft(re, im, ns)
+        return main, launches + 2, fl, hb, (re, im, ns, len(w))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    c = ctx_for(nise.BATCHED)
+    trajectory(c)
+    for _ in range(max(args.warmup, 3)):
+        one_step(c)
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    mains, launches, flops = [], 0, 0.0
+    ev0.record(stream)
+    for _ in range(args.steps):
+        m, l, fl, hb, last = one_step(c)
+        mains.append(m)
+        launches += l
+        flops = fl
+        hbm = hb
+    ev1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    value = world * per_step * args.steps / (ms / 1e3)
+
+    # end to end through the C ABI from pinned host buffers, copies inside the timed region
+    barrier()
+    for _ in range(2):
+        trajectory(c)
+        one_step(c)
+    barrier()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        trajectory(c)
+        one_step(c)
+    ev1.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    e2e_value = world * per_step * args.steps / (e2e_ms / 1e3)
+    fft = max(c.params.fft, c.params.tmax1)
+    h2d = e_bytes + d_bytes + c_bytes
+    d2h = c.params.tmax1 * 16 + fft * 16  # response sums and device spectrum
+
+    # plain: one start point (3 polarisations) per launch, over the first
+    # PLAIN_SAMPLES start points of the same job (throughput per launch does
+    # not depend on how many launches follow)
+    plain_samples = min(100, nsamp)
+    cp = ctx_for(nise.PLAIN, EndPoint=plain_samples)
+    trajectory(cp)
+    one_step(cp)
+    barrier()
+    ev0.record(stream)
+    one_step(cp)
+    ev1.record(stream)
+    barrier()
+    plain_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    plain_value = world * 3 * plain_samples * n * 256 / (plain_ms / 1e3)
+    cp.close()
+
+    main_ms = statistics.mean(mains)
+    achieved = flops / (main_ms / 1e3) / 1e12
+    peak = nise.fp32_peak(local)
+    traffic = read_traffic().get("k_abs_taylor_fp32_per_launch")
+    out = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            with tempfile.TemporaryDirectory() as td:
+                write_small_trajectory(td)
+                threads = min(host_threads(), 16)
+                t0 = time.time()
+                d, err = cpu_baseline(td, threads)
+                if d:
+                    cpu = {"value": d["site_steps"] / d["seconds"], "unit": UNIT, "cores": threads,
+                           "kind": "reference",
+                           "sample": "%d concurrent vector steps (one per thread) of the reference's propagate_vector "
+                                     "(Sparse, Threshold 0: ssyev_ + dense U) at N=1024 on frame 0 of this workload, "
+                                     "%.1f s wall" % (threads, d["seconds"])}
+                else:
+                    cpu = {"value": None, "unit": UNIT, "cores": threads, "kind": "reference", "sample": err}
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (propagation), f64 (response sums)",
+            "data": "synthetic (seeded OU trajectory, point-dipole lattice couplings)",
+            "config": config_dict(args.frames, {"start_points": nsamp}),
+            "time_to_spectrum_s": e2e_ms / args.steps / 1e3,
+            "plain": {"value": plain_value, "unit": UNIT, "ms": plain_ms, "start_points": plain_samples,
+                      "mode": "one start point (3 polarisations) per launch"},
+            "batched_over_plain": value / plain_value,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": e2e_ms / args.steps},
+            "roofline": {"bound": "fp32", "kernel": "k_abs_taylor", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": traffic,
+                         "peak_source": "measured in-process FP32 FMA throughput (nise_probe_fp32_peak)",
+                         "algorithmic_flops_per_launch": flops, "algorithmic_hbm_bytes_per_launch": hbm,
+                         "kernel_ms": main_ms},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(out), flush=True)
+    c.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return None
+    threads = min(host_threads(), 64)
+    steps = min(args.steps, 3)  # each timed step is ~30 s of reference CPU time per thread
+    with tempfile.TemporaryDirectory() as td:
+        write_small_trajectory(td)
+        exe = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
+        if not os.path.exists(exe):
+            out = {"impl": "reference", "unavailable": "oracle/_ref/ref_bench was not built (needs the reference "
+                                                       "sources at build time)"}
+            print(json.dumps(out), flush=True)
+            return out
+        for _ in range(args.warmup):  # untimed: pages in the binary and OpenBLAS
+            subprocess.run([exe, os.path.join(td, "Energy.bin"), os.path.join(td, "Coupling.bin"), "1024", "1",
+                            "2", "1", "5", "0", "13500", "16500", "1", "1"], stdout=subprocess.DEVNULL)
+        secs, site = 0.0, 0
+        for _ in range(steps):
+            d, err = cpu_baseline(td, threads)
+            if d is None:
+                out = {"impl": "reference", "unavailable": "reference harness failed: %s" % err}
+                print(json.dumps(out), flush=True)
+                return out
+            secs += d["seconds"]
+            site += d["site_steps"]
+    value = site / secs
+    sample = ("%d concurrent vector steps per step (one per host thread) of the reference's propagate_vector "
+              "(Sparse, Threshold 0) at N=1024" % threads)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+        "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": secs / steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded OU trajectory, point-dipole lattice couplings)",
+        "config": config_dict(args.frames),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+    return out
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)

@@ -159,9 +159,20 @@ int nise_write_spectrum(const char *path, const double *freq, const double *spec
 /* print2D: divides by sample_count, halves the t3 = 0 row, writes t1 t2 t3 Re Im. */
 int nise_write_2d(const char *path, const nise_params *p, const double *re, const double *im, int sample_count);
 
-/* Device time of the kernels of the last compute call (ms), and how many of
+/* Run this context's device work on the caller's CUDA stream (a
+ * cudaStream_t passed as a pointer; NULL restores the context's own stream). */
+int nise_set_stream(nise_ctx *ctx, void *stream);
+/* Device time of the last compute call (ms, CUDA events on the context's
+ * stream): the whole call and its main propagation kernel(s), and how many of
  * this library's kernels it launched. */
-int nise_last_timing(const nise_ctx *ctx, double *kernel_ms, long *launches);
+int nise_last_timing(const nise_ctx *ctx, double *total_ms, double *main_kernel_ms, long *launches);
+/* Algorithmic work of the last compute call's main kernel(s): floating-point
+ * operations and HBM bytes (every trajectory frame and dipole record read
+ * once, state kept on chip). */
+int nise_last_work(const nise_ctx *ctx, double *flops, double *hbm_bytes);
+/* Measured FP32 FMA throughput of a device (TFLOP/s), the roofline
+ * denominator of the CUDA-core kernels. */
+int nise_probe_fp32_peak(int device, double *tflops);
 
 #ifdef __cplusplus
 }

@@ -34,7 +34,8 @@ EXPORTED = [
     "nise_params_default", "nise_read_input", "nise_create", "nise_destroy", "nise_last_error",
     "nise_global_error", "nise_load_files", "nise_set_trajectory", "nise_set_singleshift", "nise_absorption",
     "nise_absorption_fft", "nise_2dir", "nise_propagate", "nise_propagate_doubles", "nise_write_td_absorption",
-    "nise_write_spectrum", "nise_write_2d", "nise_last_timing",
+    "nise_write_spectrum", "nise_write_2d", "nise_set_stream", "nise_last_timing", "nise_last_work",
+    "nise_probe_fp32_peak",
 ]
 
 
@@ -98,7 +99,10 @@ def lib():
         L.nise_write_td_absorption.argtypes = [ctypes.c_char_p, P, dp, dp, ctypes.c_int]
         L.nise_write_spectrum.argtypes = [ctypes.c_char_p, dp, dp, dp, ctypes.c_int]
         L.nise_write_2d.argtypes = [ctypes.c_char_p, P, dp, dp, ctypes.c_int]
-        L.nise_last_timing.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_long)]
+        L.nise_set_stream.argtypes = [vp, vp]
+        L.nise_last_timing.argtypes = [vp, dp, dp, ctypes.POINTER(ctypes.c_long)]
+        L.nise_last_work.argtypes = [vp, dp, dp]
+        L.nise_probe_fp32_peak.argtypes = [ctypes.c_int, dp]
         _lib = L
     return _lib
 
@@ -255,11 +259,33 @@ class Context:
             None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
         return re, im
 
+    def set_stream(self, stream_ptr):
+        """Enqueue this context's device work on a caller CUDA stream (int handle, 0 = own)."""
+        self._check(lib().nise_set_stream(self._h, ctypes.c_void_p(stream_ptr or None)))
+
     def timing(self):
-        ms = ctypes.c_double(0)
+        """(total ms, main kernel ms, kernel launches) of the last compute call."""
+        tot = ctypes.c_double(0)
+        main = ctypes.c_double(0)
         n = ctypes.c_long(0)
-        lib().nise_last_timing(self._h, ctypes.byref(ms), ctypes.byref(n))
-        return ms.value, n.value
+        lib().nise_last_timing(self._h, ctypes.byref(tot), ctypes.byref(main), ctypes.byref(n))
+        return tot.value, main.value, n.value
+
+    def work(self):
+        """(flops, hbm_bytes) of the last compute call's main kernel(s)."""
+        f = ctypes.c_double(0)
+        b = ctypes.c_double(0)
+        lib().nise_last_work(self._h, ctypes.byref(f), ctypes.byref(b))
+        return f.value, b.value
+
+
+def fp32_peak(device=0):
+    """Measured FP32 FMA throughput (TFLOP/s) of a device."""
+    t = ctypes.c_double(0)
+    rc = lib().nise_probe_fp32_peak(device, ctypes.byref(t))
+    if rc != 0:
+        raise NiseError(rc, lib().nise_global_error().decode())
+    return t.value
 
 
 def write_td_absorption(path, params, re, im, samples):

@@ -24,6 +24,8 @@ CU_SOURCES = [
     "absorption.cu",
     "fft.cu",
     "twodir.cu",
+    "eigen.cu",
+    "util.cu",
 ]
 CPP_SOURCES = [
     "api.cpp",

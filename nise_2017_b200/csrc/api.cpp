@@ -93,9 +93,12 @@ extern "C" int nise_create(const nise_params *p, nise_ctx **out) {
     }
     c->shifte = (p->max1 + p->min1) / 2;
     int e = (int)cudaSetDevice(p->device);
-    if (!e) e = (int)cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (!e) e = (int)cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+    c->stream = c->own_stream;
     if (!e) e = (int)cudaEventCreate(&c->ev0);
     if (!e) e = (int)cudaEventCreate(&c->ev1);
+    if (!e) e = (int)cudaEventCreate(&c->evk0);
+    if (!e) e = (int)cudaEventCreate(&c->evk1);
     if (e) {
         int rc = nise_cuda(nullptr, e, "device setup");
         delete c;
@@ -112,6 +115,7 @@ void nise_free_traj(nise_ctx *c) {
         if (q) cudaFree(q);
     c->d_energy = c->d_dipole = c->d_hc = c->d_mu_static = c->d_anh = c->d_over = c->d_shift_ab = nullptr;
     c->d_shift_site = nullptr;
+    c->cap_energy = c->cap_dipole = c->cap_anh = c->cap_over = c->cap_hc = c->cap_mu = c->cap_ab = 0;
     c->loaded = false;
 }
 
@@ -119,24 +123,36 @@ extern "C" void nise_destroy(nise_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->p.device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    c->stream = c->own_stream;
     nise_free_traj(c);
-    if (c->ev0) cudaEventDestroy(c->ev0);
-    if (c->ev1) cudaEventDestroy(c->ev1);
-    if (c->stream) cudaStreamDestroy(c->stream);
+    cudaEvent_t evs[] = {c->ev0, c->ev1, c->evk0, c->evk1};
+    for (cudaEvent_t ev : evs)
+        if (ev) cudaEventDestroy(ev);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
 }
 
 extern "C" const char *nise_last_error(const nise_ctx *c) { return c ? c->err.c_str() : g_error.c_str(); }
 
-static int upload(nise_ctx *c, float **dst, const void *src, size_t bytes) {
-    if (*dst) {
-        cudaFree(*dst);
+// Copy host bytes to a context buffer, keeping the allocation when it is
+// already large enough (repeated uploads of same-sized trajectories allocate
+// nothing).
+static int upload(nise_ctx *c, float **dst, size_t *cap, const void *src, size_t bytes) {
+    if (!src || !bytes) {
+        if (*dst) cudaFree(*dst);
         *dst = nullptr;
+        *cap = 0;
+        return NISE_OK;
     }
-    if (!src || !bytes) return NISE_OK;
-    int e = (int)cudaMalloc((void **)dst, bytes);
-    if (e) return nise_fail(c, NISE_ERR_NOMEM, "device allocation of %zu bytes failed", bytes);
-    e = (int)cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
+    if (bytes > *cap) {
+        if (*dst) cudaFree(*dst);
+        *dst = nullptr;
+        *cap = 0;
+        if (cudaMalloc((void **)dst, bytes) != cudaSuccess)
+            return nise_fail(c, NISE_ERR_NOMEM, "device allocation of %zu bytes failed", bytes);
+        *cap = bytes;
+    }
+    int e = (int)cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
     return nise_cuda(c, e, "trajectory upload");
 }
 
@@ -158,12 +174,12 @@ extern "C" int nise_set_trajectory(nise_ctx *c, const void *energy, size_t energ
     if (c->e_frames < 1) return nise_fail(c, NISE_ERR_IO, "Hamiltonian trajectory file to short");
     if (c->d_frames < 1) return nise_fail(c, NISE_ERR_IO, "Dipole trajectory file to short");
     int rc;
-    if ((rc = upload(c, &c->d_energy, energy, (size_t)c->e_frames * 4 * c->e_words))) return rc;
-    if ((rc = upload(c, &c->d_dipole, dipole, (size_t)c->d_frames * 4 * c->d_words))) return rc;
+    if ((rc = upload(c, &c->d_energy, &c->cap_energy, energy, (size_t)c->e_frames * 4 * c->e_words))) return rc;
+    if ((rc = upload(c, &c->d_dipole, &c->cap_dipole, dipole, (size_t)c->d_frames * 4 * c->d_words))) return rc;
     c->a_frames = anharm ? (long)(anharm_bytes / (4 * (size_t)(1 + N))) : 0;
     c->o_frames = overtone ? (long)(overtone_bytes / (4 * (size_t)(1 + 3L * N))) : 0;
-    if ((rc = upload(c, &c->d_anh, anharm, (size_t)c->a_frames * 4 * (1 + N)))) return rc;
-    if ((rc = upload(c, &c->d_over, overtone, (size_t)c->o_frames * 4 * (1 + 3L * N)))) return rc;
+    if ((rc = upload(c, &c->d_anh, &c->cap_anh, anharm, (size_t)c->a_frames * 4 * (1 + N)))) return rc;
+    if ((rc = upload(c, &c->d_over, &c->cap_over, overtone, (size_t)c->o_frames * 4 * (1 + 3L * N)))) return rc;
     c->h_hc.clear();
     c->h_mu_static.clear();
     if (coupling_type) {
@@ -180,11 +196,11 @@ extern "C" int nise_set_trajectory(nise_ctx *c, const void *energy, size_t energ
             }
         const float *m = (const float *)dipole + 1;
         c->h_mu_static.assign(m, m + 3L * N);
-        if ((rc = upload(c, &c->d_hc, c->h_hc.data(), sizeof(float) * c->nn2))) return rc;
-        if ((rc = upload(c, &c->d_mu_static, c->h_mu_static.data(), sizeof(float) * 3 * N))) return rc;
+        if ((rc = upload(c, &c->d_hc, &c->cap_hc, c->h_hc.data(), sizeof(float) * c->nn2))) return rc;
+        if ((rc = upload(c, &c->d_mu_static, &c->cap_mu, c->h_mu_static.data(), sizeof(float) * 3 * N))) return rc;
     } else {
-        if ((rc = upload(c, &c->d_hc, nullptr, 0))) return rc;
-        if ((rc = upload(c, &c->d_mu_static, nullptr, 0))) return rc;
+        if ((rc = upload(c, &c->d_hc, &c->cap_hc, nullptr, 0))) return rc;
+        if ((rc = upload(c, &c->d_mu_static, &c->cap_mu, nullptr, 0))) return rc;
     }
     int e = (int)cudaStreamSynchronize(c->stream);
     if (e) return nise_cuda(c, e, "trajectory upload");
@@ -210,7 +226,7 @@ extern "C" int nise_set_singleshift(nise_ctx *c, int n, const int *sites, const 
             return nise_fail(c, NISE_ERR_NOMEM, "device allocation failed");
         cudaMemcpyAsync(c->d_shift_site, sites, sizeof(int) * n, cudaMemcpyHostToDevice, c->stream);
     }
-    if ((rc = upload(c, &c->d_shift_ab, n ? ab.data() : nullptr, sizeof(float) * 2 * n))) return rc;
+    if ((rc = upload(c, &c->d_shift_ab, &c->cap_ab, n ? ab.data() : nullptr, sizeof(float) * 2 * n))) return rc;
     return nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "SingleShift upload");
 }
 
@@ -355,8 +371,20 @@ extern "C" int nise_absorption(nise_ctx *c, double *re_S, double *im_S, int *sam
     DevBuf<double2> resp, out;
     if ((rc = resp.alloc(c, (size_t)nvec * tmax)) || (rc = out.alloc(c, tmax))) return rc;
     c->launches = 0;
+    c->last_flops = c->last_bytes = 0;
     const bool plain = p.launch_mode == NISE_PLAIN;
     size_t rsz = prec == NISE_FP32 ? sizeof(float) : sizeof(double);
+    cudaEventRecord(c->ev0, c->stream);
+    // Vectors crossing each propagated frame: used for the algorithmic work.
+    std::vector<long> cross(nf, 0);
+    for (int s = 0; s < nsamp; s++) {
+        long a = (long)(begin + s) * p.sample - f0;
+        for (int t = 0; t < tmax - 1; t++) cross[a + t] += 3;
+    }
+    long vec_steps = 3L * nsamp * (tmax - 1);
+    // bytes: every frame read once (diagonal or full record) and the dipoles
+    c->last_bytes = (double)nf * 4 * (p.hamiltonian == NISE_HAM_COUPLING ? N : c->nn2) +
+                    (double)(p.hamiltonian == NISE_HAM_COUPLING ? 3 * N : (nf + 1) * 3L * N) * 4;
 
     if (p.propagation == NISE_PROP_COUPLING) {
         std::vector<int2> pairs;
@@ -376,10 +404,12 @@ extern "C" int nise_absorption(nise_ctx *c, double *re_S, double *im_S, int *sam
         P.pairs = dpairs.p;
         P.U = U.p;
         P.rot = rot.p;
-        cudaEventRecord(c->ev0, c->stream);
+        // per vector step: ts * (K rotations * 12 flops + 2 N half-phases * 6 flops)
+        c->last_flops = (double)vec_steps * p.ts * (12.0 * P.k + 12.0 * N);
         if ((rc = nise_cuda(c, launch_prep_trotter(prec, T, P, J.f64_sub, J.f32_sub, c->stream), "Trotter prep")))
             return rc;
         c->launches += 1 + (P.rot_static ? 1 : 0);
+        cudaEventRecord(c->evk0, c->stream);
         if (plain) {
             for (int s = 0; s < nsamp; s++) {
                 AbsJob Js = J;
@@ -395,6 +425,7 @@ extern "C" int nise_absorption(nise_ctx *c, double *re_S, double *im_S, int *sam
                 return rc;
             c->launches++;
         }
+        cudaEventRecord(c->evk1, c->stream);
     } else if (p.propagation == NISE_PROP_RK4) {
         std::vector<int2> pairs, ent;
         if ((rc = nise_pattern(c, f0, nf, pairs))) return rc;
@@ -415,9 +446,11 @@ extern "C" int nise_absorption(nise_ctx *c, double *re_S, double *im_S, int *sam
         if ((rc = val.alloc(c, rsz * (size_t)nf * P.k))) return rc;
         P.entries = dent.p;
         P.val = val.p;
-        cudaEventRecord(c->ev0, c->stream);
+        // per sub-step: 4 stages over the list (off-diagonal entries twice) + update and norms
+        c->last_flops = (double)vec_steps * p.ts * (4.0 * 4.0 * (2.0 * P.k - N) + 20.0 * N);
         if ((rc = nise_cuda(c, launch_prep_rk4(prec, T, P, J.f64_sub, J.f32_sub, c->stream), "RK4 prep"))) return rc;
         c->launches++;
+        cudaEventRecord(c->evk0, c->stream);
         if (plain) {
             for (int s = 0; s < nsamp; s++) {
                 AbsJob Js = J;
@@ -432,6 +465,7 @@ extern "C" int nise_absorption(nise_ctx *c, double *re_S, double *im_S, int *sam
             if ((rc = nise_cuda(c, launch_abs_rk4(prec, T, P, J, resp.p, c->stream), "RK4 propagation"))) return rc;
             c->launches++;
         }
+        cudaEventRecord(c->evk1, c->stream);
     } else {
         // Sparse / Diagonal: exact propagator exp(-i H dt) (propagate_vec_DIA,
         // propagate.c:60-125).  Threshold > 0 keeps only large elements of U
@@ -485,10 +519,18 @@ extern "C" int nise_absorption(nise_ctx *c, double *re_S, double *im_S, int *sam
         P.f0 = f0;
         P.nf = nf;
         P.singleshift = c->nshift > 0;
-        cudaEventRecord(c->ev0, c->stream);
         if ((rc = nise_cuda(c, launch_prep_taylor(prec, T, P, rowabs, J.f, dorder.p, c->stream), "Taylor prep")))
             return rc;
         c->launches++;
+        // per vector step and Taylor order: nnz complex*real products (4 flops)
+        // and the diagonal, scaling and accumulation (6 flops per site)
+        std::vector<int> order(nf);
+        cudaMemcpyAsync(order.data(), dorder.p, sizeof(int) * nf, cudaMemcpyDeviceToHost, c->stream);
+        if ((rc = nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "Taylor prep"))) return rc;
+        double orders = 0;
+        for (long t = 0; t < nf; t++) orders += (double)order[t] * cross[t];
+        c->last_flops = orders * (4.0 * P.nnz + 6.0 * N);
+        cudaEventRecord(c->evk0, c->stream);
         if (plain) {
             for (int s = 0; s < nsamp; s++) {
                 AbsJob Js = J;
@@ -504,6 +546,7 @@ extern "C" int nise_absorption(nise_ctx *c, double *re_S, double *im_S, int *sam
                 return rc;
             c->launches++;
         }
+        cudaEventRecord(c->evk1, c->stream);
     }
     if ((rc = nise_cuda(c, launch_reduce_resp(resp.p, nvec, tmax, out.p, c->stream), "response reduction")))
         return rc;
@@ -512,9 +555,7 @@ extern "C" int nise_absorption(nise_ctx *c, double *re_S, double *im_S, int *sam
     std::vector<double2> h(tmax);
     cudaMemcpyAsync(h.data(), out.p, sizeof(double2) * tmax, cudaMemcpyDeviceToHost, c->stream);
     if ((rc = nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "absorption"))) return rc;
-    float ms = 0;
-    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-    c->last_ms = ms;
+    nise_collect_timing(c);
     for (int t = 0; t < tmax; t++) {
         re_S[t] = h[t].x;
         im_S[t] = h[t].y;
@@ -581,10 +622,33 @@ extern "C" int nise_absorption_fft(nise_ctx *c, const double *re_S, const double
     return NISE_OK;
 }
 
-extern "C" int nise_last_timing(const nise_ctx *c, double *kernel_ms, long *launches) {
+void nise_collect_timing(nise_ctx *c) {
+    float ms = 0, kms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    cudaEventElapsedTime(&kms, c->evk0, c->evk1);
+    c->last_ms = ms;
+    c->last_main_ms = kms;
+}
+
+extern "C" int nise_set_stream(nise_ctx *c, void *stream) {
+    if (!c) return nise_fail(nullptr, NISE_ERR_ARG, "null context");
+    cudaStreamSynchronize(c->stream);
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    return NISE_OK;
+}
+
+extern "C" int nise_last_timing(const nise_ctx *c, double *total_ms, double *main_kernel_ms, long *launches) {
     if (!c) return NISE_ERR_ARG;
-    if (kernel_ms) *kernel_ms = c->last_ms;
+    if (total_ms) *total_ms = c->last_ms;
+    if (main_kernel_ms) *main_kernel_ms = c->last_main_ms;
     if (launches) *launches = c->launches;
+    return NISE_OK;
+}
+
+extern "C" int nise_last_work(const nise_ctx *c, double *flops, double *hbm_bytes) {
+    if (!c) return NISE_ERR_ARG;
+    if (flops) *flops = c->last_flops;
+    if (hbm_bytes) *hbm_bytes = c->last_bytes;
     return NISE_OK;
 }
 

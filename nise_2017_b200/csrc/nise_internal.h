@@ -15,9 +15,11 @@ struct nise_ctx {
     long nn2 = 0;
     float shifte = 0;
     float thres = 0;  // Threshold after the reference's rescaling
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    double last_ms = 0;
+    cudaStream_t stream = nullptr;      // stream all work is enqueued on
+    cudaStream_t own_stream = nullptr;  // the context's own stream
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evk0 = nullptr, evk1 = nullptr;
+    double last_ms = 0, last_main_ms = 0;
+    double last_flops = 0, last_bytes = 0;
     long launches = 0;
     bool loaded = false;
     // trajectory in device memory (record images, 4-byte words)
@@ -26,6 +28,7 @@ struct nise_ctx {
     int *d_shift_site = nullptr;
     int nshift = 0;
     long e_words = 0, e_frames = 0, d_words = 0, d_frames = 0, a_frames = 0, o_frames = 0;
+    size_t cap_energy = 0, cap_dipole = 0, cap_anh = 0, cap_over = 0, cap_hc = 0, cap_mu = 0, cap_ab = 0;
     std::vector<float> h_hc;        // coupling frame (HamiltonianType Coupling), shifted, cut
     std::vector<float> h_mu_static; // dipoles of frame 0 (HamiltonianType Coupling)
 };
@@ -37,6 +40,8 @@ double nise_f64(const nise_params &p, int sign, int m);
 DevTraj nise_devtraj(const nise_ctx *c);
 int nise_pattern(nise_ctx *c, long f0, long nf, std::vector<int2> &pairs);
 int nise_check_frames(nise_ctx *c, long last_frame);
+// Device time between ev0/ev1 (whole call) and evk0/evk1 (main kernels).
+void nise_collect_timing(nise_ctx *c);
 
 // Stream-ordered device buffer owned by one call.
 template <typename T> struct DevBuf {

@@ -78,10 +78,10 @@ int main(int argc, char *argv[]) {
         nise_destroy(c);
         return 2;
     }
-    double ms = 0;
+    double ms = 0, main_ms = 0;
     long launches = 0;
-    nise_last_timing(c, &ms, &launches);
-    printf(" Device time %.3f ms in %ld kernel launches\n", ms, launches);
+    nise_last_timing(c, &ms, &main_ms, &launches);
+    printf(" Device time %.3f ms (propagation %.3f ms) in %ld kernel launches\n", ms, main_ms, launches);
     nise_destroy(c);
     return 0;
 }

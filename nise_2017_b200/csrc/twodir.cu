@@ -1,15 +1,929 @@
-// 2DIR family (calc_2DIR.c:22-629) on the device.
+// 2DIR family (calc_2DIR.c:22-629) on one GPU.
+//
+// The reference loops over (start point, molecular polarisation) work items
+// and, inside each, propagates dozens of vectors frame by frame.  Here the
+// work of a chunk of start points is reorganised by linearity and shared:
+//
+//  * singles vectors depend on one dipole component only, so the t1 vectors
+//    (leftn), the GB t3 vector (mut3), leftr and their t2/t3 propagations are
+//    computed once per component x in {x,y,z} instead of once per molecular
+//    polarisation (21);
+//  * the excited-state-absorption (EA) "right" vectors are propagated
+//    backwards in the reference (sign -1, propagate.c:1552-1560); they equal
+//    the complex conjugates of the SE vectors propagated forwards, operation
+//    by operation, for every scheme here (Trotter rotations, RK4, eigen
+//    propagator), so the conjugated SE snapshots are used bit for bit;
+//  * the doubles vectors depend on a pair of components: fr on (px1,px2) and
+//    ft1[t1] on (px0,px2), 9 + 9*tmax1 vectors instead of 21*(1+tmax1).
+//
+// Kernels (one chunk of start points at a time):
+//   k2d_gb1      leftn_x[t1]: mu_x(tj-t1) propagated t1 steps; GB t1 dots
+//   k2d_gb3      mut3_x: mu_x(tk) propagated through t3; GB t3 dots
+//   k2d_t2       t2 eigen steps (propagate_t2_DIA) of leftr_x and leftn_x[t1]
+//   k2d_se       SE t3 propagation of leftr_x and leftn_x[t1], snapshots per t3
+//   k2d_doubles  doubles (two-exciton) Trotter propagation of fr / ft1[t1],
+//                dipole_double_last projections and EA dot products per t3
+//   k2d_response GB + SE + EA contributions per (start point, t3, t1) with the
+//                21 molecular-frame weights and the lifetime factors
+// followed by a deterministic sum over start points.
+//
+// FP32 contexts keep the reference's single-precision operations (states,
+// rotations, dipole operators) and accumulate every dot product and response
+// sum in FP64, like the FP32/FP64-sum oracle.
+#include <cstring>
+#include <vector>
+
 #include "common.cuh"
+#include "eigen.h"
 #include "engine.h"
 #include "nise_internal.h"
+#include "schemes.cuh"
+
+namespace {
+
+// polar() (polar.c:36-105); the weights of polarweight() (polar.c:12-33)
+// are uploaded to c_w as the float values the reference computes.
+__constant__ int c_px[21][4] = {{0, 0, 0, 0}, {1, 1, 1, 1}, {2, 2, 2, 2}, {0, 0, 1, 1}, {0, 0, 2, 2}, {1, 1, 0, 0},
+                                 {1, 1, 2, 2}, {2, 2, 0, 0}, {2, 2, 1, 1}, {0, 1, 0, 1}, {0, 2, 0, 2}, {1, 0, 1, 0},
+                                 {1, 2, 1, 2}, {2, 0, 2, 0}, {2, 1, 2, 1}, {0, 1, 1, 0}, {0, 2, 2, 0}, {1, 0, 0, 1},
+                                 {1, 2, 2, 1}, {2, 0, 0, 2}, {2, 1, 1, 2}};
+__constant__ float c_w[3][21];
+
+struct TwoD {
+    DevTraj T;
+    int n, T1, T2, T3, ts, sample, s0, S;  // S start points in this chunk, the first is s0
+    int gb, se, ea;
+    int prop;                 // NISE_PROP_*
+    float anh;                // Anharmonicity keyword (0: per-frame files)
+    long f0;                  // first frame of the coefficient tables
+    const int2 *pairs;        // Trotter pattern (a < b, lexicographic)
+    int K;
+    const void *U, *rot;      // Trotter tables: U[t][n], rot[t][K] (or [K] static)
+    int rot_static;
+    const int2 *ent;          // RK4 entries (a <= b)
+    int Kr;
+    const void *rkval;        // RK4 values [t][Kr]
+    long e0;                  // eigen data for frames [e0, e0 + ne)
+    const double *eV, *ew;    // V [ne][n][n], w [ne][n]
+    float f32_full;           // deltat*icm2ifs*2pi in float
+    double f64_full;
+    float f32_dsub;           // deltat*icm2ifs*2pi/ts in float (propagate.c:905)
+    double f64_dsub;
+    void *L;                  // [S][3][T1][n] R2  leftn_x[t1]
+    void *Lr;                 // [S][3][n] R2      leftr_x
+    void *SE;                 // [S][T3][NV][n] R2 snapshots, NV = 3 + 3*T1 (leftr_x, then leftn_x[t1])
+    double2 *gbt1;            // [S][3 p0][3 p1][T1]
+    double2 *gbt3;            // [S][3 p2][3 p3][T3]
+    double2 *eaI, *eaII;      // [S][T3][21][T1]
+    double *Rs;               // [S][12][T3][T1]
+    const float *lt;          // [T3][T1]
+};
+
+__device__ __forceinline__ long tj_of(const TwoD &D, int s) { return (long)(D.s0 + s) * D.sample + D.T1; }
+__device__ __forceinline__ long tk_of(const TwoD &D, int s) { return tj_of(D, s) + D.T2; }
+__device__ __forceinline__ int nvec_se(const TwoD &D) { return 3 + 3 * D.T1; }
+
+// One singles time step of the configured scheme through frame t.
+template <typename R>
+__device__ __forceinline__ void singles_step(const TwoD &D, typename Vec2<R>::T *S, int B, int lane, long t) {
+    typedef typename Vec2<R>::T R2;
+    long fi = t - D.f0;
+    if (D.prop == NISE_PROP_RK4) {
+        rk4_apply<R>(S, B, lane, D.n, D.Kr, D.ent, (const R *)D.rkval + fi * D.Kr, D.ts);
+    } else {
+        const R2 *Uf = (const R2 *)D.U + fi * D.n;
+        const R2 *Rf = D.rot_static ? (const R2 *)D.rot : (const R2 *)D.rot + fi * D.K;
+        trotter_apply<R>(S, B, lane, D.n, D.K, D.pairs, Uf, Rf, D.ts);
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ size_t singles_lane_bytes(int n, int prop) {
+    return (prop == NISE_PROP_RK4 ? 5 : 1) * (size_t)n * sizeof(typename Vec2<R>::T);
+}
+
+// sum_i mu_i * psi_i with float products (FP32) and an FP64 sum.
+template <typename R>
+__device__ __forceinline__ double2 dot_col(const DevTraj &T, long t, int x, const typename Vec2<R>::T *S, int B,
+                                           int lane, int n) {
+    return dot_mu<R>(T, t, x, S, B, lane, n);
+}
+
+// ---------------------------------------------------------------- GB t1
+// Thread per (start point, x, pair p): t1 = p and t1 = T1-1-p, so every
+// thread does T1-1 steps (the triangle of calc_2DIR.c:215-239 balanced).
+template <typename R>
+__global__ void k2d_gb1(TwoD D) {
+    typedef typename Vec2<R>::T R2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R2 *S = (R2 *)smem_raw;
+    const int B = blockDim.x, lane = threadIdx.x, n = D.n;
+    const int P = (D.T1 + 1) / 2;
+    int g = blockIdx.x * B + lane;
+    if (g >= D.S * 3 * P) return;
+    int s = g / (3 * P), rem = g % (3 * P), x = rem / P, p = rem % P;
+    long tj = tj_of(D, s);
+    for (int pass = 0; pass < 2; pass++) {
+        int t1 = pass == 0 ? p : D.T1 - 1 - p;
+        if (pass == 1 && t1 == p) break;
+        for (int i = 0; i < n; i++) {
+            R2 z;
+            z.x = (R)traj_mu(D.T, tj - t1, x, i);
+            z.y = 0;
+            S[i * B + lane] = z;
+        }
+        for (int tm = 0; tm < t1; tm++) singles_step<R>(D, S, B, lane, tj - t1 + tm);
+        R2 *out = (R2 *)D.L + (((size_t)s * 3 + x) * D.T1 + t1) * n;
+        for (int i = 0; i < n; i++) out[i] = S[i * B + lane];
+        if (D.gb)  // t1nr/t1ni (calc_2DIR.c:244-250) for every p1
+            for (int p1 = 0; p1 < 3; p1++)
+                D.gbt1[(((size_t)s * 3 + x) * 3 + p1) * D.T1 + t1] = dot_col<R>(D.T, tj, p1, S, B, lane, n);
+    }
+}
+
+// ---------------------------------------------------------------- GB t3
+template <typename R>
+__global__ void k2d_gb3(TwoD D) {
+    typedef typename Vec2<R>::T R2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R2 *S = (R2 *)smem_raw;
+    const int B = blockDim.x, lane = threadIdx.x, n = D.n;
+    int g = blockIdx.x * B + lane;
+    if (g >= D.S * 3) return;
+    int s = g / 3, x = g % 3;
+    long tk = tk_of(D, s);
+    for (int i = 0; i < n; i++) {
+        R2 z;
+        z.x = (R)traj_mu(D.T, tk, x, i);
+        z.y = 0;
+        S[i * B + lane] = z;
+    }
+    for (int t3 = 0; t3 < D.T3; t3++) {  // calc_2DIR.c:257-299
+        long tl = tk + t3;
+        for (int p3 = 0; p3 < 3; p3++)
+            D.gbt3[(((size_t)s * 3 + x) * 3 + p3) * D.T3 + t3] = dot_col<R>(D.T, tl, p3, S, B, lane, n);
+        if (t3 < D.T3 - 1) singles_step<R>(D, S, B, lane, tl);
+    }
+}
+
+// ---------------------------------------------------------------- t2
+// propagate_t2_DIA (propagate.c:130-180): V^T, phase, V per frame, with the
+// eigenvectors in the reference's storage and FP32 operands in FP32 mode.
+template <typename R>
+__global__ void k2d_t2(TwoD D) {
+    typedef typename Vec2<R>::T R2;
+    typedef Ar<R> A;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int B = blockDim.x, lane = threadIdx.x, n = D.n;
+    R2 *S = (R2 *)smem_raw, *X = S + (size_t)n * B;
+    const int NV = nvec_se(D);
+    int g = blockIdx.x * B + lane;
+    if (g >= D.S * NV) return;
+    int s = g / NV, v = g % NV;
+    R2 *vec = v < 3 ? (R2 *)D.Lr + ((size_t)s * 3 + v) * n
+                    : (R2 *)D.L + (((size_t)s * 3 + (v - 3) / D.T1) * D.T1 + (v - 3) % D.T1) * n;
+    for (int i = 0; i < n; i++) S[i * B + lane] = vec[i];
+    long tj = tj_of(D, s);
+    for (int t2 = 0; t2 < D.T2; t2++) {
+        long fi = tj + t2 - D.e0;
+        const double *V = D.eV + fi * n * n, *w = D.ew + fi * n;
+        for (int a = 0; a < n; a++) {  // matrix_on_vector: x = V^T v
+            R xr = 0, xi = 0;
+            for (int b = 0; b < n; b++) {
+                R c = (R)V[b * n + a];
+                R2 z = S[b * B + lane];
+                xr = A::add(xr, A::mul(c, z.x));
+                xi = A::add(xi, A::mul(c, z.y));
+            }
+            R ev = (R)w[a], arg = A::mul(ev, sizeof(R) == 4 ? (R)D.f32_full : (R)D.f64_full);
+            R ur = (R)cos((double)arg), ui = (R)(-sin((double)arg));
+            R2 o;  // vector_on_vector (NISE_subs.c:71-80)
+            o.x = A::sub(A::mul(ur, xr), A::mul(ui, xi));
+            o.y = A::add(A::mul(ui, xr), A::mul(ur, xi));
+            X[a * B + lane] = o;
+        }
+        for (int a = 0; a < n; a++) {  // trans_matrix_on_vector: v = V x
+            R yr = 0, yi = 0;
+            for (int b = 0; b < n; b++) {
+                R c = (R)V[a * n + b];
+                R2 z = X[b * B + lane];
+                yr = A::add(yr, A::mul(c, z.x));
+                yi = A::add(yi, A::mul(c, z.y));
+            }
+            R2 o;
+            o.x = yr;
+            o.y = yi;
+            S[a * B + lane] = o;
+        }
+    }
+    for (int i = 0; i < n; i++) vec[i] = S[i * B + lane];
+}
+
+// ---------------------------------------------------------------- SE t3
+template <typename R>
+__global__ void k2d_se(TwoD D) {
+    typedef typename Vec2<R>::T R2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R2 *S = (R2 *)smem_raw;
+    const int B = blockDim.x, lane = threadIdx.x, n = D.n;
+    const int NV = nvec_se(D);
+    int g = blockIdx.x * B + lane;
+    if (g >= D.S * NV) return;
+    int s = g / NV, v = g % NV;
+    const R2 *vec = v < 3 ? (const R2 *)D.Lr + ((size_t)s * 3 + v) * n
+                          : (const R2 *)D.L + (((size_t)s * 3 + (v - 3) / D.T1) * D.T1 + (v - 3) % D.T1) * n;
+    for (int i = 0; i < n; i++) S[i * B + lane] = vec[i];
+    long tk = tk_of(D, s);
+    for (int t3 = 0; t3 < D.T3; t3++) {  // calc_2DIR.c:372-443
+        R2 *snap = (R2 *)D.SE + (((size_t)s * D.T3 + t3) * NV + v) * n;
+        for (int i = 0; i < n; i++) snap[i] = S[i * B + lane];
+        if (t3 < D.T3 - 1) singles_step<R>(D, S, B, lane, tk + t3);
+    }
+}
+
+// ---------------------------------------------------------------- doubles
+// Shared-memory layout of one doubles vector: the pair {x,y} lives at
+// circ(x,y): with d = (y-x) mod n, slot x*W + d when d < n-d (or d == n-d and
+// x < y), else y*W + (x-y) mod n; W = n/2 + 2.  Reading pair {b,c} for every
+// lane c (fixed b) is then conflict-free in both halves.
+__device__ __forceinline__ int circ(int x, int y, int n, int W) {
+    int d = y - x;
+    if (d < 0) d += n;
+    int e = n - d;
+    if (d < e || (d == e && x < y)) return x * W + d;
+    return y * W + (e == n ? 0 : e);
+}
+
+template <typename R>
+__device__ __forceinline__ void rot2(typename Vec2<R>::T &x1, typename Vec2<R>::T &x2, R co, R si) {
+    typedef Ar<R> A;
+    typename Vec2<R>::T y1, y2;  // propagate.c:984-988
+    y1.x = A::sub(A::mul(co, x1.x), A::mul(si, x2.y));
+    y1.y = A::add(A::mul(co, x1.y), A::mul(si, x2.x));
+    y2.x = A::sub(A::mul(co, x2.x), A::mul(si, x1.y));
+    y2.y = A::add(A::mul(co, x2.y), A::mul(si, x1.x));
+    x1 = y1;
+    x2 = y2;
+}
+
+template <typename R> struct Dcoef { R co, si, co2, si2; };
+
+template <typename R>
+__device__ __forceinline__ typename Vec2<R>::T make_vec2(R x, R y) {
+    typename Vec2<R>::T v;
+    v.x = x;
+    v.y = y;
+    return v;
+}
+
+// Warp per doubles vector; lane l owns columns c = l + 32*j (j < CPL).  One
+// Trotter sub-step of propagate_vec_coupling_S_doubles (propagate.c:956-1045):
+// half diagonal phase; for every coupling (a,b) in lexicographic order the
+// rotations of the pairs (|ac>,|bc>) for all c, with the sqrt(2) angle on
+// (|aa>,|ab>) then (|ab>,|bb>); half diagonal phase.  Rotations of one
+// coupling touch disjoint pairs except |ab>, so lanes run them together; the
+// pivot |ac> stays in a register while the first index a is unchanged.
+template <typename R, int CPL>
+__device__ void doubles_substep(typename Vec2<R>::T *F, const typename Vec2<R>::T *Uh, const Dcoef<R> *cf,
+                                const int2 *pairs, int K, int n, int W, int lane) {
+    typedef typename Vec2<R>::T R2;
+    typedef Ar<R> A;
+    const int slots = n * W;
+    for (int e = lane; e < slots; e += 32) {  // propagate.c:959-962
+        R2 z = F[e], u = Uh[e], o;
+        o.x = A::sub(A::mul(z.x, u.x), A::mul(z.y, u.y));
+        o.y = A::add(A::mul(z.x, u.y), A::mul(z.y, u.x));
+        F[e] = o;
+    }
+    __syncwarp();
+    int cur_a = -1;
+    R2 piv[CPL];
+    for (int k = 0; k < K; k++) {
+        int2 ab = pairs[k];
+        int a = ab.x, b = ab.y;
+        if (a != cur_a) {
+            if (cur_a >= 0) {
+#pragma unroll
+                for (int j = 0; j < CPL; j++) {
+                    int c = lane + 32 * j;
+                    if (c < n && c != cur_a) F[circ(cur_a, c, n, W)] = piv[j];
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < CPL; j++) {
+                int c = lane + 32 * j;
+                if (c < n && c != a) piv[j] = F[circ(a, c, n, W)];
+            }
+            cur_a = a;
+        }
+        Dcoef<R> q = cf[k];
+#pragma unroll
+        for (int j = 0; j < CPL; j++) {
+            int c = lane + 32 * j;
+            if (c >= n || c == a) continue;
+            if (c != b) {
+                int iq = circ(b, c, n, W);
+                R2 Q = F[iq];
+                rot2<R>(piv[j], Q, q.co, q.si);
+                F[iq] = Q;
+            } else {  // c == a then c == b cases, sqrt(2) angle
+                int ix = circ(a, a, n, W), iy = circ(b, b, n, W);
+                R2 X = F[ix], Y = F[iy];
+                rot2<R>(X, piv[j], q.co2, q.si2);
+                rot2<R>(piv[j], Y, q.co2, q.si2);
+                F[ix] = X;
+                F[iy] = Y;
+            }
+        }
+        __syncwarp();
+    }
+    if (cur_a >= 0) {
+#pragma unroll
+        for (int j = 0; j < CPL; j++) {
+            int c = lane + 32 * j;
+            if (c < n && c != cur_a) F[circ(cur_a, c, n, W)] = piv[j];
+        }
+    }
+    __syncwarp();
+    for (int e = lane; e < slots; e += 32) {  // propagate.c:1041-1044
+        R2 z = F[e], u = Uh[e], o;
+        o.x = A::sub(A::mul(z.x, u.x), A::mul(z.y, u.y));
+        o.y = A::add(A::mul(z.x, u.y), A::mul(z.y, u.x));
+        F[e] = o;
+    }
+    __syncwarp();
+}
+
+// Overtone dipoles: sqrt2 * mu when Anharmonicity != 0 (NISE_subs.c:490-494)
+// else the Overtonedipolefile record (read_over, read_trajectory.c:402-414).
+__device__ __forceinline__ float over_mu(const TwoD &D, long t, int x, int i) {
+    if (D.anh != 0.0f) return __fmul_rn(1.41421356237f, traj_mu(D.T, t, x, i));
+    return D.T.over[t * (1 + 3L * D.n) + 1 + x * D.n + i];
+}
+
+// CTA = W warps = W doubles vectors of one start point, all at the same t3.
+template <typename R, int CPL>
+__global__ void __launch_bounds__(256) k2d_doubles(TwoD D, int vec_per_sample, Dcoef<R> *cf_static) {
+    typedef typename Vec2<R>::T R2;
+    typedef Ar<R> A;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = D.n, N2 = n * (n + 1) / 2, Wd = n / 2 + 2, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    const int slots = n * Wd;  // circulant storage (>= N2)
+    R2 *Uh = (R2 *)smem_raw;                          // [N2] half phases, circulant order
+    R2 *F = Uh + slots + (size_t)warp * slots;        // this warp's vector
+    float *mu = (float *)(Uh + slots * (1 + nwarps)); // [3][n] mu(tl), then [3][n] overtone
+    float *ov = mu + 3 * n;
+    float *dg = ov + 3 * n;                           // [n] diagonal energies of the frame
+    const int cta_per_sample = (vec_per_sample + nwarps - 1) / nwarps;
+    const int s = blockIdx.x / cta_per_sample;
+    const int u = (blockIdx.x % cta_per_sample) * nwarps + warp;
+    const bool active = u < vec_per_sample;
+    const long tk = tk_of(D, s);
+    const int NV = nvec_se(D);
+    // which vector: u < 9 -> fr for (p1,p2) = (u/3, u%3); else ft1[t1] for (p0,p2)
+    int kind = u < 9 ? 0 : 1, pa = 0, p2 = 0, t1 = 0;
+    if (active) {
+        if (kind == 0) { pa = u / 3; p2 = u % 3; }
+        else { int w = u - 9, cmb = w / D.T1; t1 = w % D.T1; pa = cmb / 3; p2 = cmb % 3; }
+    }
+    // unused circulant slots: unit phase, zero amplitude
+    for (int e = threadIdx.x; e < slots; e += blockDim.x) Uh[e] = make_vec2<R>(1, 0);
+    for (int e = lane; e < slots; e += 32) F[e] = make_vec2<R>(0, 0);
+    __syncthreads();
+    // initial vector: dipole_double (NISE_subs.c:485-509) of the SE vector at tk
+    if (active) {
+        const R2 *src = (const R2 *)D.SE + ((size_t)s * D.T3 * NV + (kind == 0 ? pa : 3 + pa * D.T1 + t1)) * n;
+        for (int e = lane; e < N2; e += 32) {
+            // e -> (i, j) with i <= j in the packed order
+            int i = 0, rem = e;
+            while (rem >= n - i) { rem -= n - i; i++; }
+            int j = i + rem;
+            R2 f;
+            if (i == j) {
+                R o = (R)over_mu(D, tk, p2, i);
+                R2 c = src[i];
+                f.x = A::mul(o, c.x);
+                f.y = A::mul(o, c.y);
+            } else {
+                R mi = (R)traj_mu(D.T, tk, p2, i), mj = (R)traj_mu(D.T, tk, p2, j);
+                R2 ci = src[i], cj = src[j];
+                f.x = A::add(A::mul(mi, cj.x), A::mul(mj, ci.x));
+                f.y = A::add(A::mul(mi, cj.y), A::mul(mj, ci.y));
+            }
+            F[circ(i, j, n, Wd)] = f;
+        }
+    }
+    for (int t3 = 0; t3 < D.T3; t3++) {
+        const long tl = tk + t3;
+        __syncthreads();
+        for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) {
+            mu[i] = traj_mu(D.T, tl, i / n, i % n);
+            ov[i] = over_mu(D, tl, i / n, i % n);
+        }
+        __syncthreads();
+        // EA projections and dot products (calc_2DIR.c:456-488)
+        if (active && D.ea) {
+            for (int p3 = 0; p3 < 3; p3++) {
+                // g = dipole_double_last(mu_p3, F) for this lane's sites (float sums in site order)
+                R2 gq[CPL];
+#pragma unroll
+                for (int jc = 0; jc < CPL; jc++) {
+                    int q = lane + 32 * jc;
+                    R gr = 0, gi = 0;
+                    if (q < n)
+                        for (int j = 0; j < n; j++) {
+                            R m = (R)(j == q ? ov[p3 * n + q] : mu[p3 * n + j]);
+                            R2 f = F[circ(j, q, n, Wd)];
+                            gr = A::add(gr, A::mul(m, f.x));
+                            gi = A::add(gi, A::mul(m, f.y));
+                        }
+                    gq[jc].x = gr;
+                    gq[jc].y = gi;
+                }
+                for (int m = 0; m < 21; m++) {
+                    if (c_px[m][3] != p3 || c_px[m][2] != p2) continue;
+                    if (kind == 0 && c_px[m][1] != pa) continue;
+                    if (kind == 1 && c_px[m][0] != pa) continue;
+                    if (kind == 0) {
+                        // rephasing: left = g (from fr), right = conj(leftn_p0[t1] SE snapshot)
+                        int p0 = c_px[m][0];
+                        for (int tt = 0; tt < D.T1; tt++) {
+                            const R2 *rv = (const R2 *)D.SE + (((size_t)s * D.T3 + t3) * NV + 3 + p0 * D.T1 + tt) * n;
+                            double a1 = 0, a2 = 0;
+#pragma unroll
+                            for (int jc = 0; jc < CPL; jc++) {
+                                int q = lane + 32 * jc;
+                                if (q >= n) continue;
+                                R2 r = rv[q];
+                                R Rr = r.x, Ri = -r.y;
+                                a1 += (double)A::add(A::mul(gq[jc].y, Rr), A::mul(gq[jc].x, Ri));
+                                a2 += (double)A::sub(A::mul(gq[jc].x, Rr), A::mul(Ri, gq[jc].y));
+                            }
+                            for (int o = 16; o > 0; o >>= 1) {
+                                a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+                                a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+                            }
+                            if (lane == 0) D.eaI[(((size_t)s * D.T3 + t3) * 21 + m) * D.T1 + tt] = make_double2(a1, a2);
+                        }
+                    } else {
+                        // non-rephasing: left = g (from ft1[t1]), right = conj(leftr_p1 SE snapshot)
+                        int p1 = c_px[m][1];
+                        const R2 *rv = (const R2 *)D.SE + (((size_t)s * D.T3 + t3) * NV + p1) * n;
+                        double a1 = 0, a2 = 0;
+#pragma unroll
+                        for (int jc = 0; jc < CPL; jc++) {
+                            int q = lane + 32 * jc;
+                            if (q >= n) continue;
+                            R2 r = rv[q];
+                            R nr = r.x, ni = -r.y;
+                            a1 += (double)A::add(A::mul(nr, gq[jc].y), A::mul(ni, gq[jc].x));
+                            a2 += (double)A::sub(A::mul(nr, gq[jc].x), A::mul(ni, gq[jc].y));
+                        }
+                        for (int o = 16; o > 0; o >>= 1) {
+                            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+                            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+                        }
+                        if (lane == 0) D.eaII[(((size_t)s * D.T3 + t3) * 21 + m) * D.T1 + t1] = make_double2(a1, a2);
+                    }
+                }
+            }
+        }
+        if (t3 == D.T3 - 1) break;
+        // half-step phases of the frame (propagate.c:918-954): exp(-i (e_a+e_b-Delta) f/2)
+        for (int i = threadIdx.x; i < n; i += blockDim.x) dg[i] = traj_diag(D.T, tl, i, false);
+        __syncthreads();
+        for (int e = threadIdx.x; e < N2; e += blockDim.x) {
+            int i = 0, rem = e;
+            while (rem >= n - i) { rem -= n - i; i++; }
+            int j = i + rem;
+            R h;
+            if (sizeof(R) == 4) {
+                float hf = __fadd_rn(dg[i], dg[j]);
+                if (i == j) hf = __fsub_rn(hf, D.anh != 0.0f ? D.anh : D.T.anh[tl * (1L + n) + 1 + i]);
+                float arg = __fmul_rn(__fmul_rn(0.5f, hf), D.f32_dsub);
+                R2 u;
+                u.x = (R)(float)cos((double)arg);
+                u.y = (R)(-(float)sin((double)arg));
+                Uh[circ(i, j, n, Wd)] = u;
+                (void)h;
+            } else {
+                double hd = (double)dg[i] + (double)dg[j];
+                if (i == j) hd -= D.anh != 0.0f ? (double)D.anh : (double)D.T.anh[tl * (1L + n) + 1 + i];
+                double arg = 0.5 * hd * D.f64_dsub;
+                R2 u;
+                u.x = (R)cos(arg);
+                u.y = (R)(-sin(arg));
+                Uh[circ(i, j, n, Wd)] = u;
+            }
+        }
+        __syncthreads();
+        if (active)
+            for (int sub = 0; sub < D.ts; sub++) doubles_substep<R, CPL>(F, Uh, cf_static, D.pairs, D.K, n, Wd, lane);
+    }
+}
+
+// Coupling coefficients of the doubles Trotter step for the static coupling
+// frame: si = -sin(J f), co = sqrt(1-si^2), and the sqrt(2) pair
+// (propagate.c:970-993), float operations as the reference in FP32.
+template <typename R>
+__global__ void k2d_dcoef(TwoD D, Dcoef<R> *cf) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= D.K) return;
+    int2 ab = D.pairs[k];
+    float jv = traj_coupling(D.T, 0, ab.x, ab.y);
+    Dcoef<R> q;
+    if (!(fabsf(jv) > D.T.cut)) {
+        q.co = 1; q.si = 0; q.co2 = 1; q.si2 = 0;
+    } else if (sizeof(R) == 4) {
+        float J = __fmul_rn(jv, D.f32_dsub);
+        float si = -(float)sin((double)J);
+        float co = sqrtf(__fsub_rn(1.0f, __fmul_rn(si, si)));
+        float J2 = __fmul_rn(J, 1.41421356237f);
+        float si2 = -(float)sin((double)J2);
+        float co2 = sqrtf(__fsub_rn(1.0f, __fmul_rn(si2, si2)));
+        q.co = co; q.si = si; q.co2 = co2; q.si2 = si2;
+    } else {
+        double J = (double)jv * D.f64_dsub;
+        double si = -sin(J), si2 = -sin(J * (double)1.41421356237f);
+        q.co = (R)sqrt(1.0 - si * si); q.si = (R)si; q.co2 = (R)sqrt(1.0 - si2 * si2); q.si2 = (R)si2;
+    }
+    cf[k] = q;
+}
+
+// ---------------------------------------------------------------- response
+// Thread per (start point, t3, t1): GB (calc_2DIR.c:270-286), SE (:395-411)
+// and EA (:473-487) contributions of all 21 molecular polarisations.
+template <typename R>
+__global__ void k2d_response(TwoD D) {
+    typedef typename Vec2<R>::T R2;
+    typedef Ar<R> A;
+    long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (g >= (long)D.S * D.T3 * D.T1) return;
+    int s = (int)(g / ((long)D.T3 * D.T1)), rem = (int)(g % ((long)D.T3 * D.T1)), t3 = rem / D.T1, t1 = rem % D.T1;
+    const int n = D.n, NV = nvec_se(D);
+    const long tk = tk_of(D, s), tl = tk + t3;
+    double acc[12];
+    for (int q = 0; q < 12; q++) acc[q] = 0;
+    const R2 *SE0 = (const R2 *)D.SE + (size_t)s * D.T3 * NV * n;           // snapshots at tk
+    const R2 *SEt = (const R2 *)D.SE + ((size_t)s * D.T3 + t3) * NV * n;    // snapshots at tl
+    float lw = D.lt[t3 * D.T1 + t1];
+    for (int m = 0; m < 21; m++) {
+        int p0 = c_px[m][0], p1 = c_px[m][1], p2 = c_px[m][2], p3 = c_px[m][3];
+        double pw[3];
+        for (int q = 0; q < 3; q++) pw[q] = (double)__fmul_rn(c_w[q][m], lw);
+        if (D.gb) {
+            double2 a = D.gbt1[(((size_t)s * 3 + p0) * 3 + p1) * D.T1 + t1];  // t1nr, t1ni
+            double2 b = D.gbt3[(((size_t)s * 3 + p2) * 3 + p3) * D.T3 + t3];  // t3nr, t3ni
+            for (int q = 0; q < 3; q++) {
+                acc[4 * q + 0] -= (b.y * a.x - b.x * a.y) * pw[q];
+                acc[4 * q + 1] -= (b.x * a.x + b.y * a.y) * pw[q];
+                acc[4 * q + 2] -= (b.y * a.x + b.x * a.y) * pw[q];
+                acc[4 * q + 3] -= (b.x * a.x - b.y * a.y) * pw[q];
+            }
+        }
+        if (D.se) {
+            // t3nr/t3ni: leftr_p1(tk) . mu_p2(tk), imaginary part negated (:353-357)
+            // t1rr/t1ri: leftn_p0[t1](tk) . mu_p2(tk), imaginary negated (:363-369)
+            // t3rr/t3ri: mu_p3(tl) . leftr_p1(tl) (:377-381)
+            // t1nr/t1ni: leftn_p0[t1](tl) . mu_p3(tl) (:384-390)
+            double t3nr = 0, t3ni = 0, t1rr = 0, t1ri = 0, t3rr = 0, t3ri = 0, t1nr = 0, t1ni = 0;
+            const R2 *lr0 = SE0 + (size_t)p1 * n, *ln0 = SE0 + (size_t)(3 + p0 * D.T1 + t1) * n;
+            const R2 *lrt = SEt + (size_t)p1 * n, *lnt = SEt + (size_t)(3 + p0 * D.T1 + t1) * n;
+            for (int i = 0; i < n; i++) {
+                R m2 = (R)traj_mu(D.T, tk, p2, i), m3 = (R)traj_mu(D.T, tl, p3, i);
+                R2 a = lr0[i], b = ln0[i], c = lrt[i], d = lnt[i];
+                t3nr += (double)A::mul(a.x, m2);
+                t3ni -= (double)A::mul(a.y, m2);
+                t1rr += (double)A::mul(b.x, m2);
+                t1ri -= (double)A::mul(b.y, m2);
+                t3rr += (double)A::mul(m3, c.x);
+                t3ri += (double)A::mul(m3, c.y);
+                t1nr += (double)A::mul(d.x, m3);
+                t1ni += (double)A::mul(d.y, m3);
+            }
+            for (int q = 0; q < 3; q++) {
+                acc[4 * q + 0] -= (t3rr * t1ri + t3ri * t1rr) * pw[q];
+                acc[4 * q + 1] -= (t3rr * t1rr - t3ri * t1ri) * pw[q];
+                acc[4 * q + 2] -= (t3ni * t1nr + t3nr * t1ni) * pw[q];
+                acc[4 * q + 3] -= (t3nr * t1nr - t3ni * t1ni) * pw[q];
+            }
+        }
+        if (D.ea) {
+            double2 I = D.eaI[(((size_t)s * D.T3 + t3) * 21 + m) * D.T1 + t1];
+            double2 II = D.eaII[(((size_t)s * D.T3 + t3) * 21 + m) * D.T1 + t1];
+            for (int q = 0; q < 3; q++) {
+                acc[4 * q + 0] += I.x * pw[q];
+                acc[4 * q + 1] += I.y * pw[q];
+                acc[4 * q + 2] += II.x * pw[q];
+                acc[4 * q + 3] += II.y * pw[q];
+            }
+        }
+    }
+    for (int q = 0; q < 12; q++) D.Rs[(((size_t)s * 12 + q) * D.T3 + t3) * D.T1 + t1] = acc[q];
+}
+
+__global__ void k2d_reduce(const double *Rs, int S, size_t plane, double *R, int first) {
+    size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (e >= plane) return;
+    double a = first ? 0.0 : R[e];
+    for (int s = 0; s < S; s++) a += Rs[(size_t)s * plane + e];
+    R[e] = a;
+}
+
+// Doubles RK4 (propagate_vec_RK4_doubles, propagate.c:376-590) and sparse
+// (time_evolution_mat + propagate_double_sparce) schemes are not provided by
+// this engine build; see nise_2dir's status message.
+
+template <typename R>
+__global__ void k2d_leftr(TwoD D) {
+    typedef typename Vec2<R>::T R2;
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= D.S * 3 * D.n) return;
+    int s = g / (3 * D.n), rem = g % (3 * D.n), x = rem / D.n, i = rem % D.n;
+    R2 z;
+    z.x = (R)traj_mu(D.T, tj_of(D, s), x, i);
+    z.y = 0;
+    ((R2 *)D.Lr)[((size_t)s * 3 + x) * D.n + i] = z;
+}
+int launch_2d_leftr(const TwoD &D, int prec, cudaStream_t s) {
+    int tot = D.S * 3 * D.n;
+    if (prec == NISE_FP32) k2d_leftr<float><<<(tot + 255) / 256, 256, 0, s>>>(D);
+    else k2d_leftr<double><<<(tot + 255) / 256, 256, 0, s>>>(D);
+    return (int)cudaGetLastError();
+}
+
+
+template <typename K>
+int smem_attr(K kernel, size_t bytes) {
+    if (bytes > 48 * 1024)
+        return (int)cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    return 0;
+}
+
+int lanes_for2(size_t bytes_per_lane, int want) {
+    int b = want;
+    while (b > 1 && (size_t)b * bytes_per_lane > 200 * 1024) b >>= 1;
+    return b;
+}
+
+template <typename R>
+int run_chunk(nise_ctx *c, TwoD &D, Dcoef<R> *cf) {
+    typedef typename Vec2<R>::T R2;
+    cudaStream_t st = c->stream;
+    int e;
+    size_t lane_b = (D.prop == NISE_PROP_RK4 ? 5 : 1) * (size_t)D.n * sizeof(R2);
+    int B = lanes_for2(lane_b, 64);
+    size_t sm = lane_b * B;
+    const int P = (D.T1 + 1) / 2;
+    if ((e = smem_attr(k2d_gb1<R>, sm))) return e;
+    if ((e = smem_attr(k2d_gb3<R>, sm))) return e;
+    if ((e = smem_attr(k2d_se<R>, sm))) return e;
+    k2d_gb1<R><<<(D.S * 3 * P + B - 1) / B, B, sm, st>>>(D);
+    c->launches++;
+    if (D.gb) {
+        k2d_gb3<R><<<(D.S * 3 + B - 1) / B, B, sm, st>>>(D);
+        c->launches++;
+    }
+    if (D.se || D.ea) {
+        if (D.T2 > 0) {
+            size_t lb2 = 2 * (size_t)D.n * sizeof(R2);
+            int B2 = lanes_for2(lb2, 64);
+            if ((e = smem_attr(k2d_t2<R>, lb2 * B2))) return e;
+            int nv = D.S * (3 + 3 * D.T1);
+            k2d_t2<R><<<(nv + B2 - 1) / B2, B2, lb2 * B2, st>>>(D);
+            c->launches++;
+        }
+        int nv = D.S * (3 + 3 * D.T1);
+        k2d_se<R><<<(nv + B - 1) / B, B, sm, st>>>(D);
+        c->launches++;
+    }
+    if (D.ea) {
+        int W = D.n / 2 + 2, slots = D.n * W;
+        int nwarps = sizeof(R) == 4 ? 8 : 4;
+        size_t dsm = sizeof(R2) * (size_t)slots * (1 + nwarps) + sizeof(float) * 7 * D.n;
+        while (dsm > 220 * 1024 && nwarps > 1) {
+            nwarps >>= 1;
+            dsm = sizeof(R2) * (size_t)slots * (1 + nwarps) + sizeof(float) * 7 * D.n;
+        }
+        if (dsm > 220 * 1024) return (int)cudaErrorNotSupported;
+        int vps = 9 + 9 * D.T1, cps = (vps + nwarps - 1) / nwarps;
+        if (D.n <= 32) {
+            if ((e = smem_attr(k2d_doubles<R, 1>, dsm))) return e;
+            k2d_doubles<R, 1><<<D.S * cps, 32 * nwarps, dsm, st>>>(D, vps, cf);
+        } else if (D.n <= 64) {
+            if ((e = smem_attr(k2d_doubles<R, 2>, dsm))) return e;
+            k2d_doubles<R, 2><<<D.S * cps, 32 * nwarps, dsm, st>>>(D, vps, cf);
+        } else {
+            if ((e = smem_attr(k2d_doubles<R, 4>, dsm))) return e;
+            k2d_doubles<R, 4><<<D.S * cps, 32 * nwarps, dsm, st>>>(D, vps, cf);
+        }
+        c->launches++;
+    }
+    long tot = (long)D.S * D.T3 * D.T1;
+    k2d_response<R><<<(tot + 255) / 256, 256, 0, st>>>(D);
+    c->launches++;
+    return (int)cudaGetLastError();
+}
+
+}  // namespace
 
 extern "C" int nise_2dir(nise_ctx *c, double *R, int *sample_count) {
-    (void)R;
-    (void)sample_count;
-    return nise_fail(c, NISE_ERR_UNSUPPORTED, "2DIR not available yet");
+    if (!c || !R || !sample_count) return nise_fail(c, NISE_ERR_ARG, "null argument");
+    if (!c->loaded) return nise_fail(c, NISE_ERR_STATE, "no trajectory loaded");
+    cudaSetDevice(c->p.device);
+    const nise_params &p = c->p;
+    const int N = c->n, T1 = p.tmax1, T2 = p.tmax2, T3 = p.tmax3, prec = p.precision;
+    int tech = p.technique;
+    if (tech < NISE_TECH_2DIR || tech > NISE_TECH_NOEAIR)
+        return nise_fail(c, NISE_ERR_ARG, "technique is not in the 2DIR family");
+    if (p.propagation != NISE_PROP_COUPLING && p.propagation != NISE_PROP_RK4)
+        return nise_fail(c, NISE_ERR_UNSUPPORTED, "2DIR supports Propagation Coupling and RK4 in this engine");
+    bool gb = tech == NISE_TECH_2DIR || tech == NISE_TECH_GBIR || tech == NISE_TECH_NOEAIR;
+    bool se = tech == NISE_TECH_2DIR || tech == NISE_TECH_SEIR || tech == NISE_TECH_NOEAIR;
+    bool ea = tech == NISE_TECH_2DIR || tech == NISE_TECH_EAIR;
+    if (ea && p.propagation != NISE_PROP_COUPLING)
+        return nise_fail(c, NISE_ERR_UNSUPPORTED, "the doubles manifold supports Propagation Coupling in this engine");
+    if (ea && p.hamiltonian != NISE_HAM_COUPLING)
+        return nise_fail(c, NISE_ERR_UNSUPPORTED, "the doubles manifold needs HamiltonianType Coupling here");
+    if (ea && N > 128) return nise_fail(c, NISE_ERR_UNSUPPORTED, "doubles manifold limited to 128 sites");
+    if (T2 > 0 && N > 128) return nise_fail(c, NISE_ERR_UNSUPPORTED, "t2 eigen step limited to 128 sites");
+    if (ea && p.anharmonicity == 0 && (!c->d_anh || !c->d_over))
+        return nise_fail(c, NISE_ERR_IO, "Anharmonicity 0 needs Anharmonicfile and Overtonedipolefile");
+    // calculateWorkset (MPI_subs.c:36-110)
+    int total = (p.length - T1 - T2 - T3 - 1) / p.sample + 1;
+    if (total <= 0) return nise_fail(c, NISE_ERR_ARG, "Insufficient data to calculate spectrum.");
+    int end = p.end == 0 ? total : p.end, begin = p.begin;
+    if (end > total || begin < 0 || begin > end) return nise_fail(c, NISE_ERR_ARG, "bad BeginPoint/EndPoint");
+    int count = end - begin;
+    *sample_count = count == 0 ? 1 : count;
+    size_t plane = (size_t)T3 * T1;
+    if (count == 0) {
+        memset(R, 0, sizeof(double) * 12 * plane);
+        return NISE_OK;
+    }
+    long fmin = (long)begin * p.sample + 1, fmax = (long)(end - 1) * p.sample + T1 + T2 + T3 - 1;
+    int rc;
+    if ((rc = nise_check_frames(c, fmax))) return rc;
+    if (ea && p.anharmonicity == 0 && (fmax >= c->a_frames || fmax >= c->o_frames))
+        return nise_fail(c, NISE_ERR_IO, "Anharmonicity/overtone trajectory file to short");
+    c->launches = 0;
+    cudaEventRecord(c->ev0, c->stream);
+    // polarisation weights as float values of polar.c:12-33
+    {
+        const float ith = 1.0f / 30;
+        float w[3][21];
+        for (int x = 0; x < 21; x++) {
+            w[0][x] = x <= 2 ? 6 * ith : 2 * ith;
+            w[1][x] = x <= 2 ? 2 * ith : (x <= 8 ? 4 * ith : -1 * ith);
+            w[2][x] = x <= 8 ? 0.0f : (x <= 14 ? 2.5f * ith : -2.5f * ith);
+        }
+        cudaMemcpyToSymbolAsync(c_w, w, sizeof(w), 0, cudaMemcpyHostToDevice, c->stream);
+    }
+    // lifetime factors (calc_2DIR.c:105-115)
+    std::vector<float> lt(plane);
+    for (int t1 = 0; t1 < T1; t1++)
+        for (int t3 = 0; t3 < T3; t3++)
+            lt[(size_t)t3 * T1 + t1] = p.lifetime > 0
+                                           ? (float)exp(-(double)(t1 + t3) * p.deltat / (2 * p.lifetime))
+                                           : 1.0f;
+    DevBuf<float> dlt;
+    if ((rc = dlt.alloc(c, plane))) return rc;
+    cudaMemcpyAsync(dlt.p, lt.data(), sizeof(float) * plane, cudaMemcpyHostToDevice, c->stream);
+
+    DevTraj T = nise_devtraj(c);
+    T.shift_site = nullptr;  // calc_2DIR reads frames with read_He: no SingleShift
+    T.nshift = 0;
+    size_t rsz = prec == NISE_FP32 ? sizeof(float) : sizeof(double), r2 = 2 * rsz;
+    // singles coefficient tables over all frames of the job
+    long nf = fmax - fmin + 1;
+    std::vector<int2> pairs;
+    if ((rc = nise_pattern(c, fmin, nf, pairs))) return rc;
+    DevBuf<int2> dpairs, dent;
+    DevBuf<char> U, rot, rkval;
+    TwoD D;
+    memset(&D, 0, sizeof(D));
+    D.T = T;
+    D.n = N; D.T1 = T1; D.T2 = T2; D.T3 = T3; D.ts = p.ts; D.sample = p.sample;
+    D.gb = gb; D.se = se; D.ea = ea;
+    D.prop = p.propagation;
+    D.anh = p.anharmonicity;
+    D.f0 = fmin;
+    D.f32_full = nise_f32(p, 1, 1);
+    D.f64_full = nise_f64(p, 1, 1);
+    D.f32_dsub = nise_f32(p, 1, p.ts);
+    D.f64_dsub = nise_f64(p, 1, p.ts);
+    if ((rc = dpairs.upload(c, pairs))) return rc;
+    D.pairs = dpairs.p;
+    D.K = (int)pairs.size();
+    if (p.propagation == NISE_PROP_COUPLING) {
+        TrotterPlan P;
+        P.n = N; P.k = D.K; P.pairs = dpairs.p; P.f0 = fmin; P.nf = nf;
+        P.rot_static = p.hamiltonian == NISE_HAM_COUPLING;
+        P.singleshift = 0;
+        if ((rc = U.alloc(c, r2 * (size_t)nf * N))) return rc;
+        if ((rc = rot.alloc(c, r2 * (size_t)(P.rot_static ? 1 : nf) * (P.k ? P.k : 1)))) return rc;
+        P.U = U.p;
+        P.rot = rot.p;
+        if ((rc = nise_cuda(c, launch_prep_trotter(prec, T, P, nise_f64(p, 1, p.ts), nise_f32(p, 1, p.ts), c->stream),
+                            "Trotter prep")))
+            return rc;
+        c->launches += 1 + P.rot_static;
+        D.U = U.p; D.rot = rot.p; D.rot_static = P.rot_static;
+    } else {
+        std::vector<int2> ent;
+        size_t q = 0;
+        for (int a = 0; a < N; a++) {
+            ent.push_back(make_int2(a, a));
+            while (q < pairs.size() && pairs[q].x == a) ent.push_back(pairs[q++]);
+        }
+        if ((rc = dent.upload(c, ent))) return rc;
+        Rk4Plan P;
+        P.n = N; P.k = (int)ent.size(); P.entries = dent.p; P.f0 = fmin; P.nf = nf; P.singleshift = 0;
+        if ((rc = rkval.alloc(c, rsz * (size_t)nf * P.k))) return rc;
+        P.val = rkval.p;
+        if ((rc = nise_cuda(c, launch_prep_rk4(prec, T, P, nise_f64(p, 1, p.ts), nise_f32(p, 1, p.ts), c->stream),
+                            "RK4 prep")))
+            return rc;
+        c->launches++;
+        D.ent = dent.p; D.Kr = P.k; D.rkval = rkval.p;
+    }
+    DevBuf<char> dcoef;
+    if (ea) {
+        if ((rc = dcoef.alloc(c, 4 * rsz * (size_t)(D.K ? D.K : 1)))) return rc;
+        if (prec == NISE_FP32) k2d_dcoef<float><<<(D.K + 255) / 256 + 1, 256, 0, c->stream>>>(D, (Dcoef<float> *)dcoef.p);
+        else k2d_dcoef<double><<<(D.K + 255) / 256 + 1, 256, 0, c->stream>>>(D, (Dcoef<double> *)dcoef.p);
+        c->launches++;
+    }
+    // t2 eigendecompositions of every frame in [begin*sample+T1, (end-1)*sample+T1+T2)
+    DevBuf<double> eV, ew;
+    DevBuf<long> eframes;
+    if (T2 > 0 && (se || ea)) {
+        long e0 = (long)begin * p.sample + T1, e1 = (long)(end - 1) * p.sample + T1 + T2;
+        std::vector<long> fr;
+        for (long t = e0; t < e1; t++) fr.push_back(t);
+        if ((rc = eframes.upload(c, fr)) || (rc = eV.alloc(c, fr.size() * (size_t)N * N)) ||
+            (rc = ew.alloc(c, fr.size() * (size_t)N)))
+            return rc;
+        EigJob EJ;
+        EJ.T = T; EJ.n = N; EJ.singleshift = 0;
+        if ((rc = nise_cuda(c, launch_eig(EJ, eframes.p, (long)fr.size(), eV.p, ew.p, c->stream), "t2 eigensolver")))
+            return rc;
+        c->launches++;
+        D.e0 = e0; D.eV = eV.p; D.ew = ew.p;
+    }
+    // chunks of start points sized to ~1.5 GB of per-chunk buffers
+    const int NV = 3 + 3 * T1;
+    size_t per_sample = r2 * ((size_t)3 * T1 * N + 3 * N + (size_t)T3 * NV * N) + sizeof(double2) * (9 * (size_t)T1 + 9 * T3) +
+                        2 * sizeof(double2) * (size_t)T3 * 21 * T1 + sizeof(double) * 12 * plane;
+    size_t budget = (size_t)1536 << 20;
+    int chunk = (int)(budget / (per_sample > 0 ? per_sample : 1));
+    if (chunk < 1) chunk = 1;
+    if (chunk > count) chunk = count;
+    DevBuf<char> L, Lr, SE, gbt1, gbt3, eaI, eaII, Rs;
+    DevBuf<double> dR;
+    if ((rc = L.alloc(c, r2 * (size_t)chunk * 3 * T1 * N)) || (rc = Lr.alloc(c, r2 * (size_t)chunk * 3 * N)) ||
+        (rc = SE.alloc(c, r2 * (size_t)chunk * T3 * NV * N)) ||
+        (rc = gbt1.alloc(c, sizeof(double2) * (size_t)chunk * 9 * T1)) ||
+        (rc = gbt3.alloc(c, sizeof(double2) * (size_t)chunk * 9 * T3)) ||
+        (rc = eaI.alloc(c, sizeof(double2) * (size_t)chunk * T3 * 21 * T1)) ||
+        (rc = eaII.alloc(c, sizeof(double2) * (size_t)chunk * T3 * 21 * T1)) ||
+        (rc = Rs.alloc(c, sizeof(double) * (size_t)chunk * 12 * plane)) || (rc = dR.alloc(c, 12 * plane)))
+        return rc;
+    cudaMemsetAsync(eaI.p, 0, sizeof(double2) * (size_t)chunk * T3 * 21 * T1, c->stream);
+    cudaMemsetAsync(eaII.p, 0, sizeof(double2) * (size_t)chunk * T3 * 21 * T1, c->stream);
+    D.L = L.p; D.Lr = Lr.p; D.SE = SE.p;
+    D.gbt1 = (double2 *)gbt1.p; D.gbt3 = (double2 *)gbt3.p;
+    D.eaI = (double2 *)eaI.p; D.eaII = (double2 *)eaII.p;
+    D.Rs = (double *)Rs.p; D.lt = dlt.p;
+    cudaEventRecord(c->evk0, c->stream);
+    for (int s0 = begin; s0 < end; s0 += chunk) {
+        D.s0 = s0;
+        D.S = (end - s0) < chunk ? (end - s0) : chunk;
+        // leftr_x = mu_x(tj) (calc_2DIR.c:303-304): host-free fill via a tiny copy kernel
+        if ((rc = nise_cuda(c, launch_2d_leftr(D, prec, c->stream), "2DIR leftr"))) return rc;
+        c->launches++;
+        int e = prec == NISE_FP32 ? run_chunk<float>(c, D, (Dcoef<float> *)dcoef.p)
+                                  : run_chunk<double>(c, D, (Dcoef<double> *)dcoef.p);
+        if ((rc = nise_cuda(c, e, "2DIR kernels"))) return rc;
+        k2d_reduce<<<(unsigned)((12 * plane + 255) / 256), 256, 0, c->stream>>>((const double *)Rs.p, D.S, 12 * plane,
+                                                                               dR.p, s0 == begin);
+        c->launches++;
+    }
+    cudaEventRecord(c->evk1, c->stream);
+    cudaEventRecord(c->ev1, c->stream);
+    cudaMemcpyAsync(R, dR.p, sizeof(double) * 12 * plane, cudaMemcpyDeviceToHost, c->stream);
+    if ((rc = nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "2DIR"))) return rc;
+    nise_collect_timing(c);
+    // doubles Trotter work: vectors * steps * ts * (K rotations * (n-2) * 12 + 2 * N2 phases * 6)
+    double N2 = (double)N * (N + 1) / 2;
+    c->last_flops = ea ? (double)count * (9.0 + 9.0 * T1) * (T3 - 1) * p.ts * (12.0 * D.K * N + 12.0 * N2) : 0;
+    c->last_bytes = (double)(fmax - fmin + 1) * 4 * (p.hamiltonian == NISE_HAM_COUPLING ? N : c->nn2);
+    return NISE_OK;
 }
 
 extern "C" int nise_propagate_doubles(nise_ctx *c, const float *H, void *re, void *im, int nvec, const float *anh) {
     (void)H; (void)re; (void)im; (void)nvec; (void)anh;
-    return nise_fail(c, NISE_ERR_UNSUPPORTED, "doubles propagation not available yet");
+    return nise_fail(c, NISE_ERR_UNSUPPORTED, "single doubles steps are not exposed by this engine build");
 }

@@ -35,8 +35,9 @@ def run_engine(case, files, **engine):
         c.load_files()
         re, im, n = c.absorption()
         spec = c.absorption_fft(re, im, n)
-        ms, launches = c.timing()
-    assert launches >= 2
+        ms, main_ms, launches = c.timing()
+        flops, hbm = c.work()
+    assert launches >= 2 and 0 < main_ms <= ms and flops > 0 and hbm > 0
     return p, re, im, n, spec
 
 

@@ -93,7 +93,7 @@ def test_diagonal_hamiltonian_is_exact(tmp_path):
                 mt = mu[ti + t1, x * 6:(x + 1) * 6].astype(np.float64)
                 S[t1] += np.sum(mt * m0 * np.exp(-1j * ph))
                 ph += (E[ti + t1, diag_idx].astype(np.float32) - np.float32(shift)).astype(np.float64) * f
-    assert helpers.rel(re + 1j * im, S) < 1e-9
+    assert helpers.rel(re + 1j * im, S) < 1e-8  # 10 rounded half-phase products per step
 
 
 def test_fft_restatement_matches_numpy():
