@@ -289,6 +289,103 @@ __global__ void k_pattern_scan(DevTraj T, long f0, long nf, int *flag) {
     flag[tid] = any;
 }
 
+
+// Sparse Taylor propagation, vectors across lanes.  A CTA owns G vectors
+// (G in {4, 8}); lane = g + G*q handles vector g for row slot q, so one warp
+// instruction covers 32/G consecutive rows of G vectors and reads, for each
+// neighbour j, the G contiguous vector entries of row j (rows padded to G+2
+// complex numbers to spread the rows over the shared-memory banks).  Rows
+// are interleaved over warps (row = q + QR*(warp + NW*it)); the current
+// Taylor term lives in shared memory (double buffered) and the partial sum
+// psi and the frame diagonals in registers.
+template <typename R, int G, int IT>
+__global__ void __launch_bounds__(512) k_abs_taylor2(DevTraj T, TaylorPlan P, AbsJob J, double2 *resp, int nvec) {
+    typedef typename Vec2<R>::T R2;
+    constexpr int QR = 32 / G, RS = G + 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = P.n, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, NW = blockDim.x >> 5;
+    const int g = lane % G, q = lane / G;
+    R2 *cur = (R2 *)smem_raw, *nxt = cur + (size_t)n * RS;
+    double *red = (double *)(nxt + (size_t)n * RS);  // [NW][G][2]
+    const int v = blockIdx.x * G + g;
+    const bool valid = v < nvec;
+    const int vv = valid ? v : blockIdx.x * G;
+    const int x = vv % 3;
+    const long ti = (long)(J.begin + vv / 3) * J.sample;
+    int rows[IT];
+    R2 psi[IT];
+    float dg[IT];
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+        int i = q + QR * (warp + NW * it);
+        rows[it] = i < n ? i : -1;
+        psi[it].x = i < n ? (R)traj_mu(T, ti, x, i) : (R)0;
+        psi[it].y = 0;
+    }
+    const R *jval = (const R *)P.val;
+    for (int t1 = 0; t1 < J.tmax; t1++) {
+        const long tj = ti + t1;
+        double re = 0, im = 0;
+#pragma unroll
+        for (int it = 0; it < IT; it++)
+            if (rows[it] >= 0) {
+                R m = (R)traj_mu(T, tj, x, rows[it]);
+                re += (double)(m * psi[it].x);
+                im += (double)(m * psi[it].y);
+            }
+        for (int o = G; o < 32; o <<= 1) {
+            re += __shfl_xor_sync(0xffffffffu, re, o);
+            im += __shfl_xor_sync(0xffffffffu, im, o);
+        }
+        if (q == 0) { red[(warp * G + g) * 2] = re; red[(warp * G + g) * 2 + 1] = im; }
+        __syncthreads();
+        if (tid < G && blockIdx.x * G + tid < nvec) {
+            double sr = 0, si = 0;
+            for (int w = 0; w < NW; w++) { sr += red[(w * G + tid) * 2]; si += red[(w * G + tid) * 2 + 1]; }
+            resp[(size_t)(blockIdx.x * G + tid) * J.tmax + t1] = make_double2(sr, si);
+        }
+        if (t1 == J.tmax - 1) break;
+        // series order: the largest over the CTA's vectors (their frames differ)
+        int K = P.order[tj - P.f0];
+        for (int o = 1; o < G; o <<= 1) K = max(K, __shfl_xor_sync(0xffffffffu, K, o));
+#pragma unroll
+        for (int it = 0; it < IT; it++) {
+            dg[it] = rows[it] >= 0 ? traj_diag(T, tj, rows[it], P.singleshift != 0) : 0.0f;
+            if (rows[it] >= 0) cur[(size_t)rows[it] * RS + g] = psi[it];
+        }
+        R2 *a = cur, *b = nxt;
+        for (int k = 1; k <= K; k++) {
+            __syncthreads();
+            const R c = (R)(J.f / k);
+#pragma unroll
+            for (int it = 0; it < IT; it++) {
+                const int i = rows[it];
+                if (i < 0) continue;
+                R2 z = a[(size_t)i * RS + g];
+                R yr = (R)dg[it] * z.x, yi = (R)dg[it] * z.y;
+                const int e1 = P.row_ptr[i + 1];
+                for (int e = P.row_ptr[i]; e < e1; e++) {
+                    const int j = P.col[e];
+                    const R w = jval[e];
+                    R2 zz = a[(size_t)j * RS + g];
+                    yr += w * zz.x;
+                    yi += w * zz.y;
+                }
+                R2 nz;
+                nz.x = c * yi;  // (-i)(c)(y)
+                nz.y = -c * yr;
+                b[(size_t)i * RS + g] = nz;
+                psi[it].x += nz.x;
+                psi[it].y += nz.y;
+            }
+            R2 *tmp = a;
+            a = b;
+            b = tmp;
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void k_reduce_resp(const double2 *resp, int nvec, int tmax, double2 *out) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= tmax) return;
@@ -545,8 +642,49 @@ static int run_taylor(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, do
     return (int)cudaGetLastError();
 }
 
+template <typename R, int G, int IT>
+static int run_taylor2(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int nvec,
+                       cudaStream_t s) {
+    const int NT = 512;
+    size_t smem = 2 * (size_t)P.n * (G + 2) * sizeof(typename Vec2<R>::T) + (NT / 32) * G * 2 * sizeof(double);
+    int e;
+    if ((e = set_smem(k_abs_taylor2<R, G, IT>, smem))) return e;
+    k_abs_taylor2<R, G, IT><<<(nvec + G - 1) / G, NT, smem, s>>>(T, P, J, resp, nvec);
+    return (int)cudaGetLastError();
+}
+
 int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp,
                       int vec_per_cta, cudaStream_t s) {
+    {
+        // vectors across lanes (k_abs_taylor2): 16 warps cover 512 rows per
+        // iteration at G = 8 (4 rows per warp) and 128 at G = 4... rows per
+        // thread IT = ceil(n / (16 * 32 / G)).
+        int nvec = 3 * J.nsamp;
+        if (P.static_j) {
+            int G = vec_per_cta <= 4 ? 4 : 8;
+            if (prec != 0) G = 4;
+            int per_iter = 16 * (32 / G);
+            int it = (P.n + per_iter - 1) / per_iter;
+            int IT = it <= 1 ? 1 : it <= 2 ? 2 : it <= 4 ? 4 : it <= 8 ? 8 : it <= 16 ? 16 : 32;
+            if (it <= 32) {
+#define T2(R, GG)                                                                              \
+    switch (IT) {                                                                              \
+    case 1: return run_taylor2<R, GG, 1>(T, P, J, resp, nvec, s);                              \
+    case 2: return run_taylor2<R, GG, 2>(T, P, J, resp, nvec, s);                              \
+    case 4: return run_taylor2<R, GG, 4>(T, P, J, resp, nvec, s);                              \
+    case 8: return run_taylor2<R, GG, 8>(T, P, J, resp, nvec, s);                              \
+    case 16: return run_taylor2<R, GG, 16>(T, P, J, resp, nvec, s);                            \
+    default: return run_taylor2<R, GG, 32>(T, P, J, resp, nvec, s);                            \
+    }
+                if (prec == 0) {
+                    if (G == 4) { T2(float, 4) }
+                    T2(float, 8)
+                }
+                T2(double, 4)
+#undef T2
+            }
+        }
+    }
     int nvec = 3 * J.nsamp;
     int rpt = (P.n + 511) / 512;
     if (rpt > 4 || !P.static_j) return (int)cudaErrorNotSupported;

@@ -519,8 +519,9 @@ __global__ void __launch_bounds__(256) k2d_doubles(TwoD D, int vec_per_sample, D
             }
         }
         __syncthreads();
+        const Dcoef<R> *cf = D.rot_static ? cf_static : cf_static + (tl - D.f0) * D.K;
         if (active)
-            for (int sub = 0; sub < D.ts; sub++) doubles_substep<R, CPL>(F, Uh, cf_static, D.pairs, D.K, n, Wd, lane);
+            for (int sub = 0; sub < D.ts; sub++) doubles_substep<R, CPL>(F, Uh, cf, D.pairs, D.K, n, Wd, lane);
     }
 }
 
@@ -528,11 +529,13 @@ __global__ void __launch_bounds__(256) k2d_doubles(TwoD D, int vec_per_sample, D
 // frame: si = -sin(J f), co = sqrt(1-si^2), and the sqrt(2) pair
 // (propagate.c:970-993), float operations as the reference in FP32.
 template <typename R>
-__global__ void k2d_dcoef(TwoD D, Dcoef<R> *cf) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= D.K) return;
+__global__ void k2d_dcoef(TwoD D, Dcoef<R> *cf, long nframes) {
+    long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (g >= nframes * D.K) return;
+    int k = (int)(g % D.K);
+    long fi = g / D.K;
     int2 ab = D.pairs[k];
-    float jv = traj_coupling(D.T, 0, ab.x, ab.y);
+    float jv = traj_coupling(D.T, D.f0 + fi, ab.x, ab.y);
     Dcoef<R> q;
     if (!(fabsf(jv) > D.T.cut)) {
         q.co = 1; q.si = 0; q.co2 = 1; q.si2 = 0;
@@ -549,7 +552,7 @@ __global__ void k2d_dcoef(TwoD D, Dcoef<R> *cf) {
         double si = -sin(J), si2 = -sin(J * (double)1.41421356237f);
         q.co = (R)sqrt(1.0 - si * si); q.si = (R)si; q.co2 = (R)sqrt(1.0 - si2 * si2); q.si2 = (R)si2;
     }
-    cf[k] = q;
+    cf[g] = q;
 }
 
 // ---------------------------------------------------------------- response
@@ -745,8 +748,6 @@ extern "C" int nise_2dir(nise_ctx *c, double *R, int *sample_count) {
     bool ea = tech == NISE_TECH_2DIR || tech == NISE_TECH_EAIR;
     if (ea && p.propagation != NISE_PROP_COUPLING)
         return nise_fail(c, NISE_ERR_UNSUPPORTED, "the doubles manifold supports Propagation Coupling in this engine");
-    if (ea && p.hamiltonian != NISE_HAM_COUPLING)
-        return nise_fail(c, NISE_ERR_UNSUPPORTED, "the doubles manifold needs HamiltonianType Coupling here");
     if (ea && N > 128) return nise_fail(c, NISE_ERR_UNSUPPORTED, "doubles manifold limited to 128 sites");
     if (T2 > 0 && N > 128) return nise_fail(c, NISE_ERR_UNSUPPORTED, "t2 eigen step limited to 128 sites");
     if (ea && p.anharmonicity == 0 && (!c->d_anh || !c->d_over))
@@ -850,11 +851,18 @@ extern "C" int nise_2dir(nise_ctx *c, double *R, int *sample_count) {
         D.ent = dent.p; D.Kr = P.k; D.rkval = rkval.p;
     }
     DevBuf<char> dcoef;
-    if (ea) {
-        if ((rc = dcoef.alloc(c, 4 * rsz * (size_t)(D.K ? D.K : 1)))) return rc;
-        if (prec == NISE_FP32) k2d_dcoef<float><<<(D.K + 255) / 256 + 1, 256, 0, c->stream>>>(D, (Dcoef<float> *)dcoef.p);
-        else k2d_dcoef<double><<<(D.K + 255) / 256 + 1, 256, 0, c->stream>>>(D, (Dcoef<double> *)dcoef.p);
-        c->launches++;
+    D.rot_static = p.hamiltonian == NISE_HAM_COUPLING;
+    if (ea) {  // doubles coupling coefficients: once (static couplings) or per frame
+        long ncf = D.rot_static ? 1 : nf;
+        if ((rc = dcoef.alloc(c, 4 * rsz * (size_t)ncf * (D.K ? D.K : 1)))) return rc;
+        long tot = ncf * D.K;
+        if (tot > 0) {
+            if (prec == NISE_FP32)
+                k2d_dcoef<float><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(D, (Dcoef<float> *)dcoef.p, ncf);
+            else
+                k2d_dcoef<double><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(D, (Dcoef<double> *)dcoef.p, ncf);
+            c->launches++;
+        }
     }
     // t2 eigendecompositions of every frame in [begin*sample+T1, (end-1)*sample+T1+T2)
     DevBuf<double> eV, ew;
