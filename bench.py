@@ -51,6 +51,10 @@ def parse():
     a.add_argument("--impl", choices=["ours", "reference"], default="ours")
     a.add_argument("--frames", type=int, default=100000, help="trajectory length (default: the full workload)")
     a.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline (profiling runs)")
+    a.add_argument("--config", choices=["c1", "c2"], default="c1",
+                   help="c1: the headline (batched absorption, N=1024); c2: 2DIR, N=64 cluster (secondary)")
+    a.add_argument("--t2", type=int, default=0, help="c2 only: waiting-time steps (RunTimes 64 t2 64)")
+    a.add_argument("--end", type=int, default=0, help="c2 only: EndPoint (0 = all start points)")
     return a.parse_args()
 
 
@@ -331,6 +335,49 @@ def run_ours(args):
     return out
 
 
+# ---------------------------------------------------------------- 2DIR (secondary)
+def run_c2(args):
+    """2DIR, N = 64 random cluster, Tmax1 = Tmax3 = 64, Samplerate 100, 20000 x 2 fs frames.
+
+    value = reference-equivalent doubles site-steps per second: the reference
+    propagates 21 * (tmax1 + 1) doubles vectors of N(N+1)/2 states through
+    tmax3 steps per start point (calc_2DIR.c:448-505)."""
+    import torch
+    import nise_2017_b200 as nise
+    from nise_2017_b200 import synth
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    s = synth.c2_spec()
+    kw = synth.c2_keywords(RunTimes="64 %d 64" % args.t2)
+    if args.end:
+        kw["EndPoint"] = args.end
+    with tempfile.TemporaryDirectory() as td:
+        files = synth.write(s, td)
+        p = nise.params_from_keywords(kw, files, device=local)
+        with nise.Context(p) as c:
+            c.load_files()
+            for _ in range(max(args.warmup, 1)):
+                c.twodir()
+            times, mains = [], []
+            for _ in range(args.steps):
+                R, n = c.twodir()
+                tot, main, launches = c.timing()
+                times.append(tot)
+                mains.append(main)
+            flops, _ = c.work()
+    n2 = 64 * 65 // 2
+    site_steps = n * 21 * 65 * 64 * n2
+    ms = statistics.mean(times)
+    out = {"metric": "2DIR time-to-spectrum and doubles site-steps/s (secondary workload)",
+           "value": site_steps / (ms / 1e3), "unit": "site-steps/s", "n_gpus": 1, "steps": args.steps,
+           "warmup": max(args.warmup, 1), "ms_per_step": ms, "time_to_spectrum_s": ms / 1e3,
+           "config": {"workload": "2DIR, Propagation Coupling, N=64 random cluster, RunTimes 64 %d 64, "
+                                  "Samplerate 100, 20000 x 2 fs" % args.t2, "start_points": n},
+           "doubles_fp32_tflops": flops / (statistics.mean(mains) / 1e3) / 1e12, "gpu_launches": launches}
+    print(json.dumps(out), flush=True)
+    return out
+
+
 # ---------------------------------------------------------------- reference arm
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
@@ -379,5 +426,7 @@ if __name__ == "__main__":
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.config == "c2":
+        run_c2(a)
     else:
         run_ours(a)
