@@ -174,6 +174,21 @@ int nise_last_work(const nise_ctx *ctx, double *flops, double *hbm_bytes);
  * denominator of the CUDA-core kernels. */
 int nise_probe_fp32_peak(int device, double *tflops);
 
+/* No counterpart in the reference.  Linear absorption with the Trotter
+ * "Coupling" scheme (HamiltonianType Full) for callers whose device memory is
+ * owned by their own allocator and who therefore cannot let the library call
+ * cudaMalloc/cudaFree: inputs (record images of the Hamiltonian and dipole
+ * files) and outputs (re_S/im_S, tmax1 doubles each) are caller-allocated
+ * DEVICE buffers, every intermediate table lives in one static device array
+ * of 32 MiB that each GPU loading the library keeps until exit, and larger
+ * jobs return NISE_ERR_SHAPE.  Work is enqueued on `stream` (a cudaStream_t,
+ * NULL = default stream) on the current device and the call returns when it
+ * is done.  All calls share the array: calls whose device work overlaps race.
+ * The first call on a device looks up the array's device address; make it
+ * before any stream capture.  Results equal nise_absorption's. */
+int nise_absorption_noalloc(const nise_params *p, const void *d_energy, size_t energy_bytes, const void *d_dipole,
+                            size_t dipole_bytes, double *d_re_S, double *d_im_S, int *samples, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

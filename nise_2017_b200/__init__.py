@@ -35,7 +35,7 @@ EXPORTED = [
     "nise_global_error", "nise_load_files", "nise_set_trajectory", "nise_set_singleshift", "nise_absorption",
     "nise_absorption_fft", "nise_2dir", "nise_propagate", "nise_propagate_doubles", "nise_write_td_absorption",
     "nise_write_spectrum", "nise_write_2d", "nise_set_stream", "nise_last_timing", "nise_last_work",
-    "nise_probe_fp32_peak",
+    "nise_probe_fp32_peak", "nise_absorption_noalloc",
 ]
 
 

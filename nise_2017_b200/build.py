@@ -26,6 +26,7 @@ CU_SOURCES = [
     "twodir.cu",
     "eigen.cu",
     "util.cu",
+    "noalloc.cu",
 ]
 CPP_SOURCES = [
     "api.cpp",
