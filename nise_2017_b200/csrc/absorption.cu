@@ -386,6 +386,112 @@ __global__ void __launch_bounds__(512) k_abs_taylor2(DevTraj T, TaylorPlan P, Ab
     }
 }
 
+// Sparse Taylor propagation with the coupling matrix in shared memory as a
+// sliced ELL: slice s = rows 4s..4s+3 (the rows of one warp instruction at
+// G = 8), Ls entries per row (the slice's longest row, shorter rows padded
+// with zero weights), entry = (offset of the neighbour row in the state,
+// weight), stored [slot][row in slice] so a warp instruction reads 4
+// consecutive entries.  The state is single-buffered: the next Taylor term of
+// a thread's rows is kept in registers until every warp has read the current
+// term, then written back.
+template <typename R> struct EllEnt;
+template <> struct EllEnt<float> { int off; float v; };
+template <> struct EllEnt<double> { int off; int pad; double v; };
+
+template <typename R, int IT>
+__global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, AbsJob J, double2 *resp, int nvec,
+                                                    const EllEnt<R> *__restrict__ ell_g, const int *__restrict__ sptr_g,
+                                                    int nslices, int nent) {
+    typedef typename Vec2<R>::T R2;
+    constexpr int G = 8, QR = 4, RS = G + 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = P.n, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, NW = blockDim.x >> 5;
+    const int g = lane % G, q = lane / G;
+    R2 *cur = (R2 *)smem_raw;
+    EllEnt<R> *ell = (EllEnt<R> *)(cur + (size_t)n * RS);
+    int *sptr = (int *)(ell + nent);
+    double *red = (double *)(((uintptr_t)(sptr + nslices + 1) + 15) & ~(uintptr_t)15);
+    for (int e = tid; e < nent; e += blockDim.x) ell[e] = ell_g[e];
+    for (int e = tid; e <= nslices; e += blockDim.x) sptr[e] = sptr_g[e];
+    const int v = blockIdx.x * G + g;
+    const bool valid = v < nvec;
+    const int vv = valid ? v : blockIdx.x * G;
+    const int x = vv % 3;
+    const long ti = (long)(J.begin + vv / 3) * J.sample;
+    R2 psi[IT], nx[IT];
+    float dg[IT];
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+        int i = q + QR * (warp + NW * it);
+        psi[it].x = i < n ? (R)traj_mu(T, ti, x, i) : (R)0;
+        psi[it].y = 0;
+    }
+    __syncthreads();
+    for (int t1 = 0; t1 < J.tmax; t1++) {
+        const long tj = ti + t1;
+        double re = 0, im = 0;
+#pragma unroll
+        for (int it = 0; it < IT; it++) {
+            int i = q + QR * (warp + NW * it);
+            if (i < n) {
+                R m = (R)traj_mu(T, tj, x, i);
+                re += (double)(m * psi[it].x);
+                im += (double)(m * psi[it].y);
+            }
+        }
+        for (int o = G; o < 32; o <<= 1) {
+            re += __shfl_xor_sync(0xffffffffu, re, o);
+            im += __shfl_xor_sync(0xffffffffu, im, o);
+        }
+        if (q == 0) { red[(warp * G + g) * 2] = re; red[(warp * G + g) * 2 + 1] = im; }
+        __syncthreads();
+        if (tid < G && blockIdx.x * G + tid < nvec) {
+            double sr = 0, si = 0;
+            for (int w = 0; w < NW; w++) { sr += red[(w * G + tid) * 2]; si += red[(w * G + tid) * 2 + 1]; }
+            resp[(size_t)(blockIdx.x * G + tid) * J.tmax + t1] = make_double2(sr, si);
+        }
+        if (t1 == J.tmax - 1) break;
+        int K = P.order[tj - P.f0];
+        for (int o = 1; o < G; o <<= 1) K = max(K, __shfl_xor_sync(0xffffffffu, K, o));
+#pragma unroll
+        for (int it = 0; it < IT; it++) {
+            int i = q + QR * (warp + NW * it);
+            dg[it] = i < n ? traj_diag(T, tj, i, P.singleshift != 0) : 0.0f;
+            if (i < n) cur[(size_t)i * RS + g] = psi[it];
+        }
+        for (int k = 1; k <= K; k++) {
+            __syncthreads();
+            const R c = (R)(J.f / k);
+#pragma unroll
+            for (int it = 0; it < IT; it++) {
+                const int sl = warp + NW * it, i = q + QR * sl;
+                if (sl >= nslices) continue;
+                R2 z = cur[(size_t)(i < n ? i : 0) * RS + g];
+                R yr = (R)dg[it] * z.x, yi = (R)dg[it] * z.y;
+                const int b0 = sptr[sl], b1 = sptr[sl + 1];
+                for (int e = b0 + q; e < b1; e += QR) {
+                    EllEnt<R> en = ell[e];
+                    R2 zz = cur[en.off + g];
+                    yr += en.v * zz.x;
+                    yi += en.v * zz.y;
+                }
+                nx[it].x = c * yi;  // (-i)(c)(y)
+                nx[it].y = -c * yr;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int it = 0; it < IT; it++) {
+                const int sl = warp + NW * it, i = q + QR * sl;
+                if (sl >= nslices || i >= n) continue;
+                cur[(size_t)i * RS + g] = nx[it];
+                psi[it].x += nx[it].x;
+                psi[it].y += nx[it].y;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void k_reduce_resp(const double2 *resp, int nvec, int tmax, double2 *out) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= tmax) return;
@@ -653,8 +759,46 @@ static int run_taylor2(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, d
     return (int)cudaGetLastError();
 }
 
+size_t taylor3_smem(const TaylorPlan &P, size_t rsz) {
+    size_t ent = rsz == 4 ? 8 : 16;
+    return (size_t)P.n * 10 * 2 * rsz + (size_t)P.ell_nent * ent + sizeof(int) * (P.ell_nslices + 1) + 16 +
+           16 * 8 * 2 * sizeof(double);
+}
+
+template <typename R, int IT>
+static int run_taylor3(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int nvec,
+                       cudaStream_t s) {
+    const int NT = 512;
+    size_t smem = taylor3_smem(P, sizeof(R));
+    int e;
+    if ((e = set_smem(k_abs_taylor3<R, IT>, smem))) return e;
+    k_abs_taylor3<R, IT><<<(nvec + 7) / 8, NT, smem, s>>>(T, P, J, resp, nvec, (const EllEnt<R> *)P.ell,
+                                                          P.ell_sptr, P.ell_nslices, P.ell_nent);
+    (void)NT;
+    return (int)cudaGetLastError();
+}
+
 int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp,
                       int vec_per_cta, cudaStream_t s) {
+    if (P.static_j && P.ell && vec_per_cta > 4 && taylor3_smem(P, prec == 0 ? 4 : 8) <= 220 * 1024) {
+        int nvec = 3 * J.nsamp;
+        int it = (P.ell_nslices + 15) / 16;  // 16 warps, one slice (4 rows) per warp instruction
+        int IT = it <= 1 ? 1 : it <= 2 ? 2 : it <= 4 ? 4 : it <= 8 ? 8 : it <= 16 ? 16 : 32;
+        if (it <= 32) {
+#define T3(R)                                                                    \
+    switch (IT) {                                                                \
+    case 1: return run_taylor3<R, 1>(T, P, J, resp, nvec, s);                    \
+    case 2: return run_taylor3<R, 2>(T, P, J, resp, nvec, s);                    \
+    case 4: return run_taylor3<R, 4>(T, P, J, resp, nvec, s);                    \
+    case 8: return run_taylor3<R, 8>(T, P, J, resp, nvec, s);                    \
+    case 16: return run_taylor3<R, 16>(T, P, J, resp, nvec, s);                  \
+    default: return run_taylor3<R, 32>(T, P, J, resp, nvec, s);                  \
+    }
+            if (prec == 0) { T3(float) }
+            T3(double)
+#undef T3
+        }
+    }
     {
         // vectors across lanes (k_abs_taylor2): 16 warps cover 512 rows per
         // iteration at G = 8 (4 rows per warp) and 128 at G = 4... rows per

@@ -7,6 +7,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -508,6 +509,49 @@ extern "C" int nise_absorption(nise_ctx *c, double *re_S, double *im_S, int *sam
             cudaMemcpyAsync(dval.p, vd.data(), sizeof(double) * vd.size(), cudaMemcpyHostToDevice, c->stream);
         }
         if ((rc = dorder.alloc(c, (size_t)nf))) return rc;
+        // sliced ELL (4-row slices, [slot][row]) of the same couplings for the
+        // shared-memory kernel; entry offsets address rows of 10 complex numbers
+        const int nsl = (N + 3) / 4;
+        std::vector<int> sptr(nsl + 1, 0);
+        for (int sl = 0; sl < nsl; sl++) {
+            int L = 0;
+            for (int r = 0; r < 4; r++) {
+                int row = 4 * sl + r;
+                if (row < N) L = std::max(L, rp[row + 1] - rp[row]);
+            }
+            sptr[sl + 1] = sptr[sl] + 4 * L;
+        }
+        const int nent = sptr[nsl];
+        DevBuf<char> dell;
+        DevBuf<int> dsptr;
+        {
+            size_t esz = prec == NISE_FP32 ? 8 : 16;
+            std::vector<unsigned char> ell((size_t)(nent > 0 ? nent : 1) * esz, 0);
+            for (int sl = 0; sl < nsl; sl++) {
+                int L = (sptr[sl + 1] - sptr[sl]) / 4;
+                for (int slot = 0; slot < L; slot++)
+                    for (int r = 0; r < 4; r++) {
+                        int row = 4 * sl + r, e = sptr[sl] + slot * 4 + r;
+                        int off = (row < N ? row : 0) * 10;
+                        double v = 0;
+                        if (row < N && slot < rp[row + 1] - rp[row]) {
+                            off = col[rp[row] + slot] * 10;
+                            v = vd.empty() ? 0 : vd[rp[row] + slot];
+                        }
+                        unsigned char *dst = ell.data() + (size_t)e * esz;
+                        memcpy(dst, &off, 4);
+                        if (prec == NISE_FP32) {
+                            float fv = (float)v;
+                            memcpy(dst + 4, &fv, 4);
+                        } else {
+                            memcpy(dst + 8, &v, 8);
+                        }
+                    }
+            }
+            if ((rc = dell.alloc(c, ell.size()))) return rc;
+            cudaMemcpyAsync(dell.p, ell.data(), ell.size(), cudaMemcpyHostToDevice, c->stream);
+            if ((rc = dsptr.upload(c, sptr))) return rc;
+        }
         TaylorPlan P;
         memset(&P, 0, sizeof(P));
         P.n = N;
@@ -516,6 +560,10 @@ extern "C" int nise_absorption(nise_ctx *c, double *re_S, double *im_S, int *sam
         P.col = dcol.p;
         P.val = dval.p;
         P.static_j = 1;
+        P.ell = dell.p;
+        P.ell_sptr = dsptr.p;
+        P.ell_nslices = nsl;
+        P.ell_nent = nent;
         P.f0 = f0;
         P.nf = nf;
         P.singleshift = c->nshift > 0;

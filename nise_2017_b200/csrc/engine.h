@@ -44,6 +44,11 @@ struct TaylorPlan {
     long f0, nf;
     const int *order;      // [nf] Taylor order per frame
     int singleshift;
+    // sliced-ELL copy of the couplings for the shared-memory kernel: slices of
+    // 4 rows, entries (state offset, weight) [slot][row in slice]
+    const void *ell;
+    const int *ell_sptr;   // [nslices + 1] entry offset of each slice
+    int ell_nslices, ell_nent;
 };
 
 // A batch of linear-absorption start points: vectors v = 3*(s-begin)+x for
