@@ -159,6 +159,15 @@ int nise_write_spectrum(const char *path, const double *freq, const double *spec
 /* print2D: divides by sample_count, halves the t3 = 0 row, writes t1 t2 t3 Re Im. */
 int nise_write_2d(const char *path, const nise_params *p, const double *re, const double *im, int sample_count);
 
+/* The reference's 2DFFT program (2DFFT.c:20-830): reads the keyword file at
+ * `input_path` (FFT, Timestep, RunTimes, Min/MaxFrequencies, Homogeneous,
+ * Inhomogeneous, Window, Format, Technique) and the 2D response files
+ * R{par,per,cro}{I,II}.dat of the current directory (per waiting time when a
+ * Waitingtime.dat lists them, the .IRraman files for 2DIRraman), and writes
+ * Rw*.dat, 2D.*.dat and PP.*.dat there.  The fft x fft transforms run on
+ * `device`. */
+int nise_2dfft_files(const char *input_path, int device);
+
 /* Run this context's device work on the caller's CUDA stream (a
  * cudaStream_t passed as a pointer; NULL restores the context's own stream). */
 int nise_set_stream(nise_ctx *ctx, void *stream);

@@ -35,7 +35,7 @@ EXPORTED = [
     "nise_global_error", "nise_load_files", "nise_set_trajectory", "nise_set_singleshift", "nise_absorption",
     "nise_absorption_fft", "nise_2dir", "nise_propagate", "nise_propagate_doubles", "nise_write_td_absorption",
     "nise_write_spectrum", "nise_write_2d", "nise_set_stream", "nise_last_timing", "nise_last_work",
-    "nise_probe_fp32_peak", "nise_absorption_noalloc",
+    "nise_probe_fp32_peak", "nise_absorption_noalloc", "nise_2dfft_files",
 ]
 
 
@@ -307,3 +307,11 @@ def write_2d(path, params, re, im, count):
                              _dp(np.ascontiguousarray(im)), count)
     if rc != 0:
         raise NiseError(rc, "cannot write %s" % path)
+
+
+def fft2d_files(input_path, device=0):
+    """The 2DFFT program (2DFFT.c): 2D spectra from the R*.dat files of the
+    current directory, with the keyword file `input_path`."""
+    rc = lib().nise_2dfft_files(os.fsencode(input_path), device)
+    if rc != 0:
+        raise NiseError(rc, lib().nise_global_error().decode())

@@ -27,6 +27,7 @@ CU_SOURCES = [
     "eigen.cu",
     "util.cu",
     "noalloc.cu",
+    "fft2d.cu",
 ]
 CPP_SOURCES = [
     "api.cpp",
@@ -93,12 +94,14 @@ def build_engine(force=False, verbose_ptxas=False):
 
 
 def build_driver(force=False):
-    out = os.path.join(HERE, "nise")
-    src = os.path.join(CSRC, "nise_main.c")
-    if force or _newer(out, [src, os.path.join(INCLUDE, "nise_b200.h")]):
-        _run(["gcc", "-std=gnu99", "-O2", "-I" + INCLUDE, "-o", out, src,
-              "-L" + HERE, "-lnise_b200", "-Wl,-rpath,$ORIGIN", "-lm"])
-    return out
+    """The drop-in executables: nise (NISE's propagation path) and nise2dfft (2DFFT)."""
+    for exe, c in (("nise", "nise_main.c"), ("nise2dfft", "nise2dfft_main.c")):
+        out = os.path.join(HERE, exe)
+        src = os.path.join(CSRC, c)
+        if force or _newer(out, [src, os.path.join(INCLUDE, "nise_b200.h")]):
+            _run(["gcc", "-std=gnu99", "-O2", "-I" + INCLUDE, "-o", out, src,
+                  "-L" + HERE, "-lnise_b200", "-Wl,-rpath,$ORIGIN", "-lm"])
+    return os.path.join(HERE, "nise")
 
 
 def build_all(force=False):
@@ -109,4 +112,4 @@ def build_all(force=False):
 
 if __name__ == "__main__":
     build_all(force="--force" in sys.argv)
-    print("built:", ", ".join(f for f in os.listdir(HERE) if f.endswith(".so") or f == "nise"))
+    print("built:", ", ".join(f for f in os.listdir(HERE) if f.endswith(".so") or f in ("nise", "nise2dfft")))

@@ -141,7 +141,7 @@ size_t eig_smem_bytes(int n) {
 }
 
 int launch_eig(const EigJob &J, const long *frames_dev, long nframes, double *V, double *w, cudaStream_t s) {
-    if (J.n > 128) return (int)cudaErrorNotSupported;
+    if (J.n > NISE_EIG_MAX_N) return (int)cudaErrorNotSupported;
     size_t smem = eig_smem_bytes(J.n);
     cudaError_t e = cudaFuncSetAttribute(k_eig_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e) return (int)e;

@@ -298,9 +298,17 @@ __device__ void doubles_substep(typename Vec2<R>::T *F, const typename Vec2<R>::
     __syncwarp();
     int cur_a = -1;
     R2 piv[CPL];
+    // the next coupling and its coefficients are loaded one step ahead
+    int2 ab_next = K > 0 ? pairs[0] : make_int2(0, 0);
+    Dcoef<R> q_next;
+    if (K > 0) q_next = cf[0];
     for (int k = 0; k < K; k++) {
-        int2 ab = pairs[k];
-        int a = ab.x, b = ab.y;
+        const int a = ab_next.x, b = ab_next.y;
+        const Dcoef<R> q = q_next;
+        if (k + 1 < K) {
+            ab_next = pairs[k + 1];
+            q_next = cf[k + 1];
+        }
         if (a != cur_a) {
             if (cur_a >= 0) {
 #pragma unroll
@@ -317,24 +325,26 @@ __device__ void doubles_substep(typename Vec2<R>::T *F, const typename Vec2<R>::
             }
             cur_a = a;
         }
-        Dcoef<R> q = cf[k];
+        // c == a case: (|aa>,|ab>) with the sqrt(2) angle, by the lane owning c = b
+        if (b - lane >= 0 && ((b - lane) & 31) == 0) {
+            const int j = (b - lane) >> 5;
+            const int ix = circ(a, a, n, W);
+            R2 X = F[ix];
+#pragma unroll
+            for (int jj = 0; jj < CPL; jj++)
+                if (jj == j) rot2<R>(X, piv[jj], q.co2, q.si2);
+            F[ix] = X;
+        }
+        // every other lane c != a: (|ac>,|bc>); for c == b that is (|ab>,|bb>) at sqrt(2)
 #pragma unroll
         for (int j = 0; j < CPL; j++) {
-            int c = lane + 32 * j;
+            const int c = lane + 32 * j;
             if (c >= n || c == a) continue;
-            if (c != b) {
-                int iq = circ(b, c, n, W);
-                R2 Q = F[iq];
-                rot2<R>(piv[j], Q, q.co, q.si);
-                F[iq] = Q;
-            } else {  // c == a then c == b cases, sqrt(2) angle
-                int ix = circ(a, a, n, W), iy = circ(b, b, n, W);
-                R2 X = F[ix], Y = F[iy];
-                rot2<R>(X, piv[j], q.co2, q.si2);
-                rot2<R>(piv[j], Y, q.co2, q.si2);
-                F[ix] = X;
-                F[iy] = Y;
-            }
+            const bool sp = c == b;
+            const int iq = circ(b, c, n, W);
+            R2 Q = F[iq];
+            rot2<R>(piv[j], Q, sp ? q.co2 : q.co, sp ? q.si2 : q.si);
+            F[iq] = Q;
         }
         __syncwarp();
     }
@@ -364,7 +374,7 @@ __device__ __forceinline__ float over_mu(const TwoD &D, long t, int x, int i) {
 
 // CTA = W warps = W doubles vectors of one start point, all at the same t3.
 template <typename R, int CPL>
-__global__ void __launch_bounds__(256) k2d_doubles(TwoD D, int vec_per_sample, Dcoef<R> *cf_static) {
+__global__ void __launch_bounds__(512) k2d_doubles(TwoD D, int vec_per_sample, Dcoef<R> *cf_static) {
     typedef typename Vec2<R>::T R2;
     typedef Ar<R> A;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -555,6 +565,207 @@ __global__ void k2d_dcoef(TwoD D, Dcoef<R> *cf, long nframes) {
     cf[g] = q;
 }
 
+
+// ---------------------------------------------------------------- doubles, RK4
+// propagate_vec_RK4_doubles (propagate.c:376-590): thread per doubles vector,
+// in the reference's sequential order (stage sums accumulate element by
+// element in the order of its loops), state and stage vectors in global
+// memory in packed order.  The EA projections and dot products per t3 are
+// those of k2d_doubles, summed in site order.
+template <typename R> struct Rk4D;
+template <> struct Rk4D<float> {
+    // k += H * (c + k' * 0.5) * factor, evaluated in double like the reference
+    static __device__ __forceinline__ float half(float k, float h, float c, float kp, float fac, bool minus) {
+        double y = __dmul_rn(__dmul_rn((double)h, __dadd_rn((double)c, __dmul_rn((double)kp, 0.5))), (double)fac);
+        return (float)(minus ? __dsub_rn((double)k, y) : __dadd_rn((double)k, y));
+    }
+    static __device__ __forceinline__ float full(float k, float h, float c, float kp, float fac, bool minus) {
+        float y = __fmul_rn(__fmul_rn(h, __fadd_rn(c, kp)), fac);
+        return minus ? __fsub_rn(k, y) : __fadd_rn(k, y);
+    }
+    static __device__ __forceinline__ float first(float k, float h, float c, float fac, bool minus) {
+        float y = __fmul_rn(__fmul_rn(h, c), fac);
+        return minus ? __fsub_rn(k, y) : __fadd_rn(k, y);
+    }
+    static __device__ __forceinline__ float update(float c, float k1, float k2, float k3, float k4) {
+        double sum = __dadd_rn(__dadd_rn(__dadd_rn((double)k1, __dmul_rn(2.0, (double)k2)), __dmul_rn(2.0, (double)k3)),
+                               (double)k4);
+        return (float)__dadd_rn((double)c, __ddiv_rn(sum, 6.0));
+    }
+};
+template <> struct Rk4D<double> {
+    static __device__ __forceinline__ double half(double k, double h, double c, double kp, double fac, bool minus) {
+        double y = h * (c + kp * 0.5) * fac;
+        return minus ? k - y : k + y;
+    }
+    static __device__ __forceinline__ double full(double k, double h, double c, double kp, double fac, bool minus) {
+        double y = h * (c + kp) * fac;
+        return minus ? k - y : k + y;
+    }
+    static __device__ __forceinline__ double first(double k, double h, double c, double fac, bool minus) {
+        double y = h * c * fac;
+        return minus ? k - y : k + y;
+    }
+    static __device__ __forceinline__ double update(double c, double k1, double k2, double k3, double k4) {
+        return c + (k1 + 2.0 * k2 + 2.0 * k3 + k4) / 6.0;
+    }
+};
+
+template <typename R>
+__device__ void rk4_doubles_step(const TwoD &D, long t, typename Vec2<R>::T *F, typename Vec2<R>::T *Kq, R *hd) {
+    typedef typename Vec2<R>::T R2;
+    typedef Ar<R> A;
+    typedef Rk4D<R> O;
+    const int n = D.n, N2 = n * (n + 1) / 2;
+    const R f = sizeof(R) == 4 ? (R)D.f32_dsub : (R)D.f64_dsub;
+    const R sq2 = (R)1.41421356237f;
+    R2 *K1 = Kq, *K2 = K1 + N2, *K3 = K2 + N2, *K4 = K3 + N2;
+    for (int a = 0; a < n; a++) {  // HD (propagate.c:427-442)
+        R ea = (R)traj_diag(D.T, t, a, false);
+        for (int b = a; b < n; b++) {
+            R hsum = A::add(ea, (R)traj_diag(D.T, t, b, false));
+            R h = A::mul(f, hsum);
+            if (a == b) {
+                R an = D.anh != 0.0f ? (R)D.anh : (R)D.T.anh[t * (1L + n) + 1 + a];
+                h = A::sub(h, A::mul(an, f));
+            }
+            hd[sindex(a, b, n)] = h;
+        }
+    }
+    for (int sub = 0; sub < D.ts; sub++) {
+        for (int e = 0; e < 4 * N2; e++) { Kq[e].x = 0; Kq[e].y = 0; }
+        for (int stage = 0; stage < 4; stage++) {
+            R2 *Kn = stage == 0 ? K1 : stage == 1 ? K2 : stage == 2 ? K3 : K4;
+            const R2 *Kp = stage == 1 ? K1 : stage == 2 ? K2 : K3;
+            for (int e = 0; e < N2; e++) {
+                R2 c = F[e], k = Kn[e];
+                R h = hd[e];
+                if (stage == 0) { k.x = O::first(k.x, h, c.y, (R)1, false); k.y = O::first(k.y, h, c.x, (R)1, true); }
+                else if (stage < 3) { k.x = O::half(k.x, h, c.y, Kp[e].y, (R)1, false); k.y = O::half(k.y, h, c.x, Kp[e].x, (R)1, true); }
+                else { k.x = O::full(k.x, h, c.y, Kp[e].y, (R)1, false); k.y = O::full(k.y, h, c.x, Kp[e].x, (R)1, true); }
+                Kn[e] = k;
+            }
+            for (int kk = 0; kk < D.K; kk++) {
+                int2 ab = D.pairs[kk];
+                int a = ab.x, b = ab.y;
+                float jv = traj_coupling(D.T, t, a, b);
+                R h0 = fabsf(jv) > D.T.cut ? A::mul(f, (R)jv) : (R)0;
+                for (int c = 0; c < n; c++) {
+                    int i1 = sindex(a, c, n), i2 = sindex(b, c, n);
+                    R fac = (c == a || c == b) ? sq2 : (R)1;
+                    R2 c1 = F[i1], c2 = F[i2], k1 = Kn[i1];
+                    if (stage == 0) {
+                        k1.x = O::first(k1.x, h0, c2.y, fac, false); k1.y = O::first(k1.y, h0, c2.x, fac, true);
+                    } else if (stage < 3) {
+                        k1.x = O::half(k1.x, h0, c2.y, Kp[i2].y, fac, false);
+                        k1.y = O::half(k1.y, h0, c2.x, Kp[i2].x, fac, true);
+                    } else {
+                        k1.x = O::full(k1.x, h0, c2.y, Kp[i2].y, fac, false);
+                        k1.y = O::full(k1.y, h0, c2.x, Kp[i2].x, fac, true);
+                    }
+                    Kn[i1] = k1;
+                    R2 k2 = Kn[i2];
+                    if (stage == 0) {
+                        k2.x = O::first(k2.x, h0, c1.y, fac, false); k2.y = O::first(k2.y, h0, c1.x, fac, true);
+                    } else if (stage < 3) {
+                        k2.x = O::half(k2.x, h0, c1.y, Kp[i1].y, fac, false);
+                        k2.y = O::half(k2.y, h0, c1.x, Kp[i1].x, fac, true);
+                    } else {
+                        k2.x = O::full(k2.x, h0, c1.y, Kp[i1].y, fac, false);
+                        k2.y = O::full(k2.y, h0, c1.x, Kp[i1].x, fac, true);
+                    }
+                    Kn[i2] = k2;
+                }
+            }
+        }
+        R norm = 0;  // find_norm / re_normalize (NISE_subs.c:125-148)
+        for (int e = 0; e < N2; e++) norm = A::add(norm, A::add(A::mul(F[e].x, F[e].x), A::mul(F[e].y, F[e].y)));
+        for (int e = 0; e < N2; e++) {
+            R2 z = F[e];
+            z.x = O::update(z.x, K1[e].x, K2[e].x, K3[e].x, K4[e].x);
+            z.y = O::update(z.y, K1[e].y, K2[e].y, K3[e].y, K4[e].y);
+            F[e] = z;
+        }
+        R nn = 0;
+        for (int e = 0; e < N2; e++) nn = A::add(nn, A::add(A::mul(F[e].x, F[e].x), A::mul(F[e].y, F[e].y)));
+        if (norm != nn) {
+            R factor = (R)sqrt((double)(norm / nn));
+            for (int e = 0; e < N2; e++) { F[e].x = A::mul(F[e].x, factor); F[e].y = A::mul(F[e].y, factor); }
+        }
+    }
+}
+
+// Thread per doubles vector: dipole_double at tk, then per t3 the EA
+// projections (dipole_double_last) and dot products, then one RK4 step.
+template <typename R>
+__global__ void k2d_doubles_seq(TwoD D, int vec_per_sample, void *Fbuf, void *Kbuf, void *hdbuf) {
+    typedef typename Vec2<R>::T R2;
+    typedef Ar<R> A;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= D.S * vec_per_sample) return;
+    const int s = g / vec_per_sample, u = g % vec_per_sample, n = D.n, N2 = n * (n + 1) / 2, NV = nvec_se(D);
+    R2 *F = (R2 *)Fbuf + (size_t)g * N2, *Kq = (R2 *)Kbuf + (size_t)g * 4 * N2;
+    R *hd = (R *)hdbuf + (size_t)g * N2;
+    const long tk = tk_of(D, s);
+    int kind = u < 9 ? 0 : 1, pa, p2, t1 = 0;
+    if (kind == 0) { pa = u / 3; p2 = u % 3; }
+    else { int w = u - 9, cmb = w / D.T1; t1 = w % D.T1; pa = cmb / 3; p2 = cmb % 3; }
+    const R2 *src = (const R2 *)D.SE + ((size_t)s * D.T3 * NV + (kind == 0 ? pa : 3 + pa * D.T1 + t1)) * n;
+    for (int i = 0; i < n; i++)
+        for (int j = i; j < n; j++) {
+            R2 f;
+            if (i == j) {
+                R o = (R)over_mu(D, tk, p2, i);
+                f.x = A::mul(o, src[i].x);
+                f.y = A::mul(o, src[i].y);
+            } else {
+                R mi = (R)traj_mu(D.T, tk, p2, i), mj = (R)traj_mu(D.T, tk, p2, j);
+                f.x = A::add(A::mul(mi, src[j].x), A::mul(mj, src[i].x));
+                f.y = A::add(A::mul(mi, src[j].y), A::mul(mj, src[i].y));
+            }
+            F[sindex(i, j, n)] = f;
+        }
+    for (int t3 = 0; t3 < D.T3; t3++) {
+        const long tl = tk + t3;
+        if (D.ea)
+            for (int p3 = 0; p3 < 3; p3++)
+                for (int m = 0; m < 21; m++) {
+                    if (c_px[m][3] != p3 || c_px[m][2] != p2) continue;
+                    if (kind == 0 && c_px[m][1] != pa) continue;
+                    if (kind == 1 && c_px[m][0] != pa) continue;
+                    const int p0 = c_px[m][0], p1 = c_px[m][1];
+                    int tt0 = kind == 0 ? 0 : t1, tt1 = kind == 0 ? D.T1 : t1 + 1;
+                    for (int tt = tt0; tt < tt1; tt++) {
+                        const R2 *rv = (const R2 *)D.SE +
+                                       (((size_t)s * D.T3 + t3) * NV + (kind == 0 ? 3 + p0 * D.T1 + tt : p1)) * n;
+                        double a1 = 0, a2 = 0;
+                        for (int q = 0; q < n; q++) {
+                            R gr = 0, gi = 0;  // dipole_double_last for site q
+                            for (int j = 0; j < n; j++) {
+                                R mm = (R)(j == q ? over_mu(D, tl, p3, q) : traj_mu(D.T, tl, p3, j));
+                                R2 ff = F[sindex(j, q, n)];
+                                gr = A::add(gr, A::mul(mm, ff.x));
+                                gi = A::add(gi, A::mul(mm, ff.y));
+                            }
+                            R rr = rv[q].x, ri = -rv[q].y;
+                            if (kind == 0) {
+                                a1 += (double)A::add(A::mul(gi, rr), A::mul(gr, ri));
+                                a2 += (double)A::sub(A::mul(gr, rr), A::mul(ri, gi));
+                            } else {
+                                a1 += (double)A::add(A::mul(rr, gi), A::mul(ri, gr));
+                                a2 += (double)A::sub(A::mul(rr, gr), A::mul(ri, gi));
+                            }
+                        }
+                        size_t o = (((size_t)s * D.T3 + t3) * 21 + m) * D.T1 + tt;
+                        if (kind == 0) D.eaI[o] = make_double2(a1, a2);
+                        else D.eaII[o] = make_double2(a1, a2);
+                    }
+                }
+        if (t3 == D.T3 - 1) break;
+        rk4_doubles_step<R>(D, tl, F, Kq, hd);
+    }
+}
+
 // ---------------------------------------------------------------- response
 // Thread per (start point, t3, t1): GB (calc_2DIR.c:270-286), SE (:395-411)
 // and EA (:473-487) contributions of all 21 molecular polarisations.
@@ -702,12 +913,24 @@ int run_chunk(nise_ctx *c, TwoD &D, Dcoef<R> *cf) {
         k2d_se<R><<<(nv + B - 1) / B, B, sm, st>>>(D);
         c->launches++;
     }
-    if (D.ea) {
+    if (D.ea && D.prop == NISE_PROP_RK4) {
+        int vps = 9 + 9 * D.T1, tot = D.S * vps, N2 = D.n * (D.n + 1) / 2;
+        void *Fb = nullptr, *Kb = nullptr, *Hb = nullptr;
+        if ((e = (int)cudaMallocAsync(&Fb, sizeof(R2) * (size_t)tot * N2, st))) return e;
+        if ((e = (int)cudaMallocAsync(&Kb, sizeof(R2) * (size_t)tot * 4 * N2, st))) return e;
+        if ((e = (int)cudaMallocAsync(&Hb, sizeof(R) * (size_t)tot * N2, st))) return e;
+        k2d_doubles_seq<R><<<(tot + 63) / 64, 64, 0, st>>>(D, vps, Fb, Kb, Hb);
+        c->launches++;
+        cudaFreeAsync(Fb, st);
+        cudaFreeAsync(Kb, st);
+        cudaFreeAsync(Hb, st);
+    } else if (D.ea) {
         int W = D.n / 2 + 2, slots = D.n * W;
-        int nwarps = sizeof(R) == 4 ? 8 : 4;
+        // as many vectors (warps) as fit next to the phase table in shared memory
+        int nwarps = 16;
         size_t dsm = sizeof(R2) * (size_t)slots * (1 + nwarps) + sizeof(float) * 7 * D.n;
         while (dsm > 220 * 1024 && nwarps > 1) {
-            nwarps >>= 1;
+            nwarps -= 1;
             dsm = sizeof(R2) * (size_t)slots * (1 + nwarps) + sizeof(float) * 7 * D.n;
         }
         if (dsm > 220 * 1024) return (int)cudaErrorNotSupported;
@@ -746,10 +969,9 @@ extern "C" int nise_2dir(nise_ctx *c, double *R, int *sample_count) {
     bool gb = tech == NISE_TECH_2DIR || tech == NISE_TECH_GBIR || tech == NISE_TECH_NOEAIR;
     bool se = tech == NISE_TECH_2DIR || tech == NISE_TECH_SEIR || tech == NISE_TECH_NOEAIR;
     bool ea = tech == NISE_TECH_2DIR || tech == NISE_TECH_EAIR;
-    if (ea && p.propagation != NISE_PROP_COUPLING)
-        return nise_fail(c, NISE_ERR_UNSUPPORTED, "the doubles manifold supports Propagation Coupling in this engine");
     if (ea && N > 128) return nise_fail(c, NISE_ERR_UNSUPPORTED, "doubles manifold limited to 128 sites");
-    if (T2 > 0 && N > 128) return nise_fail(c, NISE_ERR_UNSUPPORTED, "t2 eigen step limited to 128 sites");
+    if (T2 > 0 && N > NISE_EIG_MAX_N)
+        return nise_fail(c, NISE_ERR_UNSUPPORTED, "t2 eigen step limited to 120 sites");
     if (ea && p.anharmonicity == 0 && (!c->d_anh || !c->d_over))
         return nise_fail(c, NISE_ERR_IO, "Anharmonicity 0 needs Anharmonicfile and Overtonedipolefile");
     // calculateWorkset (MPI_subs.c:36-110)
@@ -885,6 +1107,8 @@ extern "C" int nise_2dir(nise_ctx *c, double *R, int *sample_count) {
     const int NV = 3 + 3 * T1;
     size_t per_sample = r2 * ((size_t)3 * T1 * N + 3 * N + (size_t)T3 * NV * N) + sizeof(double2) * (9 * (size_t)T1 + 9 * T3) +
                         2 * sizeof(double2) * (size_t)T3 * 21 * T1 + sizeof(double) * 12 * plane;
+    if (D.ea && D.prop == NISE_PROP_RK4)  // RK4 doubles: state, 4 stages and the diagonal per doubles vector
+        per_sample += (9 + 9 * (size_t)T1) * (size_t)N * (N + 1) / 2 * (5 * r2 + r2 / 2);
     size_t budget = (size_t)1536 << 20;
     int chunk = (int)(budget / (per_sample > 0 ? per_sample : 1));
     if (chunk < 1) chunk = 1;

@@ -44,3 +44,45 @@ def uses_eigen(case):
     kw = case["keywords"]
     t2 = int(str(kw.get("RunTimes", "0 0 0")).split()[1])
     return kw.get("Propagation") in ("Sparse", "Diagonal") or (kw["Technique"] != "Absorption" and t2 > 0)
+
+
+def fft2d_case(name):
+    """Inputs and reference outputs of a 2D FFT golden case: ({name: text}, {name: text})."""
+    d = np.load(os.path.join(GOLDEN, "fft2d_%s.npz" % name))
+    return json.loads(str(d["inputs"])), json.loads(str(d["outputs"]))
+
+
+def fft2d_case_names():
+    with open(os.path.join(GOLDEN, "fft2d_cases.json")) as f:
+        return sorted(json.load(f))
+
+
+def compare_spectrum_text(got, ref, tol):
+    """Compare two text files of the 2D FFT step.
+
+    The line structure (blank lines, tokens per line, the '###' header) must be
+    identical; "%f" tokens (frequency axes) must be identical text; "%e" tokens
+    (spectral values) must agree within tol times the largest |value| in the
+    file.  Returns the worst relative value difference.
+    """
+    a, b = got.splitlines(), ref.splitlines()
+    assert len(a) == len(b), "line count %d != %d" % (len(a), len(b))
+    worst, vals_a, vals_b = 0.0, [], []
+    for la, lb in zip(a, b):
+        ta, tb = la.split(), lb.split()
+        assert len(ta) == len(tb), (la, lb)
+        if lb.startswith("#"):
+            assert la == lb
+            continue
+        for x, y in zip(ta, tb):
+            if "e" in y:
+                vals_a.append(float(x))
+                vals_b.append(float(y))
+            else:
+                assert x == y, "axis token %s != %s" % (x, y)
+    if vals_b:
+        va, vb = np.array(vals_a), np.array(vals_b)
+        scale = np.abs(vb).max() or 1.0
+        worst = float(np.abs(va - vb).max() / scale)
+        assert worst <= tol, "values differ by %.3g of the largest (tolerance %.3g)" % (worst, tol)
+    return worst

@@ -21,7 +21,7 @@ pytestmark = pytest.mark.gpu
 
 CASES = helpers.cases()
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-SUPPORTED = ["2d_coupling", "2d_coupling_t2", "2d_full_anhfile", "2d_gbir", "2d_seir", "2d_eair"]
+SUPPORTED = ["2d_coupling", "2d_coupling_t2", "2d_rk4", "2d_full_anhfile", "2d_gbir", "2d_seir", "2d_eair"]
 
 SUM_ORDER = 1e-10   # same single-precision operations, FP64 sums in another order
 T2_EIGEN = 1e-5     # t2 eigenvectors from a different Jacobi ordering (rounded to float)
@@ -63,8 +63,8 @@ def test_fp64_matches_fp64_oracle(name, tmp_path):
     assert helpers.rel2d(R, oR) < (1e-9 if helpers.uses_eigen(case) else 1e-11)
 
 
-@pytest.mark.parametrize("tech", ["GBIR", "SEIR", "noEAIR"])
-def test_rk4_singles_techniques(tech, tmp_path):
+@pytest.mark.parametrize("tech", ["GBIR", "SEIR", "noEAIR", "EAIR", "2DIR"])
+def test_rk4_techniques(tech, tmp_path):
     s = synth.c2_spec(n_sites=6, frames=300, seed=31)
     files = synth.write(s, str(tmp_path))
     kw = synth.c2_keywords(Singles=6, Length=300, RunTimes="8 2 8", Samplerate=40, Propagation="RK4", Technique=tech)
