@@ -288,7 +288,7 @@ def run_ours(args):
     main_ms = statistics.mean(mains)
     achieved = flops / (main_ms / 1e3) / 1e12
     peak = nise.fp32_peak(local)
-    traffic = read_traffic().get("k_abs_taylor_fp32_per_launch")
+    traffic = read_traffic().get("k_abs_taylor3_fp32_per_launch")
     out = None
     if rank == 0:
         cpu = None
@@ -318,7 +318,7 @@ def run_ours(args):
             "batched_over_plain": value / plain_value,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_ms / args.steps},
-            "roofline": {"bound": "fp32", "kernel": "k_abs_taylor", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "fp32", "kernel": "k_abs_taylor3", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": traffic,
                          "peak_source": "measured in-process FP32 FMA throughput (nise_probe_fp32_peak)",
                          "algorithmic_flops_per_launch": flops, "algorithmic_hbm_bytes_per_launch": hbm,

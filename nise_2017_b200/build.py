@@ -28,6 +28,8 @@ CU_SOURCES = [
     "util.cu",
     "noalloc.cu",
     "fft2d.cu",
+    "diag.cu",
+    "adjoint.cu",
 ]
 CPP_SOURCES = [
     "api.cpp",

@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "eigen.h"
 #include "engine.h"
 #include "nise_b200.h"
 #include "nise_internal.h"
@@ -338,6 +339,65 @@ int nise_check_frames(nise_ctx *c, long last_frame) {
 }
 
 // ------------------------------------------------------------ absorption
+// Eigen route of the exact propagators (diag.cu): every frame of [f0, f0+nf)
+// is diagonalised in FP64 (chunks of frames), its one-step propagator U is
+// built (truncated when a Threshold is active) and applied to every start
+// point crossing it.  Records evk0/evk1 around the device work.
+static int abs_eigen(nise_ctx *c, const DevTraj &T, const AbsJob &J, long f0, long nf, double2 *resp, bool plain,
+                     bool truncated) {
+    const int N = c->n, prec = c->p.precision;
+    const size_t r2 = prec == NISE_FP32 ? sizeof(float2) : sizeof(double2);
+    const size_t ubytes = r2 * (size_t)nf * N * N;
+    if (ubytes > ((size_t)64 << 30))
+        return nise_fail(c, NISE_ERR_NOMEM, "eigen route: %ld frames of %d sites need more than 64 GB of propagators",
+                         nf, N);
+    int rc;
+    DevBuf<char> U;
+    DevBuf<long> fr;
+    DevBuf<double> V, w;
+    std::vector<long> frames(nf);
+    for (long t = 0; t < nf; t++) frames[t] = f0 + t;
+    const long FC = std::max(1L, std::min(nf, (long)(((size_t)512 << 20) / (sizeof(double) * (size_t)N * N))));
+    if ((rc = U.alloc(c, ubytes)) || (rc = fr.upload(c, frames)) || (rc = V.alloc(c, (size_t)FC * N * N)) ||
+        (rc = w.alloc(c, (size_t)FC * N)))
+        return rc;
+    EigJob EJ;
+    EJ.T = T;
+    EJ.n = N;
+    EJ.singleshift = c->nshift > 0;
+    // propagate_vec_DIA: f = deltat*icm2ifs*twoPi*sign in float, one full step
+    const double f = prec == NISE_FP32 ? (double)J.f32_full : J.f;
+    cudaEventRecord(c->evk0, c->stream);
+    for (long q = 0; q < nf; q += FC) {
+        long m = std::min(FC, nf - q);
+        if ((rc = nise_cuda(c, launch_eig(EJ, fr.p + q, m, V.p, w.p, c->stream), "eigensolver"))) return rc;
+        if ((rc = nise_cuda(c, launch_build_u(prec == NISE_FP32 ? 0 : 1, V.p, w.p, m, N, f, c->thres, truncated,
+                                              U.p + r2 * (size_t)q * N * N, c->stream),
+                            "propagator build")))
+            return rc;
+        c->launches += 2;
+    }
+    if (plain) {
+        for (int s = 0; s < J.nsamp; s++) {
+            AbsJob Js = J;
+            Js.begin = J.begin + s;
+            Js.nsamp = 1;
+            if ((rc = nise_cuda(c, launch_abs_dia(prec == NISE_FP32 ? 0 : 1, T, U.p, f0, N, Js,
+                                                  resp + (size_t)3 * s * J.tmax, c->stream),
+                                "eigen propagation")))
+                return rc;
+            c->launches++;
+        }
+    } else {
+        if ((rc = nise_cuda(c, launch_abs_dia(prec == NISE_FP32 ? 0 : 1, T, U.p, f0, N, J, resp, c->stream),
+                            "eigen propagation")))
+            return rc;
+        c->launches++;
+    }
+    cudaEventRecord(c->evk1, c->stream);
+    return NISE_OK;
+}
+
 extern "C" int nise_absorption(nise_ctx *c, double *re_S, double *im_S, int *samples) {
     if (!c || !re_S || !im_S || !samples) return nise_fail(c, NISE_ERR_ARG, "null argument");
     if (!c->loaded) return nise_fail(c, NISE_ERR_STATE, "no trajectory loaded");
@@ -470,12 +530,22 @@ extern "C" int nise_absorption(nise_ctx *c, double *re_S, double *im_S, int *sam
     } else {
         // Sparse / Diagonal: exact propagator exp(-i H dt) (propagate_vec_DIA,
         // propagate.c:60-125).  Threshold > 0 keeps only large elements of U
-        // (propagate_vec_DIA_S) and needs the explicit eigen propagator.
-        if (c->thres != 0 && !(c->thres > 1))
-            return nise_fail(c, NISE_ERR_UNSUPPORTED, "Sparse with Threshold > 0 (truncated U) is not supported");
-        if (p.hamiltonian != NISE_HAM_COUPLING)
-            return nise_fail(c, NISE_ERR_UNSUPPORTED,
-                             "Sparse absorption needs HamiltonianType Coupling (static couplings)");
+        // (propagate_vec_DIA_S, propagate.c:185-258) and needs the explicit
+        // eigen propagator, as do per-frame couplings (HamiltonianType Full)
+        // and the Diagonal scheme up to NISE_EIG_MAX_N sites.  Otherwise the
+        // static couplings go through the sparse Taylor series below.
+        const bool truncated = c->thres != 0 && !(c->thres > 1);
+        const bool eigen_route = truncated || p.hamiltonian != NISE_HAM_COUPLING ||
+                                 (p.propagation == NISE_PROP_DIAGONAL && N <= NISE_EIG_MAX_N);
+        if (eigen_route) {
+            if (N > NISE_EIG_MAX_N)
+                return nise_fail(c, NISE_ERR_UNSUPPORTED,
+                                 truncated ? "Sparse with Threshold > 0 is limited to 120 sites (eigen route)"
+                                           : "exact propagation of per-frame couplings (HamiltonianType Full) is "
+                                             "limited to 120 sites (eigen route)");
+            if ((rc = abs_eigen(c, T, J, f0, nf, resp.p, plain, truncated))) return rc;
+            c->last_flops = (double)nf * 6.7 * N * (double)N * N + (double)vec_steps * 8.0 * N * N;
+        } else {
         // CSR of the static couplings (read cut applied, |J| >= cut kept)
         std::vector<int> rp(N + 1, 0), col;
         std::vector<double> vd;
@@ -595,6 +665,7 @@ extern "C" int nise_absorption(nise_ctx *c, double *re_S, double *im_S, int *sam
             c->launches++;
         }
         cudaEventRecord(c->evk1, c->stream);
+        }
     }
     if ((rc = nise_cuda(c, launch_reduce_resp(resp.p, nvec, tmax, out.p, c->stream), "response reduction")))
         return rc;

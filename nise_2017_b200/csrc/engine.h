@@ -89,3 +89,32 @@ int launch_step_coupling(int prec, int n, float cut, const float *H, void *re, v
 int launch_step_rk4(int prec, int n, float cut, const float *H, void *re, void *im, int nvec, int ts,
                     double fsub, float fsub32, cudaStream_t s);
 int launch_step_taylor(int prec, int n, const float *H, void *re, void *im, int nvec, double f, cudaStream_t s);
+
+// Eigen route (diag.cu).  U[t][a][c] = sum_k V[t][a][k] V[t][c][k] exp(-i w[t][k] f)
+// for nfr frames, rounded to the working precision (prec 0 FP32, 1 FP64) and,
+// when `truncate`, zeroed where |U_ac|^2 <= thres (propagate_vec_DIA_S).
+int launch_build_u(int prec, const double *V, const double *w, long nfr, int n, double f, float thres, int truncate,
+                   void *U, cudaStream_t s);
+// Linear absorption of the start points of J with the per-frame propagators
+// U (frames from f0): one CTA per start point, n <= 1024.
+int launch_abs_dia(int prec, const DevTraj &T, const void *U, long f0, int n, const AbsJob &J, double2 *resp,
+                   cudaStream_t s);
+
+// Differentiable FP64 Trotter absorption (adjoint.cu).  Tables for frames
+// [f0, f0+nf): U[t][a] half-step phases with the site shifts, rot[t][k]
+// (co, si) of the scaled couplings, jf[t][k] = J f; checkpoints every K
+// steps plus the last state (nck slots per vector).
+struct AdjPlan {
+    int n, k, ts, K, nck;
+    const int2 *pairs;
+    long f0, nf;
+    const double *shift;   // [n] device
+    double scale, f;       // coupling scale, deltat*icm2ifs*2pi/ts
+    double2 *U, *rot;
+    double *jf;
+};
+int launch_adj_prep(const DevTraj &T, const AdjPlan &P, cudaStream_t s);
+int launch_adj_fwd(const DevTraj &T, const AdjPlan &P, const AbsJob &J, double2 *resp, double2 *ckpt,
+                   cudaStream_t s);
+int launch_adj_bwd(const DevTraj &T, const AdjPlan &P, const AbsJob &J, const double2 *G, const double2 *ckpt,
+                   double *gshift_part, double *gscale_part, double *gshift, double *gscale, cudaStream_t s);

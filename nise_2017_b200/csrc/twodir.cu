@@ -30,6 +30,7 @@
 // FP32 contexts keep the reference's single-precision operations (states,
 // rotations, dipole operators) and accumulate every dot product and response
 // sum in FP64, like the FP32/FP64-sum oracle.
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -63,6 +64,8 @@ struct TwoD {
     const int2 *ent;          // RK4 entries (a <= b)
     int Kr;
     const void *rkval;        // RK4 values [t][Kr]
+    const void *Ud;           // Sparse/Diagonal: full-step propagators U[t][n][n] (truncated by Threshold)
+    const void *Us;           // Sparse/Diagonal doubles: substep propagators U[t][n][n] (f/ts, truncated)
     long e0;                  // eigen data for frames [e0, e0 + ne)
     const double *eV, *ew;    // V [ne][n][n], w [ne][n]
     float f32_full;           // deltat*icm2ifs*2pi in float
@@ -83,12 +86,41 @@ __device__ __forceinline__ long tj_of(const TwoD &D, int s) { return (long)(D.s0
 __device__ __forceinline__ long tk_of(const TwoD &D, int s) { return tj_of(D, s) + D.T2; }
 __device__ __forceinline__ int nvec_se(const TwoD &D) { return 3 + 3 * D.T1; }
 
+__host__ __device__ __forceinline__ bool is_eigen_scheme(int prop) {
+    return prop == NISE_PROP_SPARSE || prop == NISE_PROP_DIAGONAL;
+}
+
+// propagate_vec_DIA / propagate_vec_DIA_S (propagate.c:60-125, 185-258) on
+// one vector of the [site][lane] layout: c_a <- sum_b U_ab c_b, accumulated
+// in b order (float operations in FP32 mode); truncated elements of U are
+// zero.  The temporary is the second half of the lane's shared memory.
+template <typename R>
+__device__ __forceinline__ void dia_apply(typename Vec2<R>::T *S, int B, int lane, int n,
+                                          const typename Vec2<R>::T *U) {
+    typedef typename Vec2<R>::T R2;
+    typedef Ar<R> A;
+    R2 *Tm = S + (size_t)n * B;
+    for (int a = 0; a < n; a++) {
+        R2 acc;
+        acc.x = acc.y = 0;
+        for (int b = 0; b < n; b++) {
+            R2 u = U[(size_t)a * n + b], z = S[b * B + lane];
+            acc.x = A::add(acc.x, A::sub(A::mul(u.x, z.x), A::mul(u.y, z.y)));
+            acc.y = A::add(acc.y, A::add(A::mul(u.x, z.y), A::mul(u.y, z.x)));
+        }
+        Tm[a * B + lane] = acc;
+    }
+    for (int a = 0; a < n; a++) S[a * B + lane] = Tm[a * B + lane];
+}
+
 // One singles time step of the configured scheme through frame t.
 template <typename R>
 __device__ __forceinline__ void singles_step(const TwoD &D, typename Vec2<R>::T *S, int B, int lane, long t) {
     typedef typename Vec2<R>::T R2;
     long fi = t - D.f0;
-    if (D.prop == NISE_PROP_RK4) {
+    if (is_eigen_scheme(D.prop)) {
+        dia_apply<R>(S, B, lane, D.n, (const R2 *)D.Ud + fi * D.n * D.n);
+    } else if (D.prop == NISE_PROP_RK4) {
         rk4_apply<R>(S, B, lane, D.n, D.Kr, D.ent, (const R *)D.rkval + fi * D.Kr, D.ts);
     } else {
         const R2 *Uf = (const R2 *)D.U + fi * D.n;
@@ -99,7 +131,7 @@ __device__ __forceinline__ void singles_step(const TwoD &D, typename Vec2<R>::T 
 
 template <typename R>
 __device__ __forceinline__ size_t singles_lane_bytes(int n, int prop) {
-    return (prop == NISE_PROP_RK4 ? 5 : 1) * (size_t)n * sizeof(typename Vec2<R>::T);
+    return (prop == NISE_PROP_RK4 ? 5 : is_eigen_scheme(prop) ? 2 : 1) * (size_t)n * sizeof(typename Vec2<R>::T);
 }
 
 // sum_i mu_i * psi_i with float products (FP32) and an FP64 sum.
@@ -695,8 +727,70 @@ __device__ void rk4_doubles_step(const TwoD &D, long t, typename Vec2<R>::T *F, 
     }
 }
 
+// propagate_double_sparce (propagate.c:1304-1394) through frame t: ts times
+// an anharmonic half phase on |aa>, the symmetrised U (x) U update over the
+// element pairs of the truncated substep propagator (time_evolution_mat,
+// propagate.c:1241-1299, called with its row and column lists exchanged,
+// propagate.c:1496), and the second half phase.  Elements are enumerated in
+// time_evolution_mat's order (row a outer, column b inner); zero (truncated)
+// elements are not in the list.  V is the temporary of the update.
+template <typename R>
+__device__ void sparse_doubles_step(const TwoD &D, long t, typename Vec2<R>::T *F, typename Vec2<R>::T *V) {
+    typedef typename Vec2<R>::T R2;
+    typedef Ar<R> A;
+    const int n = D.n, N2 = n * (n + 1) / 2, nn = n * n;
+    const R2 *Us = (const R2 *)D.Us + (t - D.f0) * nn;
+    const R sq2 = (R)1.41421356237f;
+    // fm = f * 0.5 / m with f = deltat*icm2ifs*twoPi (float), the product in double
+    const R fm = sizeof(R) == 4 ? (R)(float)((double)D.f32_full * 0.5 / D.ts) : (R)(D.f64_full * 0.5 / D.ts);
+    for (int sub = 0; sub < D.ts; sub++) {
+        for (int half = 0; half < 2; half++) {
+            if (half == 1)
+                for (int e = 0; e < N2; e++) F[e] = V[e];
+            else
+                for (int e = 0; e < N2; e++) V[e] = F[e];
+            for (int a = 0; a < n; a++) {
+                R an = D.anh != 0.0f ? (R)D.anh : (R)D.T.anh[t * (1L + n) + 1 + a];
+                R arg = A::mul(fm, an);
+                R co = (R)cos((double)arg), si = (R)sin((double)arg);
+                int ia = sindex(a, a, n);
+                R2 v = V[ia], o;
+                o.x = A::sub(A::mul(co, v.x), A::mul(si, v.y));
+                o.y = A::add(A::mul(co, v.y), A::mul(si, v.x));
+                F[ia] = o;
+            }
+            if (half == 1) break;
+            for (int e = 0; e < N2; e++) V[e].x = V[e].y = 0;
+            for (int ea = 0; ea < nn; ea++) {
+                R2 ua = Us[ea];
+                if (ua.x == (R)0 && ua.y == (R)0) continue;
+                const int sA = ea % n, tA = ea / n;  // R = column, C = row (exchanged lists)
+                for (int eb = 0; eb <= ea; eb++) {
+                    R2 ub = Us[eb];
+                    if (ub.x == (R)0 && ub.y == (R)0) continue;
+                    const int u = eb % n, v = eb / n;
+                    R g = 1;
+                    if (sA != u) g = sq2;
+                    if (v != tA) g = sq2;
+                    if (sA != u && v != tA) g = 1;
+                    const int iA = sindex(sA, u, n), iB = sindex(tA, v, n);
+                    R pr = A::sub(A::mul(ua.x, ub.x), A::mul(ua.y, ub.y));
+                    R pi = A::add(A::mul(ua.y, ub.x), A::mul(ua.x, ub.y));
+                    R2 fb = F[iB], acc = V[iA];
+                    acc.x = A::add(acc.x, A::mul(A::mul(pr, fb.x), g));
+                    acc.x = A::sub(acc.x, A::mul(A::mul(pi, fb.y), g));
+                    acc.y = A::add(acc.y, A::mul(A::mul(pr, fb.y), g));
+                    acc.y = A::add(acc.y, A::mul(A::mul(pi, fb.x), g));
+                    V[iA] = acc;
+                }
+            }
+        }
+    }
+}
+
 // Thread per doubles vector: dipole_double at tk, then per t3 the EA
-// projections (dipole_double_last) and dot products, then one RK4 step.
+// projections (dipole_double_last) and dot products, then one doubles step
+// (RK4, or the Sparse/Diagonal U (x) U step).
 template <typename R>
 __global__ void k2d_doubles_seq(TwoD D, int vec_per_sample, void *Fbuf, void *Kbuf, void *hdbuf) {
     typedef typename Vec2<R>::T R2;
@@ -762,7 +856,8 @@ __global__ void k2d_doubles_seq(TwoD D, int vec_per_sample, void *Fbuf, void *Kb
                     }
                 }
         if (t3 == D.T3 - 1) break;
-        rk4_doubles_step<R>(D, tl, F, Kq, hd);
+        if (is_eigen_scheme(D.prop)) sparse_doubles_step<R>(D, tl, F, Kq);
+        else rk4_doubles_step<R>(D, tl, F, Kq, hd);
     }
 }
 
@@ -887,7 +982,7 @@ int run_chunk(nise_ctx *c, TwoD &D, Dcoef<R> *cf) {
     typedef typename Vec2<R>::T R2;
     cudaStream_t st = c->stream;
     int e;
-    size_t lane_b = (D.prop == NISE_PROP_RK4 ? 5 : 1) * (size_t)D.n * sizeof(R2);
+    size_t lane_b = (D.prop == NISE_PROP_RK4 ? 5 : is_eigen_scheme(D.prop) ? 2 : 1) * (size_t)D.n * sizeof(R2);
     int B = lanes_for2(lane_b, 64);
     size_t sm = lane_b * B;
     const int P = (D.T1 + 1) / 2;
@@ -913,7 +1008,7 @@ int run_chunk(nise_ctx *c, TwoD &D, Dcoef<R> *cf) {
         k2d_se<R><<<(nv + B - 1) / B, B, sm, st>>>(D);
         c->launches++;
     }
-    if (D.ea && D.prop == NISE_PROP_RK4) {
+    if (D.ea && (D.prop == NISE_PROP_RK4 || is_eigen_scheme(D.prop))) {
         int vps = 9 + 9 * D.T1, tot = D.S * vps, N2 = D.n * (D.n + 1) / 2;
         void *Fb = nullptr, *Kb = nullptr, *Hb = nullptr;
         if ((e = (int)cudaMallocAsync(&Fb, sizeof(R2) * (size_t)tot * N2, st))) return e;
@@ -964,8 +1059,9 @@ extern "C" int nise_2dir(nise_ctx *c, double *R, int *sample_count) {
     int tech = p.technique;
     if (tech < NISE_TECH_2DIR || tech > NISE_TECH_NOEAIR)
         return nise_fail(c, NISE_ERR_ARG, "technique is not in the 2DIR family");
-    if (p.propagation != NISE_PROP_COUPLING && p.propagation != NISE_PROP_RK4)
-        return nise_fail(c, NISE_ERR_UNSUPPORTED, "2DIR supports Propagation Coupling and RK4 in this engine");
+    const bool eig_scheme = p.propagation == NISE_PROP_SPARSE || p.propagation == NISE_PROP_DIAGONAL;
+    if (eig_scheme && N > NISE_EIG_MAX_N)
+        return nise_fail(c, NISE_ERR_UNSUPPORTED, "2DIR with Propagation Sparse/Diagonal is limited to 120 sites");
     bool gb = tech == NISE_TECH_2DIR || tech == NISE_TECH_GBIR || tech == NISE_TECH_NOEAIR;
     bool se = tech == NISE_TECH_2DIR || tech == NISE_TECH_SEIR || tech == NISE_TECH_NOEAIR;
     bool ea = tech == NISE_TECH_2DIR || tech == NISE_TECH_EAIR;
@@ -1054,6 +1150,43 @@ extern "C" int nise_2dir(nise_ctx *c, double *R, int *sample_count) {
             return rc;
         c->launches += 1 + P.rot_static;
         D.U = U.p; D.rot = rot.p; D.rot_static = P.rot_static;
+    } else if (eig_scheme) {
+        // propagate_vector's Sparse scheme for the singles (DIA, or DIA_S when
+        // 0 < Threshold <= 1) and time_evolution_mat's truncated substep
+        // propagator for the doubles (Threshold always applied); Diagonal is
+        // the untruncated exact propagator.
+        const float thr = p.propagation == NISE_PROP_DIAGONAL ? 0.0f : c->thres;
+        const bool trunc_singles = thr != 0 && !(thr > 1);
+        const long FC = std::max(1L, std::min(nf, (long)(((size_t)512 << 20) / (sizeof(double) * (size_t)N * N))));
+        std::vector<long> frs(nf);
+        for (long t = 0; t < nf; t++) frs[t] = fmin + t;
+        DevBuf<long> dfr;
+        DevBuf<double> V, w;
+        if ((rc = dfr.upload(c, frs)) || (rc = V.alloc(c, (size_t)FC * N * N)) || (rc = w.alloc(c, (size_t)FC * N)) ||
+            (rc = U.alloc(c, r2 * (size_t)nf * N * N)))
+            return rc;
+        if (ea && (rc = rot.alloc(c, r2 * (size_t)nf * N * N))) return rc;
+        EigJob EJ;
+        EJ.T = T; EJ.n = N; EJ.singleshift = 0;
+        const int pr = prec == NISE_FP32 ? 0 : 1;
+        const double ffull = prec == NISE_FP32 ? (double)D.f32_full : D.f64_full;
+        const double fsub = prec == NISE_FP32 ? (double)D.f32_dsub : D.f64_dsub;
+        for (long q = 0; q < nf; q += FC) {
+            long m = std::min(FC, nf - q);
+            if ((rc = nise_cuda(c, launch_eig(EJ, dfr.p + q, m, V.p, w.p, c->stream), "eigensolver"))) return rc;
+            if ((rc = nise_cuda(c, launch_build_u(pr, V.p, w.p, m, N, ffull, thr, trunc_singles,
+                                                  U.p + r2 * (size_t)q * N * N, c->stream), "propagator build")))
+                return rc;
+            c->launches += 2;
+            if (ea) {
+                if ((rc = nise_cuda(c, launch_build_u(pr, V.p, w.p, m, N, fsub, thr, 1, rot.p + r2 * (size_t)q * N * N,
+                                                      c->stream), "doubles propagator build")))
+                    return rc;
+                c->launches++;
+            }
+        }
+        D.Ud = U.p;
+        D.Us = rot.p;
     } else {
         std::vector<int2> ent;
         size_t q = 0;
@@ -1107,7 +1240,7 @@ extern "C" int nise_2dir(nise_ctx *c, double *R, int *sample_count) {
     const int NV = 3 + 3 * T1;
     size_t per_sample = r2 * ((size_t)3 * T1 * N + 3 * N + (size_t)T3 * NV * N) + sizeof(double2) * (9 * (size_t)T1 + 9 * T3) +
                         2 * sizeof(double2) * (size_t)T3 * 21 * T1 + sizeof(double) * 12 * plane;
-    if (D.ea && D.prop == NISE_PROP_RK4)  // RK4 doubles: state, 4 stages and the diagonal per doubles vector
+    if (D.ea && (D.prop == NISE_PROP_RK4 || is_eigen_scheme(D.prop)))  // sequential doubles: state, 4 stages, diagonal
         per_sample += (9 + 9 * (size_t)T1) * (size_t)N * (N + 1) / 2 * (5 * r2 + r2 / 2);
     size_t budget = (size_t)1536 << 20;
     int chunk = (int)(budget / (per_sample > 0 ? per_sample : 1));

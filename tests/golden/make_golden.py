@@ -7,7 +7,7 @@ oracle/Makefile).  The reference's output files are stored as arrays:
   absorption cases: td = TD_Absorption.dat columns, spec = Absorption.dat columns
   2D cases:         R  = [6 files][Re, Im][t3][t1] of RparI.dat ... RcroII.dat
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root:  python tests/golden/make_golden.py [case ...]
 """
 import json
 import os
@@ -49,6 +49,19 @@ CASES = {
         keywords=synth.c0_keywords(Singles=10, Length=400, RunTimes="50 0 0", Samplerate=30, Window="Hann",
                                    Homogeneous=800, Inhomogeneous=300, FFT=256, BeginPoint=1, EndPoint=9),
         shift=[(2, 1.0, 5.0), (7, 1.02, -3.0)]),
+    "abs_sparse_full": dict(
+        spec=dict(n_sites=12, frames=400, dt_fs=2.0, geometry=synth.CHAIN, seed=16),
+        keywords=synth.c0_keywords(Singles=12, Length=400, RunTimes="48 0 0", Samplerate=30, Propagation="Sparse",
+                                   Threshold=0, FFT=512)),
+    "abs_sparse_trunc": dict(
+        spec=dict(n_sites=10, frames=400, dt_fs=2.0, geometry=synth.CHAIN, j_nn=-12.0, seed=17),
+        keywords=synth.c0_keywords(Singles=10, Length=400, RunTimes="40 0 0", Samplerate=30, Propagation="Sparse",
+                                   Threshold=100000, FFT=256)),
+    "abs_sparse_trunc_static": dict(
+        spec=dict(n_sites=24, frames=300, dt_fs=1.0, geometry=L, spacing=8.0, eps0=15000.0, sigma=300.0,
+                  tau_fs=50.0, jcut=2.0, mu_jitter=0.0, ham_type=synth.COUPLING, dipole_frames=1, seed=18),
+        keywords=synth.c1_keywords(Singles=24, Length=300, RunTimes="40 0 0", Samplerate=40, Threshold=20000,
+                                   FFT=512)),
     # 2DIR family
     "2d_coupling": dict(
         spec=dict(n_sites=5, frames=300, dt_fs=2.0, geometry=C, spacing=6.0, sigma=12.0, tau_fs=200.0,
@@ -67,6 +80,11 @@ CASES = {
                   mu_jitter=0.0, ham_type=synth.COUPLING, dipole_frames=1, seed=24),
         keywords=synth.c2_keywords(Singles=5, Length=300, RunTimes="8 0 8", Samplerate=40, Propagation="Sparse",
                                    Threshold=0)),
+    "2d_sparse_trunc": dict(
+        spec=dict(n_sites=5, frames=300, dt_fs=2.0, geometry=C, spacing=5.0, sigma=12.0, tau_fs=200.0,
+                  mu_jitter=0.0, ham_type=synth.COUPLING, dipole_frames=1, seed=27),
+        keywords=synth.c2_keywords(Singles=5, Length=300, RunTimes="8 0 8", Samplerate=40, Propagation="Sparse",
+                                   Threshold=20000)),
     "2d_full_anhfile": dict(
         spec=dict(n_sites=4, frames=260, dt_fs=2.0, geometry=synth.CHAIN, j_nn=-6.0, j_sigma=1.5, seed=25),
         keywords=synth.c2_keywords(Singles=4, Length=260, RunTimes="6 0 6", Samplerate=30, Anharmonicity=0,
@@ -101,9 +119,15 @@ def materialise(case, directory):
     return files
 
 
-def main():
+def main(names=None):
+    """Regenerate every case, or only `names` (kept in cases.json with the rest)."""
     manifest = {}
+    if names:
+        with open(os.path.join(HERE, "cases.json")) as f:
+            manifest = json.load(f)
     for name, case in CASES.items():
+        if names and name not in names:
+            continue
         work = tempfile.mkdtemp(prefix="golden_")
         try:
             files = materialise(case, work)
@@ -129,4 +153,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -94,6 +94,42 @@ def test_plain_equals_batched(name, tmp_path):
         assert np.array_equal(re_b, re_p) and np.array_equal(im_b, im_p)
 
 
+@pytest.mark.parametrize("name", ["abs_sparse_full", "abs_sparse_trunc"])
+def test_eigen_route_plain_equals_batched(name, tmp_path):
+    """The eigen route runs the same per-start-point kernel batched or one start point per launch."""
+    case = CASES[name]
+    files = helpers.materialise(case, str(tmp_path))
+    _, re_b, im_b, n_b, _ = run_engine(case, files)
+    _, re_p, im_p, n_p, _ = run_engine(case, files, launch_mode=nise.PLAIN)
+    assert n_b == n_p
+    assert np.array_equal(re_b, re_p) and np.array_equal(im_b, im_p)
+
+
+def test_diagonal_scheme_matches_reference_sparse(tmp_path):
+    """Propagation Diagonal (rejected by the reference) is checked against the
+    reference's Sparse + Threshold 0 output on the same trajectory."""
+    case = CASES["abs_sparse_full"]
+    files = helpers.materialise(case, str(tmp_path))
+    kw = dict(case["keywords"], Propagation="Diagonal")
+    p, re, im, n, (w, sr, si) = run_engine(dict(case, keywords=kw), files)
+    g = helpers.golden("abs_sparse_full")
+    assert helpers.rel(np.stack([re / n, im / n], 1), g["td"][:, 1:]) < REF_EIGEN
+    assert helpers.rel(np.stack([sr, si], 1), g["spec"][:, 1:]) < REF_EIGEN
+    ore, oim, on = oracle.absorption(oracle.params(case["keywords"], files), "f64")
+    assert helpers.rel(re + 1j * im, ore + 1j * oim) < SPARSE_FP32
+
+
+def test_eigen_route_matches_taylor_route(tmp_path):
+    """Two exact propagators of static couplings: the eigen route (Diagonal)
+    and the sparse Taylor series (Sparse, Threshold 0), both in FP64."""
+    case = CASES["abs_sparse_static"]
+    files = helpers.materialise(case, str(tmp_path))
+    _, re_t, im_t, _, _ = run_engine(case, files, precision=nise.FP64)
+    kw = dict(case["keywords"], Propagation="Diagonal")
+    _, re_e, im_e, _, _ = run_engine(dict(case, keywords=kw), files, precision=nise.FP64)
+    assert helpers.rel(re_e + 1j * im_e, re_t + 1j * im_t) < 1e-9
+
+
 def random_hamiltonians(rng, nvec, n, cut):
     nn2 = n * (n + 1) // 2
     H = np.zeros((nvec, nn2), np.float32)

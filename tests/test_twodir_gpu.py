@@ -21,7 +21,8 @@ pytestmark = pytest.mark.gpu
 
 CASES = helpers.cases()
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-SUPPORTED = ["2d_coupling", "2d_coupling_t2", "2d_rk4", "2d_full_anhfile", "2d_gbir", "2d_seir", "2d_eair"]
+SUPPORTED = ["2d_coupling", "2d_coupling_t2", "2d_rk4", "2d_sparse", "2d_sparse_trunc", "2d_full_anhfile", "2d_gbir",
+             "2d_seir", "2d_eair"]
 
 SUM_ORDER = 1e-10   # same single-precision operations, FP64 sums in another order
 T2_EIGEN = 1e-5     # t2 eigenvectors from a different Jacobi ordering (rounded to float)
@@ -48,12 +49,18 @@ def test_fp32_matches_oracle_and_reference(name, tmp_path):
     oR, on = oracle.twodir(po, "f32a64")
     assert n == on
     eig = helpers.uses_eigen(case)
-    assert helpers.rel2d(R, oR) < (T2_EIGEN if eig else SUM_ORDER)
+    if case["keywords"].get("Propagation") in ("Sparse", "Diagonal"):
+        # Exact propagators from FP64 eigenvectors: the engine's FP32 run must be
+        # at least as close to the FP64 result as the FP32 restatement is.
+        oR64, _ = oracle.twodir(po, "f64")
+        assert helpers.rel2d(R, oR64) <= max(helpers.rel2d(oR, oR64), T2_EIGEN)
+    else:
+        assert helpers.rel2d(R, oR) < (T2_EIGEN if eig else SUM_ORDER)
     Rn = helpers.R12_to_files(oracle.normalize_2d(po, R, n, "f64"))
     assert helpers.rel2d(Rn, helpers.golden(name)["R"]) < (REF_EIGEN if eig else REF_FP32_SUMS)
 
 
-@pytest.mark.parametrize("name", ["2d_coupling", "2d_coupling_t2", "2d_eair"])
+@pytest.mark.parametrize("name", ["2d_coupling", "2d_coupling_t2", "2d_eair", "2d_sparse"])
 def test_fp64_matches_fp64_oracle(name, tmp_path):
     case = CASES[name]
     files = helpers.materialise(case, str(tmp_path))
@@ -95,10 +102,25 @@ def test_cluster_n40(tmp_path):
     assert helpers.rel2d(R, oR) < SUM_ORDER
 
 
-def test_unsupported_schemes_fail_cleanly(tmp_path):
+def test_diagonal_scheme_matches_reference_sparse(tmp_path):
+    """Propagation Diagonal (rejected by the reference) against the reference's
+    Sparse + Threshold 0 response files on the same trajectory."""
     case = CASES["2d_sparse"]
     files = helpers.materialise(case, str(tmp_path))
-    p = nise.params_from_keywords(case["keywords"], files)
+    kw = dict(case["keywords"], Propagation="Diagonal")
+    p, R, n = run(kw, files)
+    po = oracle.params(case["keywords"], files)
+    Rn = helpers.R12_to_files(oracle.normalize_2d(po, R, n, "f64"))
+    assert helpers.rel2d(Rn, helpers.golden("2d_sparse")["R"]) < REF_EIGEN
+
+
+def test_eigen_schemes_size_limit(tmp_path):
+    """Sparse/Diagonal 2DIR needs the per-frame eigensolver (at most 120 sites)."""
+    s = synth.c2_spec(n_sites=121, frames=40, seed=5)
+    files = synth.write(s, str(tmp_path))
+    kw = synth.c2_keywords(Singles=121, Length=40, RunTimes="2 0 2", Samplerate=10, Propagation="Sparse",
+                           Threshold=0)
+    p = nise.params_from_keywords(kw, files)
     with nise.Context(p) as c:
         c.load_files()
         with pytest.raises(nise.NiseError) as e:
