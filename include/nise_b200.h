@@ -183,6 +183,24 @@ int nise_last_work(const nise_ctx *ctx, double *flops, double *hbm_bytes);
  * denominator of the CUDA-core kernels. */
 int nise_probe_fp32_peak(int device, double *tflops);
 
+/* No counterpart in the reference (it has no derivatives).  A differentiable
+ * FP64 model of linear absorption with Propagation Coupling: the Trotter
+ * scheme of propagate_vec_coupling_S (propagate.c:821-899) on the loaded
+ * trajectory with site_shift[a] (cm^-1, N values) added to every shifted
+ * diagonal energy (a SingleShift with a = 1), every coupling multiplied by
+ * coupling_scale after the read cut, and the transform of do_1DFFT
+ * (1DFFT.c:144-228) with the given lifetime (fs; 0 = none).  A SingleShift
+ * loaded in the context is not applied.  Writes the Absorption.dat rows. */
+int nise_absorption_model(nise_ctx *ctx, const double *site_shift, double coupling_scale, double lifetime,
+                          double *freq, double *spec_re, double *spec_im, int max_rows, int *rows);
+/* Gradient of a loss L of that spectrum: given dL/dspec_re and dL/dspec_im at
+ * its `rows` rows, returns dL/dsite_shift (N values), dL/dcoupling_scale and
+ * dL/dlifetime, by reverse-time propagation from checkpoints stored every 32
+ * steps of a forward recomputation. */
+int nise_backward_absorption(nise_ctx *ctx, const double *site_shift, double coupling_scale, double lifetime,
+                             const double *dL_dspec_re, const double *dL_dspec_im, int rows, double *g_shift,
+                             double *g_scale, double *g_lifetime);
+
 /* No counterpart in the reference.  Linear absorption with the Trotter
  * "Coupling" scheme (HamiltonianType Full) for callers whose device memory is
  * owned by their own allocator and who therefore cannot let the library call

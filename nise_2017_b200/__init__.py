@@ -35,7 +35,8 @@ EXPORTED = [
     "nise_global_error", "nise_load_files", "nise_set_trajectory", "nise_set_singleshift", "nise_absorption",
     "nise_absorption_fft", "nise_2dir", "nise_propagate", "nise_propagate_doubles", "nise_write_td_absorption",
     "nise_write_spectrum", "nise_write_2d", "nise_set_stream", "nise_last_timing", "nise_last_work",
-    "nise_probe_fp32_peak", "nise_absorption_noalloc", "nise_2dfft_files",
+    "nise_probe_fp32_peak", "nise_absorption_noalloc", "nise_2dfft_files", "nise_absorption_model",
+    "nise_backward_absorption",
 ]
 
 
@@ -258,6 +259,30 @@ class Context:
             self._h, H.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), re.ctypes.data, im.ctypes.data, re.shape[0],
             None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
         return re, im
+
+    def absorption_model(self, shift, scale, lifetime):
+        """Differentiable FP64 spectrum (nise_absorption_model): site shifts
+        (cm^-1), coupling scale and lifetime (fs) -> (w, spec_re, spec_im)."""
+        fft = max(self.params.fft, self.params.tmax1)
+        w, sr, si = np.zeros(fft), np.zeros(fft), np.zeros(fft)
+        rows = ctypes.c_int(0)
+        shift = np.ascontiguousarray(shift, dtype=np.float64)
+        self._check(lib().nise_absorption_model(self._h, _dp(shift), ctypes.c_double(scale), ctypes.c_double(lifetime),
+                                                _dp(w), _dp(sr), _dp(si), fft, ctypes.byref(rows)))
+        r = rows.value
+        return w[:r], sr[:r], si[:r]
+
+    def backward_absorption(self, shift, scale, lifetime, dl_dre, dl_dim):
+        """Adjoint of absorption_model: (dL/dshift [N], dL/dscale, dL/dlifetime)."""
+        shift = np.ascontiguousarray(shift, dtype=np.float64)
+        dl_dre = np.ascontiguousarray(dl_dre, dtype=np.float64)
+        dl_dim = np.ascontiguousarray(dl_dim, dtype=np.float64)
+        g = np.zeros(self.params.singles)
+        gs, gl = ctypes.c_double(0), ctypes.c_double(0)
+        self._check(lib().nise_backward_absorption(self._h, _dp(shift), ctypes.c_double(scale),
+                                                   ctypes.c_double(lifetime), _dp(dl_dre), _dp(dl_dim), len(dl_dre),
+                                                   _dp(g), ctypes.byref(gs), ctypes.byref(gl)))
+        return g, gs.value, gl.value
 
     def set_stream(self, stream_ptr):
         """Enqueue this context's device work on a caller CUDA stream (int handle, 0 = own)."""

@@ -1,0 +1,476 @@
+// Adjoint of linear absorption (no reference counterpart; the reference has
+// no derivatives).  The differentiable model is the Trotter "Coupling"
+// absorption of propagate_vec_coupling_S (propagate.c:821-899) and
+// absorption.c:119-145 in FP64, with three parameters:
+//   b_a  per-site energy shifts added to the shifted diagonal (the b of a
+//        SingleShift with a = 1, hamshift.c:59-66),
+//   s    a global scale of every coupling (after the read cut),
+//   T1   the Lifetime of the 1D transform (1DFFT.c:178-181).
+// Rotations are applied for every nonzero coupling of the pattern (the
+// read cut removes |J| < Couplingcut), so the model is smooth in s.
+//
+// Forward (k_adj_fwd): thread per vector (start point, polarisation), the
+// state in shared memory ([site][lane]); the response is recorded and the
+// state is stored every K steps (checkpoints) and at the last step.
+// Backward (k_adj_bwd): reverse-time propagation from the last state, each
+// Trotter operation undone in reverse order (they are unitary, the inverse
+// is the conjugate operation) while the adjoint state is carried back through
+// the same operations; the state is reset from the checkpoint whenever the
+// reverse sweep reaches one, which bounds the drift of the reconstruction.
+// Per operation the derivative terms are accumulated:
+//   half phase  y_a = exp(-i h_a f/2) x_a:   dL/db_a += (f/2) Im(conj(l_a) y_a)
+//   rotation    y = R(theta) x, theta = s J f:  dL/ds += J f Re(l . dR/dtheta x)
+// and the response gradient G(t1) is injected as l_a += mu_a(t) G(t1).
+#include <vector>
+
+#include "common.cuh"
+#include "engine.h"
+
+namespace {
+
+// FP64 tables for frames [f0, f0+nf): U[t][a] = (cos(h f/2), -sin(h f/2)),
+// rot[t][k] = (co, si) with si = -sin(s J f), co = sqrt(1 - si^2), and
+// jf[t][k] = J f (the derivative of the angle with respect to s).
+__global__ void k_adj_prep(DevTraj T, AdjPlan P) {
+    long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const long nU = P.nf * P.n, nR = P.nf * P.k;
+    if (g < nU) {
+        long t = g / P.n;
+        int a = (int)(g % P.n);
+        double h = (double)traj_diag_raw(T, P.f0 + t, a) + P.shift[a];
+        double s, c;
+        sincos(0.5 * h * P.f, &s, &c);
+        P.U[g] = make_double2(c, -s);
+        return;
+    }
+    g -= nU;
+    if (g < nR) {
+        long t = g / P.k;
+        int k = (int)(g % P.k);
+        int2 ab = P.pairs[k];
+        double jf = (double)traj_coupling(T, P.f0 + t, ab.x, ab.y) * P.f;
+        double si = -sin(P.scale * jf);
+        P.rot[g] = make_double2(sqrt(1.0 - si * si), si);
+        P.jf[g] = jf;
+    }
+}
+
+__device__ __forceinline__ void adj_phase(double2 *X, int B, int lane, int n, const double2 *U) {
+    for (int a = 0; a < n; a++) {
+        double2 u = U[a], z = X[a * B + lane];
+        X[a * B + lane] = make_double2(z.x * u.x - z.y * u.y, z.y * u.x + z.x * u.y);
+    }
+}
+
+// One forward Trotter step through frame table row fi (ts sub-steps).
+__device__ void adj_step(double2 *X, int B, int lane, const AdjPlan &P, long fi) {
+    const double2 *U = P.U + fi * P.n, *Rt = P.rot + fi * P.k;
+    for (int sub = 0; sub < P.ts; sub++) {
+        adj_phase(X, B, lane, P.n, U);
+        for (int k = 0; k < P.k; k++) {
+            int2 ab = P.pairs[k];
+            double2 cs = Rt[k], xa = X[ab.x * B + lane], xb = X[ab.y * B + lane];
+            // ya = co xa + i si xb, yb = co xb + i si xa
+            X[ab.x * B + lane] = make_double2(cs.x * xa.x - cs.y * xb.y, cs.x * xa.y + cs.y * xb.x);
+            X[ab.y * B + lane] = make_double2(cs.x * xb.x - cs.y * xa.y, cs.x * xb.y + cs.y * xa.x);
+        }
+        adj_phase(X, B, lane, P.n, U);
+    }
+}
+
+__global__ void k_adj_fwd(DevTraj T, AdjPlan P, AbsJob J, double2 *resp, double2 *ckpt) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *X = (double2 *)smem_raw;
+    const int B = blockDim.x, lane = threadIdx.x, n = P.n;
+    const int v = blockIdx.x * B + lane;
+    if (v >= 3 * J.nsamp) return;
+    const int x = v % 3;
+    const long ti = (long)(J.begin + v / 3) * J.sample;
+    for (int a = 0; a < n; a++) X[a * B + lane] = make_double2((double)traj_mu(T, ti, x, a), 0.0);
+    double2 *ck = ckpt + (size_t)v * P.nck * n;
+    for (int t1 = 0; t1 < J.tmax; t1++) {
+        const long t = ti + t1;
+        double re = 0, im = 0;
+        for (int a = 0; a < n; a++) {
+            double m = (double)traj_mu(T, t, x, a);
+            double2 z = X[a * B + lane];
+            re += m * z.x;
+            im += m * z.y;
+        }
+        resp[(size_t)v * J.tmax + t1] = make_double2(re, im);
+        if (t1 % P.K == 0)
+            for (int a = 0; a < n; a++) ck[(size_t)(t1 / P.K) * n + a] = X[a * B + lane];
+        if (t1 == J.tmax - 1) {
+            for (int a = 0; a < n; a++) ck[(size_t)(P.nck - 1) * n + a] = X[a * B + lane];
+            break;
+        }
+        adj_step(X, B, lane, P, t - P.f0);
+    }
+}
+
+// Undo a half phase (x = conj(u) y) and carry the adjoint back (l <- conj(u) l);
+// the derivative of y_a with respect to b_a is (-i f/2) y_a, whose pairing
+// with the adjoint is Re(conj(l_a) (-i f/2) y_a) = (f/2)(l.x y.y - l.y y.x).
+__device__ __forceinline__ void adj_phase_back(double2 *X, double2 *L, double *gs, int B, int lane, int n,
+                                               const double2 *U, double hf) {
+    for (int a = 0; a < n; a++) {
+        double2 u = U[a], y = X[a * B + lane], l = L[a * B + lane];
+        gs[a * B + lane] += hf * (l.x * y.y - l.y * y.x);
+        X[a * B + lane] = make_double2(y.x * u.x + y.y * u.y, y.y * u.x - y.x * u.y);
+        L[a * B + lane] = make_double2(l.x * u.x + l.y * u.y, l.y * u.x - l.x * u.y);
+    }
+}
+
+__global__ void k_adj_bwd(DevTraj T, AdjPlan P, AbsJob J, const double2 *G, const double2 *ckpt, double *gshift,
+                          double *gscale) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int B = blockDim.x, lane = threadIdx.x, n = P.n;
+    double2 *X = (double2 *)smem_raw, *L = X + (size_t)n * B;
+    double *gs = (double *)(L + (size_t)n * B);
+    const int v = blockIdx.x * B + lane;
+    if (v >= 3 * J.nsamp) return;
+    const int x = v % 3;
+    const long ti = (long)(J.begin + v / 3) * J.sample;
+    const double2 *ck = ckpt + (size_t)v * P.nck * n;
+    const double hf = 0.5 * P.f;
+    double gsc = 0;
+    {
+        const long t = ti + J.tmax - 1;
+        const double2 g = G[J.tmax - 1];
+        for (int a = 0; a < n; a++) {
+            double m = (double)traj_mu(T, t, x, a);
+            X[a * B + lane] = ck[(size_t)(P.nck - 1) * n + a];
+            L[a * B + lane] = make_double2(m * g.x, m * g.y);
+            gs[a * B + lane] = 0;
+        }
+    }
+    for (int t1 = J.tmax - 2; t1 >= 0; t1--) {
+        const long t = ti + t1, fi = t - P.f0;
+        const double2 *U = P.U + fi * n, *Rt = P.rot + fi * P.k;
+        const double *Jf = P.jf + fi * P.k;
+        for (int sub = P.ts - 1; sub >= 0; sub--) {
+            adj_phase_back(X, L, gs, B, lane, n, U, hf);
+            for (int k = P.k - 1; k >= 0; k--) {
+                int2 ab = P.pairs[k];
+                double co = Rt[k].x, si = Rt[k].y;
+                double2 ya = X[ab.x * B + lane], yb = X[ab.y * B + lane];
+                double2 la = L[ab.x * B + lane], lb = L[ab.y * B + lane];
+                // inputs: xa = co ya - i si yb, xb = co yb - i si ya
+                double2 xa = make_double2(co * ya.x + si * yb.y, co * ya.y - si * yb.x);
+                double2 xb = make_double2(co * yb.x + si * ya.y, co * yb.y - si * ya.x);
+                // dy/dtheta with sin(theta) = -si, cos(theta) = co:
+                // dya = si xa - i co xb, dyb = si xb - i co xa
+                double2 da = make_double2(si * xa.x + co * xb.y, si * xa.y - co * xb.x);
+                double2 db = make_double2(si * xb.x + co * xa.y, si * xb.y - co * xa.x);
+                gsc += Jf[k] * (la.x * da.x + la.y * da.y + lb.x * db.x + lb.y * db.y);
+                X[ab.x * B + lane] = xa;
+                X[ab.y * B + lane] = xb;
+                L[ab.x * B + lane] = make_double2(co * la.x + si * lb.y, co * la.y - si * lb.x);
+                L[ab.y * B + lane] = make_double2(co * lb.x + si * la.y, co * lb.y - si * la.x);
+            }
+            adj_phase_back(X, L, gs, B, lane, n, U, hf);
+        }
+        if (t1 % P.K == 0)
+            for (int a = 0; a < n; a++) X[a * B + lane] = ck[(size_t)(t1 / P.K) * n + a];
+        const double2 g = G[t1];
+        for (int a = 0; a < n; a++) {
+            double m = (double)traj_mu(T, t, x, a);
+            double2 l = L[a * B + lane];
+            L[a * B + lane] = make_double2(l.x + m * g.x, l.y + m * g.y);
+        }
+    }
+    for (int a = 0; a < n; a++) gshift[(size_t)v * n + a] = gs[a * B + lane];
+    gscale[v] = gsc;
+}
+
+// Deterministic sums over vectors: g[a] = sum_v part[v][a] (a < n), in v order.
+__global__ void k_adj_reduce(const double *part, int nvec, int n, double *g) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n) return;
+    double s = 0;
+    for (int v = 0; v < nvec; v++) s += part[(size_t)v * n + a];
+    g[a] = s;
+}
+
+int lanes_adj(size_t lane_bytes) {
+    int B = 64;
+    while (B > 1 && lane_bytes * B > 200 * 1024) B >>= 1;
+    return B;
+}
+
+}  // namespace
+
+int launch_adj_prep(const DevTraj &T, const AdjPlan &P, cudaStream_t s) {
+    long tot = P.nf * P.n + P.nf * P.k;
+    if (tot <= 0) return 0;
+    k_adj_prep<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(T, P);
+    return (int)cudaGetLastError();
+}
+
+int launch_adj_fwd(const DevTraj &T, const AdjPlan &P, const AbsJob &J, double2 *resp, double2 *ckpt,
+                   cudaStream_t s) {
+    const int nvec = 3 * J.nsamp;
+    const size_t lb = sizeof(double2) * P.n;
+    const int B = lanes_adj(lb);
+    const size_t sm = lb * B;
+    cudaError_t e = cudaFuncSetAttribute(k_adj_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e) return (int)e;
+    k_adj_fwd<<<(nvec + B - 1) / B, B, sm, s>>>(T, P, J, resp, ckpt);
+    return (int)cudaGetLastError();
+}
+
+int launch_adj_bwd(const DevTraj &T, const AdjPlan &P, const AbsJob &J, const double2 *G, const double2 *ckpt,
+                   double *gshift_part, double *gscale_part, double *gshift, double *gscale, cudaStream_t s) {
+    const int nvec = 3 * J.nsamp;
+    const size_t lb = (2 * sizeof(double2) + sizeof(double)) * P.n;
+    const int B = lanes_adj(lb);
+    const size_t sm = lb * B;
+    cudaError_t e = cudaFuncSetAttribute(k_adj_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e) return (int)e;
+    k_adj_bwd<<<(nvec + B - 1) / B, B, sm, s>>>(T, P, J, G, ckpt, gshift_part, gscale_part);
+    k_adj_reduce<<<(P.n + 127) / 128, 128, 0, s>>>(gshift_part, nvec, P.n, gshift);
+    k_adj_reduce<<<1, 1, 0, s>>>(gscale_part, nvec, 1, gscale);
+    return (int)cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ host
+#include <cmath>
+#include <cstring>
+
+#include "nise_internal.h"
+
+namespace {
+
+const float kCv32 = 2.99792458e-5f;
+const float kTwoPi32 = (float)(2 * 3.14159265359);
+
+struct AdjRun {
+    int begin = 0, end = 0, nsamp = 0;
+    long f0 = 0, nf = 0;
+    std::vector<double2> S;  // response sums (tmax)
+};
+
+// FP64 forward of the model; leaves the tables and checkpoints in the
+// caller's buffers for the backward sweep.
+int adj_forward(nise_ctx *c, const double *shift, double scale, int K, AdjRun &R, DevBuf<double> &dshift,
+                DevBuf<int2> &dpairs, DevBuf<double2> &U, DevBuf<double2> &rot, DevBuf<double> &jf,
+                DevBuf<double2> &ckpt, AdjPlan &P, AbsJob &J) {
+    const nise_params &p = c->p;
+    if (p.propagation != NISE_PROP_COUPLING)
+        return nise_fail(c, NISE_ERR_UNSUPPORTED, "the absorption adjoint differentiates Propagation Coupling");
+    if (!c->loaded) return nise_fail(c, NISE_ERR_STATE, "no trajectory loaded");
+    if (!shift || !(scale == scale)) return nise_fail(c, NISE_ERR_ARG, "null shifts or invalid scale");
+    const int N = c->n, tmax = p.tmax1;
+    int n_samples = (p.length - p.tmax1 - 1) / p.sample + 1;
+    if (n_samples <= 0) return nise_fail(c, NISE_ERR_ARG, "Insufficient data to calculate spectrum.");
+    R.end = p.end == 0 ? n_samples : p.end;
+    R.begin = p.begin;
+    if (R.end > n_samples || R.begin < 0 || R.begin >= R.end) return nise_fail(c, NISE_ERR_ARG, "bad BeginPoint/EndPoint");
+    R.nsamp = R.end - R.begin;
+    R.f0 = (long)R.begin * p.sample;
+    long f1 = (long)(R.end - 1) * p.sample + tmax - 1;
+    int rc;
+    if ((rc = nise_check_frames(c, f1))) return rc;
+    R.nf = f1 - R.f0 > 0 ? f1 - R.f0 : 1;
+    std::vector<int2> pairs;
+    if ((rc = nise_pattern(c, R.f0, R.nf, pairs))) return rc;
+    const int nvec = 3 * R.nsamp;
+    memset(&P, 0, sizeof(P));
+    P.n = N;
+    P.k = (int)pairs.size();
+    P.ts = p.ts;
+    P.K = K;
+    P.nck = (tmax - 1) / K + 2;
+    P.f0 = R.f0;
+    P.nf = R.nf;
+    P.scale = scale;
+    P.f = nise_f64(p, 1, p.ts);
+    std::vector<double> hs(shift, shift + N);
+    if ((rc = dshift.upload(c, hs)) || (rc = dpairs.upload(c, pairs.empty() ? std::vector<int2>(1) : pairs)) ||
+        (rc = U.alloc(c, (size_t)R.nf * N)) || (rc = rot.alloc(c, (size_t)R.nf * (P.k ? P.k : 1))) ||
+        (rc = jf.alloc(c, (size_t)R.nf * (P.k ? P.k : 1))) || (rc = ckpt.alloc(c, (size_t)nvec * P.nck * N)))
+        return rc;
+    P.shift = dshift.p;
+    P.pairs = dpairs.p;
+    P.U = U.p;
+    P.rot = rot.p;
+    P.jf = jf.p;
+    memset(&J, 0, sizeof(J));
+    J.begin = R.begin;
+    J.nsamp = R.nsamp;
+    J.sample = p.sample;
+    J.tmax = tmax;
+    J.ts = p.ts;
+    DevTraj T = nise_devtraj(c);
+    DevBuf<double2> resp, out;
+    if ((rc = resp.alloc(c, (size_t)nvec * tmax)) || (rc = out.alloc(c, tmax))) return rc;
+    c->launches = 0;
+    cudaEventRecord(c->ev0, c->stream);
+    cudaEventRecord(c->evk0, c->stream);
+    if ((rc = nise_cuda(c, launch_adj_prep(T, P, c->stream), "adjoint tables"))) return rc;
+    if ((rc = nise_cuda(c, launch_adj_fwd(T, P, J, resp.p, ckpt.p, c->stream), "adjoint forward"))) return rc;
+    if ((rc = nise_cuda(c, launch_reduce_resp(resp.p, nvec, tmax, out.p, c->stream), "response reduction")))
+        return rc;
+    c->launches += 3;
+    R.S.resize(tmax);
+    cudaMemcpyAsync(R.S.data(), out.p, sizeof(double2) * tmax, cudaMemcpyDeviceToHost, c->stream);
+    return nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "adjoint forward");
+}
+
+// The FP64 branch of the 1D transform input factors (1DFFT.c:170-200) for
+// point j, lifetime given explicitly.
+double fft_factor(const nise_params &p, int j, double lifetime) {
+    double d = 1;
+    if (lifetime > 0) d *= exp(-j * (double)p.deltat / (2 * lifetime));
+    if (p.homogen > 0) d *= exp(-j * (double)p.deltat / (2 * (double)p.homogen));
+    if (p.inhomogen > 0)
+        d *= exp(-j * (double)p.deltat * j * (double)p.deltat / (2 * (double)p.inhomogen * p.inhomogen));
+    if (p.window == 1) {
+        double a = j * (double)kTwoPi32 / (4 * p.tmax1 - 4);
+        d *= cos(a) * cos(a);
+    }
+    if (j == 0) d *= 0.5;
+    return d;
+}
+
+// Rows of Absorption.dat in FP64 (1DFFT.c:208-228): FFT index and frequency.
+void fft_rows(const nise_ctx *c, int fft, std::vector<int> &idx, std::vector<double> &w) {
+    const nise_params &p = c->p;
+    auto emit = [&](int i, int num) {
+        double x = -((double)num / p.deltat / (double)kCv32 / fft - (double)c->shifte);
+        if (!(x > p.min1 && x < p.max1)) return;
+        idx.push_back(i);
+        w.push_back(x);
+    };
+    for (int i = fft / 2; i <= fft - 1; i++) emit(i, fft - i);
+    for (int i = 0; i <= fft / 2 - 1; i++) emit(i, -i);
+}
+
+// Spectrum rows of the response S in FP64 on the host (direct DFT at the
+// emitted indices): spec = (Im Out, Re Out) * 2 dt c_v.
+void model_spectrum(const nise_ctx *c, const std::vector<double2> &S, int samples, double lifetime,
+                    const std::vector<int> &idx, std::vector<double> &sr, std::vector<double> &si) {
+    const nise_params &p = c->p;
+    const int tmax = p.tmax1, fft = p.fft < tmax ? tmax : p.fft;
+    std::vector<double2> in(tmax);
+    for (int j = 0; j < tmax; j++) {
+        double d = fft_factor(p, j, lifetime);
+        in[j] = make_double2(S[j].y / samples * d, S[j].x / samples * d);
+    }
+    const double scale = 2.0 * (double)p.deltat * (double)kCv32;
+    sr.assign(idx.size(), 0);
+    si.assign(idx.size(), 0);
+    for (size_t r = 0; r < idx.size(); r++) {
+        double ore = 0, oim = 0;
+        for (int j = 0; j < tmax; j++) {
+            long m = ((long)j * idx[r]) % fft;
+            double ang = -2.0 * M_PI * (double)m / fft, cs = cos(ang), sn = sin(ang);
+            ore += in[j].x * cs - in[j].y * sn;
+            oim += in[j].x * sn + in[j].y * cs;
+        }
+        sr[r] = oim * scale;
+        si[r] = ore * scale;
+    }
+}
+
+}  // namespace
+
+extern "C" int nise_absorption_model(nise_ctx *c, const double *site_shift, double coupling_scale, double lifetime,
+                                     double *freq, double *spec_re, double *spec_im, int max_rows, int *rows) {
+    if (!c || !freq || !spec_re || !spec_im || !rows) return nise_fail(c, NISE_ERR_ARG, "null argument");
+    cudaSetDevice(c->p.device);
+    AdjRun R;
+    DevBuf<double> dshift, jf;
+    DevBuf<int2> dpairs;
+    DevBuf<double2> U, rot, ckpt;
+    AdjPlan P;
+    AbsJob J;
+    int rc = adj_forward(c, site_shift, coupling_scale, c->p.tmax1, R, dshift, dpairs, U, rot, jf, ckpt, P, J);
+    if (rc) return rc;
+    cudaEventRecord(c->evk1, c->stream);
+    cudaEventRecord(c->ev1, c->stream);
+    cudaStreamSynchronize(c->stream);
+    nise_collect_timing(c);
+    const int fft = c->p.fft < c->p.tmax1 ? c->p.tmax1 : c->p.fft;
+    std::vector<int> idx;
+    std::vector<double> w, sr, si;
+    fft_rows(c, fft, idx, w);
+    model_spectrum(c, R.S, R.end, lifetime, idx, sr, si);
+    int n = (int)idx.size() < max_rows ? (int)idx.size() : max_rows;
+    for (int r = 0; r < n; r++) {
+        freq[r] = w[r];
+        spec_re[r] = sr[r];
+        spec_im[r] = si[r];
+    }
+    *rows = n;
+    return NISE_OK;
+}
+
+extern "C" int nise_backward_absorption(nise_ctx *c, const double *site_shift, double coupling_scale,
+                                        double lifetime, const double *dL_dspec_re, const double *dL_dspec_im,
+                                        int rows, double *g_shift, double *g_scale, double *g_lifetime) {
+    if (!c || !dL_dspec_re || !dL_dspec_im || !g_shift || !g_scale || !g_lifetime)
+        return nise_fail(c, NISE_ERR_ARG, "null argument");
+    cudaSetDevice(c->p.device);
+    const nise_params &p = c->p;
+    const int fft = p.fft < p.tmax1 ? p.tmax1 : p.fft, tmax = p.tmax1, N = c->n;
+    std::vector<int> idx;
+    std::vector<double> w;
+    fft_rows(c, fft, idx, w);
+    if (rows != (int)idx.size())
+        return nise_fail(c, NISE_ERR_SHAPE, "dL/dspec has %d rows, the spectrum has %d", rows, (int)idx.size());
+    AdjRun R;
+    DevBuf<double> dshift, jf;
+    DevBuf<int2> dpairs;
+    DevBuf<double2> U, rot, ckpt;
+    AdjPlan P;
+    AbsJob J;
+    const int K = 32;  // checkpoint interval (steps)
+    int rc = adj_forward(c, site_shift, coupling_scale, K, R, dshift, dpairs, U, rot, jf, ckpt, P, J);
+    if (rc) return rc;
+    // adjoint of the transform: dL/dOut_k = (dL/dspec_im + i dL/dspec_re) * 2 dt c_v,
+    // dL/din_j = sum_k exp(+2 pi i jk/fft) dL/dOut_k, then through the input factors
+    const double scale = 2.0 * (double)p.deltat * (double)kCv32;
+    std::vector<double2> G(tmax);
+    double gl = 0;
+    for (int j = 0; j < tmax; j++) {
+        double gr = 0, gi = 0;
+        for (size_t r = 0; r < idx.size(); r++) {
+            long m = ((long)j * idx[r]) % fft;
+            double ang = 2.0 * M_PI * (double)m / fft, cs = cos(ang), sn = sin(ang);
+            double orr = dL_dspec_im[r] * scale, oii = dL_dspec_re[r] * scale;
+            gr += cs * orr - sn * oii;
+            gi += sn * orr + cs * oii;
+        }
+        double d = fft_factor(p, j, lifetime);
+        // in_j = d * (Im S_j + i Re S_j) / samples
+        G[j] = make_double2(gi * d / R.end, gr * d / R.end);
+        if (lifetime > 0) {
+            double inr = R.S[j].y / R.end * d, ini = R.S[j].x / R.end * d;
+            gl += (gr * inr + gi * ini) * (j * (double)p.deltat / (2 * lifetime * lifetime));
+        }
+    }
+    DevBuf<double2> dG;
+    DevBuf<double> gsp, gcp, gs, gc;
+    const int nvec = 3 * R.nsamp;
+    if ((rc = dG.upload(c, G)) || (rc = gsp.alloc(c, (size_t)nvec * N)) || (rc = gcp.alloc(c, nvec)) ||
+        (rc = gs.alloc(c, N)) || (rc = gc.alloc(c, 1)))
+        return rc;
+    DevTraj T = nise_devtraj(c);
+    if ((rc = nise_cuda(c, launch_adj_bwd(T, P, J, dG.p, ckpt.p, gsp.p, gcp.p, gs.p, gc.p, c->stream),
+                        "adjoint backward")))
+        return rc;
+    c->launches += 3;
+    cudaEventRecord(c->evk1, c->stream);
+    std::vector<double> hs(N);
+    double hc = 0;
+    cudaMemcpyAsync(hs.data(), gs.p, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream);
+    cudaMemcpyAsync(&hc, gc.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    cudaEventRecord(c->ev1, c->stream);
+    if ((rc = nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "adjoint backward"))) return rc;
+    nise_collect_timing(c);
+    for (int a = 0; a < N; a++) g_shift[a] = hs[a];
+    *g_scale = hc;
+    *g_lifetime = gl;
+    return NISE_OK;
+}
