@@ -43,6 +43,22 @@ UNIT = "site-steps/s"
 WORKLOAD = "batched linear absorption, Propagation Sparse (exact exp(-iH dt), Threshold 0), N=1024 lattice"
 
 
+def max_over_ranks(x, world, device):
+    """Largest value of x over all ranks (the job time of replicas is the slowest rank's)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(units_per_rank, max_ms, world):
+    """Whole-job throughput of `world` independent replicas: all ranks' units over the max time."""
+    return world * units_per_rank / (max_ms / 1e3)
+
+
 def parse():
     a = argparse.ArgumentParser()
     a.add_argument("--gpus", type=int, default=1)
@@ -51,8 +67,9 @@ def parse():
     a.add_argument("--impl", choices=["ours", "reference"], default="ours")
     a.add_argument("--frames", type=int, default=100000, help="trajectory length (default: the full workload)")
     a.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline (profiling runs)")
-    a.add_argument("--config", choices=["c1", "c2"], default="c1",
-                   help="c1: the headline (batched absorption, N=1024); c2: 2DIR, N=64 cluster (secondary)")
+    a.add_argument("--config", choices=["c1", "c2", "c4"], default="c1",
+                   help="c1: the headline (batched absorption, N=1024); c2: 2DIR, N=64 cluster; c4: 64-trajectory "
+                        "mixed-size batch (secondary workloads)")
     a.add_argument("--t2", type=int, default=0, help="c2 only: waiting-time steps (RunTimes 64 t2 64)")
     a.add_argument("--end", type=int, default=0, help="c2 only: EndPoint (0 = all start points)")
     return a.parse_args()
@@ -222,13 +239,6 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     c = ctx_for(nise.BATCHED)
     trajectory(c)
     for _ in range(max(args.warmup, 3)):
@@ -248,8 +258,8 @@ def run_ours(args):
     ev1.record(stream)
     barrier()
     clk = clocks.stop()
-    ms = max_over_ranks(ev0.elapsed_time(ev1))
-    value = world * per_step * args.steps / (ms / 1e3)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world, "cuda")
+    value = replica_throughput(per_step * args.steps, ms, world)
 
     # end to end through the C ABI from pinned host buffers, copies inside the timed region
     barrier()
@@ -263,8 +273,8 @@ def run_ours(args):
         one_step(c)
     ev1.record(stream)
     barrier()
-    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
-    e2e_value = world * per_step * args.steps / (e2e_ms / 1e3)
+    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1), world, "cuda")
+    e2e_value = replica_throughput(per_step * args.steps, e2e_ms, world)
     fft = max(c.params.fft, c.params.tmax1)
     h2d = e_bytes + d_bytes + c_bytes
     d2h = c.params.tmax1 * 16 + fft * 16  # response sums and device spectrum
@@ -281,8 +291,8 @@ def run_ours(args):
     one_step(cp)
     ev1.record(stream)
     barrier()
-    plain_ms = max_over_ranks(ev0.elapsed_time(ev1))
-    plain_value = world * 3 * plain_samples * n * 256 / (plain_ms / 1e3)
+    plain_ms = max_over_ranks(ev0.elapsed_time(ev1), world, "cuda")
+    plain_value = replica_throughput(3 * plain_samples * n * 256, plain_ms, world)
     cp.close()
 
     main_ms = statistics.mean(mains)
@@ -378,6 +388,78 @@ def run_c2(args):
     return out
 
 
+def c4_sites():
+    """Site counts of the mixed-size batch: round(8 * 256^(i/63)), i = 0..63 (8 ... 2048)."""
+    return [int(round(8 * 256 ** (i / 63.0))) for i in range(64)]
+
+
+def run_c4(args):
+    """64 absorption trajectories, N log-spaced 8..2048, lattice couplings and OU site noise (the
+    C1 statistics), 5000 x 1 fs frames, Tmax1 128, Samplerate 25; even i Propagation Coupling,
+    odd i Propagation Diagonal; all jobs in one CUDA graph (nise_batch_*), autotuned.
+
+    value = aggregate site-steps per second of one graph launch (all 64 spectra).  The
+    sequential comparison runs the same jobs one context at a time (nise_absorption)."""
+    import torch
+    import nise_2017_b200 as nise
+    from nise_2017_b200 import synth
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    frames, tmax, sample = 5000, 128, 25
+    sizes = c4_sites()
+    nsamp = (frames - tmax - 1) // sample + 1
+    site_steps = sum(3 * nsamp * tmax * n for n in sizes)
+    ctxs = []
+    with tempfile.TemporaryDirectory() as td:
+        try:
+            for i, n in enumerate(sizes):
+                s = synth.c1_spec(n_sites=n, frames=frames, seed=40000 + i)
+                files = synth.write(s, os.path.join(td, "t%02d" % i))
+                kw = synth.c1_keywords(Singles=n, Length=frames, RunTimes="%d 0 0" % tmax, Samplerate=sample,
+                                       Propagation="Coupling" if i % 2 == 0 else "Diagonal", FFT=1024)
+                c = nise.Context(nise.params_from_keywords(kw, files, device=local))
+                c.load_files()
+                ctxs.append(c)
+            # sequential comparison: every job on its own, one after another (device time)
+            seq_ms, per_job = 0.0, []
+            for c in ctxs:
+                re, im, n = c.absorption()
+                c.absorption_fft(re, im, n)
+                re, im, n = c.absorption()
+                tot, _, _ = c.timing()
+                seq_ms += tot
+                per_job.append(tot)
+            with nise.Batch(ctxs, autotune=True) as b:
+                for _ in range(max(args.warmup, 3)):
+                    b.run()
+                times = []
+                clk = ClockSampler(local)
+                clk.start()
+                for _ in range(args.steps):
+                    b.run()
+                    ms, launches = b.timing()
+                    times.append(ms)
+                clocks = clk.stop()
+        finally:
+            for c in ctxs:
+                c.close()
+    ms = statistics.mean(times)
+    out = {"metric": "C4 mixed-size batch: aggregate site-steps/s and time-to-spectrum (secondary workload)",
+           "value": site_steps / (ms / 1e3), "unit": "site-steps/s", "n_gpus": 1, "steps": args.steps,
+           "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
+           "time_to_spectrum_s": ms / 1e3,
+           "config": {"workload": "64 trajectories, N = round(8*256^(i/63)) = 8..2048 (sum %d), lattice couplings, "
+                                  "OU sites, 5000 x 1 fs, RunTimes 128 0 0, Samplerate 25, even i Coupling, "
+                                  "odd i Diagonal, one CUDA graph, autotuned" % sum(sizes),
+                      "site_steps": site_steps},
+           "sequential": {"ms": seq_ms, "value": site_steps / (seq_ms / 1e3),
+                          "mode": "the same jobs one context at a time (nise_absorption)",
+                          "slowest_job_ms": max(per_job), "slowest_job_sites": sizes[per_job.index(max(per_job))]},
+           "batched_over_sequential": seq_ms / ms, "clocks": clocks, "gpu_launches": launches}
+    print(json.dumps(out), flush=True)
+    return out
+
+
 # ---------------------------------------------------------------- reference arm
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
@@ -428,5 +510,7 @@ if __name__ == "__main__":
         run_reference(a)
     elif a.config == "c2":
         run_c2(a)
+    elif a.config == "c4":
+        run_c4(a)
     else:
         run_ours(a)

@@ -97,6 +97,12 @@ typedef struct {
     int precision;                 /* NISE_FP32 or NISE_FP64 */
     int launch_mode;               /* NISE_BATCHED or NISE_PLAIN */
     int device;                    /* CUDA device ordinal */
+    int kernel_config;             /* absorption kernel: 0 automatic (autotuned or default);
+                                      Trotter: 1 thread per vector, 64/128/256 level-scheduled
+                                      rotations with that many threads per start point;
+                                      Sparse (static couplings): 3 or 9 k_abs_taylor2 with 4 or 8
+                                      vectors per CTA, 8 the sliced-ELL Taylor kernel, 10 the
+                                      sliced-ELL Chebyshev kernel (FP32) */
 } nise_params;
 
 typedef struct nise_ctx nise_ctx;
@@ -158,6 +164,33 @@ int nise_write_spectrum(const char *path, const double *freq, const double *spec
                         int rows);
 /* print2D: divides by sample_count, halves the t3 = 0 row, writes t1 t2 t3 Re Im. */
 int nise_write_2d(const char *path, const nise_params *p, const double *re, const double *im, int sample_count);
+
+/* Launch autotuner: times the candidate kernel configurations of this
+ * context's absorption job (Trotter: thread per vector or level-scheduled
+ * rotations with 64/128/256 threads per start point; Sparse: the Taylor
+ * kernel variants) and keeps the fastest for every later job of the same
+ * scheme, precision and size in this process.  Results do not depend on the
+ * choice (Trotter variants are bitwise identical). */
+int nise_absorption_tune(nise_ctx *ctx);
+
+/* Batched linear absorption of many contexts (trajectories of any size and
+ * scheme, one device): nise_batch_create plans every job (optionally
+ * autotuning), then captures all of them, each on its own stream, with their
+ * 1D transforms into one CUDA graph; nise_batch_run launches the graph once
+ * and waits.  Results per job: the response (as nise_absorption) and the
+ * Absorption.dat rows (as nise_absorption_fft).  Destroy the batch before its
+ * contexts.  No reference counterpart (the reference runs one trajectory per
+ * process). */
+typedef struct nise_batch nise_batch;
+int nise_batch_create(nise_ctx *const *ctxs, int n, int autotune, nise_batch **out);
+int nise_batch_run(nise_batch *batch);
+int nise_batch_result(nise_batch *batch, int job, double *re_S, double *im_S, int *samples);
+int nise_batch_spectrum(nise_batch *batch, int job, double *freq, double *spec_re, double *spec_im, int max_rows,
+                        int *rows);
+/* Device time of the last nise_batch_run (ms) and the kernels in the graph. */
+int nise_batch_timing(const nise_batch *batch, double *ms, long *kernel_launches);
+const char *nise_batch_error(const nise_batch *batch);
+void nise_batch_destroy(nise_batch *batch);
 
 /* The reference's 2DFFT program (2DFFT.c:20-830): reads the keyword file at
  * `input_path` (FFT, Timestep, RunTimes, Min/MaxFrequencies, Homogeneous,

@@ -36,7 +36,8 @@ EXPORTED = [
     "nise_absorption_fft", "nise_2dir", "nise_propagate", "nise_propagate_doubles", "nise_write_td_absorption",
     "nise_write_spectrum", "nise_write_2d", "nise_set_stream", "nise_last_timing", "nise_last_work",
     "nise_probe_fp32_peak", "nise_absorption_noalloc", "nise_2dfft_files", "nise_absorption_model",
-    "nise_backward_absorption",
+    "nise_backward_absorption", "nise_absorption_tune", "nise_batch_create", "nise_batch_run", "nise_batch_result",
+    "nise_batch_spectrum", "nise_batch_timing", "nise_batch_error", "nise_batch_destroy",
 ]
 
 
@@ -61,6 +62,7 @@ class Params(ctypes.Structure):
         ("couplingFName", ctypes.c_char * 256), ("anharFName", ctypes.c_char * 256),
         ("overdipFName", ctypes.c_char * 256), ("singleShiftFName", ctypes.c_char * 256),
         ("precision", ctypes.c_int), ("launch_mode", ctypes.c_int), ("device", ctypes.c_int),
+        ("kernel_config", ctypes.c_int),
     ]
 
 
@@ -104,6 +106,16 @@ def lib():
         L.nise_last_timing.argtypes = [vp, dp, dp, ctypes.POINTER(ctypes.c_long)]
         L.nise_last_work.argtypes = [vp, dp, dp]
         L.nise_probe_fp32_peak.argtypes = [ctypes.c_int, dp]
+        L.nise_absorption_tune.argtypes = [vp]
+        L.nise_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
+        L.nise_batch_run.argtypes = [vp]
+        L.nise_batch_result.argtypes = [vp, ctypes.c_int, dp, dp, ip]
+        L.nise_batch_spectrum.argtypes = [vp, ctypes.c_int, dp, dp, dp, ctypes.c_int, ip]
+        L.nise_batch_timing.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_long)]
+        L.nise_batch_error.argtypes = [vp]
+        L.nise_batch_error.restype = ctypes.c_char_p
+        L.nise_batch_destroy.argtypes = [vp]
+        L.nise_batch_destroy.restype = None
         _lib = L
     return _lib
 
@@ -284,6 +296,10 @@ class Context:
                                                    _dp(g), ctypes.byref(gs), ctypes.byref(gl)))
         return g, gs.value, gl.value
 
+    def tune(self):
+        """Autotune the absorption kernels for this context's job (nise_absorption_tune)."""
+        self._check(lib().nise_absorption_tune(self._h))
+
     def set_stream(self, stream_ptr):
         """Enqueue this context's device work on a caller CUDA stream (int handle, 0 = own)."""
         self._check(lib().nise_set_stream(self._h, ctypes.c_void_p(stream_ptr or None)))
@@ -340,3 +356,56 @@ def fft2d_files(input_path, device=0):
     rc = lib().nise_2dfft_files(os.fsencode(input_path), device)
     if rc != 0:
         raise NiseError(rc, lib().nise_global_error().decode())
+
+
+class Batch:
+    """Many contexts' absorption jobs as one CUDA graph (nise_batch_*)."""
+
+    def __init__(self, contexts, autotune=False):
+        self.contexts = list(contexts)
+        arr = (ctypes.c_void_p * len(self.contexts))(*[c._h for c in self.contexts])
+        h = ctypes.c_void_p()
+        rc = lib().nise_batch_create(arr, len(self.contexts), 1 if autotune else 0, ctypes.byref(h))
+        if rc != 0:
+            raise NiseError(rc, lib().nise_global_error().decode())
+        self._h = h
+
+    def _check(self, rc):
+        if rc != 0:
+            raise NiseError(rc, lib().nise_batch_error(self._h).decode())
+
+    def run(self):
+        self._check(lib().nise_batch_run(self._h))
+
+    def result(self, i):
+        t = self.contexts[i].params.tmax1
+        re, im, n = np.zeros(t), np.zeros(t), ctypes.c_int(0)
+        self._check(lib().nise_batch_result(self._h, i, _dp(re), _dp(im), ctypes.byref(n)))
+        return re, im, n.value
+
+    def spectrum(self, i):
+        p = self.contexts[i].params
+        fft = max(p.fft, p.tmax1)
+        w, sr, si = np.zeros(fft), np.zeros(fft), np.zeros(fft)
+        rows = ctypes.c_int(0)
+        self._check(lib().nise_batch_spectrum(self._h, i, _dp(w), _dp(sr), _dp(si), fft, ctypes.byref(rows)))
+        r = rows.value
+        return w[:r], sr[:r], si[:r]
+
+    def timing(self):
+        """(device ms of the last run, kernels in the graph)."""
+        ms, n = ctypes.c_double(0), ctypes.c_long(0)
+        lib().nise_batch_timing(self._h, ctypes.byref(ms), ctypes.byref(n))
+        return ms.value, n.value
+
+    def close(self):
+        if self._h:
+            lib().nise_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+

@@ -33,6 +33,7 @@ CU_SOURCES = [
 ]
 CPP_SOURCES = [
     "api.cpp",
+    "absrun.cpp",
     "input.cpp",
 ]
 

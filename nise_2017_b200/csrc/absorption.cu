@@ -82,6 +82,82 @@ __global__ void k_abs_trotter(DevTraj T, TrotterPlan P, AbsJob J, double2 *resp,
     }
 }
 
+// Trotter absorption with the rotations of a sub-step grouped into levels:
+// rotation k gets level 1 + the highest level of the earlier rotations that
+// share one of its sites, so the rotations of one level touch disjoint sites
+// and applying a level in parallel reproduces the sequential lexicographic
+// order of propagate.c:876-888 operation for operation.  CTA per start
+// point, its three polarisation vectors in shared memory; the response is
+// summed in site order by one thread per polarisation (the order of dot_mu),
+// so every Trotter kernel gives bitwise identical results.
+template <typename R>
+__global__ void k_abs_trotter_lv(DevTraj T, TrotterPlan P, AbsJob J, double2 *resp, const int *__restrict__ perm,
+                                 const int *__restrict__ lvptr, int nlev) {
+    typedef typename Vec2<R>::T R2;
+    typedef Ar<R> A;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = P.n, tid = threadIdx.x, NT = blockDim.x;
+    R2 *C = (R2 *)smem_raw;             // [3][n]
+    float *mu = (float *)(C + 3 * n);   // [3][n]
+    const int sl = blockIdx.x;
+    const long ti = (long)(J.begin + sl) * J.sample;
+    for (int e = tid; e < 3 * n; e += NT) {
+        R2 z;
+        z.x = (R)traj_mu(T, ti, e / n, e % n);
+        z.y = 0;
+        C[e] = z;
+    }
+    const R2 *U = (const R2 *)P.U, *rot = (const R2 *)P.rot;
+    for (int t1 = 0; t1 < J.tmax; t1++) {
+        const long t = ti + t1;
+        for (int e = tid; e < 3 * n; e += NT) mu[e] = traj_mu(T, t, e / n, e % n);
+        __syncthreads();
+        if (tid < 3) {
+            double re = 0, im = 0;
+            for (int a = 0; a < n; a++) {
+                R m = (R)mu[tid * n + a];
+                R2 z = C[tid * n + a];
+                re += (double)A::mul(m, z.x);
+                im += (double)A::mul(m, z.y);
+            }
+            resp[(size_t)(3 * sl + tid) * J.tmax + t1] = make_double2(re, im);
+        }
+        __syncthreads();
+        if (t1 == J.tmax - 1) break;
+        const R2 *Uf = U + (t - P.f0) * n;
+        const R2 *Rf = P.rot_static ? rot : rot + (t - P.f0) * P.k;
+        for (int sub = 0; sub < J.ts; sub++) {
+            for (int half = 0; half < 2; half++) {
+                for (int e = tid; e < 3 * n; e += NT) {  // propagate.c:870-873 / 891-894
+                    R2 z = C[e], u = Uf[e % n], o;
+                    o.x = A::sub(A::mul(z.x, u.x), A::mul(z.y, u.y));
+                    o.y = A::add(A::mul(z.y, u.x), A::mul(z.x, u.y));
+                    C[e] = o;
+                }
+                __syncthreads();
+                if (half == 1) break;
+                for (int l = 0; l < nlev; l++) {
+                    const int r0 = lvptr[l], cnt = lvptr[l + 1] - r0;
+                    for (int e = tid; e < 3 * cnt; e += NT) {
+                        const int k = perm[r0 + e / 3], x = e % 3;
+                        const int2 ab = P.pairs[k];
+                        const R2 cs = Rf[k];
+                        R2 *ca = C + x * n + ab.x, *cb = C + x * n + ab.y;
+                        R2 xa = *ca, xb = *cb, ya, yb;
+                        ya.x = A::sub(A::mul(cs.x, xa.x), A::mul(cs.y, xb.y));
+                        ya.y = A::add(A::mul(cs.x, xa.y), A::mul(cs.y, xb.x));
+                        yb.x = A::sub(A::mul(cs.x, xb.x), A::mul(cs.y, xa.y));
+                        yb.y = A::add(A::mul(cs.x, xb.y), A::mul(cs.y, xa.x));
+                        *ca = ya;
+                        *cb = yb;
+                    }
+                    __syncthreads();
+                }
+            }
+        }
+    }
+}
+
 // ------------------------------------------------------------ RK4
 template <typename R>
 __global__ void k_prep_rk4(DevTraj T, Rk4Plan P, R fsub) {
@@ -403,7 +479,7 @@ __global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, Ab
                                                     const EllEnt<R> *__restrict__ ell_g, const int *__restrict__ sptr_g,
                                                     int nslices, int nent) {
     typedef typename Vec2<R>::T R2;
-    constexpr int G = 8, QR = 4, RS = G + 2;
+    constexpr int G = 8, QR = 4, RS = NISE_T3_ROW;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = P.n, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, NW = blockDim.x >> 5;
     const int g = lane % G, q = lane / G;
@@ -486,6 +562,206 @@ __global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, Ab
                 cur[(size_t)i * RS + g] = nx[it];
                 psi[it].x += nx[it].x;
                 psi[it].y += nx[it].y;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Chebyshev expansion of the exact step (FP32, sliced ELL in shared memory).
+//
+// With R_t the Gershgorin radius of frame t (max |h_ii| + max row sum of
+// |J|) and x = f R_t, exp(-i f H) = sum_k a_k T_k(H / R_t) with a_0 = J_0(x),
+// a_k = 2 (-i)^k J_k(x) (the Jacobi-Anger expansion); the T_k(H/R) psi follow
+// the three-term recurrence T_k = 2 (H/R) T_(k-1) - T_(k-2).  For the small
+// x of a time step the Bessel coefficients fall off like (x/2)^k / k!,
+// against x^k / k! for the Taylor terms, so fewer sparse products reach the
+// same tolerance.  Per frame the prep kernel stores 1/R_t, the coefficients
+// and the order K_t (2 * sum_(k>K) |J_k(x)| <= tol).
+__global__ void k_prep_cheb(DevTraj T, TaylorPlan P, double rowabs, double f, double tol, int *order,
+                            float *inv_r, float2 *coef) {
+    long fi = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (fi >= P.nf) return;
+    long t = P.f0 + fi;
+    double dmax = 0;
+    for (int i = 0; i < P.n; i++) dmax = fmax(dmax, fabs((double)traj_diag(T, t, i, P.singleshift != 0)));
+    double R = dmax + rowabs;
+    if (!(R > 0)) R = 1;
+    const double x = fabs(f) * R;
+    // J_k(x), k = 0..KMAX+8, by Miller's downward recurrence normalised with
+    // J_0 + 2 sum J_2k = 1 (valid for every x > 0; x is below 20 here).
+    constexpr int KM = NISE_CHEB_KMAX + 8;
+    double jv[KM + 1];
+    for (int k = 0; k <= KM; k++) jv[k] = 0;
+    if (x < 1e-300) {
+        jv[0] = 1;
+    } else {
+        int M = (int)x + KM + 16;  // start well above the orders kept
+        if (M & 1) M++;
+        double jp = 0, j = 1e-280, sum = 0;
+        for (int k = M; k >= 1; k--) {
+            double jm = 2.0 * k / x * j - jp;  // J_(k-1)
+            jp = j;
+            j = jm;
+            if (fabs(j) > 1e250) {  // rescale to stay in range
+                j *= 1e-250;
+                jp *= 1e-250;
+                sum *= 1e-250;
+                for (int q = 0; q <= KM; q++) jv[q] *= 1e-250;
+            }
+            if (k - 1 <= KM) jv[k - 1] = j;
+            if (((k - 1) & 1) == 0 && k - 1 > 0) sum += 2 * j;
+        }
+        sum += jv[0];
+        for (int k = 0; k <= KM; k++) jv[k] /= sum;
+    }
+    int K = NISE_CHEB_KMAX;
+    for (int k = 1; k <= NISE_CHEB_KMAX; k++) {
+        double tail = 0;
+        for (int q = k + 1; q <= KM; q++) tail += fabs(jv[q]);
+        if (2 * tail <= tol) {
+            K = k;
+            break;
+        }
+    }
+    order[fi] = K;
+    inv_r[fi] = (float)(1.0 / R);
+    float2 *c = coef + fi * (NISE_CHEB_KMAX + 1);
+    c[0] = make_float2((float)jv[0], 0.f);
+    for (int k = 1; k <= NISE_CHEB_KMAX; k++) {
+        float a = (float)(2 * jv[k]);
+        switch (k & 3) {  // (-i)^k
+        case 0: c[k] = make_float2(a, 0.f); break;
+        case 1: c[k] = make_float2(0.f, -a); break;
+        case 2: c[k] = make_float2(-a, 0.f); break;
+        default: c[k] = make_float2(0.f, a); break;
+        }
+    }
+}
+
+// k_abs_taylor3's layout (8 vectors per CTA, sliced ELL, rows of NISE_T3_ROW)
+// with the Chebyshev recurrence: per own row the accumulated result, T_(k-2)
+// and the new T_k stay in registers, the diagonal of the current frame in
+// shared memory.
+template <int IT>
+__global__ void __launch_bounds__(512) k_abs_cheb3(DevTraj T, TaylorPlan P, AbsJob J, double2 *resp, int nvec,
+                                                  const EllEnt<float> *__restrict__ ell_g,
+                                                  const int *__restrict__ sptr_g, int nslices, int nent,
+                                                  const float *__restrict__ inv_r, const float2 *__restrict__ coef) {
+    constexpr int G = 8, QR = 4, RS = NISE_T3_ROW, KC = NISE_CHEB_KMAX + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = P.n, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, NW = blockDim.x >> 5;
+    const int g = lane % G, q = lane / G;
+    float2 *cur = (float2 *)smem_raw;
+    float *dgs = (float *)(cur + (size_t)n * RS);  // [row][g]
+    EllEnt<float> *ell = (EllEnt<float> *)(dgs + (size_t)n * G);
+    int *sptr = (int *)(ell + nent);
+    double *red = (double *)(((uintptr_t)(sptr + nslices + 1) + 15) & ~(uintptr_t)15);
+    for (int e = tid; e < nent; e += blockDim.x) ell[e] = ell_g[e];
+    for (int e = tid; e <= nslices; e += blockDim.x) sptr[e] = sptr_g[e];
+    const int v = blockIdx.x * G + g;
+    const bool valid = v < nvec;
+    const int vv = valid ? v : blockIdx.x * G;
+    const int x = vv % 3;
+    const long ti = (long)(J.begin + vv / 3) * J.sample;
+    float2 psi[IT], prev[IT], nx[IT];
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+        int i = q + QR * (warp + NW * it);
+        psi[it].x = i < n ? traj_mu(T, ti, x, i) : 0.f;
+        psi[it].y = 0;
+    }
+    __syncthreads();
+    for (int t1 = 0; t1 < J.tmax; t1++) {
+        const long tj = ti + t1;
+        double re = 0, im = 0;
+#pragma unroll
+        for (int it = 0; it < IT; it++) {
+            int i = q + QR * (warp + NW * it);
+            if (i < n) {
+                float m = traj_mu(T, tj, x, i);
+                re += (double)(m * psi[it].x);
+                im += (double)(m * psi[it].y);
+            }
+        }
+        for (int o = G; o < 32; o <<= 1) {
+            re += __shfl_xor_sync(0xffffffffu, re, o);
+            im += __shfl_xor_sync(0xffffffffu, im, o);
+        }
+        if (q == 0) { red[(warp * G + g) * 2] = re; red[(warp * G + g) * 2 + 1] = im; }
+        __syncthreads();
+        if (tid < G && blockIdx.x * G + tid < nvec) {
+            double sr = 0, si = 0;
+            for (int w = 0; w < NW; w++) { sr += red[(w * G + tid) * 2]; si += red[(w * G + tid) * 2 + 1]; }
+            resp[(size_t)(blockIdx.x * G + tid) * J.tmax + t1] = make_double2(sr, si);
+        }
+        if (t1 == J.tmax - 1) break;
+        const long fl = tj - P.f0;
+        int K = P.order[fl];
+        for (int o = 1; o < G; o <<= 1) K = max(K, __shfl_xor_sync(0xffffffffu, K, o));
+        const float ir = inv_r[fl], ir2 = 2.f * ir;
+        const float2 *cf = coef + fl * KC;
+        const float a0 = cf[0].x;
+#pragma unroll
+        for (int it = 0; it < IT; it++) {
+            int i = q + QR * (warp + NW * it);
+            if (i < n) {
+                dgs[(size_t)i * G + g] = traj_diag(T, tj, i, P.singleshift != 0);
+                cur[(size_t)i * RS + g] = psi[it];
+            }
+            prev[it] = psi[it];
+            psi[it].x *= a0;
+            psi[it].y *= a0;
+        }
+        for (int k = 1; k <= K; k++) {
+            __syncthreads();
+            const float2 a = cf[k];
+#pragma unroll
+            for (int it = 0; it < IT; it++) {
+                const int sl = warp + NW * it, i = q + QR * sl;
+                if (sl >= nslices) continue;
+                const int ic = i < n ? i : 0;
+                float2 z = cur[(size_t)ic * RS + g];
+                const float d = dgs[(size_t)ic * G + g];
+                float yr = d * z.x, yi = d * z.y;
+                const int b0 = sptr[sl], b1 = sptr[sl + 1];
+                int e = b0 + q;
+                float yr2 = 0.f, yi2 = 0.f;
+                for (; e + QR < b1; e += 2 * QR) {
+                    EllEnt<float> e0 = ell[e], e1 = ell[e + QR];
+                    float2 z0 = cur[e0.off + g], z1 = cur[e1.off + g];
+                    yr += e0.v * z0.x;
+                    yi += e0.v * z0.y;
+                    yr2 += e1.v * z1.x;
+                    yi2 += e1.v * z1.y;
+                }
+                if (e < b1) {
+                    EllEnt<float> e0 = ell[e];
+                    float2 z0 = cur[e0.off + g];
+                    yr += e0.v * z0.x;
+                    yi += e0.v * z0.y;
+                }
+                yr += yr2;
+                yi += yi2;
+                float2 tk;
+                if (k == 1) {
+                    tk.x = ir * yr;
+                    tk.y = ir * yi;
+                } else {
+                    tk.x = ir2 * yr - prev[it].x;
+                    tk.y = ir2 * yi - prev[it].y;
+                }
+                prev[it] = z;
+                nx[it] = tk;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int it = 0; it < IT; it++) {
+                const int sl = warp + NW * it, i = q + QR * sl;
+                if (sl >= nslices || i >= n) continue;
+                cur[(size_t)i * RS + g] = nx[it];
+                psi[it].x += a.x * nx[it].x - a.y * nx[it].y;
+                psi[it].y += a.x * nx[it].y + a.y * nx[it].x;
             }
         }
         __syncthreads();
@@ -659,6 +935,8 @@ int lanes_for(size_t bytes_per_lane, int want) {
     return b;
 }
 
+const size_t kMaxSmem = 227 * 1024;  // dynamic shared memory per CTA on sm_100
+
 template <typename K>
 int set_smem(K kernel, size_t bytes) {
     if (bytes > 48 * 1024)
@@ -699,6 +977,21 @@ int launch_abs_trotter(int prec, const DevTraj &T, const TrotterPlan &P, const A
     } else {
         if ((e = set_smem(k_abs_trotter<double>, smem))) return e;
         k_abs_trotter<double><<<grid, B, smem, s>>>(T, P, J, resp, nvec);
+    }
+    return (int)cudaGetLastError();
+}
+
+int launch_abs_trotter_lv(int prec, const DevTraj &T, const TrotterPlan &P, const AbsJob &J, double2 *resp,
+                          const int *perm, const int *lvptr, int nlev, int threads, cudaStream_t s) {
+    if (J.nsamp <= 0) return 0;
+    const size_t smem = (size_t)3 * P.n * ((prec == 0 ? sizeof(float2) : sizeof(double2)) + sizeof(float));
+    int e;
+    if (prec == 0) {
+        if ((e = set_smem(k_abs_trotter_lv<float>, smem))) return e;
+        k_abs_trotter_lv<float><<<J.nsamp, threads, smem, s>>>(T, P, J, resp, perm, lvptr, nlev);
+    } else {
+        if ((e = set_smem(k_abs_trotter_lv<double>, smem))) return e;
+        k_abs_trotter_lv<double><<<J.nsamp, threads, smem, s>>>(T, P, J, resp, perm, lvptr, nlev);
     }
     return (int)cudaGetLastError();
 }
@@ -761,8 +1054,23 @@ static int run_taylor2(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, d
 
 size_t taylor3_smem(const TaylorPlan &P, size_t rsz) {
     size_t ent = rsz == 4 ? 8 : 16;
-    return (size_t)P.n * 10 * 2 * rsz + (size_t)P.ell_nent * ent + sizeof(int) * (P.ell_nslices + 1) + 16 +
+    return (size_t)P.n * NISE_T3_ROW * 2 * rsz + (size_t)P.ell_nent * ent + sizeof(int) * (P.ell_nslices + 1) + 16 +
            16 * 8 * 2 * sizeof(double);
+}
+
+size_t cheb3_smem(const TaylorPlan &P) {
+    return (size_t)P.n * NISE_T3_ROW * sizeof(float2) + (size_t)P.n * 8 * sizeof(float) + (size_t)P.ell_nent * 8 +
+           sizeof(int) * (P.ell_nslices + 1) + 16 + 16 * 8 * 2 * sizeof(double);
+}
+
+template <int IT>
+static int run_cheb3(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int nvec, cudaStream_t s) {
+    size_t smem = cheb3_smem(P);
+    int e;
+    if ((e = set_smem(k_abs_cheb3<IT>, smem))) return e;
+    k_abs_cheb3<IT><<<(nvec + 7) / 8, 512, smem, s>>>(T, P, J, resp, nvec, (const EllEnt<float> *)P.ell, P.ell_sptr,
+                                                      P.ell_nslices, P.ell_nent, P.cheb_inv_r, P.cheb_coef);
+    return (int)cudaGetLastError();
 }
 
 template <typename R, int IT>
@@ -780,7 +1088,22 @@ static int run_taylor3(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, d
 
 int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp,
                       int vec_per_cta, cudaStream_t s) {
-    if (P.static_j && P.ell && vec_per_cta > 4 && taylor3_smem(P, prec == 0 ? 4 : 8) <= 220 * 1024) {
+    if (P.cheb_coef) {  // Chebyshev tables present: the FP32 sliced-ELL Chebyshev kernel
+        if (prec != 0 || !P.ell || cheb3_smem(P) > kMaxSmem) return (int)cudaErrorNotSupported;
+        int nvec = 3 * J.nsamp;
+        int it = (P.ell_nslices + 15) / 16;
+        if (it > 32) return (int)cudaErrorNotSupported;
+        int IT = it <= 1 ? 1 : it <= 2 ? 2 : it <= 4 ? 4 : it <= 8 ? 8 : it <= 16 ? 16 : 32;
+        switch (IT) {
+        case 1: return run_cheb3<1>(T, P, J, resp, nvec, s);
+        case 2: return run_cheb3<2>(T, P, J, resp, nvec, s);
+        case 4: return run_cheb3<4>(T, P, J, resp, nvec, s);
+        case 8: return run_cheb3<8>(T, P, J, resp, nvec, s);
+        case 16: return run_cheb3<16>(T, P, J, resp, nvec, s);
+        default: return run_cheb3<32>(T, P, J, resp, nvec, s);
+        }
+    }
+    if (!P.only_v2 && P.static_j && P.ell && vec_per_cta > 4 && taylor3_smem(P, prec == 0 ? 4 : 8) <= 220 * 1024) {
         int nvec = 3 * J.nsamp;
         int it = (P.ell_nslices + 15) / 16;  // 16 warps, one slice (4 rows) per warp instruction
         int IT = it <= 1 ? 1 : it <= 2 ? 2 : it <= 4 ? 4 : it <= 8 ? 8 : it <= 16 ? 16 : 32;
@@ -805,12 +1128,15 @@ int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const Abs
         // thread IT = ceil(n / (16 * 32 / G)).
         int nvec = 3 * J.nsamp;
         if (P.static_j) {
+            const size_t r2 = prec == 0 ? sizeof(float2) : sizeof(double2);
+            auto t2_smem = [&](int g) { return 2 * (size_t)P.n * (g + 2) * r2 + 16 * (size_t)g * 2 * sizeof(double); };
             int G = vec_per_cta <= 4 ? 4 : 8;
             if (prec != 0) G = 4;
+            if (G == 8 && t2_smem(8) > kMaxSmem) G = 4;
             int per_iter = 16 * (32 / G);
             int it = (P.n + per_iter - 1) / per_iter;
             int IT = it <= 1 ? 1 : it <= 2 ? 2 : it <= 4 ? 4 : it <= 8 ? 8 : it <= 16 ? 16 : 32;
-            if (it <= 32) {
+            if (it <= 32 && t2_smem(G) <= kMaxSmem) {
 #define T2(R, GG)                                                                              \
     switch (IT) {                                                                              \
     case 1: return run_taylor2<R, GG, 1>(T, P, J, resp, nvec, s);                              \
@@ -833,6 +1159,12 @@ int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const Abs
     int rpt = (P.n + 511) / 512;
     if (rpt > 4 || !P.static_j) return (int)cudaErrorNotSupported;
     rpt = rpt <= 1 ? 1 : (rpt <= 2 ? 2 : 4);
+    {  // k_abs_taylor keeps two full copies of G vectors: fall back to G = 3 where 8 (4) does not fit
+        const size_t r2 = prec == 0 ? sizeof(float2) : sizeof(double2);
+        const int gbig = prec == 0 ? 8 : 4;
+        if (2 * (size_t)P.n * gbig * r2 + 16 * 2 * (size_t)gbig * sizeof(double) > kMaxSmem) vec_per_cta = 3;
+        if (2 * (size_t)P.n * 3 * r2 + 16 * 2 * 3 * sizeof(double) > kMaxSmem) return (int)cudaErrorNotSupported;
+    }
 #define TAY(R, G)                                                                                  \
     do {                                                                                           \
         if (rpt == 1) return run_taylor<R, G, 1>(T, P, J, resp, nvec, s);                          \
@@ -847,6 +1179,15 @@ int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const Abs
         TAY(double, 4);
     }
 #undef TAY
+}
+
+int launch_prep_cheb(const DevTraj &T, TaylorPlan &P, double rowabs_max, double f, int *order, float *inv_r,
+                     float2 *coef, cudaStream_t s) {
+    if (P.nf) k_prep_cheb<<<(P.nf + 127) / 128, 128, 0, s>>>(T, P, rowabs_max, f, 1e-10, order, inv_r, coef);
+    P.order = order;
+    P.cheb_inv_r = inv_r;
+    P.cheb_coef = coef;
+    return (int)cudaGetLastError();
 }
 
 int launch_pattern_scan(const DevTraj &T, long f0, long nf, int *flag, cudaStream_t s) {

@@ -1,0 +1,756 @@
+// Linear absorption jobs (absorption.c:18-202): planning, enqueueing and
+// collection of one context's job, the launch autotuner, and the batch API
+// that runs many contexts' jobs as one CUDA graph.
+//
+// A job is split so that everything that allocates or synchronises happens
+// in plan() (validation, coupling pattern, CSR/ELL tables, rotation levels,
+// device buffers, autotuning) and enqueue() only launches kernels on a given
+// stream.  nise_absorption runs plan/enqueue/collect on the context's stream;
+// nise_batch_create plans every job, then captures all enqueues, each on its
+// own forked stream, into one graph that nise_batch_run launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "eigen.h"
+#include "engine.h"
+#include "nise_b200.h"
+#include "nise_internal.h"
+
+namespace {
+
+enum Scheme { SCHEME_TROTTER, SCHEME_RK4, SCHEME_TAYLOR, SCHEME_EIGEN };
+
+// Launch configurations the autotuner chooses from.
+//   Trotter: 0 = thread per vector (k_abs_trotter), T > 0 = level-scheduled
+//            rotations with T threads per start point (k_abs_trotter_lv);
+//            all are bitwise identical.
+//   Taylor:  3 = k_abs_taylor2 with 4 vectors per CTA, 8 = the sliced-ELL
+//            kernel with 8 (k_abs_taylor2 with 8 where it does not fit),
+//            -8 = k_abs_taylor2 with 8, 10 = the FP32 sliced-ELL kernel with
+//            the Chebyshev expansion of the step (k_abs_cheb3).
+typedef std::tuple<int, int, int, int, int> TuneKey;  // scheme, precision, sites, couplings, static
+std::map<TuneKey, int> g_tuned;
+std::mutex g_tune_mu;
+
+int default_config(int scheme, int N, bool plain, bool cheb) {
+    if (scheme == SCHEME_TROTTER) return N >= 96 ? 128 : 0;
+    if (plain) return 3;  // one start point per launch: 3 vectors
+    (void)cheb;           // the Chebyshev kernel is a tuned alternative: fewer terms, more work per term
+    return 8;
+}
+
+// Rotation levels of the lexicographic coupling list: perm holds the
+// rotation indices ordered by (level, index), lvptr the level boundaries.
+void rotation_levels(const std::vector<int2> &pairs, int n, std::vector<int> &perm, std::vector<int> &lvptr) {
+    std::vector<int> last(n, 0), lv(pairs.size());
+    int nlev = 0;
+    for (size_t k = 0; k < pairs.size(); k++) {
+        int l = std::max(last[pairs[k].x], last[pairs[k].y]) + 1;
+        last[pairs[k].x] = last[pairs[k].y] = l;
+        lv[k] = l - 1;
+        nlev = std::max(nlev, l);
+    }
+    lvptr.assign(nlev + 1, 0);
+    for (int l : lv) lvptr[l + 1]++;
+    for (int l = 0; l < nlev; l++) lvptr[l + 1] += lvptr[l];
+    perm.assign(pairs.size(), 0);
+    std::vector<int> fill(lvptr.begin(), lvptr.end() - 1);
+    for (size_t k = 0; k < pairs.size(); k++) perm[fill[lv[k]]++] = (int)k;
+}
+
+}  // namespace
+
+struct AbsRun {
+    nise_ctx *c = nullptr;
+    int N = 0, tmax = 0, prec = 0, begin = 0, end = 0, nsamp = 0, nvec = 0;
+    long f0 = 0, nf = 0;
+    bool plain = false;
+    int scheme = SCHEME_TROTTER;
+    int config = 0;
+    DevTraj T;
+    AbsJob J;
+    DevBuf<double2> resp, out;
+    // Trotter
+    DevBuf<int2> dpairs;
+    DevBuf<char> U, rot;
+    DevBuf<int> perm, lvptr;
+    int nlev = 0;
+    TrotterPlan TP;
+    // RK4
+    DevBuf<int2> dent;
+    DevBuf<char> rkval;
+    Rk4Plan RP;
+    // Taylor
+    DevBuf<int> drp, dcol, dorder, dsptr, dcorder;
+    DevBuf<char> dval, dell;
+    DevBuf<float> dinvr;
+    DevBuf<float2> dcoef;
+    TaylorPlan XP;
+    double rowabs = 0;
+    bool cheb = false;  // Chebyshev tables allocated (FP32, sliced ELL fits)
+    // eigen route
+    DevBuf<char> Ue;
+    DevBuf<long> efr;
+    DevBuf<double> eV, ew;
+    long FC = 1;
+    bool truncated = false;
+    double fe = 0;
+    // work accounting
+    std::vector<long> cross;
+    long vec_steps = 0;
+
+    int plan(nise_ctx *ctx, bool autotune);
+    int enqueue(cudaStream_t s, bool events);
+    int run_main(cudaStream_t s, int cfg, double2 *dst);
+    double flops() const;
+    int tune();
+};
+
+int AbsRun::plan(nise_ctx *ctx, bool autotune) {
+    c = ctx;
+    if (!c->loaded) return nise_fail(c, NISE_ERR_STATE, "no trajectory loaded");
+    const nise_params &p = c->p;
+    N = c->n;
+    tmax = p.tmax1;
+    prec = p.precision;
+    // determine_samples (NISE_subs.c:197-221)
+    int n_samples = (p.length - p.tmax1 - 1) / p.sample + 1;
+    if (n_samples <= 0) return nise_fail(c, NISE_ERR_ARG, "Insufficient data to calculate spectrum.");
+    end = p.end == 0 ? n_samples : p.end;
+    if (end > n_samples) return nise_fail(c, NISE_ERR_ARG, "Endpoint larger than number of samples was specified.");
+    begin = p.begin;
+    if (begin < 0 || begin >= end) return nise_fail(c, NISE_ERR_ARG, "BeginPoint must be below EndPoint");
+    nsamp = end - begin;
+    nvec = 3 * nsamp;
+    f0 = (long)begin * p.sample;
+    long f1 = (long)(end - 1) * p.sample + tmax - 1;  // last frame read
+    int rc;
+    if ((rc = nise_check_frames(c, f1))) return rc;
+    nf = f1 - f0;  // frames propagated through: [f0, f1)
+    if (nf < 1) nf = 1;
+    T = nise_devtraj(c);
+    memset(&J, 0, sizeof(J));
+    J.begin = begin;
+    J.nsamp = nsamp;
+    J.sample = p.sample;
+    J.tmax = tmax;
+    J.ts = p.ts;
+    J.f = nise_f64(p, 1, 1);
+    J.f32_sub = nise_f32(p, 1, p.ts);
+    J.f64_sub = nise_f64(p, 1, p.ts);
+    J.f32_full = nise_f32(p, 1, 1);
+    plain = p.launch_mode == NISE_PLAIN;
+    if ((rc = resp.alloc(c, (size_t)nvec * tmax)) || (rc = out.alloc(c, tmax))) return rc;
+    cross.assign(nf, 0);
+    for (int s = 0; s < nsamp; s++) {
+        long a = (long)(begin + s) * p.sample - f0;
+        for (int t = 0; t < tmax - 1; t++) cross[a + t] += 3;
+    }
+    vec_steps = 3L * nsamp * (tmax - 1);
+    // bytes: every frame read once (diagonal or full record) and the dipoles
+    c->last_bytes = (double)nf * 4 * (p.hamiltonian == NISE_HAM_COUPLING ? N : c->nn2) +
+                    (double)(p.hamiltonian == NISE_HAM_COUPLING ? 3 * N : (nf + 1) * 3L * N) * 4;
+    const size_t rsz = prec == NISE_FP32 ? sizeof(float) : sizeof(double), r2 = 2 * rsz;
+
+    if (p.propagation == NISE_PROP_COUPLING) {
+        scheme = SCHEME_TROTTER;
+        std::vector<int2> pairs;
+        if ((rc = nise_pattern(c, f0, nf, pairs))) return rc;
+        memset(&TP, 0, sizeof(TP));
+        TP.n = N;
+        TP.k = (int)pairs.size();
+        TP.f0 = f0;
+        TP.nf = nf;
+        TP.rot_static = p.hamiltonian == NISE_HAM_COUPLING;
+        TP.singleshift = c->nshift > 0;
+        std::vector<int> hperm, hlv;
+        rotation_levels(pairs, N, hperm, hlv);
+        nlev = (int)hlv.size() - 1;
+        if ((rc = dpairs.upload(c, pairs.empty() ? std::vector<int2>(1) : pairs)) ||
+            (rc = U.alloc(c, r2 * (size_t)nf * N)) ||
+            (rc = rot.alloc(c, r2 * (size_t)(TP.rot_static ? 1 : nf) * (TP.k ? TP.k : 1))) ||
+            (rc = perm.upload(c, hperm.empty() ? std::vector<int>(1) : hperm)) || (rc = lvptr.upload(c, hlv)))
+            return rc;
+        TP.pairs = dpairs.p;
+        TP.U = U.p;
+        TP.rot = rot.p;
+    } else if (p.propagation == NISE_PROP_RK4) {
+        scheme = SCHEME_RK4;
+        std::vector<int2> pairs, ent;
+        if ((rc = nise_pattern(c, f0, nf, pairs))) return rc;
+        size_t q = 0;
+        for (int a = 0; a < N; a++) {  // propagate.c:294-305 order: (a,a) then (a,b>a)
+            ent.push_back(make_int2(a, a));
+            while (q < pairs.size() && pairs[q].x == a) ent.push_back(pairs[q++]);
+        }
+        memset(&RP, 0, sizeof(RP));
+        RP.n = N;
+        RP.k = (int)ent.size();
+        RP.f0 = f0;
+        RP.nf = nf;
+        RP.singleshift = c->nshift > 0;
+        if ((rc = dent.upload(c, ent)) || (rc = rkval.alloc(c, rsz * (size_t)nf * RP.k))) return rc;
+        RP.entries = dent.p;
+        RP.val = rkval.p;
+    } else {
+        // Sparse / Diagonal: the exact propagator exp(-i H dt) (propagate_vec_DIA,
+        // propagate.c:60-125).  Threshold > 0 keeps only large elements of U
+        // (propagate_vec_DIA_S, propagate.c:185-258) and needs the explicit
+        // eigen propagator, as do per-frame couplings (HamiltonianType Full)
+        // and the Diagonal scheme up to NISE_EIG_MAX_N sites.  Otherwise the
+        // static couplings go through the sparse Taylor series.
+        truncated = c->thres != 0 && !(c->thres > 1);
+        const bool eigen_route = truncated || p.hamiltonian != NISE_HAM_COUPLING ||
+                                 (p.propagation == NISE_PROP_DIAGONAL && N <= NISE_EIG_MAX_N);
+        if (eigen_route) {
+            scheme = SCHEME_EIGEN;
+            if (N > NISE_EIG_MAX_N)
+                return nise_fail(c, NISE_ERR_UNSUPPORTED,
+                                 truncated ? "Sparse with Threshold > 0 is limited to 120 sites (eigen route)"
+                                           : "exact propagation of per-frame couplings (HamiltonianType Full) is "
+                                             "limited to 120 sites (eigen route)");
+            const size_t ubytes = r2 * (size_t)nf * N * N;
+            if (ubytes > ((size_t)64 << 30))
+                return nise_fail(c, NISE_ERR_NOMEM,
+                                 "eigen route: %ld frames of %d sites need more than 64 GB of propagators", nf, N);
+            std::vector<long> frames(nf);
+            for (long t = 0; t < nf; t++) frames[t] = f0 + t;
+            FC = std::max(1L, std::min(nf, (long)(((size_t)512 << 20) / (sizeof(double) * (size_t)N * N))));
+            if ((rc = Ue.alloc(c, ubytes)) || (rc = efr.upload(c, frames)) || (rc = eV.alloc(c, (size_t)FC * N * N)) ||
+                (rc = ew.alloc(c, (size_t)FC * N)))
+                return rc;
+            // propagate_vec_DIA: f = deltat*icm2ifs*twoPi*sign in float, one full step
+            fe = prec == NISE_FP32 ? (double)J.f32_full : J.f;
+        } else {
+            scheme = SCHEME_TAYLOR;
+            // CSR of the static couplings (read cut applied, |J| >= cut kept)
+            std::vector<int> rp(N + 1, 0), col;
+            std::vector<double> vd;
+            for (int i = 0; i < N; i++) {
+                double rs = 0;
+                for (int j = 0; j < N; j++) {
+                    if (j == i) continue;
+                    int a = i < j ? i : j, b = i < j ? j : i;
+                    float v = c->h_hc[b + (long)a * ((N << 1) - a - 1) / 2];
+                    if (v != 0.0f) {
+                        col.push_back(j);
+                        vd.push_back(v);
+                        rs += fabs(v);
+                    }
+                }
+                rp[i + 1] = (int)col.size();
+                rowabs = rs > rowabs ? rs : rowabs;
+            }
+            if ((rc = drp.upload(c, rp)) || (rc = dcol.upload(c, col.empty() ? std::vector<int>(1, 0) : col)))
+                return rc;
+            if (prec == NISE_FP32) {
+                std::vector<float> vf(vd.begin(), vd.end());
+                if (vf.empty()) vf.push_back(0);
+                if ((rc = dval.alloc(c, sizeof(float) * vf.size()))) return rc;
+                cudaMemcpyAsync(dval.p, vf.data(), sizeof(float) * vf.size(), cudaMemcpyHostToDevice, c->stream);
+            } else {
+                std::vector<double> v2 = vd;
+                if (v2.empty()) v2.push_back(0);
+                if ((rc = dval.alloc(c, sizeof(double) * v2.size()))) return rc;
+                cudaMemcpyAsync(dval.p, v2.data(), sizeof(double) * v2.size(), cudaMemcpyHostToDevice, c->stream);
+            }
+            if ((rc = dorder.alloc(c, (size_t)nf))) return rc;
+            // sliced ELL (4-row slices, [slot][row]) of the same couplings for the
+            // shared-memory kernel; entry offsets address rows of NISE_T3_ROW
+            // complex numbers.  Each row lists its neighbours of the other
+            // parity first: the four rows of a slice alternate in parity, so a
+            // slot whose rows all pick the same relative parity gathers two even
+            // and two odd rows, which share no shared-memory banks (FP32).
+            std::vector<int> ecol(col.size());
+            std::vector<double> evd(col.size());
+            for (int i = 0; i < N; i++) {
+                int w = rp[i];
+                for (int pass = 0; pass < 2; pass++)
+                    for (int q = rp[i]; q < rp[i + 1]; q++)
+                        if ((((col[q] ^ i) & 1) == 1) == (pass == 0)) {
+                            ecol[w] = col[q];
+                            evd[w] = vd[q];
+                            w++;
+                        }
+            }
+            const int nsl = (N + 3) / 4;
+            std::vector<int> sptr(nsl + 1, 0);
+            for (int sl = 0; sl < nsl; sl++) {
+                int L = 0;
+                for (int r = 0; r < 4; r++) {
+                    int row = 4 * sl + r;
+                    if (row < N) L = std::max(L, rp[row + 1] - rp[row]);
+                }
+                sptr[sl + 1] = sptr[sl] + 4 * L;
+            }
+            const int nent = sptr[nsl];
+            const size_t esz = prec == NISE_FP32 ? 8 : 16;
+            std::vector<unsigned char> ell((size_t)(nent > 0 ? nent : 1) * esz, 0);
+            for (int sl = 0; sl < nsl; sl++) {
+                int L = (sptr[sl + 1] - sptr[sl]) / 4;
+                for (int slot = 0; slot < L; slot++)
+                    for (int r = 0; r < 4; r++) {
+                        int row = 4 * sl + r, e = sptr[sl] + slot * 4 + r;
+                        int off = (row < N ? row : 0) * NISE_T3_ROW;
+                        double v = 0;
+                        if (row < N && slot < rp[row + 1] - rp[row]) {
+                            off = ecol[rp[row] + slot] * NISE_T3_ROW;
+                            v = evd[rp[row] + slot];
+                        }
+                        unsigned char *dst = ell.data() + (size_t)e * esz;
+                        memcpy(dst, &off, 4);
+                        if (prec == NISE_FP32) {
+                            float fv = (float)v;
+                            memcpy(dst + 4, &fv, 4);
+                        } else {
+                            memcpy(dst + 8, &v, 8);
+                        }
+                    }
+            }
+            if ((rc = dell.alloc(c, ell.size()))) return rc;
+            cudaMemcpyAsync(dell.p, ell.data(), ell.size(), cudaMemcpyHostToDevice, c->stream);
+            if ((rc = dsptr.upload(c, sptr))) return rc;
+            memset(&XP, 0, sizeof(XP));
+            XP.n = N;
+            XP.nnz = (int)col.size();
+            XP.row_ptr = drp.p;
+            XP.col = dcol.p;
+            XP.val = dval.p;
+            XP.static_j = 1;
+            XP.ell = dell.p;
+            XP.ell_sptr = dsptr.p;
+            XP.ell_nslices = nsl;
+            XP.ell_nent = nent;
+            XP.f0 = f0;
+            XP.nf = nf;
+            XP.singleshift = c->nshift > 0;
+            // Chebyshev kernel: FP32, its shared-memory footprint (state, diagonal, ELL)
+            const size_t csm = (size_t)N * NISE_T3_ROW * 8 + (size_t)N * 32 + (size_t)nent * 8 + 4 * (nsl + 1) + 4096;
+            cheb = prec == NISE_FP32 && csm <= 227 * 1024 && (nsl + 15) / 16 <= 32;
+            if (cheb && ((rc = dcorder.alloc(c, (size_t)nf)) || (rc = dinvr.alloc(c, (size_t)nf)) ||
+                         (rc = dcoef.alloc(c, (size_t)nf * (NISE_CHEB_KMAX + 1)))))
+                return rc;
+        }
+    }
+    config = default_config(scheme, N, plain, cheb);
+    if (p.kernel_config != 0) {  // forced by the caller
+        const int k = p.kernel_config;
+        if (scheme == SCHEME_TROTTER && (k == 1 || k == 64 || k == 128 || k == 256)) config = k == 1 ? 0 : k;
+        else if (scheme == SCHEME_TAYLOR && (k == 3 || k == 8 || k == 9 || (k == 10 && cheb)))
+            config = k == 9 ? -8 : k;
+        else return nise_fail(c, NISE_ERR_ARG, "kernel_config %d does not apply to this scheme", k);
+        return NISE_OK;
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tuned.find(TuneKey(scheme, prec, N, scheme == SCHEME_TROTTER ? TP.k : 0,
+                                       scheme == SCHEME_TROTTER ? TP.rot_static : 0));
+        if (it != g_tuned.end()) config = it->second;
+    }
+    if (autotune && (scheme == SCHEME_TROTTER || scheme == SCHEME_TAYLOR) && !plain)
+        if ((rc = tune())) return rc;
+    return NISE_OK;
+}
+
+// The propagation kernel(s) of the job with launch configuration cfg.
+int AbsRun::run_main(cudaStream_t s, int cfg, double2 *dst) {
+    const int pr = prec == NISE_FP32 ? 0 : 1;
+    int e = 0;
+    auto one = [&](const AbsJob &Js, double2 *r) -> int {
+        switch (scheme) {
+        case SCHEME_TROTTER:
+            if (cfg > 0) return launch_abs_trotter_lv(pr, T, TP, Js, r, perm.p, lvptr.p, nlev, cfg, s);
+            return launch_abs_trotter(pr, T, TP, Js, r, s);
+        case SCHEME_RK4:
+            return launch_abs_rk4(pr, T, RP, Js, r, s);
+        case SCHEME_TAYLOR: {
+            TaylorPlan P = XP;
+            P.only_v2 = cfg < 0;
+            if (cfg == 10) {
+                P.order = dcorder.p;
+                P.cheb_inv_r = dinvr.p;
+                P.cheb_coef = dcoef.p;
+            } else {
+                P.order = dorder.p;
+                P.cheb_inv_r = nullptr;
+                P.cheb_coef = nullptr;
+            }
+            return launch_abs_taylor(pr, T, P, Js, r, cfg == 10 ? 8 : cfg < 0 ? -cfg : cfg, s);
+        }
+        default:
+            return launch_abs_dia(pr, T, Ue.p, f0, N, Js, r, s);
+        }
+    };
+    if (plain) {
+        for (int q = 0; q < nsamp && !e; q++) {
+            AbsJob Js = J;
+            Js.begin = begin + q;
+            Js.nsamp = 1;
+            e = one(Js, dst + (size_t)3 * q * tmax);
+            c->launches++;
+        }
+    } else {
+        e = one(J, dst);
+        c->launches++;
+    }
+    return e;
+}
+
+// Time every candidate configuration on the job itself (into the response
+// buffer, which enqueue() overwrites) and keep the fastest.
+int AbsRun::tune() {
+    std::vector<int> cand;
+    if (scheme == SCHEME_TROTTER) {
+        cand = {0, 64, 128, 256};
+    } else {
+        cand = {3, -8, 8};
+        if (cheb) cand.push_back(10);
+    }
+    // the tables the kernels read (both series for the Taylor route)
+    int rc;
+    if ((rc = enqueue(c->stream, false))) return rc;
+    if (scheme == SCHEME_TAYLOR) {
+        TaylorPlan P = XP;
+        if ((rc = nise_cuda(c, launch_prep_taylor(prec, T, P, rowabs, J.f, dorder.p, c->stream), "Taylor prep")))
+            return rc;
+        if (cheb && (rc = nise_cuda(c, launch_prep_cheb(T, P, rowabs, J.f, dcorder.p, dinvr.p, dcoef.p, c->stream),
+                                    "Chebyshev prep")))
+            return rc;
+    }
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    float best = 1e30f;
+    int best_cfg = config;
+    for (int cfg : cand) {
+        cudaEventRecord(a, c->stream);
+        int e = run_main(c->stream, cfg, resp.p);
+        cudaEventRecord(b, c->stream);
+        if (e) continue;  // a configuration that cannot launch (shared memory) is skipped
+        if (cudaEventSynchronize(b) != cudaSuccess) break;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        if (ms < best) {
+            best = ms;
+            best_cfg = cfg;
+        }
+    }
+    cudaGetLastError();
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    config = best_cfg;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[TuneKey(scheme, prec, N, scheme == SCHEME_TROTTER ? TP.k : 0,
+                    scheme == SCHEME_TROTTER ? TP.rot_static : 0)] = best_cfg;
+    return nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "autotuner");
+}
+
+// Kernels of the job on stream s: tables, propagation, response sum.
+int AbsRun::enqueue(cudaStream_t s, bool events) {
+    const int pr = prec == NISE_FP32 ? 0 : 1;
+    int rc;
+    if (events) cudaEventRecord(c->evk0, s);
+    switch (scheme) {
+    case SCHEME_TROTTER:
+        if ((rc = nise_cuda(c, launch_prep_trotter(prec, T, TP, J.f64_sub, J.f32_sub, s), "Trotter prep"))) return rc;
+        c->launches += 1 + (TP.rot_static ? 1 : 0);
+        break;
+    case SCHEME_RK4:
+        if ((rc = nise_cuda(c, launch_prep_rk4(prec, T, RP, J.f64_sub, J.f32_sub, s), "RK4 prep"))) return rc;
+        c->launches++;
+        break;
+    case SCHEME_TAYLOR: {
+        TaylorPlan P = XP;
+        if (config == 10)
+            rc = nise_cuda(c, launch_prep_cheb(T, P, rowabs, J.f, dcorder.p, dinvr.p, dcoef.p, s), "Chebyshev prep");
+        else
+            rc = nise_cuda(c, launch_prep_taylor(prec, T, P, rowabs, J.f, dorder.p, s), "Taylor prep");
+        if (rc) return rc;
+        c->launches++;
+        break;
+    }
+    default: {
+        EigJob EJ;
+        EJ.T = T;
+        EJ.n = N;
+        EJ.singleshift = c->nshift > 0;
+        const size_t r2 = prec == NISE_FP32 ? sizeof(float2) : sizeof(double2);
+        for (long q = 0; q < nf; q += FC) {
+            long m = std::min(FC, nf - q);
+            if ((rc = nise_cuda(c, launch_eig(EJ, efr.p + q, m, eV.p, ew.p, s), "eigensolver"))) return rc;
+            if ((rc = nise_cuda(c, launch_build_u(pr, eV.p, ew.p, m, N, fe, c->thres, truncated,
+                                                  Ue.p + r2 * (size_t)q * N * N, s),
+                                "propagator build")))
+                return rc;
+            c->launches += 2;
+        }
+    }
+    }
+    if ((rc = nise_cuda(c, run_main(s, config, resp.p), "propagation"))) return rc;
+    if (events) cudaEventRecord(c->evk1, s);
+    if ((rc = nise_cuda(c, launch_reduce_resp(resp.p, nvec, tmax, out.p, s), "response reduction"))) return rc;
+    c->launches++;
+    return NISE_OK;
+}
+
+// Algorithmic flops of the propagation (after the job ran: the Taylor orders
+// are read back from the device).
+double AbsRun::flops() const {
+    const nise_params &p = c->p;
+    switch (scheme) {
+    case SCHEME_TROTTER:
+        // per vector step: ts * (K rotations * 12 flops + 2 N half-phases * 6 flops)
+        return (double)vec_steps * p.ts * (12.0 * TP.k + 12.0 * N);
+    case SCHEME_RK4:
+        // per sub-step: 4 stages over the list (off-diagonal entries twice) + update and norms
+        return (double)vec_steps * p.ts * (4.0 * 4.0 * (2.0 * RP.k - N) + 20.0 * N);
+    case SCHEME_TAYLOR: {
+        // per vector step and Taylor order: nnz complex*real products (4 flops)
+        // and the diagonal, scaling and accumulation (6 flops per site)
+        // (Chebyshev: the same products per term plus the recurrence, 10 flops per site)
+        std::vector<int> order(nf);
+        cudaMemcpy(order.data(), config == 10 ? dcorder.p : dorder.p, sizeof(int) * nf, cudaMemcpyDeviceToHost);
+        double orders = 0;
+        for (long t = 0; t < nf; t++) orders += (double)order[t] * cross[t];
+        return orders * (4.0 * XP.nnz + (config == 10 ? 10.0 : 6.0) * N);
+    }
+    default:
+        return (double)nf * 6.7 * N * (double)N * N + (double)vec_steps * 8.0 * N * N;
+    }
+}
+
+extern "C" int nise_absorption(nise_ctx *c, double *re_S, double *im_S, int *samples) {
+    if (!c || !re_S || !im_S || !samples) return nise_fail(c, NISE_ERR_ARG, "null argument");
+    cudaSetDevice(c->p.device);
+    AbsRun R;
+    c->launches = 0;
+    c->last_flops = c->last_bytes = 0;
+    int rc;
+    if ((rc = R.plan(c, false))) return rc;
+    cudaEventRecord(c->ev0, c->stream);
+    if ((rc = R.enqueue(c->stream, true))) return rc;
+    cudaEventRecord(c->ev1, c->stream);
+    std::vector<double2> h(R.tmax);
+    cudaMemcpyAsync(h.data(), R.out.p, sizeof(double2) * R.tmax, cudaMemcpyDeviceToHost, c->stream);
+    if ((rc = nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "absorption"))) return rc;
+    nise_collect_timing(c);
+    c->last_flops = R.flops();
+    for (int t = 0; t < R.tmax; t++) {
+        re_S[t] = h[t].x;
+        im_S[t] = h[t].y;
+    }
+    *samples = R.end;  // absorption.c:185 divides by `samples`, which equals end after the loop
+    return NISE_OK;
+}
+
+extern "C" int nise_absorption_tune(nise_ctx *c) {
+    if (!c) return nise_fail(nullptr, NISE_ERR_ARG, "null context");
+    cudaSetDevice(c->p.device);
+    AbsRun R;
+    c->launches = 0;
+    return R.plan(c, true);
+}
+
+// ------------------------------------------------------------------ batch
+struct nise_batch {
+    std::vector<nise_ctx *> ctx;
+    std::vector<std::unique_ptr<AbsRun>> runs;
+    std::vector<std::unique_ptr<DevBuf<double2>>> spec, fftin;
+    std::vector<FftJob> fj;
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> done;
+    cudaStream_t master = nullptr;
+    cudaEvent_t start = nullptr, stop = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<std::vector<double2>> host_out, host_spec;
+    double last_ms = 0;
+    std::vector<double> job_ms;
+    int device = 0;
+    std::string err;
+};
+
+static int batch_fail(nise_batch *b, int code, const std::string &msg) {
+    b->err = msg;
+    nise_set_global_error(msg.c_str());
+    return code;
+}
+
+extern "C" void nise_batch_destroy(nise_batch *b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    if (b->master) cudaStreamSynchronize(b->master);
+    for (auto s : b->side) cudaStreamDestroy(s);
+    for (auto e : b->done) cudaEventDestroy(e);
+    if (b->start) cudaEventDestroy(b->start);
+    if (b->stop) cudaEventDestroy(b->stop);
+    b->spec.clear();
+    b->fftin.clear();
+    b->runs.clear();
+    if (b->master) cudaStreamDestroy(b->master);
+    delete b;
+}
+
+extern "C" int nise_batch_create(nise_ctx *const *ctxs, int n, int autotune, nise_batch **out) {
+    if (!ctxs || n <= 0 || !out) return nise_fail(nullptr, NISE_ERR_ARG, "nise_batch_create: bad arguments");
+    *out = nullptr;
+    nise_batch *b = new nise_batch();
+    b->device = ctxs[0]->p.device;
+    cudaSetDevice(b->device);
+    for (int i = 0; i < n; i++) {
+        nise_ctx *c = ctxs[i];
+        if (!c || c->p.device != b->device) {
+            nise_batch_destroy(b);
+            return nise_fail(nullptr, NISE_ERR_ARG, "nise_batch_create: all contexts must be valid and on one device");
+        }
+        b->ctx.push_back(c);
+        b->runs.emplace_back(new AbsRun());
+        c->launches = 0;
+        int rc = b->runs.back()->plan(c, autotune != 0);
+        if (rc) {
+            std::string m = "job " + std::to_string(i) + ": " + c->err;
+            nise_batch_destroy(b);
+            return nise_fail(nullptr, rc, "%s", m.c_str());
+        }
+        const nise_params &p = c->p;
+        FftJob J;
+        J.tmax = p.tmax1;
+        J.fft = p.fft < p.tmax1 ? p.tmax1 : p.fft;
+        J.samples = b->runs.back()->end;
+        J.window = p.window;
+        J.fp32 = p.precision == NISE_FP32;
+        J.deltat = p.deltat;
+        J.lifetime = p.lifetime;
+        J.homogen = p.homogen;
+        J.inhomogen = p.inhomogen;
+        b->fj.push_back(J);
+        b->spec.emplace_back(new DevBuf<double2>());
+        b->fftin.emplace_back(new DevBuf<double2>());
+        if ((rc = b->spec.back()->alloc(c, J.fft)) || (rc = b->fftin.back()->alloc(c, J.fft))) {
+            nise_batch_destroy(b);
+            return rc;
+        }
+    }
+    for (auto c : b->ctx) cudaStreamSynchronize(c->stream);  // tables and buffers in place
+    if (cudaStreamCreateWithFlags(&b->master, cudaStreamNonBlocking) || cudaEventCreate(&b->start) ||
+        cudaEventCreate(&b->stop)) {
+        nise_batch_destroy(b);
+        return nise_fail(nullptr, NISE_ERR_DEVICE, "nise_batch_create: stream/event creation failed");
+    }
+    b->side.resize(n);
+    b->done.resize(n);
+    for (int i = 0; i < n; i++)
+        if (cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking) || cudaEventCreate(&b->done[i])) {
+            nise_batch_destroy(b);
+            return nise_fail(nullptr, NISE_ERR_DEVICE, "nise_batch_create: stream/event creation failed");
+        }
+    // capture: fork every job onto its own stream, join them back
+    cudaEvent_t fork;
+    cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+    int rc = NISE_OK;
+    if (cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaEventDestroy(fork);
+        nise_batch_destroy(b);
+        return nise_fail(nullptr, NISE_ERR_DEVICE, "nise_batch_create: stream capture failed to begin");
+    }
+    cudaEventRecord(fork, b->master);
+    for (int i = 0; i < n && rc == NISE_OK; i++) {
+        cudaStreamWaitEvent(b->side[i], fork, 0);
+        rc = b->runs[i]->enqueue(b->side[i], false);
+        if (rc == NISE_OK)
+            rc = nise_cuda(b->ctx[i], launch_fft1d_buf(b->fj[i], b->runs[i]->out.p, b->spec[i]->p, b->fftin[i]->p,
+                                                       b->side[i]),
+                           "1D FFT");
+        cudaEventRecord(b->done[i], b->side[i]);
+        cudaStreamWaitEvent(b->master, b->done[i], 0);
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(b->master, &g);
+    cudaEventDestroy(fork);
+    if (rc != NISE_OK || ce != cudaSuccess || !g) {
+        if (g) cudaGraphDestroy(g);
+        std::string m = rc ? "capture: job kernels failed to enqueue" : cudaGetErrorString(ce);
+        nise_batch_destroy(b);
+        return nise_fail(nullptr, rc ? rc : NISE_ERR_DEVICE, "nise_batch_create: %s", m.c_str());
+    }
+    b->graph = g;
+    if (cudaGraphInstantiate(&b->exec, g, 0) != cudaSuccess) {
+        nise_batch_destroy(b);
+        return nise_fail(nullptr, NISE_ERR_DEVICE, "nise_batch_create: graph instantiation failed");
+    }
+    b->host_out.resize(n);
+    b->host_spec.resize(n);
+    b->job_ms.assign(n, 0);
+    *out = b;
+    return NISE_OK;
+}
+
+extern "C" int nise_batch_run(nise_batch *b) {
+    if (!b) return nise_fail(nullptr, NISE_ERR_ARG, "null batch");
+    cudaSetDevice(b->device);
+    cudaEventRecord(b->start, b->master);
+    if (cudaGraphLaunch(b->exec, b->master) != cudaSuccess)
+        return batch_fail(b, NISE_ERR_DEVICE, "nise_batch_run: graph launch failed");
+    cudaEventRecord(b->stop, b->master);
+    const int n = (int)b->runs.size();
+    for (int i = 0; i < n; i++) {
+        AbsRun &R = *b->runs[i];
+        b->host_out[i].resize(R.tmax);
+        b->host_spec[i].resize(b->fj[i].fft);
+        cudaMemcpyAsync(b->host_out[i].data(), R.out.p, sizeof(double2) * R.tmax, cudaMemcpyDeviceToHost, b->master);
+        cudaMemcpyAsync(b->host_spec[i].data(), b->spec[i]->p, sizeof(double2) * b->fj[i].fft,
+                        cudaMemcpyDeviceToHost, b->master);
+    }
+    cudaError_t e = cudaStreamSynchronize(b->master);
+    if (e != cudaSuccess) return batch_fail(b, NISE_ERR_DEVICE, std::string("nise_batch_run: ") + cudaGetErrorString(e));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, b->start, b->stop);
+    b->last_ms = ms;
+    return NISE_OK;
+}
+
+extern "C" int nise_batch_result(nise_batch *b, int i, double *re_S, double *im_S, int *samples) {
+    if (!b || i < 0 || i >= (int)b->runs.size() || !re_S || !im_S || !samples)
+        return nise_fail(nullptr, NISE_ERR_ARG, "nise_batch_result: bad arguments");
+    const auto &h = b->host_out[i];
+    if (h.empty()) return batch_fail(b, NISE_ERR_STATE, "nise_batch_result: the batch has not run");
+    for (size_t t = 0; t < h.size(); t++) {
+        re_S[t] = h[t].x;
+        im_S[t] = h[t].y;
+    }
+    *samples = b->runs[i]->end;
+    return NISE_OK;
+}
+
+extern "C" int nise_batch_spectrum(nise_batch *b, int i, double *freq, double *spec_re, double *spec_im, int max_rows,
+                                   int *rows) {
+    if (!b || i < 0 || i >= (int)b->runs.size() || !freq || !spec_re || !spec_im || !rows)
+        return nise_fail(nullptr, NISE_ERR_ARG, "nise_batch_spectrum: bad arguments");
+    if (b->host_spec[i].empty()) return batch_fail(b, NISE_ERR_STATE, "nise_batch_spectrum: the batch has not run");
+    *rows = nise_spectrum_rows(b->ctx[i], b->host_spec[i].data(), b->fj[i].fft, freq, spec_re, spec_im, max_rows);
+    return NISE_OK;
+}
+
+extern "C" int nise_batch_timing(const nise_batch *b, double *ms, long *kernel_launches) {
+    if (!b) return NISE_ERR_ARG;
+    if (ms) *ms = b->last_ms;
+    if (kernel_launches) {
+        long n = 0;
+        for (auto c : b->ctx) n += c->launches;
+        *kernel_launches = n + (long)b->runs.size() * 2;  // + the two transform kernels per job
+    }
+    return NISE_OK;
+}
+
+extern "C" const char *nise_batch_error(const nise_batch *b) { return b ? b->err.c_str() : nise_global_error(); }

@@ -5,6 +5,7 @@
 
 #include <cmath>
 #include <cstdarg>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <algorithm>
@@ -95,6 +96,17 @@ extern "C" int nise_create(const nise_params *p, nise_ctx **out) {
     }
     c->shifte = (p->max1 + p->min1) / 2;
     int e = (int)cudaSetDevice(p->device);
+    if (!e) {
+        // Jobs allocate their tables stream-ordered from the device's default
+        // pool; keep freed blocks in the pool (this process only) instead of
+        // returning them to the driver at every synchronisation, so repeated
+        // jobs do not remap memory.
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, p->device) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     if (!e) e = (int)cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
     c->stream = c->own_stream;
     if (!e) e = (int)cudaEventCreate(&c->ev0);
@@ -339,350 +351,6 @@ int nise_check_frames(nise_ctx *c, long last_frame) {
 }
 
 // ------------------------------------------------------------ absorption
-// Eigen route of the exact propagators (diag.cu): every frame of [f0, f0+nf)
-// is diagonalised in FP64 (chunks of frames), its one-step propagator U is
-// built (truncated when a Threshold is active) and applied to every start
-// point crossing it.  Records evk0/evk1 around the device work.
-static int abs_eigen(nise_ctx *c, const DevTraj &T, const AbsJob &J, long f0, long nf, double2 *resp, bool plain,
-                     bool truncated) {
-    const int N = c->n, prec = c->p.precision;
-    const size_t r2 = prec == NISE_FP32 ? sizeof(float2) : sizeof(double2);
-    const size_t ubytes = r2 * (size_t)nf * N * N;
-    if (ubytes > ((size_t)64 << 30))
-        return nise_fail(c, NISE_ERR_NOMEM, "eigen route: %ld frames of %d sites need more than 64 GB of propagators",
-                         nf, N);
-    int rc;
-    DevBuf<char> U;
-    DevBuf<long> fr;
-    DevBuf<double> V, w;
-    std::vector<long> frames(nf);
-    for (long t = 0; t < nf; t++) frames[t] = f0 + t;
-    const long FC = std::max(1L, std::min(nf, (long)(((size_t)512 << 20) / (sizeof(double) * (size_t)N * N))));
-    if ((rc = U.alloc(c, ubytes)) || (rc = fr.upload(c, frames)) || (rc = V.alloc(c, (size_t)FC * N * N)) ||
-        (rc = w.alloc(c, (size_t)FC * N)))
-        return rc;
-    EigJob EJ;
-    EJ.T = T;
-    EJ.n = N;
-    EJ.singleshift = c->nshift > 0;
-    // propagate_vec_DIA: f = deltat*icm2ifs*twoPi*sign in float, one full step
-    const double f = prec == NISE_FP32 ? (double)J.f32_full : J.f;
-    cudaEventRecord(c->evk0, c->stream);
-    for (long q = 0; q < nf; q += FC) {
-        long m = std::min(FC, nf - q);
-        if ((rc = nise_cuda(c, launch_eig(EJ, fr.p + q, m, V.p, w.p, c->stream), "eigensolver"))) return rc;
-        if ((rc = nise_cuda(c, launch_build_u(prec == NISE_FP32 ? 0 : 1, V.p, w.p, m, N, f, c->thres, truncated,
-                                              U.p + r2 * (size_t)q * N * N, c->stream),
-                            "propagator build")))
-            return rc;
-        c->launches += 2;
-    }
-    if (plain) {
-        for (int s = 0; s < J.nsamp; s++) {
-            AbsJob Js = J;
-            Js.begin = J.begin + s;
-            Js.nsamp = 1;
-            if ((rc = nise_cuda(c, launch_abs_dia(prec == NISE_FP32 ? 0 : 1, T, U.p, f0, N, Js,
-                                                  resp + (size_t)3 * s * J.tmax, c->stream),
-                                "eigen propagation")))
-                return rc;
-            c->launches++;
-        }
-    } else {
-        if ((rc = nise_cuda(c, launch_abs_dia(prec == NISE_FP32 ? 0 : 1, T, U.p, f0, N, J, resp, c->stream),
-                            "eigen propagation")))
-            return rc;
-        c->launches++;
-    }
-    cudaEventRecord(c->evk1, c->stream);
-    return NISE_OK;
-}
-
-extern "C" int nise_absorption(nise_ctx *c, double *re_S, double *im_S, int *samples) {
-    if (!c || !re_S || !im_S || !samples) return nise_fail(c, NISE_ERR_ARG, "null argument");
-    if (!c->loaded) return nise_fail(c, NISE_ERR_STATE, "no trajectory loaded");
-    cudaSetDevice(c->p.device);
-    const nise_params &p = c->p;
-    int N = c->n, tmax = p.tmax1, prec = p.precision;
-    // determine_samples (NISE_subs.c:197-221)
-    int n_samples = (p.length - p.tmax1 - 1) / p.sample + 1;
-    if (n_samples <= 0) return nise_fail(c, NISE_ERR_ARG, "Insufficient data to calculate spectrum.");
-    int end = p.end == 0 ? n_samples : p.end;
-    if (end > n_samples) return nise_fail(c, NISE_ERR_ARG, "Endpoint larger than number of samples was specified.");
-    int begin = p.begin;
-    if (begin < 0 || begin >= end) return nise_fail(c, NISE_ERR_ARG, "BeginPoint must be below EndPoint");
-    int nsamp = end - begin, nvec = 3 * nsamp;
-    long f0 = (long)begin * p.sample;
-    long f1 = (long)(end - 1) * p.sample + tmax - 1;  // last frame read
-    int rc;
-    if ((rc = nise_check_frames(c, f1))) return rc;
-    long nf = f1 - f0;  // frames that are propagated through: [f0, f1)
-    if (nf < 1) nf = 1;
-    DevTraj T = nise_devtraj(c);
-    AbsJob J;
-    J.begin = begin;
-    J.nsamp = nsamp;
-    J.sample = p.sample;
-    J.tmax = tmax;
-    J.ts = p.ts;
-    J.f = nise_f64(p, 1, 1);
-    J.f32_sub = nise_f32(p, 1, p.ts);
-    J.f64_sub = nise_f64(p, 1, p.ts);
-    J.f32_full = nise_f32(p, 1, 1);
-    DevBuf<double2> resp, out;
-    if ((rc = resp.alloc(c, (size_t)nvec * tmax)) || (rc = out.alloc(c, tmax))) return rc;
-    c->launches = 0;
-    c->last_flops = c->last_bytes = 0;
-    const bool plain = p.launch_mode == NISE_PLAIN;
-    size_t rsz = prec == NISE_FP32 ? sizeof(float) : sizeof(double);
-    cudaEventRecord(c->ev0, c->stream);
-    // Vectors crossing each propagated frame: used for the algorithmic work.
-    std::vector<long> cross(nf, 0);
-    for (int s = 0; s < nsamp; s++) {
-        long a = (long)(begin + s) * p.sample - f0;
-        for (int t = 0; t < tmax - 1; t++) cross[a + t] += 3;
-    }
-    long vec_steps = 3L * nsamp * (tmax - 1);
-    // bytes: every frame read once (diagonal or full record) and the dipoles
-    c->last_bytes = (double)nf * 4 * (p.hamiltonian == NISE_HAM_COUPLING ? N : c->nn2) +
-                    (double)(p.hamiltonian == NISE_HAM_COUPLING ? 3 * N : (nf + 1) * 3L * N) * 4;
-
-    if (p.propagation == NISE_PROP_COUPLING) {
-        std::vector<int2> pairs;
-        if ((rc = nise_pattern(c, f0, nf, pairs))) return rc;
-        DevBuf<int2> dpairs;
-        DevBuf<char> U, rot;
-        TrotterPlan P;
-        P.n = N;
-        P.k = (int)pairs.size();
-        P.f0 = f0;
-        P.nf = nf;
-        P.rot_static = p.hamiltonian == NISE_HAM_COUPLING;
-        P.singleshift = c->nshift > 0;
-        if ((rc = dpairs.upload(c, pairs))) return rc;
-        if ((rc = U.alloc(c, 2 * rsz * (size_t)nf * N))) return rc;
-        if ((rc = rot.alloc(c, 2 * rsz * (size_t)(P.rot_static ? 1 : nf) * (P.k ? P.k : 1)))) return rc;
-        P.pairs = dpairs.p;
-        P.U = U.p;
-        P.rot = rot.p;
-        // per vector step: ts * (K rotations * 12 flops + 2 N half-phases * 6 flops)
-        c->last_flops = (double)vec_steps * p.ts * (12.0 * P.k + 12.0 * N);
-        if ((rc = nise_cuda(c, launch_prep_trotter(prec, T, P, J.f64_sub, J.f32_sub, c->stream), "Trotter prep")))
-            return rc;
-        c->launches += 1 + (P.rot_static ? 1 : 0);
-        cudaEventRecord(c->evk0, c->stream);
-        if (plain) {
-            for (int s = 0; s < nsamp; s++) {
-                AbsJob Js = J;
-                Js.begin = begin + s;
-                Js.nsamp = 1;
-                if ((rc = nise_cuda(c, launch_abs_trotter(prec, T, P, Js, resp.p + (size_t)3 * s * tmax, c->stream),
-                                    "Trotter propagation")))
-                    return rc;
-                c->launches++;
-            }
-        } else {
-            if ((rc = nise_cuda(c, launch_abs_trotter(prec, T, P, J, resp.p, c->stream), "Trotter propagation")))
-                return rc;
-            c->launches++;
-        }
-        cudaEventRecord(c->evk1, c->stream);
-    } else if (p.propagation == NISE_PROP_RK4) {
-        std::vector<int2> pairs, ent;
-        if ((rc = nise_pattern(c, f0, nf, pairs))) return rc;
-        size_t q = 0;
-        for (int a = 0; a < N; a++) {  // propagate.c:294-305 order: (a,a) then (a,b>a)
-            ent.push_back(make_int2(a, a));
-            while (q < pairs.size() && pairs[q].x == a) ent.push_back(pairs[q++]);
-        }
-        DevBuf<int2> dent;
-        DevBuf<char> val;
-        Rk4Plan P;
-        P.n = N;
-        P.k = (int)ent.size();
-        P.f0 = f0;
-        P.nf = nf;
-        P.singleshift = c->nshift > 0;
-        if ((rc = dent.upload(c, ent))) return rc;
-        if ((rc = val.alloc(c, rsz * (size_t)nf * P.k))) return rc;
-        P.entries = dent.p;
-        P.val = val.p;
-        // per sub-step: 4 stages over the list (off-diagonal entries twice) + update and norms
-        c->last_flops = (double)vec_steps * p.ts * (4.0 * 4.0 * (2.0 * P.k - N) + 20.0 * N);
-        if ((rc = nise_cuda(c, launch_prep_rk4(prec, T, P, J.f64_sub, J.f32_sub, c->stream), "RK4 prep"))) return rc;
-        c->launches++;
-        cudaEventRecord(c->evk0, c->stream);
-        if (plain) {
-            for (int s = 0; s < nsamp; s++) {
-                AbsJob Js = J;
-                Js.begin = begin + s;
-                Js.nsamp = 1;
-                if ((rc = nise_cuda(c, launch_abs_rk4(prec, T, P, Js, resp.p + (size_t)3 * s * tmax, c->stream),
-                                    "RK4 propagation")))
-                    return rc;
-                c->launches++;
-            }
-        } else {
-            if ((rc = nise_cuda(c, launch_abs_rk4(prec, T, P, J, resp.p, c->stream), "RK4 propagation"))) return rc;
-            c->launches++;
-        }
-        cudaEventRecord(c->evk1, c->stream);
-    } else {
-        // Sparse / Diagonal: exact propagator exp(-i H dt) (propagate_vec_DIA,
-        // propagate.c:60-125).  Threshold > 0 keeps only large elements of U
-        // (propagate_vec_DIA_S, propagate.c:185-258) and needs the explicit
-        // eigen propagator, as do per-frame couplings (HamiltonianType Full)
-        // and the Diagonal scheme up to NISE_EIG_MAX_N sites.  Otherwise the
-        // static couplings go through the sparse Taylor series below.
-        const bool truncated = c->thres != 0 && !(c->thres > 1);
-        const bool eigen_route = truncated || p.hamiltonian != NISE_HAM_COUPLING ||
-                                 (p.propagation == NISE_PROP_DIAGONAL && N <= NISE_EIG_MAX_N);
-        if (eigen_route) {
-            if (N > NISE_EIG_MAX_N)
-                return nise_fail(c, NISE_ERR_UNSUPPORTED,
-                                 truncated ? "Sparse with Threshold > 0 is limited to 120 sites (eigen route)"
-                                           : "exact propagation of per-frame couplings (HamiltonianType Full) is "
-                                             "limited to 120 sites (eigen route)");
-            if ((rc = abs_eigen(c, T, J, f0, nf, resp.p, plain, truncated))) return rc;
-            c->last_flops = (double)nf * 6.7 * N * (double)N * N + (double)vec_steps * 8.0 * N * N;
-        } else {
-        // CSR of the static couplings (read cut applied, |J| >= cut kept)
-        std::vector<int> rp(N + 1, 0), col;
-        std::vector<double> vd;
-        double rowabs = 0;
-        for (int i = 0; i < N; i++) {
-            double rs = 0;
-            for (int j = 0; j < N; j++) {
-                if (j == i) continue;
-                int a = i < j ? i : j, b = i < j ? j : i;
-                float v = c->h_hc[b + (long)a * ((N << 1) - a - 1) / 2];
-                if (v != 0.0f) {
-                    col.push_back(j);
-                    vd.push_back(v);
-                    rs += fabs(v);
-                }
-            }
-            rp[i + 1] = (int)col.size();
-            rowabs = rs > rowabs ? rs : rowabs;
-        }
-        DevBuf<int> drp, dcol, dorder;
-        DevBuf<char> dval;
-        if ((rc = drp.upload(c, rp)) || (rc = dcol.upload(c, col.empty() ? std::vector<int>(1, 0) : col))) return rc;
-        if (prec == NISE_FP32) {
-            std::vector<float> vf(vd.begin(), vd.end());
-            if (vf.empty()) vf.push_back(0);
-            if ((rc = dval.alloc(c, sizeof(float) * vf.size()))) return rc;
-            cudaMemcpyAsync(dval.p, vf.data(), sizeof(float) * vf.size(), cudaMemcpyHostToDevice, c->stream);
-        } else {
-            if (vd.empty()) vd.push_back(0);
-            if ((rc = dval.alloc(c, sizeof(double) * vd.size()))) return rc;
-            cudaMemcpyAsync(dval.p, vd.data(), sizeof(double) * vd.size(), cudaMemcpyHostToDevice, c->stream);
-        }
-        if ((rc = dorder.alloc(c, (size_t)nf))) return rc;
-        // sliced ELL (4-row slices, [slot][row]) of the same couplings for the
-        // shared-memory kernel; entry offsets address rows of 10 complex numbers
-        const int nsl = (N + 3) / 4;
-        std::vector<int> sptr(nsl + 1, 0);
-        for (int sl = 0; sl < nsl; sl++) {
-            int L = 0;
-            for (int r = 0; r < 4; r++) {
-                int row = 4 * sl + r;
-                if (row < N) L = std::max(L, rp[row + 1] - rp[row]);
-            }
-            sptr[sl + 1] = sptr[sl] + 4 * L;
-        }
-        const int nent = sptr[nsl];
-        DevBuf<char> dell;
-        DevBuf<int> dsptr;
-        {
-            size_t esz = prec == NISE_FP32 ? 8 : 16;
-            std::vector<unsigned char> ell((size_t)(nent > 0 ? nent : 1) * esz, 0);
-            for (int sl = 0; sl < nsl; sl++) {
-                int L = (sptr[sl + 1] - sptr[sl]) / 4;
-                for (int slot = 0; slot < L; slot++)
-                    for (int r = 0; r < 4; r++) {
-                        int row = 4 * sl + r, e = sptr[sl] + slot * 4 + r;
-                        int off = (row < N ? row : 0) * 10;
-                        double v = 0;
-                        if (row < N && slot < rp[row + 1] - rp[row]) {
-                            off = col[rp[row] + slot] * 10;
-                            v = vd.empty() ? 0 : vd[rp[row] + slot];
-                        }
-                        unsigned char *dst = ell.data() + (size_t)e * esz;
-                        memcpy(dst, &off, 4);
-                        if (prec == NISE_FP32) {
-                            float fv = (float)v;
-                            memcpy(dst + 4, &fv, 4);
-                        } else {
-                            memcpy(dst + 8, &v, 8);
-                        }
-                    }
-            }
-            if ((rc = dell.alloc(c, ell.size()))) return rc;
-            cudaMemcpyAsync(dell.p, ell.data(), ell.size(), cudaMemcpyHostToDevice, c->stream);
-            if ((rc = dsptr.upload(c, sptr))) return rc;
-        }
-        TaylorPlan P;
-        memset(&P, 0, sizeof(P));
-        P.n = N;
-        P.nnz = (int)col.size();
-        P.row_ptr = drp.p;
-        P.col = dcol.p;
-        P.val = dval.p;
-        P.static_j = 1;
-        P.ell = dell.p;
-        P.ell_sptr = dsptr.p;
-        P.ell_nslices = nsl;
-        P.ell_nent = nent;
-        P.f0 = f0;
-        P.nf = nf;
-        P.singleshift = c->nshift > 0;
-        if ((rc = nise_cuda(c, launch_prep_taylor(prec, T, P, rowabs, J.f, dorder.p, c->stream), "Taylor prep")))
-            return rc;
-        c->launches++;
-        // per vector step and Taylor order: nnz complex*real products (4 flops)
-        // and the diagonal, scaling and accumulation (6 flops per site)
-        std::vector<int> order(nf);
-        cudaMemcpyAsync(order.data(), dorder.p, sizeof(int) * nf, cudaMemcpyDeviceToHost, c->stream);
-        if ((rc = nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "Taylor prep"))) return rc;
-        double orders = 0;
-        for (long t = 0; t < nf; t++) orders += (double)order[t] * cross[t];
-        c->last_flops = orders * (4.0 * P.nnz + 6.0 * N);
-        cudaEventRecord(c->evk0, c->stream);
-        if (plain) {
-            for (int s = 0; s < nsamp; s++) {
-                AbsJob Js = J;
-                Js.begin = begin + s;
-                Js.nsamp = 1;
-                if ((rc = nise_cuda(c, launch_abs_taylor(prec, T, P, Js, resp.p + (size_t)3 * s * tmax, 3, c->stream),
-                                    "Taylor propagation")))
-                    return rc;
-                c->launches++;
-            }
-        } else {
-            if ((rc = nise_cuda(c, launch_abs_taylor(prec, T, P, J, resp.p, 8, c->stream), "Taylor propagation")))
-                return rc;
-            c->launches++;
-        }
-        cudaEventRecord(c->evk1, c->stream);
-        }
-    }
-    if ((rc = nise_cuda(c, launch_reduce_resp(resp.p, nvec, tmax, out.p, c->stream), "response reduction")))
-        return rc;
-    c->launches++;
-    cudaEventRecord(c->ev1, c->stream);
-    std::vector<double2> h(tmax);
-    cudaMemcpyAsync(h.data(), out.p, sizeof(double2) * tmax, cudaMemcpyDeviceToHost, c->stream);
-    if ((rc = nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "absorption"))) return rc;
-    nise_collect_timing(c);
-    for (int t = 0; t < tmax; t++) {
-        re_S[t] = h[t].x;
-        im_S[t] = h[t].y;
-    }
-    *samples = end;  // absorption.c:185 divides by `samples`, which equals end after the loop
-    return NISE_OK;
-}
-
 // do_1DFFT (1DFFT.c:144-228): transform on the device, axis and window on the host.
 extern "C" int nise_absorption_fft(nise_ctx *c, const double *re_S, const double *im_S, int samples, double *freq,
                                    double *spec_re, double *spec_im, int max_rows, int *rows) {
@@ -712,6 +380,15 @@ extern "C" int nise_absorption_fft(nise_ctx *c, const double *re_S, const double
     std::vector<double2> spec(fft);
     cudaMemcpyAsync(spec.data(), dspec.p, sizeof(double2) * fft, cudaMemcpyDeviceToHost, c->stream);
     if ((rc = nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "1D FFT"))) return rc;
+    *rows = nise_spectrum_rows(c, spec.data(), fft, freq, spec_re, spec_im, max_rows);
+    return NISE_OK;
+}
+
+// Frequency axis and window of do_1DFFT (1DFFT.c:208-228): the rows of
+// Absorption.dat from the device spectrum spec[fft].
+int nise_spectrum_rows(const nise_ctx *c, const double2 *spec, int fft, double *freq, double *spec_re,
+                       double *spec_im, int max_rows) {
+    const nise_params &p = c->p;
     const bool f32 = p.precision == NISE_FP32;
     float shift1 = c->shifte;
     int n = 0;
@@ -737,8 +414,7 @@ extern "C" int nise_absorption_fft(nise_ctx *c, const double *re_S, const double
     };
     for (int i = fft / 2; i <= fft - 1; i++) emit(i, fft - i);
     for (int i = 0; i <= fft / 2 - 1; i++) emit(i, -i);
-    *rows = n < max_rows ? n : max_rows;
-    return NISE_OK;
+    return n < max_rows ? n : max_rows;
 }
 
 void nise_collect_timing(nise_ctx *c) {

@@ -33,6 +33,11 @@ struct Rk4Plan {
     int singleshift;
 };
 
+// Complex numbers per site row of the sliced-ELL Taylor kernel's state (the
+// 8 vectors of a CTA, unpadded): FP32 rows are 64 bytes, so even and odd rows
+// fall on the two halves of the shared-memory banks.
+#define NISE_T3_ROW 8
+
 // Sparse exact propagator exp(-i H f) by a Taylor series on a static CSR
 // coupling matrix plus the per-frame diagonal.
 struct TaylorPlan {
@@ -45,11 +50,18 @@ struct TaylorPlan {
     const int *order;      // [nf] Taylor order per frame
     int singleshift;
     // sliced-ELL copy of the couplings for the shared-memory kernel: slices of
-    // 4 rows, entries (state offset, weight) [slot][row in slice]
+    // 4 rows, entries (state offset = column * NISE_T3_ROW, weight) [slot][row]
     const void *ell;
     const int *ell_sptr;   // [nslices + 1] entry offset of each slice
     int ell_nslices, ell_nent;
+    int only_v2;           // 1: use k_abs_taylor2 even where the sliced-ELL kernel fits
+    // Chebyshev tables (set by launch_prep_cheb; then launch_abs_taylor runs
+    // the FP32 Chebyshev kernel): 1/R per frame and [nf][NISE_CHEB_KMAX+1]
+    // complex coefficients a_k
+    const float *cheb_inv_r;
+    const float2 *cheb_coef;
 };
+#define NISE_CHEB_KMAX 40
 
 // A batch of linear-absorption start points: vectors v = 3*(s-begin)+x for
 // samples s in [begin, begin+nsamp), polarisations x = 0..2.
@@ -65,12 +77,21 @@ int launch_prep_trotter(int prec, const DevTraj &T, const TrotterPlan &P, double
                         cudaStream_t s);
 int launch_abs_trotter(int prec, const DevTraj &T, const TrotterPlan &P, const AbsJob &J, double2 *resp,
                        cudaStream_t s);
+// Trotter absorption with level-scheduled rotations (CTA per start point):
+// perm lists the rotation indices level by level, lvptr[l]..lvptr[l+1] the
+// rotations of level l.  Bitwise identical to launch_abs_trotter.
+int launch_abs_trotter_lv(int prec, const DevTraj &T, const TrotterPlan &P, const AbsJob &J, double2 *resp,
+                          const int *perm, const int *lvptr, int nlev, int threads, cudaStream_t s);
 int launch_prep_rk4(int prec, const DevTraj &T, const Rk4Plan &P, double fsub, float fsub32, cudaStream_t s);
 int launch_abs_rk4(int prec, const DevTraj &T, const Rk4Plan &P, const AbsJob &J, double2 *resp, cudaStream_t s);
 int launch_prep_taylor(int prec, const DevTraj &T, TaylorPlan &P, double rowabs_max, double f, int *order,
                        cudaStream_t s);
 int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp,
                       int vec_per_cta, cudaStream_t s);
+// Chebyshev coefficients of the exact step per frame (FP32 kernel); sets
+// P.order, P.cheb_inv_r and P.cheb_coef.
+int launch_prep_cheb(const DevTraj &T, TaylorPlan &P, double rowabs_max, double f, int *order, float *inv_r,
+                     float2 *coef, cudaStream_t s);
 // flag[idx] = 1 for packed off-diagonals with |J| > cut in any frame of [f0, f0+nf).
 int launch_pattern_scan(const DevTraj &T, long f0, long nf, int *flag, cudaStream_t s);
 // Sum resp[v][t] over v in order (deterministic) into out[t].
@@ -81,6 +102,8 @@ struct FftJob {
     double deltat, lifetime, homogen, inhomogen;
 };
 int launch_fft1d(const FftJob &J, const double2 *resp, double2 *spec, cudaStream_t s);
+// Same with a caller work buffer in[fft] (no allocation: usable in stream capture).
+int launch_fft1d_buf(const FftJob &J, const double2 *resp, double2 *spec, double2 *in, cudaStream_t s);
 
 // Batched single steps on caller Hamiltonians (nise_propagate): vector v
 // uses packed H + v*n(n+1)/2.

@@ -98,6 +98,12 @@ __global__ void k_dft_spec(FftJob J, const double2 *in, double2 *spec) {
 
 }  // namespace
 
+int launch_fft1d_buf(const FftJob &J, const double2 *resp, double2 *spec, double2 *in, cudaStream_t s) {
+    k_fft_input<<<(J.fft + 255) / 256, 256, 0, s>>>(J, resp, in);
+    k_dft_spec<<<(J.fft + 255) / 256, 256, 256 * sizeof(double2), s>>>(J, in, spec);
+    return (int)cudaGetLastError();
+}
+
 int launch_fft1d(const FftJob &J, const double2 *resp, double2 *spec, cudaStream_t s) {
     double2 *in = nullptr;
     int e;

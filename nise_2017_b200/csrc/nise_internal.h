@@ -42,11 +42,19 @@ int nise_pattern(nise_ctx *c, long f0, long nf, std::vector<int2> &pairs);
 int nise_check_frames(nise_ctx *c, long last_frame);
 // Device time between ev0/ev1 (whole call) and evk0/evk1 (main kernels).
 void nise_collect_timing(nise_ctx *c);
+// Rows of Absorption.dat (1DFFT.c:208-228) from a device spectrum spec[fft];
+// returns the number of rows written (at most max_rows).
+int nise_spectrum_rows(const nise_ctx *c, const double2 *spec, int fft, double *freq, double *spec_re,
+                       double *spec_im, int max_rows);
+extern "C" void nise_set_global_error(const char *msg);
 
 // Stream-ordered device buffer owned by one call.
 template <typename T> struct DevBuf {
     T *p = nullptr;
     cudaStream_t s = nullptr;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
     int alloc(nise_ctx *c, size_t count) {
         s = c->stream;
         if (count == 0) count = 1;

@@ -130,6 +130,37 @@ def test_eigen_route_matches_taylor_route(tmp_path):
     assert helpers.rel(re_e + 1j * im_e, re_t + 1j * im_t) < 1e-9
 
 
+@pytest.mark.parametrize("cfg", [3, 8, 9, 10])
+def test_exact_propagator_kernels_agree(cfg, tmp_path):
+    """Every kernel of the static-coupling exact propagator (Taylor series with
+    4 or 8 vectors per CTA, sliced-ELL Taylor, sliced-ELL Chebyshev) against
+    the FP64 oracle's eigen-propagator."""
+    case = CASES["abs_sparse_static"]
+    files = helpers.materialise(case, str(tmp_path))
+    _, re, im, n, _ = run_engine(case, files, kernel_config=cfg)
+    ore, oim, on = oracle.absorption(oracle.params(case["keywords"], files), "f64")
+    assert n == on
+    assert helpers.rel(re + 1j * im, ore + 1j * oim) < SPARSE_FP32
+
+
+@pytest.mark.parametrize("n", [1300, 2048])
+def test_taylor_route_large_lattice(n, tmp_path):
+    """Static lattice couplings beyond what the shared-memory ELL kernel holds
+    (the launcher falls back to smaller tiles): FP32 against FP64, and plain
+    against batched."""
+    from nise_2017_b200 import synth
+    s = synth.c1_spec(n_sites=n, frames=48, seed=70 + n)
+    files = synth.write(s, str(tmp_path))
+    kw = synth.c1_keywords(Singles=n, Length=48, RunTimes="8 0 0", Samplerate=12)
+    case = dict(keywords=kw)
+    _, re32, im32, n32, _ = run_engine(case, files)
+    _, re64, im64, n64, _ = run_engine(case, files, precision=nise.FP64)
+    _, rep, imp, np_, _ = run_engine(case, files, launch_mode=nise.PLAIN)
+    assert n32 == n64 == np_
+    assert helpers.rel(re32 + 1j * im32, re64 + 1j * im64) < SPARSE_FP32
+    assert helpers.rel(rep + 1j * imp, re32 + 1j * im32) < 1e-6
+
+
 def random_hamiltonians(rng, nvec, n, cut):
     nn2 = n * (n + 1) // 2
     H = np.zeros((nvec, nn2), np.float32)
