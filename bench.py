@@ -375,15 +375,28 @@ def run_c2(args):
                 times.append(tot)
                 mains.append(main)
             flops, _ = c.work()
+        # plain: one start point per launch of every kernel, over the first 4 start points
+        plain_samples = 4
+        pp = nise.params_from_keywords(dict(kw, EndPoint=plain_samples), files, device=local,
+                                       launch_mode=nise.PLAIN)
+        with nise.Context(pp) as c:
+            c.load_files()
+            c.twodir()
+            c.twodir()
+            plain_ms, _, _ = c.timing()
     n2 = 64 * 65 // 2
     site_steps = n * 21 * 65 * 64 * n2
+    plain_value = plain_samples * 21 * 65 * 64 * n2 / (plain_ms / 1e3)
     ms = statistics.mean(times)
     out = {"metric": "2DIR time-to-spectrum and doubles site-steps/s (secondary workload)",
            "value": site_steps / (ms / 1e3), "unit": "site-steps/s", "n_gpus": 1, "steps": args.steps,
            "warmup": max(args.warmup, 1), "ms_per_step": ms, "time_to_spectrum_s": ms / 1e3,
            "config": {"workload": "2DIR, Propagation Coupling, N=64 random cluster, RunTimes 64 %d 64, "
                                   "Samplerate 100, 20000 x 2 fs" % args.t2, "start_points": n},
-           "doubles_fp32_tflops": flops / (statistics.mean(mains) / 1e3) / 1e12, "gpu_launches": launches}
+           "doubles_fp32_tflops": flops / (statistics.mean(mains) / 1e3) / 1e12, "gpu_launches": launches,
+           "plain": {"value": plain_value, "unit": "site-steps/s", "ms": plain_ms, "start_points": plain_samples,
+                     "mode": "one start point per launch of every kernel"},
+           "batched_over_plain": (site_steps / (ms / 1e3)) / plain_value}
     print(json.dumps(out), flush=True)
     return out
 

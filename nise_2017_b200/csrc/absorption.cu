@@ -477,7 +477,7 @@ template <> struct EllEnt<double> { int off; int pad; double v; };
 template <typename R, int IT>
 __global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, AbsJob J, double2 *resp, int nvec,
                                                     const EllEnt<R> *__restrict__ ell_g, const int *__restrict__ sptr_g,
-                                                    int nslices, int nent) {
+                                                    int nslices, int nent, const int *__restrict__ rows_g) {
     typedef typename Vec2<R>::T R2;
     constexpr int G = 8, QR = 4, RS = NISE_T3_ROW;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -486,9 +486,13 @@ __global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, Ab
     R2 *cur = (R2 *)smem_raw;
     EllEnt<R> *ell = (EllEnt<R> *)(cur + (size_t)n * RS);
     int *sptr = (int *)(ell + nent);
-    double *red = (double *)(((uintptr_t)(sptr + nslices + 1) + 15) & ~(uintptr_t)15);
+    int *rows = sptr + nslices + 1;  // [nslices][4] site of each slice row (n: padding)
+    double *red = (double *)(((uintptr_t)(rows + 4 * nslices) + 15) & ~(uintptr_t)15);
     for (int e = tid; e < nent; e += blockDim.x) ell[e] = ell_g[e];
     for (int e = tid; e <= nslices; e += blockDim.x) sptr[e] = sptr_g[e];
+    for (int e = tid; e < 4 * nslices; e += blockDim.x) rows[e] = rows_g[e];
+    __syncthreads();
+    auto rowof = [&](int sl) { return sl < nslices ? rows[q + QR * sl] : n; };
     const int v = blockIdx.x * G + g;
     const bool valid = v < nvec;
     const int vv = valid ? v : blockIdx.x * G;
@@ -498,7 +502,7 @@ __global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, Ab
     float dg[IT];
 #pragma unroll
     for (int it = 0; it < IT; it++) {
-        int i = q + QR * (warp + NW * it);
+        int i = rowof(warp + NW * it);
         psi[it].x = i < n ? (R)traj_mu(T, ti, x, i) : (R)0;
         psi[it].y = 0;
     }
@@ -508,7 +512,7 @@ __global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, Ab
         double re = 0, im = 0;
 #pragma unroll
         for (int it = 0; it < IT; it++) {
-            int i = q + QR * (warp + NW * it);
+            int i = rowof(warp + NW * it);
             if (i < n) {
                 R m = (R)traj_mu(T, tj, x, i);
                 re += (double)(m * psi[it].x);
@@ -531,7 +535,7 @@ __global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, Ab
         for (int o = 1; o < G; o <<= 1) K = max(K, __shfl_xor_sync(0xffffffffu, K, o));
 #pragma unroll
         for (int it = 0; it < IT; it++) {
-            int i = q + QR * (warp + NW * it);
+            int i = rowof(warp + NW * it);
             dg[it] = i < n ? traj_diag(T, tj, i, P.singleshift != 0) : 0.0f;
             if (i < n) cur[(size_t)i * RS + g] = psi[it];
         }
@@ -540,7 +544,7 @@ __global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, Ab
             const R c = (R)(J.f / k);
 #pragma unroll
             for (int it = 0; it < IT; it++) {
-                const int sl = warp + NW * it, i = q + QR * sl;
+                const int sl = warp + NW * it, i = rowof(sl);
                 if (sl >= nslices) continue;
                 R2 z = cur[(size_t)(i < n ? i : 0) * RS + g];
                 R yr = (R)dg[it] * z.x, yi = (R)dg[it] * z.y;
@@ -557,7 +561,7 @@ __global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, Ab
             __syncthreads();
 #pragma unroll
             for (int it = 0; it < IT; it++) {
-                const int sl = warp + NW * it, i = q + QR * sl;
+                const int sl = warp + NW * it, i = rowof(sl);
                 if (sl >= nslices || i >= n) continue;
                 cur[(size_t)i * RS + g] = nx[it];
                 psi[it].x += nx[it].x;
@@ -647,7 +651,8 @@ template <int IT>
 __global__ void __launch_bounds__(512) k_abs_cheb3(DevTraj T, TaylorPlan P, AbsJob J, double2 *resp, int nvec,
                                                   const EllEnt<float> *__restrict__ ell_g,
                                                   const int *__restrict__ sptr_g, int nslices, int nent,
-                                                  const float *__restrict__ inv_r, const float2 *__restrict__ coef) {
+                                                  const float *__restrict__ inv_r, const float2 *__restrict__ coef,
+                                                  const int *__restrict__ rows_g) {
     constexpr int G = 8, QR = 4, RS = NISE_T3_ROW, KC = NISE_CHEB_KMAX + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = P.n, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, NW = blockDim.x >> 5;
@@ -656,9 +661,13 @@ __global__ void __launch_bounds__(512) k_abs_cheb3(DevTraj T, TaylorPlan P, AbsJ
     float *dgs = (float *)(cur + (size_t)n * RS);  // [row][g]
     EllEnt<float> *ell = (EllEnt<float> *)(dgs + (size_t)n * G);
     int *sptr = (int *)(ell + nent);
-    double *red = (double *)(((uintptr_t)(sptr + nslices + 1) + 15) & ~(uintptr_t)15);
+    int *rows = sptr + nslices + 1;  // [nslices][4] site of each slice row (n: padding)
+    double *red = (double *)(((uintptr_t)(rows + 4 * nslices) + 15) & ~(uintptr_t)15);
     for (int e = tid; e < nent; e += blockDim.x) ell[e] = ell_g[e];
     for (int e = tid; e <= nslices; e += blockDim.x) sptr[e] = sptr_g[e];
+    for (int e = tid; e < 4 * nslices; e += blockDim.x) rows[e] = rows_g[e];
+    __syncthreads();
+    auto rowof = [&](int sl) { return sl < nslices ? rows[q + QR * sl] : n; };
     const int v = blockIdx.x * G + g;
     const bool valid = v < nvec;
     const int vv = valid ? v : blockIdx.x * G;
@@ -667,7 +676,7 @@ __global__ void __launch_bounds__(512) k_abs_cheb3(DevTraj T, TaylorPlan P, AbsJ
     float2 psi[IT], prev[IT], nx[IT];
 #pragma unroll
     for (int it = 0; it < IT; it++) {
-        int i = q + QR * (warp + NW * it);
+        int i = rowof(warp + NW * it);
         psi[it].x = i < n ? traj_mu(T, ti, x, i) : 0.f;
         psi[it].y = 0;
     }
@@ -677,7 +686,7 @@ __global__ void __launch_bounds__(512) k_abs_cheb3(DevTraj T, TaylorPlan P, AbsJ
         double re = 0, im = 0;
 #pragma unroll
         for (int it = 0; it < IT; it++) {
-            int i = q + QR * (warp + NW * it);
+            int i = rowof(warp + NW * it);
             if (i < n) {
                 float m = traj_mu(T, tj, x, i);
                 re += (double)(m * psi[it].x);
@@ -704,7 +713,7 @@ __global__ void __launch_bounds__(512) k_abs_cheb3(DevTraj T, TaylorPlan P, AbsJ
         const float a0 = cf[0].x;
 #pragma unroll
         for (int it = 0; it < IT; it++) {
-            int i = q + QR * (warp + NW * it);
+            int i = rowof(warp + NW * it);
             if (i < n) {
                 dgs[(size_t)i * G + g] = traj_diag(T, tj, i, P.singleshift != 0);
                 cur[(size_t)i * RS + g] = psi[it];
@@ -718,7 +727,7 @@ __global__ void __launch_bounds__(512) k_abs_cheb3(DevTraj T, TaylorPlan P, AbsJ
             const float2 a = cf[k];
 #pragma unroll
             for (int it = 0; it < IT; it++) {
-                const int sl = warp + NW * it, i = q + QR * sl;
+                const int sl = warp + NW * it, i = rowof(sl);
                 if (sl >= nslices) continue;
                 const int ic = i < n ? i : 0;
                 float2 z = cur[(size_t)ic * RS + g];
@@ -757,7 +766,7 @@ __global__ void __launch_bounds__(512) k_abs_cheb3(DevTraj T, TaylorPlan P, AbsJ
             __syncthreads();
 #pragma unroll
             for (int it = 0; it < IT; it++) {
-                const int sl = warp + NW * it, i = q + QR * sl;
+                const int sl = warp + NW * it, i = rowof(sl);
                 if (sl >= nslices || i >= n) continue;
                 cur[(size_t)i * RS + g] = nx[it];
                 psi[it].x += a.x * nx[it].x - a.y * nx[it].y;
@@ -1054,13 +1063,13 @@ static int run_taylor2(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, d
 
 size_t taylor3_smem(const TaylorPlan &P, size_t rsz) {
     size_t ent = rsz == 4 ? 8 : 16;
-    return (size_t)P.n * NISE_T3_ROW * 2 * rsz + (size_t)P.ell_nent * ent + sizeof(int) * (P.ell_nslices + 1) + 16 +
+    return (size_t)P.n * NISE_T3_ROW * 2 * rsz + (size_t)P.ell_nent * ent + sizeof(int) * (5 * P.ell_nslices + 1) + 16 +
            16 * 8 * 2 * sizeof(double);
 }
 
 size_t cheb3_smem(const TaylorPlan &P) {
     return (size_t)P.n * NISE_T3_ROW * sizeof(float2) + (size_t)P.n * 8 * sizeof(float) + (size_t)P.ell_nent * 8 +
-           sizeof(int) * (P.ell_nslices + 1) + 16 + 16 * 8 * 2 * sizeof(double);
+           sizeof(int) * (5 * P.ell_nslices + 1) + 16 + 16 * 8 * 2 * sizeof(double);
 }
 
 template <int IT>
@@ -1069,7 +1078,8 @@ static int run_cheb3(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, dou
     int e;
     if ((e = set_smem(k_abs_cheb3<IT>, smem))) return e;
     k_abs_cheb3<IT><<<(nvec + 7) / 8, 512, smem, s>>>(T, P, J, resp, nvec, (const EllEnt<float> *)P.ell, P.ell_sptr,
-                                                      P.ell_nslices, P.ell_nent, P.cheb_inv_r, P.cheb_coef);
+                                                      P.ell_nslices, P.ell_nent, P.cheb_inv_r, P.cheb_coef,
+                                                      P.ell_rows);
     return (int)cudaGetLastError();
 }
 
@@ -1081,7 +1091,7 @@ static int run_taylor3(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, d
     int e;
     if ((e = set_smem(k_abs_taylor3<R, IT>, smem))) return e;
     k_abs_taylor3<R, IT><<<(nvec + 7) / 8, NT, smem, s>>>(T, P, J, resp, nvec, (const EllEnt<R> *)P.ell,
-                                                          P.ell_sptr, P.ell_nslices, P.ell_nent);
+                                                          P.ell_sptr, P.ell_nslices, P.ell_nent, P.ell_rows);
     (void)NT;
     return (int)cudaGetLastError();
 }

@@ -90,7 +90,7 @@ struct AbsRun {
     DevBuf<char> rkval;
     Rk4Plan RP;
     // Taylor
-    DevBuf<int> drp, dcol, dorder, dsptr, dcorder;
+    DevBuf<int> drp, dcol, dorder, dsptr, dcorder, drows;
     DevBuf<char> dval, dell;
     DevBuf<float> dinvr;
     DevBuf<float2> dcoef;
@@ -282,12 +282,30 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
                             w++;
                         }
             }
+            // Rows of each slice: the sites of each parity, ordered by neighbour
+            // count, interleaved even/odd, so the 4 rows of a slice keep the
+            // alternating parity and have nearly equal lengths (little ELL padding).
             const int nsl = (N + 3) / 4;
+            std::vector<int> srow(4 * (size_t)nsl, N);
+            {
+                std::vector<int> cls[2];
+                for (int i = 0; i < N; i++) cls[i & 1].push_back(i);
+                for (int k = 0; k < 2; k++)
+                    std::stable_sort(cls[k].begin(), cls[k].end(), [&](int a, int b) {
+                        return rp[a + 1] - rp[a] > rp[b + 1] - rp[b];
+                    });
+                size_t take[2] = {0, 0};
+                for (int pos = 0; pos < 4 * nsl; pos++) {
+                    int want = pos & 1;
+                    if (take[want] >= cls[want].size()) want ^= 1;
+                    if (take[want] < cls[want].size()) srow[pos] = cls[want][take[want]++];
+                }
+            }
             std::vector<int> sptr(nsl + 1, 0);
             for (int sl = 0; sl < nsl; sl++) {
                 int L = 0;
                 for (int r = 0; r < 4; r++) {
-                    int row = 4 * sl + r;
+                    int row = srow[4 * sl + r];
                     if (row < N) L = std::max(L, rp[row + 1] - rp[row]);
                 }
                 sptr[sl + 1] = sptr[sl] + 4 * L;
@@ -299,7 +317,7 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
                 int L = (sptr[sl + 1] - sptr[sl]) / 4;
                 for (int slot = 0; slot < L; slot++)
                     for (int r = 0; r < 4; r++) {
-                        int row = 4 * sl + r, e = sptr[sl] + slot * 4 + r;
+                        int row = srow[4 * sl + r], e = sptr[sl] + slot * 4 + r;
                         int off = (row < N ? row : 0) * NISE_T3_ROW;
                         double v = 0;
                         if (row < N && slot < rp[row + 1] - rp[row]) {
@@ -316,6 +334,7 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
                         }
                     }
             }
+            if ((rc = drows.upload(c, srow))) return rc;
             if ((rc = dell.alloc(c, ell.size()))) return rc;
             cudaMemcpyAsync(dell.p, ell.data(), ell.size(), cudaMemcpyHostToDevice, c->stream);
             if ((rc = dsptr.upload(c, sptr))) return rc;
@@ -328,13 +347,14 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
             XP.static_j = 1;
             XP.ell = dell.p;
             XP.ell_sptr = dsptr.p;
+            XP.ell_rows = drows.p;
             XP.ell_nslices = nsl;
             XP.ell_nent = nent;
             XP.f0 = f0;
             XP.nf = nf;
             XP.singleshift = c->nshift > 0;
             // Chebyshev kernel: FP32, its shared-memory footprint (state, diagonal, ELL)
-            const size_t csm = (size_t)N * NISE_T3_ROW * 8 + (size_t)N * 32 + (size_t)nent * 8 + 4 * (nsl + 1) + 4096;
+            const size_t csm = (size_t)N * NISE_T3_ROW * 8 + (size_t)N * 32 + (size_t)nent * 8 + 4 * (5 * nsl + 1) + 4096;
             cheb = prec == NISE_FP32 && csm <= 227 * 1024 && (nsl + 15) / 16 <= 32;
             if (cheb && ((rc = dcorder.alloc(c, (size_t)nf)) || (rc = dinvr.alloc(c, (size_t)nf)) ||
                          (rc = dcoef.alloc(c, (size_t)nf * (NISE_CHEB_KMAX + 1)))))

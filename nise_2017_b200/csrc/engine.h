@@ -53,6 +53,7 @@ struct TaylorPlan {
     // 4 rows, entries (state offset = column * NISE_T3_ROW, weight) [slot][row]
     const void *ell;
     const int *ell_sptr;   // [nslices + 1] entry offset of each slice
+    const int *ell_rows;   // [nslices][4] site of each slice row (n for padding)
     int ell_nslices, ell_nent;
     int only_v2;           // 1: use k_abs_taylor2 even where the sliced-ELL kernel fits
     // Chebyshev tables (set by launch_prep_cheb; then launch_abs_taylor runs

@@ -1246,6 +1246,7 @@ extern "C" int nise_2dir(nise_ctx *c, double *R, int *sample_count) {
     int chunk = (int)(budget / (per_sample > 0 ? per_sample : 1));
     if (chunk < 1) chunk = 1;
     if (chunk > count) chunk = count;
+    if (p.launch_mode == NISE_PLAIN) chunk = 1;  // one start point per launch of every kernel
     DevBuf<char> L, Lr, SE, gbt1, gbt3, eaI, eaII, Rs;
     DevBuf<double> dR;
     if ((rc = L.alloc(c, r2 * (size_t)chunk * 3 * T1 * N)) || (rc = Lr.alloc(c, r2 * (size_t)chunk * 3 * N)) ||

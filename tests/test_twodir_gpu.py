@@ -102,6 +102,18 @@ def test_cluster_n40(tmp_path):
     assert helpers.rel2d(R, oR) < SUM_ORDER
 
 
+@pytest.mark.parametrize("name", ["2d_coupling", "2d_coupling_t2"])
+def test_plain_matches_batched(name, tmp_path):
+    """One start point per launch of every kernel gives the batched result
+    (the start points' responses are summed in another grouping)."""
+    case = CASES[name]
+    files = helpers.materialise(case, str(tmp_path))
+    _, Rb, nb = run(case["keywords"], files)
+    _, Rp, np_ = run(case["keywords"], files, launch_mode=nise.PLAIN)
+    assert nb == np_
+    assert helpers.rel2d(Rp, Rb) < 1e-12
+
+
 def test_diagonal_scheme_matches_reference_sparse(tmp_path):
     """Propagation Diagonal (rejected by the reference) against the reference's
     Sparse + Threshold 0 response files on the same trajectory."""
