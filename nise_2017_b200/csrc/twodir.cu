@@ -317,7 +317,7 @@ __device__ __forceinline__ typename Vec2<R>::T make_vec2(R x, R y) {
 // pivot |ac> stays in a register while the first index a is unchanged.
 template <typename R, int CPL>
 __device__ void doubles_substep(typename Vec2<R>::T *F, const typename Vec2<R>::T *Uh, const Dcoef<R> *cf,
-                                const int2 *pairs, int K, int n, int W, int lane) {
+                                const int2 *pairs, int K, int n, int W, int lane, const short *__restrict__ ci) {
     typedef typename Vec2<R>::T R2;
     typedef Ar<R> A;
     const int slots = n * W;
@@ -346,21 +346,21 @@ __device__ void doubles_substep(typename Vec2<R>::T *F, const typename Vec2<R>::
 #pragma unroll
                 for (int j = 0; j < CPL; j++) {
                     int c = lane + 32 * j;
-                    if (c < n && c != cur_a) F[circ(cur_a, c, n, W)] = piv[j];
+                    if (c < n && c != cur_a) F[ci ? ci[cur_a * n + c] : circ(cur_a, c, n, W)] = piv[j];
                 }
             }
             __syncwarp();
 #pragma unroll
             for (int j = 0; j < CPL; j++) {
                 int c = lane + 32 * j;
-                if (c < n && c != a) piv[j] = F[circ(a, c, n, W)];
+                if (c < n && c != a) piv[j] = F[ci ? ci[a * n + c] : circ(a, c, n, W)];
             }
             cur_a = a;
         }
         // c == a case: (|aa>,|ab>) with the sqrt(2) angle, by the lane owning c = b
         if (b - lane >= 0 && ((b - lane) & 31) == 0) {
             const int j = (b - lane) >> 5;
-            const int ix = circ(a, a, n, W);
+            const int ix = ci ? ci[a * n + a] : circ(a, a, n, W);
             R2 X = F[ix];
 #pragma unroll
             for (int jj = 0; jj < CPL; jj++)
@@ -373,7 +373,7 @@ __device__ void doubles_substep(typename Vec2<R>::T *F, const typename Vec2<R>::
             const int c = lane + 32 * j;
             if (c >= n || c == a) continue;
             const bool sp = c == b;
-            const int iq = circ(b, c, n, W);
+            const int iq = ci ? ci[b * n + c] : circ(b, c, n, W);
             R2 Q = F[iq];
             rot2<R>(piv[j], Q, sp ? q.co2 : q.co, sp ? q.si2 : q.si);
             F[iq] = Q;
@@ -384,7 +384,7 @@ __device__ void doubles_substep(typename Vec2<R>::T *F, const typename Vec2<R>::
 #pragma unroll
         for (int j = 0; j < CPL; j++) {
             int c = lane + 32 * j;
-            if (c < n && c != cur_a) F[circ(cur_a, c, n, W)] = piv[j];
+            if (c < n && c != cur_a) F[ci ? ci[cur_a * n + c] : circ(cur_a, c, n, W)] = piv[j];
         }
     }
     __syncwarp();
@@ -406,7 +406,7 @@ __device__ __forceinline__ float over_mu(const TwoD &D, long t, int x, int i) {
 
 // CTA = W warps = W doubles vectors of one start point, all at the same t3.
 template <typename R, int CPL>
-__global__ void __launch_bounds__(512) k2d_doubles(TwoD D, int vec_per_sample, Dcoef<R> *cf_static) {
+__global__ void __launch_bounds__(512) k2d_doubles(TwoD D, int vec_per_sample, Dcoef<R> *cf_static, int use_tab) {
     typedef typename Vec2<R>::T R2;
     typedef Ar<R> A;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -418,6 +418,7 @@ __global__ void __launch_bounds__(512) k2d_doubles(TwoD D, int vec_per_sample, D
     float *mu = (float *)(Uh + slots * (1 + nwarps)); // [3][n] mu(tl), then [3][n] overtone
     float *ov = mu + 3 * n;
     float *dg = ov + 3 * n;                           // [n] diagonal energies of the frame
+    short *cidx = use_tab ? (short *)(dg + n) : nullptr;  // [n][n] circ(x, y), where it fits
     const int cta_per_sample = (vec_per_sample + nwarps - 1) / nwarps;
     const int s = blockIdx.x / cta_per_sample;
     const int u = (blockIdx.x % cta_per_sample) * nwarps + warp;
@@ -432,6 +433,8 @@ __global__ void __launch_bounds__(512) k2d_doubles(TwoD D, int vec_per_sample, D
     }
     // unused circulant slots: unit phase, zero amplitude
     for (int e = threadIdx.x; e < slots; e += blockDim.x) Uh[e] = make_vec2<R>(1, 0);
+    if (cidx)
+        for (int e = threadIdx.x; e < n * n; e += blockDim.x) cidx[e] = (short)circ(e / n, e % n, n, Wd);
     for (int e = lane; e < slots; e += 32) F[e] = make_vec2<R>(0, 0);
     __syncthreads();
     // initial vector: dipole_double (NISE_subs.c:485-509) of the SE vector at tk
@@ -477,7 +480,7 @@ __global__ void __launch_bounds__(512) k2d_doubles(TwoD D, int vec_per_sample, D
                     if (q < n)
                         for (int j = 0; j < n; j++) {
                             R m = (R)(j == q ? ov[p3 * n + q] : mu[p3 * n + j]);
-                            R2 f = F[circ(j, q, n, Wd)];
+                            R2 f = F[cidx ? cidx[j * n + q] : circ(j, q, n, Wd)];
                             gr = A::add(gr, A::mul(m, f.x));
                             gi = A::add(gi, A::mul(m, f.y));
                         }
@@ -563,7 +566,7 @@ __global__ void __launch_bounds__(512) k2d_doubles(TwoD D, int vec_per_sample, D
         __syncthreads();
         const Dcoef<R> *cf = D.rot_static ? cf_static : cf_static + (tl - D.f0) * D.K;
         if (active)
-            for (int sub = 0; sub < D.ts; sub++) doubles_substep<R, CPL>(F, Uh, cf, D.pairs, D.K, n, Wd, lane);
+            for (int sub = 0; sub < D.ts; sub++) doubles_substep<R, CPL>(F, Uh, cf, D.pairs, D.K, n, Wd, lane, cidx);
     }
 }
 
@@ -1021,24 +1024,32 @@ int run_chunk(nise_ctx *c, TwoD &D, Dcoef<R> *cf) {
         cudaFreeAsync(Hb, st);
     } else if (D.ea) {
         int W = D.n / 2 + 2, slots = D.n * W;
-        // as many vectors (warps) as fit next to the phase table in shared memory
-        int nwarps = 16;
-        size_t dsm = sizeof(R2) * (size_t)slots * (1 + nwarps) + sizeof(float) * 7 * D.n;
-        while (dsm > 220 * 1024 && nwarps > 1) {
-            nwarps -= 1;
-            dsm = sizeof(R2) * (size_t)slots * (1 + nwarps) + sizeof(float) * 7 * D.n;
-        }
+        // as many vectors (warps) as fit next to the phase table in shared memory;
+        // the n x n slot-index table only where
+        // it costs no warp
+        auto bytes = [&](int w, bool tab) {
+            return sizeof(R2) * (size_t)slots * (1 + w) + sizeof(float) * 7 * D.n +
+                   (tab ? sizeof(short) * D.n * D.n : 0);
+        };
+        auto fit = [&](bool tab) {
+            int w = 16;
+            while (bytes(w, tab) > 220 * 1024 && w > 1) w--;
+            return w;
+        };
+        int nwarps = fit(false);
+        const int use_tab = fit(true) == nwarps && bytes(nwarps, true) <= 220 * 1024;
+        size_t dsm = bytes(nwarps, use_tab);
         if (dsm > 220 * 1024) return (int)cudaErrorNotSupported;
         int vps = 9 + 9 * D.T1, cps = (vps + nwarps - 1) / nwarps;
         if (D.n <= 32) {
             if ((e = smem_attr(k2d_doubles<R, 1>, dsm))) return e;
-            k2d_doubles<R, 1><<<D.S * cps, 32 * nwarps, dsm, st>>>(D, vps, cf);
+            k2d_doubles<R, 1><<<D.S * cps, 32 * nwarps, dsm, st>>>(D, vps, cf, use_tab);
         } else if (D.n <= 64) {
             if ((e = smem_attr(k2d_doubles<R, 2>, dsm))) return e;
-            k2d_doubles<R, 2><<<D.S * cps, 32 * nwarps, dsm, st>>>(D, vps, cf);
+            k2d_doubles<R, 2><<<D.S * cps, 32 * nwarps, dsm, st>>>(D, vps, cf, use_tab);
         } else {
             if ((e = smem_attr(k2d_doubles<R, 4>, dsm))) return e;
-            k2d_doubles<R, 4><<<D.S * cps, 32 * nwarps, dsm, st>>>(D, vps, cf);
+            k2d_doubles<R, 4><<<D.S * cps, 32 * nwarps, dsm, st>>>(D, vps, cf, use_tab);
         }
         c->launches++;
     }
