@@ -102,7 +102,8 @@ typedef struct {
                                       rotations with that many threads per start point;
                                       Sparse (static couplings): 3 or 9 k_abs_taylor2 with 4 or 8
                                       vectors per CTA, 8 the sliced-ELL Taylor kernel, 10 the
-                                      sliced-ELL Chebyshev kernel (FP32) */
+                                      sliced-ELL Chebyshev kernel (FP32), 12 the sliced-ELL
+                                      Taylor kernel with 4 vectors per CTA (FP32) */
 } nise_params;
 
 typedef struct nise_ctx nise_ctx;

@@ -572,6 +572,104 @@ __global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, Ab
     }
 }
 
+// The sliced-ELL Taylor kernel with 4 vectors per CTA (FP32): half the
+// register state of k_abs_taylor3 per CTA, so two CTAs (32 warps) share an
+// SM and hide the shared-memory latency better; the ELL (8-row slices whose
+// rows cover the four residues of the site index mod 4 twice, rows of 4
+// complex numbers = 32 bytes, so each residue class owns a quarter of the
+// banks) stays in global memory and is read through the L1 cache.
+template <int IT>
+__global__ void __launch_bounds__(512, 2) k_abs_taylor4(DevTraj T, TaylorPlan P, AbsJob J, double2 *resp, int nvec) {
+    constexpr int G = 4, QR = 8, RS = 4;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = P.n, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, NW = blockDim.x >> 5;
+    const int g = lane % G, q = lane / G;
+    float2 *cur = (float2 *)smem_raw;
+    double *red = (double *)(cur + (size_t)n * RS);
+    const int2 *__restrict__ ell = (const int2 *)P.ell4;  // (state offset, weight bits)
+    const int *__restrict__ sptr = P.ell4_sptr;
+    const int *__restrict__ rows = P.ell4_rows;
+    const int nslices = P.ell4_nslices;
+    auto rowof = [&](int sl) { return sl < nslices ? __ldg(rows + q + QR * sl) : n; };
+    const int v = blockIdx.x * G + g;
+    const bool valid = v < nvec;
+    const int vv = valid ? v : blockIdx.x * G;
+    const int x = vv % 3;
+    const long ti = (long)(J.begin + vv / 3) * J.sample;
+    float2 psi[IT], nx[IT];
+    float dg[IT];
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+        int i = rowof(warp + NW * it);
+        psi[it].x = i < n ? traj_mu(T, ti, x, i) : 0.f;
+        psi[it].y = 0;
+    }
+    for (int t1 = 0; t1 < J.tmax; t1++) {
+        const long tj = ti + t1;
+        double re = 0, im = 0;
+#pragma unroll
+        for (int it = 0; it < IT; it++) {
+            int i = rowof(warp + NW * it);
+            if (i < n) {
+                float m = traj_mu(T, tj, x, i);
+                re += (double)(m * psi[it].x);
+                im += (double)(m * psi[it].y);
+            }
+        }
+        for (int o = G; o < 32; o <<= 1) {
+            re += __shfl_xor_sync(0xffffffffu, re, o);
+            im += __shfl_xor_sync(0xffffffffu, im, o);
+        }
+        if (q == 0) { red[(warp * G + g) * 2] = re; red[(warp * G + g) * 2 + 1] = im; }
+        __syncthreads();
+        if (tid < G && blockIdx.x * G + tid < nvec) {
+            double sr = 0, si = 0;
+            for (int w = 0; w < NW; w++) { sr += red[(w * G + tid) * 2]; si += red[(w * G + tid) * 2 + 1]; }
+            resp[(size_t)(blockIdx.x * G + tid) * J.tmax + t1] = make_double2(sr, si);
+        }
+        if (t1 == J.tmax - 1) break;
+        int K = P.order[tj - P.f0];
+        for (int o = 1; o < G; o <<= 1) K = max(K, __shfl_xor_sync(0xffffffffu, K, o));
+#pragma unroll
+        for (int it = 0; it < IT; it++) {
+            int i = rowof(warp + NW * it);
+            dg[it] = i < n ? traj_diag(T, tj, i, P.singleshift != 0) : 0.0f;
+            if (i < n) cur[(size_t)i * RS + g] = psi[it];
+        }
+        for (int k = 1; k <= K; k++) {
+            __syncthreads();
+            const float c = (float)(J.f / k);
+#pragma unroll
+            for (int it = 0; it < IT; it++) {
+                const int sl = warp + NW * it, i = rowof(sl);
+                if (sl >= nslices) continue;
+                float2 z = cur[(size_t)(i < n ? i : 0) * RS + g];
+                float yr = dg[it] * z.x, yi = dg[it] * z.y;
+                const int b0 = __ldg(sptr + sl), b1 = __ldg(sptr + sl + 1);
+                for (int e = b0 + q; e < b1; e += QR) {
+                    const int2 en = __ldg(ell + e);
+                    const float w = __int_as_float(en.y);
+                    float2 zz = cur[en.x + g];
+                    yr += w * zz.x;
+                    yi += w * zz.y;
+                }
+                nx[it].x = c * yi;  // (-i)(c)(y)
+                nx[it].y = -c * yr;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int it = 0; it < IT; it++) {
+                const int sl = warp + NW * it, i = rowof(sl);
+                if (sl >= nslices || i >= n) continue;
+                cur[(size_t)i * RS + g] = nx[it];
+                psi[it].x += nx[it].x;
+                psi[it].y += nx[it].y;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // Chebyshev expansion of the exact step (FP32, sliced ELL in shared memory).
 //
 // With R_t the Gershgorin radius of frame t (max |h_ii| + max row sum of
@@ -1067,6 +1165,15 @@ size_t taylor3_smem(const TaylorPlan &P, size_t rsz) {
            16 * 8 * 2 * sizeof(double);
 }
 
+template <int IT>
+static int run_taylor4(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int nvec, cudaStream_t s) {
+    size_t smem = (size_t)P.n * 4 * sizeof(float2) + 16 * 4 * 2 * sizeof(double);
+    int e;
+    if ((e = set_smem(k_abs_taylor4<IT>, smem))) return e;
+    k_abs_taylor4<IT><<<(nvec + 3) / 4, 512, smem, s>>>(T, P, J, resp, nvec);
+    return (int)cudaGetLastError();
+}
+
 size_t cheb3_smem(const TaylorPlan &P) {
     return (size_t)P.n * NISE_T3_ROW * sizeof(float2) + (size_t)P.n * 8 * sizeof(float) + (size_t)P.ell_nent * 8 +
            sizeof(int) * (5 * P.ell_nslices + 1) + 16 + 16 * 8 * 2 * sizeof(double);
@@ -1098,6 +1205,21 @@ static int run_taylor3(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, d
 
 int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp,
                       int vec_per_cta, cudaStream_t s) {
+    if (P.use_v4) {  // the 4-vector sliced-ELL kernel (FP32, ELL through L1)
+        if (prec != 0 || !P.ell4) return (int)cudaErrorNotSupported;
+        int nvec = 3 * J.nsamp;
+        int it = (P.ell4_nslices + 15) / 16;
+        if (it > 32 || (size_t)P.n * 4 * sizeof(float2) + 1024 > kMaxSmem) return (int)cudaErrorNotSupported;
+        int IT = it <= 1 ? 1 : it <= 2 ? 2 : it <= 4 ? 4 : it <= 8 ? 8 : it <= 16 ? 16 : 32;
+        switch (IT) {
+        case 1: return run_taylor4<1>(T, P, J, resp, nvec, s);
+        case 2: return run_taylor4<2>(T, P, J, resp, nvec, s);
+        case 4: return run_taylor4<4>(T, P, J, resp, nvec, s);
+        case 8: return run_taylor4<8>(T, P, J, resp, nvec, s);
+        case 16: return run_taylor4<16>(T, P, J, resp, nvec, s);
+        default: return run_taylor4<32>(T, P, J, resp, nvec, s);
+        }
+    }
     if (P.cheb_coef) {  // Chebyshev tables present: the FP32 sliced-ELL Chebyshev kernel
         if (prec != 0 || !P.ell || cheb3_smem(P) > kMaxSmem) return (int)cudaErrorNotSupported;
         int nvec = 3 * J.nsamp;

@@ -36,7 +36,8 @@ enum Scheme { SCHEME_TROTTER, SCHEME_RK4, SCHEME_TAYLOR, SCHEME_EIGEN };
 //   Taylor:  3 = k_abs_taylor2 with 4 vectors per CTA, 8 = the sliced-ELL
 //            kernel with 8 (k_abs_taylor2 with 8 where it does not fit),
 //            -8 = k_abs_taylor2 with 8, 10 = the FP32 sliced-ELL kernel with
-//            the Chebyshev expansion of the step (k_abs_cheb3).
+//            the Chebyshev expansion of the step (k_abs_cheb3), 12 = the FP32
+//            sliced-ELL kernel with 4 vectors per CTA (k_abs_taylor4).
 typedef std::tuple<int, int, int, int, int> TuneKey;  // scheme, precision, sites, couplings, static
 std::map<TuneKey, int> g_tuned;
 std::mutex g_tune_mu;
@@ -90,7 +91,9 @@ struct AbsRun {
     DevBuf<char> rkval;
     Rk4Plan RP;
     // Taylor
-    DevBuf<int> drp, dcol, dorder, dsptr, dcorder, drows;
+    DevBuf<int> drp, dcol, dorder, dsptr, dcorder, drows, dsptr4, drows4;
+    DevBuf<int2> dell4;
+    int ell4_nslices = 0, ell4_nent = 0;
     DevBuf<char> dval, dell;
     DevBuf<float> dinvr;
     DevBuf<float2> dcoef;
@@ -335,6 +338,72 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
                     }
             }
             if ((rc = drows.upload(c, srow))) return rc;
+            if (prec == NISE_FP32) {
+                // 4-vector variant: 8-row slices covering the residues of the site
+                // index mod 4 twice (rows of 32 bytes: each residue owns a quarter
+                // of the banks), neighbours ordered by residue difference, each
+                // residue class sorted by neighbour count.
+                const int ns4 = (N + 7) / 8;
+                std::vector<int> r4(8 * (size_t)ns4, N);
+                std::vector<int> cls[4];
+                for (int i = 0; i < N; i++) cls[i & 3].push_back(i);
+                for (int k = 0; k < 4; k++)
+                    std::stable_sort(cls[k].begin(), cls[k].end(), [&](int a, int b) {
+                        return rp[a + 1] - rp[a] > rp[b + 1] - rp[b];
+                    });
+                size_t take[4] = {0, 0, 0, 0};
+                for (int pos = 0; pos < 8 * ns4; pos++) {
+                    for (int d = 0; d < 4; d++) {
+                        int k = (pos + d) & 3;
+                        if (take[k] < cls[k].size()) {
+                            r4[pos] = cls[k][take[k]++];
+                            break;
+                        }
+                    }
+                }
+                std::vector<int> c4(col.size());
+                std::vector<float> v4(col.size());
+                for (int i = 0; i < N; i++) {
+                    int w = rp[i];
+                    for (int d = 0; d < 4; d++)
+                        for (int q = rp[i]; q < rp[i + 1]; q++)
+                            if (((col[q] - i) & 3) == d) {
+                                c4[w] = col[q];
+                                v4[w] = (float)vd[q];
+                                w++;
+                            }
+                }
+                std::vector<int> sp4(ns4 + 1, 0);
+                for (int sl = 0; sl < ns4; sl++) {
+                    int L = 0;
+                    for (int r = 0; r < 8; r++) {
+                        int row = r4[8 * sl + r];
+                        if (row < N) L = std::max(L, rp[row + 1] - rp[row]);
+                    }
+                    sp4[sl + 1] = sp4[sl] + 8 * L;
+                }
+                std::vector<int2> e4(sp4[ns4] > 0 ? sp4[ns4] : 1, make_int2(0, 0));
+                for (int sl = 0; sl < ns4; sl++) {
+                    int L = (sp4[sl + 1] - sp4[sl]) / 8;
+                    for (int slot = 0; slot < L; slot++)
+                        for (int r = 0; r < 8; r++) {
+                            int row = r4[8 * sl + r], e = sp4[sl] + slot * 8 + r;
+                            int off = (row < N ? row : 0) * 4;
+                            float v = 0.f;
+                            if (row < N && slot < rp[row + 1] - rp[row]) {
+                                off = c4[rp[row] + slot] * 4;
+                                v = v4[rp[row] + slot];
+                            }
+                            int vb;
+                            memcpy(&vb, &v, 4);
+                            e4[e] = make_int2(off, vb);
+                        }
+                }
+                if ((rc = dell4.upload(c, e4)) || (rc = dsptr4.upload(c, sp4)) || (rc = drows4.upload(c, r4)))
+                    return rc;
+                ell4_nslices = ns4;
+                ell4_nent = sp4[ns4];
+            }
             if ((rc = dell.alloc(c, ell.size()))) return rc;
             cudaMemcpyAsync(dell.p, ell.data(), ell.size(), cudaMemcpyHostToDevice, c->stream);
             if ((rc = dsptr.upload(c, sptr))) return rc;
@@ -348,6 +417,13 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
             XP.ell = dell.p;
             XP.ell_sptr = dsptr.p;
             XP.ell_rows = drows.p;
+            if (dell4.p) {
+                XP.ell4 = dell4.p;
+                XP.ell4_sptr = dsptr4.p;
+                XP.ell4_rows = drows4.p;
+                XP.ell4_nslices = ell4_nslices;
+                XP.ell4_nent = ell4_nent;
+            }
             XP.ell_nslices = nsl;
             XP.ell_nent = nent;
             XP.f0 = f0;
@@ -365,7 +441,7 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
     if (p.kernel_config != 0) {  // forced by the caller
         const int k = p.kernel_config;
         if (scheme == SCHEME_TROTTER && (k == 1 || k == 64 || k == 128 || k == 256)) config = k == 1 ? 0 : k;
-        else if (scheme == SCHEME_TAYLOR && (k == 3 || k == 8 || k == 9 || (k == 10 && cheb)))
+        else if (scheme == SCHEME_TAYLOR && (k == 3 || k == 8 || k == 9 || (k == 10 && cheb) || (k == 12 && dell4.p)))
             config = k == 9 ? -8 : k;
         else return nise_fail(c, NISE_ERR_ARG, "kernel_config %d does not apply to this scheme", k);
         return NISE_OK;
@@ -395,6 +471,7 @@ int AbsRun::run_main(cudaStream_t s, int cfg, double2 *dst) {
         case SCHEME_TAYLOR: {
             TaylorPlan P = XP;
             P.only_v2 = cfg < 0;
+            P.use_v4 = cfg == 12;
             if (cfg == 10) {
                 P.order = dcorder.p;
                 P.cheb_inv_r = dinvr.p;
@@ -434,6 +511,7 @@ int AbsRun::tune() {
     } else {
         cand = {3, -8, 8};
         if (cheb) cand.push_back(10);
+        if (dell4.p) cand.push_back(12);
     }
     // the tables the kernels read (both series for the Taylor route)
     int rc;

@@ -61,6 +61,12 @@ struct TaylorPlan {
     // complex coefficients a_k
     const float *cheb_inv_r;
     const float2 *cheb_coef;
+    // 4-vector variant (k_abs_taylor4, FP32): 8-row slices, entries (column * 4,
+    // weight bits) as int2 [slot][row], rows [nslices][8]
+    int use_v4;
+    const void *ell4;
+    const int *ell4_sptr, *ell4_rows;
+    int ell4_nslices, ell4_nent;
 };
 #define NISE_CHEB_KMAX 40
 

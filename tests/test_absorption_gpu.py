@@ -130,7 +130,7 @@ def test_eigen_route_matches_taylor_route(tmp_path):
     assert helpers.rel(re_e + 1j * im_e, re_t + 1j * im_t) < 1e-9
 
 
-@pytest.mark.parametrize("cfg", [3, 8, 9, 10])
+@pytest.mark.parametrize("cfg", [3, 8, 9, 10, 12])
 def test_exact_propagator_kernels_agree(cfg, tmp_path):
     """Every kernel of the static-coupling exact propagator (Taylor series with
     4 or 8 vectors per CTA, sliced-ELL Taylor, sliced-ELL Chebyshev) against
