@@ -48,7 +48,11 @@ extern "C" {
  * Coupling/Diagonal/RK4 selects SPARSE, as in the reference. */
 enum { NISE_PROP_SPARSE = 0, NISE_PROP_COUPLING = 1, NISE_PROP_DIAGONAL = 2, NISE_PROP_RK4 = 3 };
 /* HamiltonianType keyword. */
-enum { NISE_HAM_FULL = 0, NISE_HAM_COUPLING = 1 };
+/* HamiltonianType: Full records, Coupling (diagonal frames + one static
+ * coupling record), TransitionDipole / ExtendedDipole (diagonal frames,
+ * couplings computed for every frame from the Positionfile and the dipoles,
+ * read_trajectory.c:180-303). */
+enum { NISE_HAM_FULL = 0, NISE_HAM_COUPLING = 1, NISE_HAM_TDC = 2, NISE_HAM_EDC = 3 };
 /* Technique keyword (techniques on this path). */
 enum {
     NISE_TECH_ABSORPTION = 0,
@@ -104,6 +108,8 @@ typedef struct {
                                       vectors per CTA, 8 the sliced-ELL Taylor kernel, 10 the
                                       sliced-ELL Chebyshev kernel (FP32), 12 the sliced-ELL
                                       Taylor kernel with 4 vectors per CTA (FP32) */
+    char positionFName[256];       /* Positionfile (TransitionDipole / ExtendedDipole) */
+    char pbcFName[256];            /* PBCfile: periodic box per frame (optional) */
 } nise_params;
 
 typedef struct nise_ctx nise_ctx;
@@ -173,6 +179,18 @@ int nise_write_2d(const char *path, const nise_params *p, const double *re, cons
  * scheme, precision and size in this process.  Results do not depend on the
  * choice (Trotter variants are bitwise identical). */
 int nise_absorption_tune(nise_ctx *ctx);
+
+/* HamiltonianType TransitionDipole / ExtendedDipole (read_He with the TDC/EDC
+ * couplings of read_trajectory.c:180-303): energy holds the diagonal records
+ * (int32 tag + N floats per frame), position the Positionfile records (the
+ * dipole-file layout; two records per frame for extended dipoles), pbc the
+ * PBCfile records (int32 tag + box, or NULL).  Every frame's couplings are
+ * computed once on the device and kept as Full records; nise_load_files calls
+ * this for those types. */
+int nise_set_trajectory_onfly(nise_ctx *ctx, const void *energy, size_t energy_bytes, const void *dipole,
+                              size_t dipole_bytes, const void *position, size_t position_bytes, const void *pbc,
+                              size_t pbc_bytes, const void *anharm, size_t anharm_bytes, const void *overtone,
+                              size_t overtone_bytes);
 
 /* Batched linear absorption of many contexts (trajectories of any size and
  * scheme, one device): nise_batch_create plans every job (optionally

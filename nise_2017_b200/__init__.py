@@ -37,7 +37,7 @@ EXPORTED = [
     "nise_write_spectrum", "nise_write_2d", "nise_set_stream", "nise_last_timing", "nise_last_work",
     "nise_probe_fp32_peak", "nise_absorption_noalloc", "nise_2dfft_files", "nise_absorption_model",
     "nise_backward_absorption", "nise_absorption_tune", "nise_batch_create", "nise_batch_run", "nise_batch_result",
-    "nise_batch_spectrum", "nise_batch_timing", "nise_batch_error", "nise_batch_destroy",
+    "nise_batch_spectrum", "nise_batch_timing", "nise_batch_error", "nise_batch_destroy", "nise_set_trajectory_onfly",
 ]
 
 
@@ -62,7 +62,7 @@ class Params(ctypes.Structure):
         ("couplingFName", ctypes.c_char * 256), ("anharFName", ctypes.c_char * 256),
         ("overdipFName", ctypes.c_char * 256), ("singleShiftFName", ctypes.c_char * 256),
         ("precision", ctypes.c_int), ("launch_mode", ctypes.c_int), ("device", ctypes.c_int),
-        ("kernel_config", ctypes.c_int),
+        ("kernel_config", ctypes.c_int), ("positionFName", ctypes.c_char * 256), ("pbcFName", ctypes.c_char * 256),
     ]
 
 
@@ -145,7 +145,8 @@ def params_from_keywords(keywords, files=None, **engine):
     lines = []
     for k, v in (files or {}).items():
         key = {"energy": "Hamiltonianfile", "dipole": "Dipolefile", "coupling": "Couplingfile",
-               "anharm": "Anharmonicfile", "overtone": "Overtonedipolefile", "shift": "SingleShiftfile"}[k]
+               "anharm": "Anharmonicfile", "overtone": "Overtonedipolefile", "shift": "SingleShiftfile",
+               "position": "Positionfile", "pbc": "PBCfile"}[k]
         if v:
             lines.append("%s %s" % (key, v))
     lines += ["%s %s" % (k, v) for k, v in keywords.items()]

@@ -30,6 +30,7 @@ CU_SOURCES = [
     "fft2d.cu",
     "diag.cu",
     "adjoint.cu",
+    "onfly.cu",
 ]
 CPP_SOURCES = [
     "api.cpp",

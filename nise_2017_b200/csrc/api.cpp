@@ -222,6 +222,78 @@ extern "C" int nise_set_trajectory(nise_ctx *c, const void *energy, size_t energ
     return NISE_OK;
 }
 
+extern "C" int nise_set_trajectory_onfly(nise_ctx *c, const void *energy, size_t energy_bytes, const void *dipole,
+                                         size_t dipole_bytes, const void *position, size_t position_bytes,
+                                         const void *pbc, size_t pbc_bytes, const void *anharm, size_t anharm_bytes,
+                                         const void *overtone, size_t overtone_bytes) {
+    if (!c) return nise_fail(nullptr, NISE_ERR_ARG, "null context");
+    const nise_params &p = c->p;
+    if (p.hamiltonian != NISE_HAM_TDC && p.hamiltonian != NISE_HAM_EDC)
+        return nise_fail(c, NISE_ERR_ARG, "couplings on the fly need HamiltonianType TransitionDipole or ExtendedDipole");
+    if (!energy || !dipole || !position) return nise_fail(c, NISE_ERR_ARG, "energy, dipole and position records are required");
+    cudaSetDevice(p.device);
+    const int N = c->n;
+    const bool edc = p.hamiltonian == NISE_HAM_EDC;
+    const long full_words = 1 + c->nn2 + (long)p.doubles * (p.doubles + 1) / 2;
+    const long dip_words = 1 + 3L * N + 3L * N * p.doubles;
+    long frames = (long)(energy_bytes / (4 * (size_t)(1 + N)));
+    const long d_frames = (long)(dipole_bytes / (4 * (size_t)dip_words));
+    const long p_frames = (long)(position_bytes / (4 * (size_t)dip_words)) / (edc ? 2 : 1);
+    if (frames < 1) return nise_fail(c, NISE_ERR_IO, "Hamiltonian trajectory file to short");
+    // frames whose couplings can be built: every input must hold the frame
+    frames = std::min(frames, std::min(d_frames, p_frames));
+    if (pbc) frames = std::min(frames, (long)(pbc_bytes / 16));
+    if (frames < 1) return nise_fail(c, NISE_ERR_IO, "Dipole/Position/PBC trajectory file to short");
+    int rc;
+    // dipoles, anharmonicities and overtone dipoles as for a Full trajectory
+    c->d_words = dip_words;
+    c->d_frames = d_frames;
+    if ((rc = upload(c, &c->d_dipole, &c->cap_dipole, dipole, (size_t)d_frames * 4 * dip_words))) return rc;
+    c->a_frames = anharm ? (long)(anharm_bytes / (4 * (size_t)(1 + N))) : 0;
+    c->o_frames = overtone ? (long)(overtone_bytes / (4 * (size_t)(1 + 3L * N))) : 0;
+    if ((rc = upload(c, &c->d_anh, &c->cap_anh, anharm, (size_t)c->a_frames * 4 * (1 + N)))) return rc;
+    if ((rc = upload(c, &c->d_over, &c->cap_over, overtone, (size_t)c->o_frames * 4 * (1 + 3L * N)))) return rc;
+    if ((rc = upload(c, &c->d_hc, &c->cap_hc, nullptr, 0))) return rc;
+    if ((rc = upload(c, &c->d_mu_static, &c->cap_mu, nullptr, 0))) return rc;
+    c->h_hc.clear();
+    c->h_mu_static.clear();
+    // inputs of the frame builder (freed when it is done) and the built records
+    const size_t rec_bytes = (size_t)frames * 4 * full_words;
+    if (rec_bytes > c->cap_energy) {
+        if (c->d_energy) cudaFree(c->d_energy);
+        c->d_energy = nullptr;
+        c->cap_energy = 0;
+        if (cudaMalloc((void **)&c->d_energy, rec_bytes) != cudaSuccess)
+            return nise_fail(c, NISE_ERR_NOMEM, "couplings on the fly: %zu bytes of frame records do not fit", rec_bytes);
+        c->cap_energy = rec_bytes;
+    }
+    DevBuf<char> ddiag, dpos, dpbc;
+    const size_t pos_bytes = (size_t)frames * (edc ? 2 : 1) * 4 * dip_words;
+    if ((rc = ddiag.alloc(c, (size_t)frames * 4 * (1 + N))) || (rc = dpos.alloc(c, pos_bytes)) ||
+        (pbc && (rc = dpbc.alloc(c, (size_t)frames * 16))))
+        return rc;
+    cudaMemcpyAsync(ddiag.p, energy, (size_t)frames * 4 * (1 + N), cudaMemcpyHostToDevice, c->stream);
+    cudaMemcpyAsync(dpos.p, position, pos_bytes, cudaMemcpyHostToDevice, c->stream);
+    if (pbc) cudaMemcpyAsync(dpbc.p, pbc, (size_t)frames * 16, cudaMemcpyHostToDevice, c->stream);
+    OnflyJob J;
+    J.diag = (const float *)ddiag.p;
+    J.pos = (const float *)dpos.p;
+    J.dip = c->d_dipole;
+    J.pbc = pbc ? (const float *)dpbc.p : nullptr;
+    J.frames = frames;
+    J.full_words = full_words;
+    J.dip_words = dip_words;
+    J.n = N;
+    J.edc = edc;
+    if ((rc = nise_cuda(c, launch_onfly(J, c->d_energy, c->stream), "coupling frame builder"))) return rc;
+    c->e_words = full_words;
+    c->e_frames = frames;
+    int e = (int)cudaStreamSynchronize(c->stream);
+    if (e) return nise_cuda(c, e, "coupling frame builder");
+    c->loaded = true;
+    return NISE_OK;
+}
+
 extern "C" int nise_set_singleshift(nise_ctx *c, int n, const int *sites, const float *a, const float *b) {
     if (!c || n < 0) return nise_fail(c, NISE_ERR_ARG, "bad SingleShift arguments");
     cudaSetDevice(c->p.device);
@@ -259,9 +331,20 @@ extern "C" int nise_load_files(nise_ctx *c) {
         if (!read_file(p.overdipFName, O))
             return nise_fail(c, NISE_ERR_IO, "Overtone dipole file %s not found!", p.overdipFName);
     }
-    int rc = nise_set_trajectory(c, E.data(), E.size(), D.data(), D.size(), C.empty() ? nullptr : C.data(),
-                                 C.size(), A.empty() ? nullptr : A.data(), A.size(), O.empty() ? nullptr : O.data(),
-                                 O.size());
+    int rc;
+    if (p.hamiltonian == NISE_HAM_TDC || p.hamiltonian == NISE_HAM_EDC) {
+        std::vector<char> P, B;
+        if (!read_file(p.positionFName, P))
+            return nise_fail(c, NISE_ERR_IO, "Atom position file for TDC on the fly not found!");
+        if (p.pbcFName[0] && !read_file(p.pbcFName, B))
+            return nise_fail(c, NISE_ERR_IO, "Periodic Boundary Condition file not found!");
+        rc = nise_set_trajectory_onfly(c, E.data(), E.size(), D.data(), D.size(), P.data(), P.size(),
+                                       B.empty() ? nullptr : B.data(), B.size(), A.empty() ? nullptr : A.data(),
+                                       A.size(), O.empty() ? nullptr : O.data(), O.size());
+    } else {
+        rc = nise_set_trajectory(c, E.data(), E.size(), D.data(), D.size(), C.empty() ? nullptr : C.data(), C.size(),
+                                 A.empty() ? nullptr : A.data(), A.size(), O.empty() ? nullptr : O.data(), O.size());
+    }
     if (rc) return rc;
     // read_shift (hamshift.c:13-47); a missing file is reported and ignored there.
     if (p.singleShiftFName[0]) {
@@ -293,7 +376,7 @@ DevTraj nise_devtraj(const nise_ctx *c) {
     T.energy = c->d_energy;
     T.e_words = c->e_words;
     T.e_frames = c->e_frames;
-    T.full = c->p.hamiltonian == NISE_HAM_FULL;
+    T.full = c->p.hamiltonian != NISE_HAM_COUPLING;  // Full, or records built from positions
     T.dipole = c->d_dipole;
     T.d_words = c->d_words;
     T.d_frames = c->d_frames;

@@ -148,3 +148,16 @@ int launch_adj_fwd(const DevTraj &T, const AdjPlan &P, const AbsJob &J, double2 
                    cudaStream_t s);
 int launch_adj_bwd(const DevTraj &T, const AdjPlan &P, const AbsJob &J, const double2 *G, const double2 *ckpt,
                    double *gshift_part, double *gscale_part, double *gshift, double *gscale, cudaStream_t s);
+
+// Full record images for couplings computed on the fly (onfly.cu): diag are
+// the Hamiltonian file's diagonal records (int32 tag + n floats), pos the
+// Positionfile records (one per frame, two for extended dipoles), dip the
+// dipole records (dip_words words each), pbc the PBCfile records (int32 tag +
+// box, or NULL).  out receives frames records of full_words words.
+struct OnflyJob {
+    const float *diag, *pos, *dip, *pbc;
+    long frames, full_words, dip_words;
+    int n, edc;
+};
+int launch_onfly(const OnflyJob &J, float *out, cudaStream_t s);
+

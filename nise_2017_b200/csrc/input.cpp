@@ -86,9 +86,9 @@ extern "C" int nise_read_input(const char *path, nise_params *p) {
         if (match(buf, "Alphafile", L)) { kw_s(buf, dummy, sizeof(dummy)); continue; }
         if (match(buf, "Anharmonicfile", L)) { kw_s(buf, p->anharFName, sizeof(p->anharFName)); continue; }
         if (match(buf, "Overtonedipolefile", L)) { kw_s(buf, p->overdipFName, sizeof(p->overdipFName)); continue; }
-        if (match(buf, "Positionfile", L)) { kw_s(buf, dummy, sizeof(dummy)); continue; }
+        if (match(buf, "Positionfile", L)) { kw_s(buf, p->positionFName, sizeof(p->positionFName)); continue; }
         if (match(buf, "Couplingfile", L)) { kw_s(buf, p->couplingFName, sizeof(p->couplingFName)); continue; }
-        if (match(buf, "PBCfile", L)) { kw_s(buf, dummy, sizeof(dummy)); continue; }
+        if (match(buf, "PBCfile", L)) { kw_s(buf, p->pbcFName, sizeof(p->pbcFName)); continue; }
         if (match(buf, "SingleShiftfile", L)) {
             kw_s(buf, p->singleShiftFName, sizeof(p->singleShiftFName));
             continue;
@@ -148,8 +148,11 @@ extern "C" int nise_read_input(const char *path, nise_params *p) {
     p->window = !strcmp(window, "Hann") ? 1 : 0;
     if (!strcmp(hamiltonian, "Full")) p->hamiltonian = NISE_HAM_FULL;
     else if (!strcmp(hamiltonian, "Coupling")) p->hamiltonian = NISE_HAM_COUPLING;
+    else if (!strcmp(hamiltonian, "TransitionDipole")) p->hamiltonian = NISE_HAM_TDC;
+    else if (!strcmp(hamiltonian, "ExtendedDipole")) p->hamiltonian = NISE_HAM_EDC;
     else {
-        nise_set_global_error("HamiltonianType not supported by this engine (Full, Coupling)");
+        nise_set_global_error("HamiltonianType not supported by this engine (Full, Coupling, TransitionDipole, "
+                              "ExtendedDipole)");
         return NISE_ERR_UNSUPPORTED;
     }
     // readinput.c:206-233

@@ -77,6 +77,41 @@ def write(s, directory, anharm=False, prefix=""):
     return p
 
 
+def write_positions(directory, n_sites, frames, mode="tdc", seed=1, spacing=5.0, box=0.0, prefix=""):
+    """Seeded site positions for couplings computed on the fly (Positionfile,
+    dipole-file record layout: int32 tag, then the x, y and z blocks of N
+    floats).  Sites sit on a cubic grid of the given spacing (inside `box` when
+    a periodic box is given) and move by 0.05 A (standard deviation) per
+    frame.  mode "edc" writes two records per frame, the two ends of each
+    extended dipole (+-0.6 A along a fixed random direction per site).
+    With box > 0 a PBCfile (int32 tag + 3 floats per frame) is written too.
+    Returns {"position": path[, "pbc": path]}."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    side = int(np.ceil(n_sites ** (1.0 / 3)))
+    grid = np.array([(i % side, (i // side) % side, i // (side * side)) for i in range(n_sites)], float) * spacing
+    base = grid + rng.normal(0, 0.3, size=grid.shape)
+    u = rng.normal(size=(n_sites, 3))
+    u /= np.linalg.norm(u, axis=1)[:, None]
+    out = {"position": os.path.join(directory, prefix + "Position.bin")}
+    with open(out["position"], "wb") as f:
+        for t in range(frames):
+            r = base + rng.normal(0, 0.05, size=base.shape)
+            ends = [r] if mode == "tdc" else [r - 0.6 * u, r + 0.6 * u]
+            for e in ends:
+                if box > 0:
+                    e = np.mod(e, box)
+                f.write(np.int32(t).tobytes())
+                f.write(np.ascontiguousarray(e.T, dtype=np.float32).tobytes())
+    if box > 0:
+        out["pbc"] = os.path.join(directory, prefix + "PBC.bin")
+        with open(out["pbc"], "wb") as f:
+            for t in range(frames):
+                f.write(np.int32(t).tobytes())
+                f.write(np.array([box, box, box], np.float32).tobytes())
+    return out
+
+
 # ---------------------------------------------------------------- workloads
 def c0_spec(**kw):
     d = dict(n_sites=16, frames=10000, dt_fs=2.0, geometry=CHAIN, eps0=1650.0, sigma=10.0, tau_fs=100.0,
@@ -135,6 +170,10 @@ def write_input(path, keywords, files):
         lines.append("Overtonedipolefile %s" % files["overtone"])
     if files.get("shift"):
         lines.append("SingleShiftfile %s" % files["shift"])
+    if files.get("position"):
+        lines.append("Positionfile %s" % files["position"])
+    if files.get("pbc"):
+        lines.append("PBCfile %s" % files["pbc"])
     for k, v in keywords.items():
         lines.append("%s %s" % (k, v))
     with open(path, "w") as f:

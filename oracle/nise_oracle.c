@@ -68,6 +68,8 @@ typedef struct {
     char *D; long nD;
     char *A; long nA;
     char *O; long nO;
+    char *P; long nP;  /* Positionfile (TransitionDipole / ExtendedDipole) */
+    char *B; long nB;  /* PBCfile */
     float *Hc;     /* coupling frame for HamiltonianType Coupling (read_coupling) */
     float *mu_xyz; /* static dipoles for HamiltonianType Coupling */
     int nshift; int *shift_site; float *shift_ab;
@@ -87,7 +89,7 @@ static char *slurp(const char *path, long *bytes) {
 }
 
 static void traj_free(traj_t *t) {
-    free(t->E); free(t->D); free(t->A); free(t->O); free(t->Hc); free(t->mu_xyz);
+    free(t->E); free(t->D); free(t->A); free(t->O); free(t->P); free(t->B); free(t->Hc); free(t->mu_xyz);
     free(t->shift_site); free(t->shift_ab);
     memset(t, 0, sizeof(*t));
 }
@@ -96,17 +98,103 @@ static long full_frame_floats(const oracle_params *p) {
     return (long)p->singles * (p->singles + 1) / 2 + (long)p->doubles * (p->doubles + 1) / 2;
 }
 
+static int read_mue(const traj_t *t, const char *buf, long nbytes, float *mu, int pos, int x);
+
+/* pbc1 (NISE_subs.c:641-648). */
+static float pbc1(float r, int x, const float *box) {
+    if (box[0] > 0.0) {
+        if (r > box[x] / 2) r = r - box[x];
+        if (r < -box[x] / 2) r = r + box[x];
+    }
+    return r;
+}
+
+/* Couplings computed on the fly (read_trajectory.c:180-303): transition
+ * dipole coupling from one position per site, or extended dipoles from two
+ * (records 2*pos and 2*pos+1 of the Positionfile), with the periodic box of
+ * the PBCfile record pos when given.  Float arithmetic in the reference's
+ * order; sqrt and 1.0/x in double as the reference's calls are. */
+static int onfly_couplings(const traj_t *t, float *He, int pos) {
+    const oracle_params *p = t->p;
+    const int N = p->singles;
+    const float A = 5034.11861687;
+    float box[3] = {0, 0, 0};
+    if (t->B) {
+        long off = (long)pos * 16 + 4;
+        if (off + 12 > t->nB) return 0;
+        memcpy(box, t->B + off, 12);
+    }
+    float *R = (float *)calloc(3 * N, sizeof(float)), *R2 = (float *)calloc(3 * N, sizeof(float));
+    float *mu = (float *)calloc(3 * N, sizeof(float));
+    int ok = 1, rp = p->ham_onfly == 2 ? 2 * pos : pos;
+    for (int x = 0; x < 3 && ok; x++) {
+        ok = read_mue(t, t->P, t->nP, R + x * N, rp, x) && read_mue(t, t->D, t->nD, mu + x * N, pos, x);
+        if (ok && p->ham_onfly == 2) ok = read_mue(t, t->P, t->nP, R2 + x * N, rp + 1, x);
+    }
+    if (ok && p->ham_onfly == 1) {
+        for (int i = 0; i < N; i++) {
+            float m1x = mu[i], m1y = mu[N + i], m1z = mu[2 * N + i];
+            for (int j = i + 1; j < N; j++) {
+                float Rx = pbc1(R[i] - R[j], 0, box);
+                float Ry = pbc1(R[N + i] - R[N + j], 1, box);
+                float Rz = pbc1(R[2 * N + i] - R[2 * N + j], 2, box);
+                float m2x = mu[j], m2y = mu[N + j], m2z = mu[2 * N + j];
+                float dist = sqrt(Rx * Rx + Ry * Ry + Rz * Rz);
+                float idist = 1.0 / dist;
+                float idist3 = idist * idist * idist;
+                float f1 = m1x * m2x + m1y * m2y + m1z * m2z;
+                float f2 = -3 * (m1x * Rx + m1y * Ry + m1z * Rz) * (m2x * Rx + m2y * Ry + m2z * Rz) * idist * idist;
+                He[Sindex(i, j, N)] = A * (f1 + f2) * idist3;
+            }
+        }
+    } else if (ok) {
+        for (int i = 0; i < N; i++) {
+            float Rx = pbc1(R2[i] - R[i], 0, box);
+            float Ry = pbc1(R2[N + i] - R[N + i], 1, box);
+            float Rz = pbc1(R2[2 * N + i] - R[2 * N + i], 2, box);
+            float m1x = mu[i], m1y = mu[N + i], m1z = mu[2 * N + i];
+            float dist = sqrt(Rx * Rx + Ry * Ry + Rz * Rz);
+            float q1 = sqrt(m1x * m1x + m1y * m1y + m1z * m1z) / dist;
+            for (int j = i + 1; j < N; j++) {
+                Rx = pbc1(R2[j] - R[j], 0, box);
+                Ry = pbc1(R2[N + j] - R[N + j], 1, box);
+                Rz = pbc1(R2[2 * N + j] - R[2 * N + j], 2, box);
+                dist = sqrt(Rx * Rx + Ry * Ry + Rz * Rz);
+                /* the reference forms q2 from the first dipole (read_trajectory.c:246) */
+                float q2 = sqrt(m1x * m1x + m1y * m1y + m1z * m1z) / dist;
+                float J, idist;
+                Rx = pbc1(R[i] - R[j], 0, box); Ry = pbc1(R[N + i] - R[N + j], 1, box);
+                Rz = pbc1(R[2 * N + i] - R[2 * N + j], 2, box);
+                dist = sqrt(Rx * Rx + Ry * Ry + Rz * Rz); idist = 1.0 / dist; J = idist;
+                Rx = pbc1(R[i] - R2[j], 0, box); Ry = pbc1(R[N + i] - R2[N + j], 1, box);
+                Rz = pbc1(R[2 * N + i] - R2[2 * N + j], 2, box);
+                dist = sqrt(Rx * Rx + Ry * Ry + Rz * Rz); idist = 1.0 / dist; J = J - idist;
+                Rx = pbc1(R2[i] - R[j], 0, box); Ry = pbc1(R2[N + i] - R[N + j], 1, box);
+                Rz = pbc1(R2[2 * N + i] - R[2 * N + j], 2, box);
+                dist = sqrt(Rx * Rx + Ry * Ry + Rz * Rz); idist = 1.0 / dist; J = J - idist;
+                Rx = pbc1(R2[i] - R2[j], 0, box); Ry = pbc1(R2[N + i] - R2[N + j], 1, box);
+                Rz = pbc1(R2[2 * N + i] - R2[2 * N + j], 2, box);
+                dist = sqrt(Rx * Rx + Ry * Ry + Rz * Rz); idist = 1.0 / dist; J = J + idist;
+                He[Sindex(i, j, N)] = A * q1 * q2 * J;
+            }
+        }
+    }
+    free(R); free(R2); free(mu);
+    return ok;
+}
+
 /* read_He (read_trajectory.c:106-314): Full frame (:157-178) or diagonal-only
  * frame for HamiltonianType Coupling (:135-156); coupling cut (:305-311).
  * Returns 0 when the frame lies beyond the file (the reference exits). */
 static int read_He_mem(const traj_t *t, const char *buf, long nbytes, float *He, int pos) {
     const oracle_params *p = t->p;
     int N = p->singles;
-    if (p->ham_coupling && pos >= 0) {
+    if ((p->ham_coupling && pos >= 0) || p->ham_onfly) {
         long off = (long)pos * (4 + 4L * N);
         if (pos < 0 || off + 4 + 4L * N > nbytes) return 0;
         const float *h = (const float *)(buf + off + 4);
         for (int i = 0; i < N; i++) He[i * N + i - (i * (i + 1)) / 2] = h[i] - t->shifte;
+        if (p->ham_onfly && !onfly_couplings(t, He, pos)) return 0;
     } else {
         if (pos == -1) pos = 0;
         long nn = (long)N * (N + 1) / 2;
@@ -172,6 +260,11 @@ static int traj_open(traj_t *t, const oracle_params *p, float shifte, int need_a
     t->E = slurp(p->energy, &t->nE);
     t->D = slurp(p->dipole, &t->nD);
     if (!t->E || !t->D) return -1;
+    if (p->ham_onfly) {
+        t->P = slurp(p->position, &t->nP);
+        if (!t->P) return -1;
+        if (p->pbc[0] && !(t->B = slurp(p->pbc, &t->nB))) return -1;
+    }
     if (need_anh) {
         t->A = slurp(p->anharm, &t->nA);
         t->O = slurp(p->overtone, &t->nO);

@@ -33,6 +33,8 @@ typedef struct {
     int propagation;     /* 0 Sparse, 1 Coupling, 2 Diagonal, 3 RK4 */
     int technique;       /* 0 Absorption, 1 2DIR, 2 GBIR, 3 SEIR, 4 EAIR, 5 noEAIR */
     char energy[256], dipole[256], coupling[256], anharm[256], overtone[256], shift[256];
+    int ham_onfly;       /* 1: TransitionDipole, 2: ExtendedDipole (couplings from positions) */
+    char position[256], pbc[256];
 } oracle_params;
 
 int oracle_real_size(void);

@@ -34,6 +34,7 @@ class OracleParams(ctypes.Structure):
         ("ham_coupling", ctypes.c_int), ("propagation", ctypes.c_int), ("technique", ctypes.c_int),
         ("energy", ctypes.c_char * 256), ("dipole", ctypes.c_char * 256), ("coupling", ctypes.c_char * 256),
         ("anharm", ctypes.c_char * 256), ("overtone", ctypes.c_char * 256), ("shift", ctypes.c_char * 256),
+        ("ham_onfly", ctypes.c_int), ("position", ctypes.c_char * 256), ("pbc", ctypes.c_char * 256),
     ]
 
 
@@ -66,6 +67,7 @@ def params(keywords, files):
     p.min1, p.min2, p.min3 = mins
     p.max1, p.max2, p.max3 = maxs
     p.ham_coupling = 1 if kw.get("HamiltonianType", "Full") == "Coupling" else 0
+    p.ham_onfly = {"TransitionDipole": 1, "ExtendedDipole": 2}.get(kw.get("HamiltonianType", "Full"), 0)
     prop = kw.get("Propagation", "")
     p.propagation = {"Coupling": 1, "Diagonal": 2, "RK4": 3}.get(prop, 0)
     p.technique = TECHNIQUES[kw.get("Technique", "Absorption")]
@@ -76,7 +78,7 @@ def params(keywords, files):
         s = np.float32(np.float32(np.float32(p.deltat) * ICM2IFS) * TWOPI) / np.float32(p.ts)
         thres = np.float32(thres * np.float32(s * s))
     p.thres = float(thres)
-    for key in ("energy", "dipole", "coupling", "anharm", "overtone", "shift"):
+    for key in ("energy", "dipole", "coupling", "anharm", "overtone", "shift", "position", "pbc"):
         setattr(p, key, (files.get(key) or "").encode())
     return p
 

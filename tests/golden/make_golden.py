@@ -62,6 +62,24 @@ CASES = {
                   tau_fs=50.0, jcut=2.0, mu_jitter=0.0, ham_type=synth.COUPLING, dipole_frames=1, seed=18),
         keywords=synth.c1_keywords(Singles=24, Length=300, RunTimes="40 0 0", Samplerate=40, Threshold=20000,
                                    FFT=512)),
+    "abs_tdc": dict(
+        spec=dict(n_sites=10, frames=300, dt_fs=2.0, geometry=C, sigma=12.0, ham_type=synth.COUPLING,
+                  dipole_frames=300, mu_jitter=0.05, seed=31),
+        keywords=synth.c0_keywords(Singles=10, Length=300, RunTimes="40 0 0", Samplerate=30,
+                                   HamiltonianType="TransitionDipole", Couplingcut=0.1, FFT=512),
+        positions=dict(mode="tdc", seed=32, spacing=5.0)),
+    "abs_edc_pbc": dict(
+        spec=dict(n_sites=9, frames=300, dt_fs=2.0, geometry=C, sigma=12.0, ham_type=synth.COUPLING,
+                  dipole_frames=300, mu_jitter=0.05, seed=33),
+        keywords=synth.c0_keywords(Singles=9, Length=300, RunTimes="40 0 0", Samplerate=30,
+                                   HamiltonianType="ExtendedDipole", Couplingcut=0.1, FFT=512),
+        positions=dict(mode="edc", seed=34, spacing=5.0, box=14.0)),
+    "2d_tdc": dict(
+        spec=dict(n_sites=5, frames=300, dt_fs=2.0, geometry=C, sigma=12.0, ham_type=synth.COUPLING,
+                  dipole_frames=300, mu_jitter=0.05, seed=35),
+        keywords=synth.c2_keywords(Singles=5, Length=300, RunTimes="8 0 8", Samplerate=40,
+                                   HamiltonianType="TransitionDipole"),
+        positions=dict(mode="tdc", seed=36, spacing=4.5)),
     # 2DIR family
     "2d_coupling": dict(
         spec=dict(n_sites=5, frames=300, dt_fs=2.0, geometry=C, spacing=6.0, sigma=12.0, tau_fs=200.0,
@@ -116,6 +134,10 @@ def materialise(case, directory):
             for site, a, b in case["shift"]:
                 f.write("%d %f %f\n" % (site, a, b))
         files["shift"] = path
+    if case.get("positions"):
+        pos = case["positions"]
+        files.update(synth.write_positions(directory, case["spec"]["n_sites"], case["spec"]["frames"], **pos))
+        files["coupling"] = ""  # couplings come from the positions
     return files
 
 

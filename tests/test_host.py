@@ -125,3 +125,16 @@ def test_generator_layout_and_determinism(tmp_path):
     off = np.array([C[b + a * (128 - a - 1) // 2] for a in range(64) for b in range(a + 1, 64)])
     nz = off[off != 0]
     assert (np.abs(nz) >= 2.0).all() and 1 < len(nz) / 64 < 20
+
+
+@pytest.mark.parametrize("ham,code", [("TransitionDipole", 2), ("ExtendedDipole", 3)])
+def test_parser_onfly_coupling_types(tmp_path, ham, code):
+    """HamiltonianType TransitionDipole / ExtendedDipole with the Positionfile
+    and PBCfile keywords (readinput.c:94,100)."""
+    path = tmp_path / "input"
+    path.write_text("Hamiltonianfile E.bin\nDipolefile D.bin\nPositionfile P.bin\nPBCfile B.bin\n"
+                    "HamiltonianType %s\nSingles 4\nLength 100\nSamplerate 10\nTimestep 2\nRunTimes 8 0 0\n"
+                    "Technique Absorption\n" % ham)
+    p = nise.read_input(str(path))
+    assert p.hamiltonian == code
+    assert p.positionFName == b"P.bin" and p.pbcFName == b"B.bin"

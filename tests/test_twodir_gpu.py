@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 CASES = helpers.cases()
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 SUPPORTED = ["2d_coupling", "2d_coupling_t2", "2d_rk4", "2d_sparse", "2d_sparse_trunc", "2d_full_anhfile", "2d_gbir",
-             "2d_seir", "2d_eair"]
+             "2d_seir", "2d_eair", "2d_tdc"]
 
 SUM_ORDER = 1e-10   # same single-precision operations, FP64 sums in another order
 T2_EIGEN = 1e-5     # t2 eigenvectors from a different Jacobi ordering (rounded to float)
