@@ -15,7 +15,8 @@
  *   nise_set_trajectory    <- the same, from record images already in host memory
  *   nise_absorption        <- absorption() (absorption.c:18-202), the response part
  *   nise_absorption_fft    <- do_1DFFT() (1DFFT.c:144-228)
- *   nise_2dir              <- calc_2DIR() (calc_2DIR.c:22-629), one GPU instead of MPI ranks
+ *   nise_2dir              <- calc_2DIR() (calc_2DIR.c:22-629) and calc_2DES()
+ *                             (calc_2DES.c:22-586), one GPU instead of MPI ranks
  *   nise_propagate         <- propagate_vector() (propagate.c:20-39), batched
  *   nise_propagate_doubles <- propagate_vec_coupling_S_doubles / _RK4_doubles /
  *                             propagate_double_sparce (propagate.c:376-1394)
@@ -53,7 +54,9 @@ enum { NISE_PROP_SPARSE = 0, NISE_PROP_COUPLING = 1, NISE_PROP_DIAGONAL = 2, NIS
  * couplings computed for every frame from the Positionfile and the dipoles,
  * read_trajectory.c:180-303). */
 enum { NISE_HAM_FULL = 0, NISE_HAM_COUPLING = 1, NISE_HAM_TDC = 2, NISE_HAM_EDC = 3 };
-/* Technique keyword (techniques on this path). */
+/* Technique keyword (techniques on this path).  The UVvis family
+ * (calc_2DES.c) is the 2DIR family with two-level sites: no overtone, no
+ * anharmonicity, doubles |ab> with a != b only. */
 enum {
     NISE_TECH_ABSORPTION = 0,
     NISE_TECH_2DIR = 1,
@@ -61,6 +64,11 @@ enum {
     NISE_TECH_SEIR = 3,
     NISE_TECH_EAIR = 4,
     NISE_TECH_NOEAIR = 5,
+    NISE_TECH_2DUVVIS = 6,
+    NISE_TECH_GBUVVIS = 7,
+    NISE_TECH_SEUVVIS = 8,
+    NISE_TECH_EAUVVIS = 9,
+    NISE_TECH_NOEAUVVIS = 10,
     NISE_TECH_OTHER = 99
 };
 /* Arithmetic of the propagation.  FP32 reproduces the reference's single
@@ -150,7 +158,8 @@ int nise_absorption(nise_ctx *ctx, double *re_S, double *im_S, int *samples);
 int nise_absorption_fft(nise_ctx *ctx, const double *re_S, const double *im_S, int samples, double *freq,
                         double *spec_re, double *spec_im, int max_rows, int *rows);
 
-/* 2DIR family (calc_2DIR.c:22-629): raw sums of the 12 response arrays,
+/* 2DIR family (calc_2DIR.c:22-629) and, for the UVvis techniques, calc_2DES
+ * (calc_2DES.c:22-586): raw sums of the 12 response arrays,
  * R[12][tmax3][tmax1] in the order rrIpar riIpar rrIIpar riIIpar rrIper
  * riIper rrIIper riIIper rrIcro riIcro rrIIcro riIIcro, and the sample
  * count print2D divides by. */

@@ -25,7 +25,8 @@ LIB_PATH = os.path.join(HERE, "libnise_b200.so")
 
 PROP = {"Sparse": 0, "Coupling": 1, "Diagonal": 2, "RK4": 3}
 HAM = {"Full": 0, "Coupling": 1}
-TECH = {"Absorption": 0, "2DIR": 1, "GBIR": 2, "SEIR": 3, "EAIR": 4, "noEAIR": 5}
+TECH = {"Absorption": 0, "2DIR": 1, "GBIR": 2, "SEIR": 3, "EAIR": 4, "noEAIR": 5,
+        "2DUVvis": 6, "GBUVvis": 7, "SEUVvis": 8, "EAUVvis": 9, "noEAUVvis": 10}
 FP32, FP64 = 0, 1
 BATCHED, PLAIN = 0, 1
 R2D_NAMES = ["RparI.dat", "RparII.dat", "RperI.dat", "RperII.dat", "RcroI.dat", "RcroII.dat"]

@@ -324,8 +324,9 @@ extern "C" int nise_load_files(nise_ctx *c) {
     if (!read_file(p.dipoleFName, D)) return nise_fail(c, NISE_ERR_IO, "Dipole file %s not found!", p.dipoleFName);
     if (p.hamiltonian == NISE_HAM_COUPLING && !read_file(p.couplingFName, C))
         return nise_fail(c, NISE_ERR_IO, "Coupling file not found!");
-    bool two_d = p.technique >= NISE_TECH_2DIR && p.technique <= NISE_TECH_NOEAIR;
-    if (two_d && p.anharmonicity == 0) {
+    // calc_2DIR.c:130-147 opens these files; calc_2DES (UVvis) reads neither
+    bool two_d_ir = p.technique >= NISE_TECH_2DIR && p.technique <= NISE_TECH_NOEAIR;
+    if (two_d_ir && p.anharmonicity == 0) {
         if (!read_file(p.anharFName, A))
             return nise_fail(c, NISE_ERR_IO, "Anharmonicity file %s not found!", p.anharFName);
         if (!read_file(p.overdipFName, O))

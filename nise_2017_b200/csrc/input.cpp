@@ -65,6 +65,11 @@ static int technique_code(const char *t) {
     if (!strcmp(t, "SEIR")) return NISE_TECH_SEIR;
     if (!strcmp(t, "EAIR")) return NISE_TECH_EAIR;
     if (!strcmp(t, "noEAIR")) return NISE_TECH_NOEAIR;
+    if (!strcmp(t, "2DUVvis")) return NISE_TECH_2DUVVIS;
+    if (!strcmp(t, "GBUVvis")) return NISE_TECH_GBUVVIS;
+    if (!strcmp(t, "SEUVvis")) return NISE_TECH_SEUVVIS;
+    if (!strcmp(t, "EAUVvis")) return NISE_TECH_EAUVVIS;
+    if (!strcmp(t, "noEAUVvis")) return NISE_TECH_NOEAUVVIS;
     return NISE_TECH_OTHER;
 }
 
@@ -156,7 +161,7 @@ extern "C" int nise_read_input(const char *path, nise_params *p) {
         return NISE_ERR_UNSUPPORTED;
     }
     // readinput.c:206-233
-    if (p->technique >= NISE_TECH_2DIR && p->technique <= NISE_TECH_NOEAIR) {
+    if (p->technique >= NISE_TECH_2DIR && p->technique <= NISE_TECH_NOEAUVVIS) {
         p->tmax3 = p->tmax1;
         if (p->length < p->tmax1 + p->tmax2 + p->tmax3) {
             nise_set_global_error("The trajectory length is too small");

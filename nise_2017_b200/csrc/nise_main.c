@@ -60,7 +60,7 @@ int main(int argc, char *argv[]) {
         printf("----------------------------------------------\n");
         printf(" Absorption calculation succesfully completed\n");
         printf("----------------------------------------------\n\n");
-    } else if (p.technique >= NISE_TECH_2DIR && p.technique <= NISE_TECH_NOEAIR) {
+    } else if (p.technique >= NISE_TECH_2DIR && p.technique <= NISE_TECH_NOEAUVVIS) {
         size_t plane = (size_t)p.tmax3 * p.tmax1;
         double *R = calloc(12 * plane, sizeof(double));
         int count = 0;
@@ -70,10 +70,11 @@ int main(int argc, char *argv[]) {
         free(R);
         printf("Samples %d\n", count);
         printf("----------------------------------------\n");
-        printf(" 2DIR calculation succesfully completed\n");
+        printf(" %s calculation succesfully completed\n", p.technique >= NISE_TECH_2DUVVIS ? "2DES" : "2DIR");
         printf("----------------------------------------\n\n");
     } else {
-        fprintf(stderr, "Technique '%s' is not on this engine's path (Absorption, 2DIR, GBIR, SEIR, EAIR, noEAIR)\n",
+        fprintf(stderr, "Technique '%s' is not on this engine's path (Absorption, 2DIR, GBIR, SEIR, EAIR, noEAIR, "
+                "2DUVvis, GBUVvis, SEUVvis, EAUVvis, noEAUVvis)\n",
                 p.technique_name);
         nise_destroy(c);
         return 2;

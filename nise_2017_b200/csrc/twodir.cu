@@ -1,4 +1,11 @@
-// 2DIR family (calc_2DIR.c:22-629) on one GPU.
+// 2DIR family (calc_2DIR.c:22-629) on one GPU, and the UVvis family
+// (calc_2DES.c:22-586), which is the same calculation for two-level sites:
+// the doubles basis keeps |ab> with a != b only (dipole_double_ES,
+// dipole_double_last_ES, NISE_subs.c:533-592) and the doubles propagators
+// have neither anharmonicity nor the sqrt(2) couplings to |aa>
+// (propagate_vec_coupling_S_doubles_ES, propagate_vec_RK4_doubles_ES,
+// propagate_double_sparce_ES; propagate.c:593-826, 1051-1181, 1400-1473).
+// The |aa> slots stay in the packed layout and stay exactly zero.
 //
 // The reference loops over (start point, molecular polarisation) work items
 // and, inside each, propagates dozens of vectors frame by frame.  Here the
@@ -54,6 +61,7 @@ struct TwoD {
     DevTraj T;
     int n, T1, T2, T3, ts, sample, s0, S;  // S start points in this chunk, the first is s0
     int gb, se, ea;
+    int es;                   // UVvis family: two-level doubles (no |aa>)
     int prop;                 // NISE_PROP_*
     float anh;                // Anharmonicity keyword (0: per-frame files)
     long f0;                  // first frame of the coefficient tables
@@ -315,9 +323,13 @@ __device__ __forceinline__ typename Vec2<R>::T make_vec2(R x, R y) {
 // (|aa>,|ab>) then (|ab>,|bb>); half diagonal phase.  Rotations of one
 // coupling touch disjoint pairs except |ab>, so lanes run them together; the
 // pivot |ac> stays in a register while the first index a is unchanged.
+//
+// Two-level sites (es, propagate.c:1051-1181): the c == a and c == b
+// rotations are absent, |ab> is rotated only with the |ac>/|bc> pairs.
 template <typename R, int CPL>
 __device__ void doubles_substep(typename Vec2<R>::T *F, const typename Vec2<R>::T *Uh, const Dcoef<R> *cf,
-                                const int2 *pairs, int K, int n, int W, int lane, const short *__restrict__ ci) {
+                                const int2 *pairs, int K, int n, int W, int lane, const short *__restrict__ ci,
+                                bool es) {
     typedef typename Vec2<R>::T R2;
     typedef Ar<R> A;
     const int slots = n * W;
@@ -358,7 +370,7 @@ __device__ void doubles_substep(typename Vec2<R>::T *F, const typename Vec2<R>::
             cur_a = a;
         }
         // c == a case: (|aa>,|ab>) with the sqrt(2) angle, by the lane owning c = b
-        if (b - lane >= 0 && ((b - lane) & 31) == 0) {
+        if (!es && b - lane >= 0 && ((b - lane) & 31) == 0) {
             const int j = (b - lane) >> 5;
             const int ix = ci ? ci[a * n + a] : circ(a, a, n, W);
             R2 X = F[ix];
@@ -371,7 +383,7 @@ __device__ void doubles_substep(typename Vec2<R>::T *F, const typename Vec2<R>::
 #pragma unroll
         for (int j = 0; j < CPL; j++) {
             const int c = lane + 32 * j;
-            if (c >= n || c == a) continue;
+            if (c >= n || c == a || (es && c == b)) continue;
             const bool sp = c == b;
             const int iq = ci ? ci[b * n + c] : circ(b, c, n, W);
             R2 Q = F[iq];
@@ -398,8 +410,11 @@ __device__ void doubles_substep(typename Vec2<R>::T *F, const typename Vec2<R>::
 }
 
 // Overtone dipoles: sqrt2 * mu when Anharmonicity != 0 (NISE_subs.c:490-494)
-// else the Overtonedipolefile record (read_over, read_trajectory.c:402-414).
+// else the Overtonedipolefile record (read_over, read_trajectory.c:402-414);
+// none for two-level sites, whose dipole_double_ES / dipole_double_last_ES
+// have no |aa> term (a zero operator adds only zeros there).
 __device__ __forceinline__ float over_mu(const TwoD &D, long t, int x, int i) {
+    if (D.es) return 0.0f;
     if (D.anh != 0.0f) return __fmul_rn(1.41421356237f, traj_mu(D.T, t, x, i));
     return D.T.over[t * (1 + 3L * D.n) + 1 + x * D.n + i];
 }
@@ -546,7 +561,7 @@ __global__ void __launch_bounds__(512) k2d_doubles(TwoD D, int vec_per_sample, D
             R h;
             if (sizeof(R) == 4) {
                 float hf = __fadd_rn(dg[i], dg[j]);
-                if (i == j) hf = __fsub_rn(hf, D.anh != 0.0f ? D.anh : D.T.anh[tl * (1L + n) + 1 + i]);
+                if (i == j && !D.es) hf = __fsub_rn(hf, D.anh != 0.0f ? D.anh : D.T.anh[tl * (1L + n) + 1 + i]);
                 float arg = __fmul_rn(__fmul_rn(0.5f, hf), D.f32_dsub);
                 R2 u;
                 u.x = (R)(float)cos((double)arg);
@@ -555,7 +570,7 @@ __global__ void __launch_bounds__(512) k2d_doubles(TwoD D, int vec_per_sample, D
                 (void)h;
             } else {
                 double hd = (double)dg[i] + (double)dg[j];
-                if (i == j) hd -= D.anh != 0.0f ? (double)D.anh : (double)D.T.anh[tl * (1L + n) + 1 + i];
+                if (i == j && !D.es) hd -= D.anh != 0.0f ? (double)D.anh : (double)D.T.anh[tl * (1L + n) + 1 + i];
                 double arg = 0.5 * hd * D.f64_dsub;
                 R2 u;
                 u.x = (R)cos(arg);
@@ -566,7 +581,7 @@ __global__ void __launch_bounds__(512) k2d_doubles(TwoD D, int vec_per_sample, D
         __syncthreads();
         const Dcoef<R> *cf = D.rot_static ? cf_static : cf_static + (tl - D.f0) * D.K;
         if (active)
-            for (int sub = 0; sub < D.ts; sub++) doubles_substep<R, CPL>(F, Uh, cf, D.pairs, D.K, n, Wd, lane, cidx);
+            for (int sub = 0; sub < D.ts; sub++) doubles_substep<R, CPL>(F, Uh, cf, D.pairs, D.K, n, Wd, lane, cidx, D.es != 0);
     }
 }
 
@@ -660,7 +675,7 @@ __device__ void rk4_doubles_step(const TwoD &D, long t, typename Vec2<R>::T *F, 
         for (int b = a; b < n; b++) {
             R hsum = A::add(ea, (R)traj_diag(D.T, t, b, false));
             R h = A::mul(f, hsum);
-            if (a == b) {
+            if (a == b && !D.es) {
                 R an = D.anh != 0.0f ? (R)D.anh : (R)D.T.anh[t * (1L + n) + 1 + a];
                 h = A::sub(h, A::mul(an, f));
             }
@@ -686,6 +701,8 @@ __device__ void rk4_doubles_step(const TwoD &D, long t, typename Vec2<R>::T *F, 
                 float jv = traj_coupling(D.T, t, a, b);
                 R h0 = fabsf(jv) > D.T.cut ? A::mul(f, (R)jv) : (R)0;
                 for (int c = 0; c < n; c++) {
+                    // two-level sites exclude |aa> and |bb> (propagate.c:648-662)
+                    if (D.es && (c == a || c == b)) continue;
                     int i1 = sindex(a, c, n), i2 = sindex(b, c, n);
                     R fac = (c == a || c == b) ? sq2 : (R)1;
                     R2 c1 = F[i1], c2 = F[i2], k1 = Kn[i1];
@@ -753,6 +770,11 @@ __device__ void sparse_doubles_step(const TwoD &D, long t, typename Vec2<R>::T *
             else
                 for (int e = 0; e < N2; e++) V[e] = F[e];
             for (int a = 0; a < n; a++) {
+                if (D.es) {  // propagate.c:1422-1426, 1465-1469: plain copies
+                    int ia = sindex(a, a, n);
+                    F[ia] = V[ia];
+                    continue;
+                }
                 R an = D.anh != 0.0f ? (R)D.anh : (R)D.T.anh[t * (1L + n) + 1 + a];
                 R arg = A::mul(fm, an);
                 R co = (R)cos((double)arg), si = (R)sin((double)arg);
@@ -776,6 +798,9 @@ __device__ void sparse_doubles_step(const TwoD &D, long t, typename Vec2<R>::T *
                     if (sA != u) g = sq2;
                     if (v != tA) g = sq2;
                     if (sA != u && v != tA) g = 1;
+                    // two-level sites: g = 0 when exactly one index differs
+                    // (propagate.c:1448-1450); those terms add only zeros
+                    if (D.es && g != (R)1) continue;
                     const int iA = sindex(sA, u, n), iB = sindex(tA, v, n);
                     R pr = A::sub(A::mul(ua.x, ub.x), A::mul(ua.y, ub.y));
                     R pi = A::add(A::mul(ua.y, ub.x), A::mul(ua.x, ub.y));
@@ -1068,8 +1093,11 @@ extern "C" int nise_2dir(nise_ctx *c, double *R, int *sample_count) {
     const nise_params &p = c->p;
     const int N = c->n, T1 = p.tmax1, T2 = p.tmax2, T3 = p.tmax3, prec = p.precision;
     int tech = p.technique;
-    if (tech < NISE_TECH_2DIR || tech > NISE_TECH_NOEAIR)
-        return nise_fail(c, NISE_ERR_ARG, "technique is not in the 2DIR family");
+    if (tech < NISE_TECH_2DIR || tech > NISE_TECH_NOEAUVVIS)
+        return nise_fail(c, NISE_ERR_ARG, "technique is not in the 2DIR or 2DUVvis family");
+    // calc_2DES.c:244-245, 377-378, 315, 420: the same selections by name
+    const bool es = tech >= NISE_TECH_2DUVVIS;
+    if (es) tech -= NISE_TECH_2DUVVIS - NISE_TECH_2DIR;
     const bool eig_scheme = p.propagation == NISE_PROP_SPARSE || p.propagation == NISE_PROP_DIAGONAL;
     if (eig_scheme && N > NISE_EIG_MAX_N)
         return nise_fail(c, NISE_ERR_UNSUPPORTED, "2DIR with Propagation Sparse/Diagonal is limited to 120 sites");
@@ -1079,7 +1107,7 @@ extern "C" int nise_2dir(nise_ctx *c, double *R, int *sample_count) {
     if (ea && N > 128) return nise_fail(c, NISE_ERR_UNSUPPORTED, "doubles manifold limited to 128 sites");
     if (T2 > 0 && N > NISE_EIG_MAX_N)
         return nise_fail(c, NISE_ERR_UNSUPPORTED, "t2 eigen step limited to 120 sites");
-    if (ea && p.anharmonicity == 0 && (!c->d_anh || !c->d_over))
+    if (ea && !es && p.anharmonicity == 0 && (!c->d_anh || !c->d_over))
         return nise_fail(c, NISE_ERR_IO, "Anharmonicity 0 needs Anharmonicfile and Overtonedipolefile");
     // calculateWorkset (MPI_subs.c:36-110)
     int total = (p.length - T1 - T2 - T3 - 1) / p.sample + 1;
@@ -1096,7 +1124,7 @@ extern "C" int nise_2dir(nise_ctx *c, double *R, int *sample_count) {
     long fmin = (long)begin * p.sample + 1, fmax = (long)(end - 1) * p.sample + T1 + T2 + T3 - 1;
     int rc;
     if ((rc = nise_check_frames(c, fmax))) return rc;
-    if (ea && p.anharmonicity == 0 && (fmax >= c->a_frames || fmax >= c->o_frames))
+    if (ea && !es && p.anharmonicity == 0 && (fmax >= c->a_frames || fmax >= c->o_frames))
         return nise_fail(c, NISE_ERR_IO, "Anharmonicity/overtone trajectory file to short");
     c->launches = 0;
     cudaEventRecord(c->ev0, c->stream);
@@ -1137,6 +1165,7 @@ extern "C" int nise_2dir(nise_ctx *c, double *R, int *sample_count) {
     D.T = T;
     D.n = N; D.T1 = T1; D.T2 = T2; D.T3 = T3; D.ts = p.ts; D.sample = p.sample;
     D.gb = gb; D.se = se; D.ea = ea;
+    D.es = es;
     D.prop = p.propagation;
     D.anh = p.anharmonicity;
     D.f0 = fmin;

@@ -619,9 +619,11 @@ void oracle_propagate_t2(const oracle_params *p, const float *H, void *cr, void 
 /* ------------------------------------------------------------------ */
 /* Doubles (two-exciton) manifold                                      */
 
-/* propagate_vec_coupling_S_doubles (propagate.c:902-1048). */
+/* propagate_vec_coupling_S_doubles (propagate.c:902-1048); with es, the
+ * two-level variant propagate_vec_coupling_S_doubles_ES (propagate.c:1051-1181):
+ * no anharmonicity, no rotations of the c == a and c == b cases. */
 static void prop_coupling_doubles(const oracle_params *p, const float *Hp, real *cr, real *ci, int m,
-                                  const float *Anh) {
+                                  const float *Anh, int es) {
     int N = p->singles, N2 = N * (N + 1) / 2;
     const real f = (real)p->deltat * (real)icm2ifs * (real)twoPi / m;
     real *H0 = (real *)malloc(sizeof(real) * N2);
@@ -634,7 +636,7 @@ static void prop_coupling_doubles(const oracle_params *p, const float *Hp, real 
         for (int b = a; b < N; b++) {
             int index = Sindex(a, b, N);
             H0[index] = (real)Hp[ia] + (real)Hp[Sindex(b, b, N)];
-            if (a == b) {
+            if (a == b && !es) {
                 if (p->anharmonicity == 0) H0[index] -= Anh[a];
                 else H0[index] -= p->anharmonicity;
             }
@@ -672,9 +674,11 @@ static void prop_coupling_doubles(const oracle_params *p, const float *Hp, real 
             for (; c < a; c++) ROT(a + c * ((N << 1) - c - 1) / 2, b + c * ((N << 1) - c - 1) / 2, co, si);
             si2 = -RSIN(J * sqrt2);
             co2 = RSQRT(1 - si2 * si2);
-            for (; c == a; c++) ROT(a + c * ((N << 1) - c - 1) / 2, b + c * ((N << 1) - c - 1) / 2, co2, si2);
+            for (; c == a; c++)
+                if (!es) ROT(a + c * ((N << 1) - c - 1) / 2, b + c * ((N << 1) - c - 1) / 2, co2, si2);
             for (; c < b; c++) ROT(c + aN, b + c * ((N << 1) - c - 1) / 2, co, si);
-            for (; c == b; c++) ROT(c + aN, b + c * ((N << 1) - c - 1) / 2, co2, si2);
+            for (; c == b; c++)
+                if (!es) ROT(c + aN, b + c * ((N << 1) - c - 1) / 2, co2, si2);
             for (; c < N; c++) ROT(c + aN, c + bN, co, si);
 #undef ROT
         }
@@ -686,14 +690,20 @@ static void prop_coupling_doubles(const oracle_params *p, const float *Hp, real 
     free(H0); free(H1); free(col); free(row); free(re_U); free(im_U); free(ocr); free(oci);
 }
 
-/* propagate_vec_RK4_doubles (propagate.c:376-590). */
-static void prop_RK4_doubles(const oracle_params *p, const float *Hp, real *cr, real *ci, int m, const float *Anh) {
+/* propagate_vec_RK4_doubles (propagate.c:376-590); with es the two-level
+ * variant propagate_vec_RK4_doubles_ES (propagate.c:593-826): diagonal part
+ * and update over |ab>, a < b, only; coupling terms with c == a or c == b
+ * left out. */
+static void prop_RK4_doubles(const oracle_params *p, const float *Hp, real *cr, real *ci, int m, const float *Anh,
+                             int es) {
     int N = p->singles, N2 = N * (N + 1) / 2;
     real f = (real)p->deltat * (real)icm2ifs * (real)twoPi / m;
     real *H0 = (real *)malloc(sizeof(real) * N2), *HD = (real *)malloc(sizeof(real) * N2);
     int *col = (int *)malloc(sizeof(int) * N2), *row = (int *)malloc(sizeof(int) * N2);
     real *kr[4], *ki[4];
     for (int q = 0; q < 4; q++) { kr[q] = (real *)calloc(N2, sizeof(real)); ki[q] = (real *)calloc(N2, sizeof(real)); }
+    char *isdiag = (char *)calloc(N2, 1);
+    for (int a = 0; a < N; a++) isdiag[Sindex(a, a, N)] = 1;
     int kmax = 0;
     for (int a = 0; a < N; a++)
         for (int b = a + 1; b < N; b++) {
@@ -705,7 +715,7 @@ static void prop_RK4_doubles(const oracle_params *p, const float *Hp, real *cr, 
         for (int b = a; b < N; b++) {
             int index = Sindex(a, b, N);
             HD[index] = f * (Hp[ia] + Hp[Sindex(b, b, N)]);
-            if (a == b) {
+            if (a == b && !es) {
                 if (p->anharmonicity == 0) HD[index] -= Anh[a] * f;
                 else HD[index] -= p->anharmonicity * f;
             }
@@ -719,6 +729,7 @@ static void prop_RK4_doubles(const oracle_params *p, const float *Hp, real *cr, 
             const real *pr = q ? kr[q - 1] : NULL, *pi = q ? ki[q - 1] : NULL;
             real *Kr = kr[q], *Ki = ki[q];
             for (int k = 0; k < N2; k++) {
+                if (es && isdiag[k]) continue;
                 if (q == 0) { Kr[k] += HD[k] * ci[k]; Ki[k] -= HD[k] * cr[k]; }
                 else if (q < 3) { Kr[k] += HD[k] * (ci[k] + pi[k] * 0.5); Ki[k] -= HD[k] * (cr[k] + pr[k] * 0.5); }
                 else { Kr[k] += HD[k] * (ci[k] + pi[k]); Ki[k] -= HD[k] * (cr[k] + pr[k]); }
@@ -726,6 +737,7 @@ static void prop_RK4_doubles(const oracle_params *p, const float *Hp, real *cr, 
             for (int k = 0; k < kmax; k++) {
                 int a = col[k], b = row[k];
                 for (int c = 0; c < N; c++) {
+                    if (es && (c == a || c == b)) continue;
                     int i1 = Sindex(a, c, N), i2 = Sindex(b, c, N);
                     float factor = 1.0;
                     if (c == a) factor = sqrt2;
@@ -745,12 +757,13 @@ static void prop_RK4_doubles(const oracle_params *p, const float *Hp, real *cr, 
         }
         real norm = find_norm(cr, ci, N2);
         for (int k = 0; k < N2; k++) {
+            if (es && isdiag[k]) continue;
             cr[k] = cr[k] + (kr[0][k] + 2.0 * kr[1][k] + 2.0 * kr[2][k] + kr[3][k]) / 6.0;
             ci[k] = ci[k] + (ki[0][k] + 2.0 * ki[1][k] + 2.0 * ki[2][k] + ki[3][k]) / 6.0;
         }
         re_normalize(cr, ci, N2, norm);
     }
-    free(H0); free(HD); free(col); free(row);
+    free(H0); free(HD); free(col); free(row); free(isdiag);
     for (int q = 0; q < 4; q++) { free(kr[q]); free(ki[q]); }
 }
 
@@ -774,15 +787,18 @@ static int time_evolution_mat(const oracle_params *p, const float *Hp, real *Ur,
     return elements;
 }
 
-/* propagate_double_sparce (propagate.c:1304-1394). */
+/* propagate_double_sparce (propagate.c:1304-1394); with es the two-level
+ * variant propagate_double_sparce_ES (propagate.c:1400-1473): plain copies
+ * instead of the anharmonic phases, g = 0 where exactly one index differs. */
 static void prop_double_sparse(const oracle_params *p, const real *Ur, const real *Ui, const int *R, const int *C,
-                               real *fr, real *fi, int elements, int m, const float *Anh) {
+                               real *fr, real *fi, int elements, int m, const float *Anh, int es) {
     int N = p->singles, Nf = N * (N + 1) / 2;
     real f = (real)p->deltat * (real)icm2ifs * (real)twoPi;
     real fm = f * 0.5 / m;
     real *vr = (real *)calloc(Nf, sizeof(real)), *vi = (real *)calloc(Nf, sizeof(real));
     real *co = (real *)calloc(N, sizeof(real)), *si = (real *)calloc(N, sizeof(real));
     for (int i = 0; i < N; i++) {
+        if (es) { co[i] = 1, si[i] = 0; continue; }
         real an = p->anharmonicity != 0 ? (real)p->anharmonicity : (real)Anh[i];
         co[i] = cos(fm * an), si[i] = sin(fm * an);
     }
@@ -791,6 +807,7 @@ static void prop_double_sparse(const oracle_params *p, const real *Ur, const rea
         memcpy(vi, fi, sizeof(real) * Nf);
         for (int a = 0; a < N; a++) {
             int A = Sindex(a, a, N);
+            if (es) { fr[A] = vr[A], fi[A] = vi[A]; continue; }
             fr[A] = co[a] * vr[A] - si[a] * vi[A];
             fi[A] = co[a] * vi[A] + si[a] * vr[A];
         }
@@ -804,8 +821,8 @@ static void prop_double_sparse(const oracle_params *p, const real *Ur, const rea
                 real Ubr = Ur[b], Ubi = Ui[b];
                 real g = 1;
                 int iA = Sindex(s, u, N), iB = Sindex(t, v, N);
-                if (s != u) g = sqrt2;
-                if (v != t) g = sqrt2;
+                if (s != u) g = es ? 0 : sqrt2;
+                if (v != t) g = es ? 0 : sqrt2;
                 if (s != u && v != t) g = 1;
                 vr[iA] += (Uar * Ubr - Uai * Ubi) * fr[iB] * g;
                 vr[iA] -= (Uai * Ubr + Uar * Ubi) * fi[iB] * g;
@@ -817,6 +834,7 @@ static void prop_double_sparse(const oracle_params *p, const real *Ur, const rea
         memcpy(fi, vi, sizeof(real) * Nf);
         for (int a = 0; a < N; a++) {
             int A = Sindex(a, a, N);
+            if (es) { fr[A] = vr[A], fi[A] = vi[A]; continue; }
             fr[A] = co[a] * vr[A] - si[a] * vi[A];
             fi[A] = co[a] * vi[A] + si[a] * vr[A];
         }
@@ -824,16 +842,19 @@ static void prop_double_sparse(const oracle_params *p, const real *Ur, const rea
     free(vr); free(vi); free(co); free(si);
 }
 
+/* propagate_double_2DIR_control / propagate_double_2DES_control
+ * (propagate.c:1476-1591, 1594-1710) for one vector: the UVvis techniques
+ * (technique >= 6) take the two-level propagators. */
 void oracle_propagate_doubles(const oracle_params *p, const float *H, void *cr, void *ci, const float *anh) {
-    int N = p->singles;
-    if (p->propagation == 1) prop_coupling_doubles(p, H, (real *)cr, (real *)ci, p->ts, anh);
-    else if (p->propagation == 3) prop_RK4_doubles(p, H, (real *)cr, (real *)ci, p->ts, anh);
+    int N = p->singles, es = p->technique >= 6;
+    if (p->propagation == 1) prop_coupling_doubles(p, H, (real *)cr, (real *)ci, p->ts, anh, es);
+    else if (p->propagation == 3) prop_RK4_doubles(p, H, (real *)cr, (real *)ci, p->ts, anh, es);
     else {
         real *Ur = (real *)calloc((size_t)N * N, sizeof(real)), *Ui = (real *)calloc((size_t)N * N, sizeof(real));
         int *Rs = (int *)calloc((size_t)N * N, sizeof(int)), *Cs = (int *)calloc((size_t)N * N, sizeof(int));
         /* the reference passes (Cs, Rs) in swapped order (propagate.c:1495-1496) */
         int el = time_evolution_mat(p, H, Ur, Ui, Cs, Rs, p->ts);
-        prop_double_sparse(p, Ur, Ui, Rs, Cs, (real *)cr, (real *)ci, el, p->ts, anh);
+        prop_double_sparse(p, Ur, Ui, Rs, Cs, (real *)cr, (real *)ci, el, p->ts, anh, es);
         free(Ur); free(Ui); free(Rs); free(Cs);
     }
 }
@@ -878,6 +899,36 @@ static void dipole_double_last(const oracle_params *p, const float *dipole, cons
             fi[i] += dipole[j] * ci[index];
         }
     }
+}
+
+/* dipole_double_ES (NISE_subs.c:533-548): no |aa> term. */
+static void dipole_double_ES(const oracle_params *p, const float *dipole, const real *cr, const real *ci, real *fr,
+                             real *fi) {
+    int n = p->singles, N = n * (n + 1) / 2;
+    for (int i = 0; i < N; i++) fr[i] = 0, fi[i] = 0;
+    for (int i = 0; i < n; i++)
+        for (int j = i + 1; j < n; j++) {
+            int index = Sindex(i, j, n);
+            fr[index] += dipole[i] * cr[j];
+            fi[index] += dipole[i] * ci[j];
+            fr[index] += dipole[j] * cr[i];
+            fi[index] += dipole[j] * ci[i];
+        }
+}
+
+/* dipole_double_last_ES (NISE_subs.c:578-592). */
+static void dipole_double_last_ES(const oracle_params *p, const float *dipole, const real *cr, const real *ci,
+                                  real *fr, real *fi) {
+    int n = p->singles;
+    for (int i = 0; i < n; i++) fr[i] = 0, fi[i] = 0;
+    for (int i = 0; i < n; i++)
+        for (int j = i + 1; j < n; j++) {
+            int index = Sindex(i, j, n);
+            fr[j] += dipole[i] * cr[index];
+            fi[j] += dipole[i] * ci[index];
+            fr[i] += dipole[j] * cr[index];
+            fi[i] += dipole[j] * ci[index];
+        }
 }
 
 void oracle_dipole_double(const oracle_params *p, const float *dipole, const void *cr, const void *ci, void *fr,
@@ -1037,14 +1088,19 @@ void oracle_print2d_normalize(const oracle_params *p, double *re, double *im, in
         }
 }
 
+/* calc_2DIR (calc_2DIR.c:22-629); for the UVvis techniques 6-10 calc_2DES
+ * (calc_2DES.c:22-586), which differs only in the doubles operators and
+ * propagators (dipole_double_ES, dipole_double_last_ES, the _ES propagators)
+ * and in reading no anharmonicity or overtone files. */
 int oracle_2dir(const oracle_params *p, double *Rout, int *sample_count) {
     int N = p->singles, nn2 = N * (N + 1) / 2, T1 = p->tmax1, T3 = p->tmax3;
-    int tech = p->technique;
+    int tech = p->technique, es = tech >= 6;
+    if (es) tech -= 5; /* 2DUVvis GBUVvis SEUVvis EAUVvis noEAUVvis -> 2DIR ... noEAIR */
     int do_gb = (tech == 1 || tech == 2 || tech == 5), do_se = (tech == 1 || tech == 3 || tech == 5);
     int do_ea = (tech == 1 || tech == 4);
     float shift1 = (p->max1 + p->min1) / 2;
     traj_t t;
-    int need_anh = (p->anharmonicity == 0 && (tech >= 1 && tech <= 5));
+    int need_anh = (p->anharmonicity == 0 && !es && (tech >= 1 && tech <= 5));
     if (traj_open(&t, p, shift1, need_anh) != 0) { traj_free(&t); return -1; }
     /* calculateWorkset (MPI_subs.c:36-110) */
     int total = (p->length - p->tmax1 - p->tmax2 - p->tmax3 - 1) / p->sample + 1;
@@ -1133,11 +1189,18 @@ int oracle_2dir(const oracle_params *p, double *Rout, int *sample_count) {
             CHK(mu_read(&t, mtmp, tk, px[2]));
             for (int i = 0; i < N; i++) mut3r[i] = mtmp[i];
             if (do_ea) { /* calc_2DIR.c:331-348 */
-                if (p->anharmonicity == 0) CHK(read_over(&t, over, tk, px[2]));
-                dipole_double(p, mtmp, leftrr, leftri, fr, fi, over);
-                for (int t1 = 0; t1 < T1; t1++)
-                    dipole_double(p, mtmp, leftnr + t1 * N, leftni + t1 * N, ft1r + (size_t)t1 * nn2,
-                                  ft1i + (size_t)t1 * nn2, over);
+                if (es) {
+                    dipole_double_ES(p, mtmp, leftrr, leftri, fr, fi);
+                    for (int t1 = 0; t1 < T1; t1++)
+                        dipole_double_ES(p, mtmp, leftnr + t1 * N, leftni + t1 * N, ft1r + (size_t)t1 * nn2,
+                                         ft1i + (size_t)t1 * nn2);
+                } else {
+                    if (p->anharmonicity == 0) CHK(read_over(&t, over, tk, px[2]));
+                    dipole_double(p, mtmp, leftrr, leftri, fr, fi, over);
+                    for (int t1 = 0; t1 < T1; t1++)
+                        dipole_double(p, mtmp, leftnr + t1 * N, leftni + t1 * N, ft1r + (size_t)t1 * nn2,
+                                      ft1i + (size_t)t1 * nn2, over);
+                }
                 for (int i = 0; i < T1 * N; i++) rightrr[i] = leftnr[i], rightri[i] = -leftni[i];
                 for (int i = 0; i < N; i++) rightnr[i] = leftrr[i], rightni[i] = -leftri[i];
             }
@@ -1184,11 +1247,18 @@ int oracle_2dir(const oracle_params *p, double *Rout, int *sample_count) {
                 for (int t3 = 0; t3 < T3; t3++) {
                     int tl = tk + t3;
                     CHK(mu_read(&t, mut4, tl, px[3]));
-                    if (p->anharmonicity == 0) CHK(read_over(&t, over, tl, px[3]));
-                    dipole_double_last(p, mut4, fr, fi, leftrr, leftri, over);
-                    for (int t1 = 0; t1 < T1; t1++)
-                        dipole_double_last(p, mut4, ft1r + (size_t)t1 * nn2, ft1i + (size_t)t1 * nn2, leftnr + t1 * N,
-                                           leftni + t1 * N, over);
+                    if (es) {
+                        dipole_double_last_ES(p, mut4, fr, fi, leftrr, leftri);
+                        for (int t1 = 0; t1 < T1; t1++)
+                            dipole_double_last_ES(p, mut4, ft1r + (size_t)t1 * nn2, ft1i + (size_t)t1 * nn2,
+                                                  leftnr + t1 * N, leftni + t1 * N);
+                    } else {
+                        if (p->anharmonicity == 0) CHK(read_over(&t, over, tl, px[3]));
+                        dipole_double_last(p, mut4, fr, fi, leftrr, leftri, over);
+                        for (int t1 = 0; t1 < T1; t1++)
+                            dipole_double_last(p, mut4, ft1r + (size_t)t1 * nn2, ft1i + (size_t)t1 * nn2,
+                                               leftnr + t1 * N, leftni + t1 * N, over);
+                    }
                     for (int t1 = 0; t1 < T1; t1++) {
                         acc rrI = 0, riI = 0, rrII = 0, riII = 0;
                         const real *Rr = rightrr + t1 * N, *Ri = rightri + t1 * N;
@@ -1209,7 +1279,7 @@ int oracle_2dir(const oracle_params *p, double *Rout, int *sample_count) {
                         }
                     }
                     CHK(read_He(&t, H, tl));
-                    if (p->anharmonicity == 0) CHK(read_A(&t, Anh, tl));
+                    if (p->anharmonicity == 0 && !es) CHK(read_A(&t, Anh, tl));
                     /* propagate_double_2DIR_control (propagate.c:1476-1591) */
                     oracle_propagate_doubles(p, H, fr, fi, Anh);
                     for (int t1 = 0; t1 < T1; t1++)

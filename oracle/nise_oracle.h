@@ -31,7 +31,7 @@ typedef struct {
     float min1, max1, min2, max2, min3, max3;
     int ham_coupling;    /* 1: HamiltonianType Coupling, 0: Full */
     int propagation;     /* 0 Sparse, 1 Coupling, 2 Diagonal, 3 RK4 */
-    int technique;       /* 0 Absorption, 1 2DIR, 2 GBIR, 3 SEIR, 4 EAIR, 5 noEAIR */
+    int technique;       /* 0 Absorption, 1 2DIR, 2 GBIR, 3 SEIR, 4 EAIR, 5 noEAIR, 6-10 the UVvis names */
     char energy[256], dipole[256], coupling[256], anharm[256], overtone[256], shift[256];
     int ham_onfly;       /* 1: TransitionDipole, 2: ExtendedDipole (couplings from positions) */
     char position[256], pbc[256];

@@ -15,7 +15,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 
-TECHNIQUES = {"Absorption": 0, "2DIR": 1, "GBIR": 2, "SEIR": 3, "EAIR": 4, "noEAIR": 5}
+TECHNIQUES = {"Absorption": 0, "2DIR": 1, "GBIR": 2, "SEIR": 3, "EAIR": 4, "noEAIR": 5,
+              "2DUVvis": 6, "GBUVvis": 7, "SEUVvis": 8, "EAUVvis": 9, "noEAUVvis": 10}
 ICM2IFS = np.float32(2.99792458e-5)
 TWOPI = np.float32(2 * 3.14159265359)
 

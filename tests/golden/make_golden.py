@@ -120,6 +120,31 @@ CASES = {
         spec=dict(n_sites=5, frames=300, dt_fs=2.0, geometry=C, spacing=6.0, seed=26, ham_type=synth.COUPLING,
                   dipole_frames=1, mu_jitter=0.0),
         keywords=synth.c2_keywords(Singles=5, Length=300, RunTimes="8 2 8", Samplerate=40, Technique="EAIR")),
+    # 2DUVvis family (calc_2DES.c): two-level doubles, no anharmonicity or overtone files
+    "2d_uvvis": dict(
+        spec=dict(n_sites=5, frames=300, dt_fs=2.0, geometry=C, spacing=6.0, sigma=12.0, tau_fs=200.0,
+                  mu_jitter=0.0, ham_type=synth.COUPLING, dipole_frames=1, seed=41),
+        keywords=synth.c2_keywords(Singles=5, Length=300, RunTimes="8 2 8", Samplerate=40, Technique="2DUVvis",
+                                   Anharmonicity=0)),
+    "2d_uvvis_rk4": dict(
+        spec=dict(n_sites=5, frames=300, dt_fs=2.0, geometry=C, spacing=6.0, sigma=12.0, tau_fs=200.0,
+                  mu_jitter=0.0, ham_type=synth.COUPLING, dipole_frames=1, seed=42),
+        keywords=synth.c2_keywords(Singles=5, Length=300, RunTimes="8 0 8", Samplerate=40, Technique="2DUVvis",
+                                   Propagation="RK4", Anharmonicity=0)),
+    "2d_uvvis_sparse": dict(
+        spec=dict(n_sites=5, frames=300, dt_fs=2.0, geometry=C, spacing=6.0, sigma=12.0, tau_fs=200.0,
+                  mu_jitter=0.0, ham_type=synth.COUPLING, dipole_frames=1, seed=43),
+        keywords=synth.c2_keywords(Singles=5, Length=300, RunTimes="8 0 8", Samplerate=40, Technique="2DUVvis",
+                                   Propagation="Sparse", Threshold=0, Anharmonicity=0)),
+    "2d_eauvvis_full": dict(
+        spec=dict(n_sites=4, frames=260, dt_fs=2.0, geometry=synth.CHAIN, j_nn=-6.0, j_sigma=1.5, seed=44),
+        keywords=synth.c2_keywords(Singles=4, Length=260, RunTimes="6 1 6", Samplerate=30, Technique="EAUVvis",
+                                   HamiltonianType="Full", Anharmonicity=0)),
+    "2d_noeauvvis": dict(
+        spec=dict(n_sites=5, frames=300, dt_fs=2.0, geometry=C, spacing=6.0, seed=45, ham_type=synth.COUPLING,
+                  dipole_frames=1, mu_jitter=0.0),
+        keywords=synth.c2_keywords(Singles=5, Length=300, RunTimes="8 2 8", Samplerate=40,
+                                   Technique="noEAUVvis")),
 }
 
 

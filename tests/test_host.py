@@ -138,3 +138,16 @@ def test_parser_onfly_coupling_types(tmp_path, ham, code):
     p = nise.read_input(str(path))
     assert p.hamiltonian == code
     assert p.positionFName == b"P.bin" and p.pbcFName == b"B.bin"
+
+
+@pytest.mark.parametrize("tech,code", [("2DUVvis", 6), ("GBUVvis", 7), ("SEUVvis", 8), ("EAUVvis", 9),
+                                       ("noEAUVvis", 10)])
+def test_parser_uvvis_techniques(tmp_path, tech, code):
+    """The calc_2DES technique names (NISE.c:296): a waiting-time technique,
+    so tmax3 follows tmax1 and the length check covers t1 + t2 + t3
+    (readinput.c:208-218)."""
+    p = nise.read_input(write(tmp_path, "Technique %s\nLength 100\nRunTimes 20 5 3\n" % tech))
+    assert p.technique == code == nise.TECH[tech]
+    assert (p.tmax1, p.tmax2, p.tmax3) == (20, 5, 20)
+    with pytest.raises(nise.NiseError):
+        nise.read_input(write(tmp_path, "Technique %s\nLength 40\nRunTimes 20 5 3\n" % tech))

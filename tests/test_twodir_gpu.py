@@ -22,7 +22,8 @@ pytestmark = pytest.mark.gpu
 CASES = helpers.cases()
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 SUPPORTED = ["2d_coupling", "2d_coupling_t2", "2d_rk4", "2d_sparse", "2d_sparse_trunc", "2d_full_anhfile", "2d_gbir",
-             "2d_seir", "2d_eair", "2d_tdc"]
+             "2d_seir", "2d_eair", "2d_tdc", "2d_uvvis", "2d_uvvis_rk4", "2d_uvvis_sparse", "2d_eauvvis_full",
+             "2d_noeauvvis"]
 
 SUM_ORDER = 1e-10   # same single-precision operations, FP64 sums in another order
 T2_EIGEN = 1e-5     # t2 eigenvectors from a different Jacobi ordering (rounded to float)
@@ -60,7 +61,8 @@ def test_fp32_matches_oracle_and_reference(name, tmp_path):
     assert helpers.rel2d(Rn, helpers.golden(name)["R"]) < (REF_EIGEN if eig else REF_FP32_SUMS)
 
 
-@pytest.mark.parametrize("name", ["2d_coupling", "2d_coupling_t2", "2d_eair", "2d_sparse"])
+@pytest.mark.parametrize("name", ["2d_coupling", "2d_coupling_t2", "2d_eair", "2d_sparse", "2d_uvvis",
+                                  "2d_uvvis_sparse", "2d_uvvis_rk4"])
 def test_fp64_matches_fp64_oracle(name, tmp_path):
     case = CASES[name]
     files = helpers.materialise(case, str(tmp_path))
@@ -78,6 +80,31 @@ def test_rk4_techniques(tech, tmp_path):
     p, R, n = run(kw, files)
     oR, on = oracle.twodir(oracle.params(kw, files), "f32a64")
     assert n == on and helpers.rel2d(R, oR) < T2_EIGEN
+
+
+@pytest.mark.parametrize("tech", ["GBUVvis", "SEUVvis", "noEAUVvis", "EAUVvis", "2DUVvis"])
+def test_rk4_uvvis_techniques(tech, tmp_path):
+    """The two-level (calc_2DES) doubles with RK4 and t2 > 0; no anharmonicity
+    or overtone file is read."""
+    s = synth.c2_spec(n_sites=6, frames=300, seed=32)
+    files = synth.write(s, str(tmp_path))
+    kw = synth.c2_keywords(Singles=6, Length=300, RunTimes="8 2 8", Samplerate=40, Propagation="RK4", Technique=tech,
+                           Anharmonicity=0)
+    p, R, n = run(kw, files)
+    oR, on = oracle.twodir(oracle.params(kw, files), "f32a64")
+    assert n == on and helpers.rel2d(R, oR) < T2_EIGEN
+
+
+def test_uvvis_cluster_n40(tmp_path):
+    """2DUVvis at N = 40 (two columns per lane in the doubles kernel)."""
+    s = synth.c2_spec(n_sites=40, frames=200, seed=44)
+    files = synth.write(s, str(tmp_path))
+    kw = synth.c2_keywords(Singles=40, Length=200, RunTimes="6 0 6", Samplerate=80, Technique="2DUVvis",
+                           Anharmonicity=0)
+    p, R, n = run(kw, files)
+    oR, on = oracle.twodir(oracle.params(kw, files), "f32a64")
+    assert n == on
+    assert helpers.rel2d(R, oR) < SUM_ORDER
 
 
 def test_larger_cluster_and_chunks(tmp_path):
@@ -102,7 +129,7 @@ def test_cluster_n40(tmp_path):
     assert helpers.rel2d(R, oR) < SUM_ORDER
 
 
-@pytest.mark.parametrize("name", ["2d_coupling", "2d_coupling_t2"])
+@pytest.mark.parametrize("name", ["2d_coupling", "2d_coupling_t2", "2d_uvvis"])
 def test_plain_matches_batched(name, tmp_path):
     """One start point per launch of every kernel gives the batched result
     (the start points' responses are summed in another grouping)."""
