@@ -17,6 +17,8 @@
  *   nise_absorption_fft    <- do_1DFFT() (1DFFT.c:144-228)
  *   nise_2dir              <- calc_2DIR() (calc_2DIR.c:22-629) and calc_2DES()
  *                             (calc_2DES.c:22-586), one GPU instead of MPI ranks
+ *   nise_linear            <- LD(), raman(), sfg(), calc_DOS(), calc_CD() (calc_LD.c,
+ *                             raman.c, sfg.c, calc_DOS.c, calc_CD.c)
  *   nise_propagate         <- propagate_vector() (propagate.c:20-39), batched
  *   nise_propagate_doubles <- propagate_vec_coupling_S_doubles / _RK4_doubles /
  *                             propagate_double_sparce (propagate.c:376-1394)
@@ -69,6 +71,11 @@ enum {
     NISE_TECH_SEUVVIS = 8,
     NISE_TECH_EAUVVIS = 9,
     NISE_TECH_NOEAUVVIS = 10,
+    NISE_TECH_LD = 11,
+    NISE_TECH_RAMAN = 12,
+    NISE_TECH_SFG = 13,
+    NISE_TECH_DOS = 14,
+    NISE_TECH_CD = 15,
     NISE_TECH_OTHER = 99
 };
 /* Arithmetic of the propagation.  FP32 reproduces the reference's single
@@ -116,8 +123,9 @@ typedef struct {
                                       vectors per CTA, 8 the sliced-ELL Taylor kernel, 10 the
                                       sliced-ELL Chebyshev kernel (FP32), 12 the sliced-ELL
                                       Taylor kernel with 4 vectors per CTA (FP32) */
-    char positionFName[256];       /* Positionfile (TransitionDipole / ExtendedDipole) */
+    char positionFName[256];       /* Positionfile (TransitionDipole / ExtendedDipole; CD) */
     char pbcFName[256];            /* PBCfile: periodic box per frame (optional) */
+    char alphaFName[256];          /* Alphafile: polarisabilities (Raman, SFG) */
 } nise_params;
 
 typedef struct nise_ctx nise_ctx;
@@ -173,7 +181,12 @@ int nise_propagate(nise_ctx *ctx, const float *H, void *re, void *im, int nvec, 
  * step) for vectors of length N(N+1)/2; anh is per-site (or NULL). */
 int nise_propagate_doubles(nise_ctx *ctx, const float *H, void *re, void *im, int nvec, const float *anh);
 
-/* Output files in the reference's text formats. */
+/* Output files in the reference's text formats.  nise_write_td writes a
+ * time-domain response "t Re Im" per line divided by samples; the files of
+ * absorption.c:181-189 and most techniques end each line with a blank
+ * (trailing_blank 1), TD_DOS.dat does not (calc_DOS.c:207-210). */
+int nise_write_td(const char *path, const nise_params *p, const double *re_S, const double *im_S, int samples,
+                  int trailing_blank);
 int nise_write_td_absorption(const char *path, const nise_params *p, const double *re_S, const double *im_S,
                              int samples);
 int nise_write_spectrum(const char *path, const double *freq, const double *spec_re, const double *spec_im,
@@ -200,6 +213,27 @@ int nise_set_trajectory_onfly(nise_ctx *ctx, const void *energy, size_t energy_b
                               size_t dipole_bytes, const void *position, size_t position_bytes, const void *pbc,
                               size_t pbc_bytes, const void *anharm, size_t anharm_bytes, const void *overtone,
                               size_t overtone_bytes);
+
+/* Operator records of the linear techniques: alpha the Alphafile (read_alpha,
+ * read_trajectory.c:380-399: int32 tag + 6N floats per frame, components
+ * xx xy xz yy yz zz) for Raman and SFG; position the CD Positionfile (the
+ * dipole-file layout, int32 tag + 3N floats per frame).  Either may be NULL;
+ * nise_load_files calls this for Raman, SFG and CD. */
+int nise_set_operators(nise_ctx *ctx, const void *alpha, size_t alpha_bytes, const void *position,
+                       size_t position_bytes);
+
+/* Linear techniques besides absorption: LD (calc_LD.c:15-290), Raman
+ * (raman.c:15-307), SFG (sfg.c:15-297), DOS (calc_DOS.c:15-234) and CD
+ * (calc_CD.c:15-392), chosen by the context's technique.  Writes the raw
+ * response sums of each output channel, re_S/im_S[channel][tmax1] (LD, DOS,
+ * CD: one channel; Raman: VV, VH; SFG: PPP, SSP), the channel count and the
+ * sample count the reference divides by.  Each channel's spectrum is
+ * nise_absorption_fft of its response. */
+int nise_linear(nise_ctx *ctx, double *re_S, double *im_S, int max_channels, int *channels, int *samples);
+/* Output file of channel k of a linear technique: the time-domain file
+ * (td != 0, e.g. TD_Raman_VV.dat) or the spectrum (Raman_VV.dat); NULL past
+ * the last channel. */
+const char *nise_linear_file(int technique, int channel, int td);
 
 /* Batched linear absorption of many contexts (trajectories of any size and
  * scheme, one device): nise_batch_create plans every job (optionally

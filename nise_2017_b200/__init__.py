@@ -26,7 +26,8 @@ LIB_PATH = os.path.join(HERE, "libnise_b200.so")
 PROP = {"Sparse": 0, "Coupling": 1, "Diagonal": 2, "RK4": 3}
 HAM = {"Full": 0, "Coupling": 1}
 TECH = {"Absorption": 0, "2DIR": 1, "GBIR": 2, "SEIR": 3, "EAIR": 4, "noEAIR": 5,
-        "2DUVvis": 6, "GBUVvis": 7, "SEUVvis": 8, "EAUVvis": 9, "noEAUVvis": 10}
+        "2DUVvis": 6, "GBUVvis": 7, "SEUVvis": 8, "EAUVvis": 9, "noEAUVvis": 10,
+        "LD": 11, "Raman": 12, "SFG": 13, "DOS": 14, "CD": 15}
 FP32, FP64 = 0, 1
 BATCHED, PLAIN = 0, 1
 R2D_NAMES = ["RparI.dat", "RparII.dat", "RperI.dat", "RperII.dat", "RcroI.dat", "RcroII.dat"]
@@ -39,6 +40,7 @@ EXPORTED = [
     "nise_probe_fp32_peak", "nise_absorption_noalloc", "nise_2dfft_files", "nise_absorption_model",
     "nise_backward_absorption", "nise_absorption_tune", "nise_batch_create", "nise_batch_run", "nise_batch_result",
     "nise_batch_spectrum", "nise_batch_timing", "nise_batch_error", "nise_batch_destroy", "nise_set_trajectory_onfly",
+    "nise_set_operators", "nise_linear", "nise_linear_file", "nise_write_td",
 ]
 
 
@@ -64,6 +66,7 @@ class Params(ctypes.Structure):
         ("overdipFName", ctypes.c_char * 256), ("singleShiftFName", ctypes.c_char * 256),
         ("precision", ctypes.c_int), ("launch_mode", ctypes.c_int), ("device", ctypes.c_int),
         ("kernel_config", ctypes.c_int), ("positionFName", ctypes.c_char * 256), ("pbcFName", ctypes.c_char * 256),
+        ("alphaFName", ctypes.c_char * 256),
     ]
 
 
@@ -117,12 +120,28 @@ def lib():
         L.nise_batch_error.restype = ctypes.c_char_p
         L.nise_batch_destroy.argtypes = [vp]
         L.nise_batch_destroy.restype = None
+        L.nise_set_operators.argtypes = [vp, vp, ctypes.c_size_t, vp, ctypes.c_size_t]
+        L.nise_linear.argtypes = [vp, dp, dp, ctypes.c_int, ip, ip]
+        L.nise_linear_file.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.nise_linear_file.restype = ctypes.c_char_p
+        L.nise_write_td.argtypes = [ctypes.c_char_p, P, dp, dp, ctypes.c_int, ctypes.c_int]
         _lib = L
     return _lib
 
 
 def _dp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def linear_files(technique):
+    """[(TD file, spectrum file)] of each channel of a linear technique."""
+    code = TECH[technique] if isinstance(technique, str) else technique
+    out = []
+    while True:
+        td = lib().nise_linear_file(code, len(out), 1)
+        if td is None:
+            return out
+        out.append((td.decode(), lib().nise_linear_file(code, len(out), 0).decode()))
 
 
 def default_params():
@@ -147,7 +166,7 @@ def params_from_keywords(keywords, files=None, **engine):
     for k, v in (files or {}).items():
         key = {"energy": "Hamiltonianfile", "dipole": "Dipolefile", "coupling": "Couplingfile",
                "anharm": "Anharmonicfile", "overtone": "Overtonedipolefile", "shift": "SingleShiftfile",
-               "position": "Positionfile", "pbc": "PBCfile"}[k]
+               "position": "Positionfile", "pbc": "PBCfile", "alpha": "Alphafile"}[k]
         if v:
             lines.append("%s %s" % (key, v))
     lines += ["%s %s" % (k, v) for k, v in keywords.items()]
@@ -241,6 +260,31 @@ class Context:
                                               ctypes.byref(rows)))
         r = rows.value
         return w[:r], sr[:r], si[:r]
+
+    def set_operators(self, alpha=None, position=None):
+        """Alphafile (Raman, SFG) and CD Positionfile record images."""
+        keep = []
+        args = []
+        for x in (alpha, position):
+            if x is None:
+                args += [None, 0]
+                continue
+            a = np.ascontiguousarray(np.frombuffer(x, dtype=np.uint8) if isinstance(x, (bytes, bytearray)) else x)
+            keep.append(a)
+            args += [a.ctypes.data, a.nbytes]
+        self._check(lib().nise_set_operators(self._h, *args))
+        return self
+
+    def linear(self):
+        """LD, Raman, SFG, DOS or CD (the context's technique): raw response
+        sums re[channel][tmax1], im[channel][tmax1] and the normaliser."""
+        t = self.params.tmax1
+        re = np.zeros((4, t))
+        im = np.zeros((4, t))
+        ch = ctypes.c_int(0)
+        n = ctypes.c_int(0)
+        self._check(lib().nise_linear(self._h, _dp(re), _dp(im), 4, ctypes.byref(ch), ctypes.byref(n)))
+        return re[:ch.value], im[:ch.value], n.value
 
     def twodir(self):
         p = self.params

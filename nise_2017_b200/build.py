@@ -31,11 +31,13 @@ CU_SOURCES = [
     "diag.cu",
     "adjoint.cu",
     "onfly.cu",
+    "linear.cu",
 ]
 CPP_SOURCES = [
     "api.cpp",
     "absrun.cpp",
     "input.cpp",
+    "singles.cpp",
 ]
 
 

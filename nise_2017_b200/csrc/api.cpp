@@ -124,12 +124,15 @@ extern "C" int nise_create(const nise_params *p, nise_ctx **out) {
 
 void nise_free_traj(nise_ctx *c) {
     void *ptrs[] = {c->d_energy, c->d_dipole, c->d_hc, c->d_mu_static, c->d_anh, c->d_over, c->d_shift_site,
-                    c->d_shift_ab};
+                    c->d_shift_ab, c->d_alpha, c->d_pos};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     c->d_energy = c->d_dipole = c->d_hc = c->d_mu_static = c->d_anh = c->d_over = c->d_shift_ab = nullptr;
+    c->d_alpha = c->d_pos = nullptr;
     c->d_shift_site = nullptr;
     c->cap_energy = c->cap_dipole = c->cap_anh = c->cap_over = c->cap_hc = c->cap_mu = c->cap_ab = 0;
+    c->cap_alpha = c->cap_pos = 0;
+    c->al_frames = c->pos_frames = 0;
     c->loaded = false;
 }
 
@@ -294,6 +297,24 @@ extern "C" int nise_set_trajectory_onfly(nise_ctx *c, const void *energy, size_t
     return NISE_OK;
 }
 
+extern "C" int nise_set_operators(nise_ctx *c, const void *alpha, size_t alpha_bytes, const void *position,
+                                  size_t position_bytes) {
+    if (!c) return nise_fail(nullptr, NISE_ERR_ARG, "null context");
+    cudaSetDevice(c->p.device);
+    const int N = c->n;
+    // read_alpha (read_trajectory.c:380-399): int tag + 6N floats per frame;
+    // CD positions with read_mue's layout (:357-377): int tag + 3N floats
+    c->al_frames = alpha ? (long)(alpha_bytes / (4 * (size_t)(1 + 6L * N))) : 0;
+    const long pw = 1 + 3L * N + 3L * N * c->p.doubles;  // read_mue's record
+    c->pos_frames = position ? (long)(position_bytes / (4 * (size_t)pw)) : 0;
+    if (alpha && c->al_frames < 1) return nise_fail(c, NISE_ERR_IO, "Polarizability trajectory file to short");
+    if (position && c->pos_frames < 1) return nise_fail(c, NISE_ERR_IO, "Position trajectory file to short");
+    int rc;
+    if ((rc = upload(c, &c->d_alpha, &c->cap_alpha, alpha, (size_t)c->al_frames * 4 * (1 + 6L * N)))) return rc;
+    if ((rc = upload(c, &c->d_pos, &c->cap_pos, position, (size_t)c->pos_frames * 4 * pw))) return rc;
+    return nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "operator upload");
+}
+
 extern "C" int nise_set_singleshift(nise_ctx *c, int n, const int *sites, const float *a, const float *b) {
     if (!c || n < 0) return nise_fail(c, NISE_ERR_ARG, "bad SingleShift arguments");
     cudaSetDevice(c->p.device);
@@ -321,7 +342,13 @@ extern "C" int nise_load_files(nise_ctx *c) {
     const nise_params &p = c->p;
     std::vector<char> E, D, C, A, O;
     if (!read_file(p.energyFName, E)) return nise_fail(c, NISE_ERR_IO, "Hamiltonian file not found!");
-    if (!read_file(p.dipoleFName, D)) return nise_fail(c, NISE_ERR_IO, "Dipole file %s not found!", p.dipoleFName);
+    const bool no_dipoles = p.technique == NISE_TECH_DOS || p.technique == NISE_TECH_RAMAN;
+    if (no_dipoles && p.hamiltonian != NISE_HAM_TDC && p.hamiltonian != NISE_HAM_EDC) {
+        // calc_DOS and raman.c open no dipole file: one zero record stands in for it
+        if (!read_file(p.dipoleFName, D)) D.assign(4 * (1 + 3 * (size_t)c->n), 0);
+    } else if (!read_file(p.dipoleFName, D)) {
+        return nise_fail(c, NISE_ERR_IO, "Dipole file %s not found!", p.dipoleFName);
+    }
     if (p.hamiltonian == NISE_HAM_COUPLING && !read_file(p.couplingFName, C))
         return nise_fail(c, NISE_ERR_IO, "Coupling file not found!");
     // calc_2DIR.c:130-147 opens these files; calc_2DES (UVvis) reads neither
@@ -347,6 +374,18 @@ extern "C" int nise_load_files(nise_ctx *c) {
                                  A.empty() ? nullptr : A.data(), A.size(), O.empty() ? nullptr : O.data(), O.size());
     }
     if (rc) return rc;
+    // Alphafile (raman.c:74-78, sfg.c:82-86) and the CD Positionfile (calc_CD.c:84-88)
+    if (p.technique == NISE_TECH_RAMAN || p.technique == NISE_TECH_SFG || p.technique == NISE_TECH_CD) {
+        std::vector<char> Al, Ps;
+        if (p.technique != NISE_TECH_CD && !read_file(p.alphaFName, Al))
+            return nise_fail(c, NISE_ERR_IO, "%s file %s not found!",
+                             p.technique == NISE_TECH_RAMAN ? "Raman" : "Polarizability", p.alphaFName);
+        if (p.technique == NISE_TECH_CD && !read_file(p.positionFName, Ps))
+            return nise_fail(c, NISE_ERR_IO, "Position file %s not found!", p.positionFName);
+        if ((rc = nise_set_operators(c, Al.empty() ? nullptr : Al.data(), Al.size(),
+                                     Ps.empty() ? nullptr : Ps.data(), Ps.size())))
+            return rc;
+    }
     // read_shift (hamshift.c:13-47); a missing file is reported and ignored there.
     if (p.singleShiftFName[0]) {
         FILE *f = fopen(p.singleShiftFName, "r");
@@ -567,21 +606,27 @@ extern "C" int nise_propagate(nise_ctx *c, const float *H, void *re, void *im, i
 }
 
 // ------------------------------------------------------------ writers
-extern "C" int nise_write_td_absorption(const char *path, const nise_params *p, const double *re_S,
-                                        const double *im_S, int samples) {
+extern "C" int nise_write_td(const char *path, const nise_params *p, const double *re_S, const double *im_S,
+                             int samples, int trailing_blank) {
     if (!path || !p || !re_S || !im_S || samples <= 0) return NISE_ERR_ARG;
     FILE *f = fopen(path, "w");
     if (!f) return NISE_ERR_IO;
     for (int t1 = 0; t1 < p->tmax1; t1++) {  // absorption.c:181-189
         fprintf(f, "%f ", t1 * p->deltat);
+        const char *fmt = trailing_blank ? "%e %e " : "%e %e";
         if (p->precision == NISE_FP32)
-            fprintf(f, "%e %e ", (float)(re_S[t1] / samples), (float)(im_S[t1] / samples));
+            fprintf(f, fmt, (float)(re_S[t1] / samples), (float)(im_S[t1] / samples));
         else
-            fprintf(f, "%e %e ", re_S[t1] / samples, im_S[t1] / samples);
+            fprintf(f, fmt, re_S[t1] / samples, im_S[t1] / samples);
         fprintf(f, "\n");
     }
     fclose(f);
     return NISE_OK;
+}
+
+extern "C" int nise_write_td_absorption(const char *path, const nise_params *p, const double *re_S,
+                                        const double *im_S, int samples) {
+    return nise_write_td(path, p, re_S, im_S, samples, 1);
 }
 
 extern "C" int nise_write_spectrum(const char *path, const double *freq, const double *spec_re,

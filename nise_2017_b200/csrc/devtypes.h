@@ -1,5 +1,6 @@
 // Plain data types shared by host code (api.cpp) and device code.
 #pragma once
+#include <vector_types.h>
 
 // Trajectory records as the reference reads them (read_trajectory.c):
 // every record is an int32 tag followed by float32 data, addressed here in
@@ -26,3 +27,20 @@ struct DevTraj {
     float cut;               // Couplingcut
 };
 
+// Coefficient tables of one singles propagation scheme over the frames
+// [f0, f0 + nf) of a job (built by nise_singles_tables): the Trotter half
+// phases U[t][n] and rotations rot[t][K] (or [K] for static couplings), the
+// RK4 Hamiltonian entries, or the eigen route's one-step propagators
+// Ud[t][n][n].  Device code reads them through singles_step (schemes.cuh).
+struct SinglesTab {
+    int n, ts, prop;          // singles, Trotter sub-steps, NISE_PROP_*
+    long f0;                  // first frame of the tables
+    const int2 *pairs;        // Trotter pattern (a < b, lexicographic)
+    int K;
+    const void *U, *rot;      // Trotter tables
+    int rot_static;
+    const int2 *ent;          // RK4 entries (a <= b)
+    int Kr;
+    const void *rkval;        // RK4 values [t][Kr]
+    const void *Ud;           // Sparse/Diagonal: propagators U[t][n][n] (truncated by Threshold)
+};

@@ -70,6 +70,11 @@ static int technique_code(const char *t) {
     if (!strcmp(t, "SEUVvis")) return NISE_TECH_SEUVVIS;
     if (!strcmp(t, "EAUVvis")) return NISE_TECH_EAUVVIS;
     if (!strcmp(t, "noEAUVvis")) return NISE_TECH_NOEAUVVIS;
+    if (!strcmp(t, "LD")) return NISE_TECH_LD;
+    if (!strcmp(t, "Raman")) return NISE_TECH_RAMAN;
+    if (!strcmp(t, "SFG")) return NISE_TECH_SFG;
+    if (!strcmp(t, "DOS")) return NISE_TECH_DOS;
+    if (!strcmp(t, "CD")) return NISE_TECH_CD;
     return NISE_TECH_OTHER;
 }
 
@@ -88,7 +93,7 @@ extern "C" int nise_read_input(const char *path, nise_params *p) {
         if (match(buf, "Propagation", L)) { kw_s(buf, prop, sizeof(prop)); continue; }
         if (match(buf, "Hamiltonianfile", L)) { kw_s(buf, p->energyFName, sizeof(p->energyFName)); continue; }
         if (match(buf, "Dipolefile", L)) { kw_s(buf, p->dipoleFName, sizeof(p->dipoleFName)); continue; }
-        if (match(buf, "Alphafile", L)) { kw_s(buf, dummy, sizeof(dummy)); continue; }
+        if (match(buf, "Alphafile", L)) { kw_s(buf, p->alphaFName, sizeof(p->alphaFName)); continue; }
         if (match(buf, "Anharmonicfile", L)) { kw_s(buf, p->anharFName, sizeof(p->anharFName)); continue; }
         if (match(buf, "Overtonedipolefile", L)) { kw_s(buf, p->overdipFName, sizeof(p->overdipFName)); continue; }
         if (match(buf, "Positionfile", L)) { kw_s(buf, p->positionFName, sizeof(p->positionFName)); continue; }

@@ -29,6 +29,11 @@ struct nise_ctx {
     int nshift = 0;
     long e_words = 0, e_frames = 0, d_words = 0, d_frames = 0, a_frames = 0, o_frames = 0;
     size_t cap_energy = 0, cap_dipole = 0, cap_anh = 0, cap_over = 0, cap_hc = 0, cap_mu = 0, cap_ab = 0;
+    // operator records of the linear techniques: polarisabilities (Raman,
+    // SFG; 6N per frame) and positions (CD; 3N per frame)
+    float *d_alpha = nullptr, *d_pos = nullptr;
+    long al_frames = 0, pos_frames = 0;
+    size_t cap_alpha = 0, cap_pos = 0;
     std::vector<float> h_hc;        // coupling frame (HamiltonianType Coupling), shifted, cut
     std::vector<float> h_mu_static; // dipoles of frame 0 (HamiltonianType Coupling)
 };
@@ -74,3 +79,18 @@ template <typename T> struct DevBuf {
         if (p) cudaFreeAsync(p, s);
     }
 };
+
+// Device buffers behind a SinglesTab (and the eigen route's doubles sub-step
+// propagators Us[t][n][n] when requested).
+struct SinglesBufs {
+    DevBuf<int2> pairs, ent;
+    DevBuf<char> U, rot, rkval;
+    const void *Us = nullptr;
+};
+
+// Build the singles scheme's coefficient tables for frames [f0, f0 + nf)
+// of the context's trajectory (singleshift: apply SingleShift to the
+// diagonal, as read_Hamiltonian does); doubles_u adds the eigen route's
+// truncated sub-step propagators for doubles propagation.
+int nise_singles_tables(nise_ctx *c, const DevTraj &T, long f0, long nf, int singleshift, bool doubles_u,
+                        SinglesTab &S, SinglesBufs &B);

@@ -5,8 +5,10 @@
  *
  * Follows the reference driver (NISE.c:49-362) for the techniques on this
  * path: read the keywords, load the trajectory, run Absorption (writing
- * TD_Absorption.dat and Absorption.dat) or the 2DIR family (writing RparI.dat
- * ... RcroII.dat), all through the C ABI in nise_b200.h.  Engine controls come
+ * TD_Absorption.dat and Absorption.dat), the other linear techniques LD,
+ * Raman, SFG, DOS and CD (their TD_*.dat and spectrum files), or the 2DIR
+ * and 2DUVvis families (writing RparI.dat ... RcroII.dat), all through the C
+ * ABI in nise_b200.h.  Engine controls come
  * from the environment: NISE_PRECISION=fp64, NISE_LAUNCH=plain, NISE_DEVICE=<n>.
  */
 #include <stdio.h>
@@ -72,8 +74,28 @@ int main(int argc, char *argv[]) {
         printf("----------------------------------------\n");
         printf(" %s calculation succesfully completed\n", p.technique >= NISE_TECH_2DUVVIS ? "2DES" : "2DIR");
         printf("----------------------------------------\n\n");
+    } else if (p.technique >= NISE_TECH_LD && p.technique <= NISE_TECH_CD) {
+        double *re = calloc(4 * (size_t)p.tmax1, sizeof(double)), *im = calloc(4 * (size_t)p.tmax1, sizeof(double));
+        int channels = 0, samples = 0;
+        if ((rc = nise_linear(c, re, im, 4, &channels, &samples)) != NISE_OK) return fail(c, p.technique_name, rc);
+        int fft = p.fft < p.tmax1 ? p.tmax1 : p.fft, rows = 0;
+        double *w = calloc(fft, sizeof(double)), *sr = calloc(fft, sizeof(double)), *si = calloc(fft, sizeof(double));
+        for (int k = 0; k < channels; k++) {
+            const double *rk = re + (size_t)k * p.tmax1, *ik = im + (size_t)k * p.tmax1;
+            /* TD_DOS.dat has no trailing blank (calc_DOS.c:209), the others do */
+            nise_write_td(nise_linear_file(p.technique, k, 1), &p, rk, ik, samples, p.technique != NISE_TECH_DOS);
+            if ((rc = nise_absorption_fft(c, rk, ik, samples, w, sr, si, fft, &rows)) != NISE_OK)
+                return fail(c, "1D FFT", rc);
+            nise_write_spectrum(nise_linear_file(p.technique, k, 0), w, sr, si, rows);
+        }
+        free(re); free(im); free(w); free(sr); free(si);
+        static const char *done[] = {"Linear Dichroism", "Raman", "SFG", "DOS", "CD"};
+        printf("----------------------------------------------\n");
+        printf(" %s calculation succesfully completed\n", done[p.technique - NISE_TECH_LD]);
+        printf("----------------------------------------------\n\n");
     } else {
-        fprintf(stderr, "Technique '%s' is not on this engine's path (Absorption, 2DIR, GBIR, SEIR, EAIR, noEAIR, "
+        fprintf(stderr, "Technique '%s' is not on this engine's path (Absorption, LD, Raman, SFG, DOS, CD, "
+                "2DIR, GBIR, SEIR, EAIR, noEAIR, "
                 "2DUVvis, GBUVvis, SEUVvis, EAUVvis, noEAUVvis)\n",
                 p.technique_name);
         nise_destroy(c);

@@ -4,6 +4,7 @@
 // the operand order and rounding of the reference (see Ar<> in common.cuh).
 #pragma once
 #include "common.cuh"
+#include "nise_b200.h"
 
 template <typename R> struct Cst;
 template <> struct Cst<float> {
@@ -206,3 +207,53 @@ __device__ __forceinline__ double2 dot_mu(const DevTraj &T, long t, int x, const
     return make_double2(re, im);
 }
 
+__host__ __device__ __forceinline__ bool is_eigen_scheme(int prop) {
+    return prop == NISE_PROP_SPARSE || prop == NISE_PROP_DIAGONAL;
+}
+
+// propagate_vec_DIA / propagate_vec_DIA_S (propagate.c:60-125, 185-258) on
+// one vector of the [site][lane] layout: c_a <- sum_b U_ab c_b, accumulated
+// in b order (float operations in FP32 mode); truncated elements of U are
+// zero.  The temporary is the second half of the lane's shared memory.
+template <typename R>
+__device__ __forceinline__ void dia_apply(typename Vec2<R>::T *S, int B, int lane, int n,
+                                          const typename Vec2<R>::T *U) {
+    typedef typename Vec2<R>::T R2;
+    typedef Ar<R> A;
+    R2 *Tm = S + (size_t)n * B;
+    for (int a = 0; a < n; a++) {
+        R2 acc;
+        acc.x = acc.y = 0;
+        for (int b = 0; b < n; b++) {
+            R2 u = U[(size_t)a * n + b], z = S[b * B + lane];
+            acc.x = A::add(acc.x, A::sub(A::mul(u.x, z.x), A::mul(u.y, z.y)));
+            acc.y = A::add(acc.y, A::add(A::mul(u.x, z.y), A::mul(u.y, z.x)));
+        }
+        Tm[a * B + lane] = acc;
+    }
+    for (int a = 0; a < n; a++) S[a * B + lane] = Tm[a * B + lane];
+}
+
+// One singles time step (propagate_vector, propagate.c:20-39) of the
+// configured scheme through frame t, from the job's coefficient tables.
+template <typename R>
+__device__ __forceinline__ void singles_step(const SinglesTab &D, typename Vec2<R>::T *S, int B, int lane, long t) {
+    typedef typename Vec2<R>::T R2;
+    long fi = t - D.f0;
+    if (is_eigen_scheme(D.prop)) {
+        dia_apply<R>(S, B, lane, D.n, (const R2 *)D.Ud + fi * D.n * D.n);
+    } else if (D.prop == NISE_PROP_RK4) {
+        rk4_apply<R>(S, B, lane, D.n, D.Kr, D.ent, (const R *)D.rkval + fi * D.Kr, D.ts);
+    } else {
+        const R2 *Uf = (const R2 *)D.U + fi * D.n;
+        const R2 *Rf = D.rot_static ? (const R2 *)D.rot : (const R2 *)D.rot + fi * D.K;
+        trotter_apply<R>(S, B, lane, D.n, D.K, D.pairs, Uf, Rf, D.ts);
+    }
+}
+
+// Shared memory one lane of singles_step needs: the vector, plus a
+// temporary vector (eigen route) or the four RK4 stages.
+template <typename R>
+__host__ __device__ __forceinline__ size_t singles_lane_bytes(int n, int prop) {
+    return (prop == NISE_PROP_RK4 ? 5 : is_eigen_scheme(prop) ? 2 : 1) * (size_t)n * sizeof(typename Vec2<R>::T);
+}

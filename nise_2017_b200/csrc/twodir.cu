@@ -57,22 +57,14 @@ __constant__ int c_px[21][4] = {{0, 0, 0, 0}, {1, 1, 1, 1}, {2, 2, 2, 2}, {0, 0,
                                  {1, 2, 2, 1}, {2, 0, 0, 2}, {2, 1, 1, 2}};
 __constant__ float c_w[3][21];
 
-struct TwoD {
+// The singles tables (SinglesTab: n, ts, prop, f0, the Trotter/RK4/eigen
+// tables) are the base; the fields below are the 2D job's.
+struct TwoD : SinglesTab {
     DevTraj T;
-    int n, T1, T2, T3, ts, sample, s0, S;  // S start points in this chunk, the first is s0
+    int T1, T2, T3, sample, s0, S;  // S start points in this chunk, the first is s0
     int gb, se, ea;
     int es;                   // UVvis family: two-level doubles (no |aa>)
-    int prop;                 // NISE_PROP_*
     float anh;                // Anharmonicity keyword (0: per-frame files)
-    long f0;                  // first frame of the coefficient tables
-    const int2 *pairs;        // Trotter pattern (a < b, lexicographic)
-    int K;
-    const void *U, *rot;      // Trotter tables: U[t][n], rot[t][K] (or [K] static)
-    int rot_static;
-    const int2 *ent;          // RK4 entries (a <= b)
-    int Kr;
-    const void *rkval;        // RK4 values [t][Kr]
-    const void *Ud;           // Sparse/Diagonal: full-step propagators U[t][n][n] (truncated by Threshold)
     const void *Us;           // Sparse/Diagonal doubles: substep propagators U[t][n][n] (f/ts, truncated)
     long e0;                  // eigen data for frames [e0, e0 + ne)
     const double *eV, *ew;    // V [ne][n][n], w [ne][n]
@@ -93,54 +85,6 @@ struct TwoD {
 __device__ __forceinline__ long tj_of(const TwoD &D, int s) { return (long)(D.s0 + s) * D.sample + D.T1; }
 __device__ __forceinline__ long tk_of(const TwoD &D, int s) { return tj_of(D, s) + D.T2; }
 __device__ __forceinline__ int nvec_se(const TwoD &D) { return 3 + 3 * D.T1; }
-
-__host__ __device__ __forceinline__ bool is_eigen_scheme(int prop) {
-    return prop == NISE_PROP_SPARSE || prop == NISE_PROP_DIAGONAL;
-}
-
-// propagate_vec_DIA / propagate_vec_DIA_S (propagate.c:60-125, 185-258) on
-// one vector of the [site][lane] layout: c_a <- sum_b U_ab c_b, accumulated
-// in b order (float operations in FP32 mode); truncated elements of U are
-// zero.  The temporary is the second half of the lane's shared memory.
-template <typename R>
-__device__ __forceinline__ void dia_apply(typename Vec2<R>::T *S, int B, int lane, int n,
-                                          const typename Vec2<R>::T *U) {
-    typedef typename Vec2<R>::T R2;
-    typedef Ar<R> A;
-    R2 *Tm = S + (size_t)n * B;
-    for (int a = 0; a < n; a++) {
-        R2 acc;
-        acc.x = acc.y = 0;
-        for (int b = 0; b < n; b++) {
-            R2 u = U[(size_t)a * n + b], z = S[b * B + lane];
-            acc.x = A::add(acc.x, A::sub(A::mul(u.x, z.x), A::mul(u.y, z.y)));
-            acc.y = A::add(acc.y, A::add(A::mul(u.x, z.y), A::mul(u.y, z.x)));
-        }
-        Tm[a * B + lane] = acc;
-    }
-    for (int a = 0; a < n; a++) S[a * B + lane] = Tm[a * B + lane];
-}
-
-// One singles time step of the configured scheme through frame t.
-template <typename R>
-__device__ __forceinline__ void singles_step(const TwoD &D, typename Vec2<R>::T *S, int B, int lane, long t) {
-    typedef typename Vec2<R>::T R2;
-    long fi = t - D.f0;
-    if (is_eigen_scheme(D.prop)) {
-        dia_apply<R>(S, B, lane, D.n, (const R2 *)D.Ud + fi * D.n * D.n);
-    } else if (D.prop == NISE_PROP_RK4) {
-        rk4_apply<R>(S, B, lane, D.n, D.Kr, D.ent, (const R *)D.rkval + fi * D.Kr, D.ts);
-    } else {
-        const R2 *Uf = (const R2 *)D.U + fi * D.n;
-        const R2 *Rf = D.rot_static ? (const R2 *)D.rot : (const R2 *)D.rot + fi * D.K;
-        trotter_apply<R>(S, B, lane, D.n, D.K, D.pairs, Uf, Rf, D.ts);
-    }
-}
-
-template <typename R>
-__device__ __forceinline__ size_t singles_lane_bytes(int n, int prop) {
-    return (prop == NISE_PROP_RK4 ? 5 : is_eigen_scheme(prop) ? 2 : 1) * (size_t)n * sizeof(typename Vec2<R>::T);
-}
 
 // sum_i mu_i * psi_i with float products (FP32) and an FP64 sum.
 template <typename R>
@@ -1156,95 +1100,19 @@ extern "C" int nise_2dir(nise_ctx *c, double *R, int *sample_count) {
     size_t rsz = prec == NISE_FP32 ? sizeof(float) : sizeof(double), r2 = 2 * rsz;
     // singles coefficient tables over all frames of the job
     long nf = fmax - fmin + 1;
-    std::vector<int2> pairs;
-    if ((rc = nise_pattern(c, fmin, nf, pairs))) return rc;
-    DevBuf<int2> dpairs, dent;
-    DevBuf<char> U, rot, rkval;
-    TwoD D;
-    memset(&D, 0, sizeof(D));
+    TwoD D{};
+    SinglesBufs SB;
+    if ((rc = nise_singles_tables(c, T, fmin, nf, 0, ea, D, SB))) return rc;
     D.T = T;
-    D.n = N; D.T1 = T1; D.T2 = T2; D.T3 = T3; D.ts = p.ts; D.sample = p.sample;
+    D.T1 = T1; D.T2 = T2; D.T3 = T3; D.sample = p.sample;
     D.gb = gb; D.se = se; D.ea = ea;
     D.es = es;
-    D.prop = p.propagation;
     D.anh = p.anharmonicity;
-    D.f0 = fmin;
     D.f32_full = nise_f32(p, 1, 1);
     D.f64_full = nise_f64(p, 1, 1);
     D.f32_dsub = nise_f32(p, 1, p.ts);
     D.f64_dsub = nise_f64(p, 1, p.ts);
-    if ((rc = dpairs.upload(c, pairs))) return rc;
-    D.pairs = dpairs.p;
-    D.K = (int)pairs.size();
-    if (p.propagation == NISE_PROP_COUPLING) {
-        TrotterPlan P;
-        P.n = N; P.k = D.K; P.pairs = dpairs.p; P.f0 = fmin; P.nf = nf;
-        P.rot_static = p.hamiltonian == NISE_HAM_COUPLING;
-        P.singleshift = 0;
-        if ((rc = U.alloc(c, r2 * (size_t)nf * N))) return rc;
-        if ((rc = rot.alloc(c, r2 * (size_t)(P.rot_static ? 1 : nf) * (P.k ? P.k : 1)))) return rc;
-        P.U = U.p;
-        P.rot = rot.p;
-        if ((rc = nise_cuda(c, launch_prep_trotter(prec, T, P, nise_f64(p, 1, p.ts), nise_f32(p, 1, p.ts), c->stream),
-                            "Trotter prep")))
-            return rc;
-        c->launches += 1 + P.rot_static;
-        D.U = U.p; D.rot = rot.p; D.rot_static = P.rot_static;
-    } else if (eig_scheme) {
-        // propagate_vector's Sparse scheme for the singles (DIA, or DIA_S when
-        // 0 < Threshold <= 1) and time_evolution_mat's truncated substep
-        // propagator for the doubles (Threshold always applied); Diagonal is
-        // the untruncated exact propagator.
-        const float thr = p.propagation == NISE_PROP_DIAGONAL ? 0.0f : c->thres;
-        const bool trunc_singles = thr != 0 && !(thr > 1);
-        const long FC = std::max(1L, std::min(nf, (long)(((size_t)512 << 20) / (sizeof(double) * (size_t)N * N))));
-        std::vector<long> frs(nf);
-        for (long t = 0; t < nf; t++) frs[t] = fmin + t;
-        DevBuf<long> dfr;
-        DevBuf<double> V, w;
-        if ((rc = dfr.upload(c, frs)) || (rc = V.alloc(c, (size_t)FC * N * N)) || (rc = w.alloc(c, (size_t)FC * N)) ||
-            (rc = U.alloc(c, r2 * (size_t)nf * N * N)))
-            return rc;
-        if (ea && (rc = rot.alloc(c, r2 * (size_t)nf * N * N))) return rc;
-        EigJob EJ;
-        EJ.T = T; EJ.n = N; EJ.singleshift = 0;
-        const int pr = prec == NISE_FP32 ? 0 : 1;
-        const double ffull = prec == NISE_FP32 ? (double)D.f32_full : D.f64_full;
-        const double fsub = prec == NISE_FP32 ? (double)D.f32_dsub : D.f64_dsub;
-        for (long q = 0; q < nf; q += FC) {
-            long m = std::min(FC, nf - q);
-            if ((rc = nise_cuda(c, launch_eig(EJ, dfr.p + q, m, V.p, w.p, c->stream), "eigensolver"))) return rc;
-            if ((rc = nise_cuda(c, launch_build_u(pr, V.p, w.p, m, N, ffull, thr, trunc_singles,
-                                                  U.p + r2 * (size_t)q * N * N, c->stream), "propagator build")))
-                return rc;
-            c->launches += 2;
-            if (ea) {
-                if ((rc = nise_cuda(c, launch_build_u(pr, V.p, w.p, m, N, fsub, thr, 1, rot.p + r2 * (size_t)q * N * N,
-                                                      c->stream), "doubles propagator build")))
-                    return rc;
-                c->launches++;
-            }
-        }
-        D.Ud = U.p;
-        D.Us = rot.p;
-    } else {
-        std::vector<int2> ent;
-        size_t q = 0;
-        for (int a = 0; a < N; a++) {
-            ent.push_back(make_int2(a, a));
-            while (q < pairs.size() && pairs[q].x == a) ent.push_back(pairs[q++]);
-        }
-        if ((rc = dent.upload(c, ent))) return rc;
-        Rk4Plan P;
-        P.n = N; P.k = (int)ent.size(); P.entries = dent.p; P.f0 = fmin; P.nf = nf; P.singleshift = 0;
-        if ((rc = rkval.alloc(c, rsz * (size_t)nf * P.k))) return rc;
-        P.val = rkval.p;
-        if ((rc = nise_cuda(c, launch_prep_rk4(prec, T, P, nise_f64(p, 1, p.ts), nise_f32(p, 1, p.ts), c->stream),
-                            "RK4 prep")))
-            return rc;
-        c->launches++;
-        D.ent = dent.p; D.Kr = P.k; D.rkval = rkval.p;
-    }
+    D.Us = SB.Us;
     DevBuf<char> dcoef;
     D.rot_static = p.hamiltonian == NISE_HAM_COUPLING;
     if (ea) {  // doubles coupling coefficients: once (static couplings) or per frame

@@ -112,6 +112,25 @@ def write_positions(directory, n_sites, frames, mode="tdc", seed=1, spacing=5.0,
     return out
 
 
+def write_alpha(directory, n_sites, frames, seed=1, prefix=""):
+    """Seeded polarisability records (Alphafile, read_alpha layout: int32 tag,
+    then the xx, xy, xz, yy, yz, zz blocks of N floats).  Each site has an
+    anisotropic tensor (diagonal near 1, off-diagonal near 0.2) that moves by
+    2 % per frame.  Returns {"alpha": path}."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    base = np.empty((6, n_sites))
+    base[[0, 3, 5]] = rng.uniform(0.5, 1.5, size=(3, n_sites))
+    base[[1, 2, 4]] = rng.normal(0, 0.2, size=(3, n_sites))
+    out = {"alpha": os.path.join(directory, prefix + "Alpha.bin")}
+    with open(out["alpha"], "wb") as f:
+        for t in range(frames):
+            a = base * (1 + rng.normal(0, 0.02, size=base.shape))
+            f.write(np.int32(t).tobytes())
+            f.write(np.ascontiguousarray(a, dtype=np.float32).tobytes())
+    return out
+
+
 # ---------------------------------------------------------------- workloads
 def c0_spec(**kw):
     d = dict(n_sites=16, frames=10000, dt_fs=2.0, geometry=CHAIN, eps0=1650.0, sigma=10.0, tau_fs=100.0,
@@ -174,6 +193,8 @@ def write_input(path, keywords, files):
         lines.append("Positionfile %s" % files["position"])
     if files.get("pbc"):
         lines.append("PBCfile %s" % files["pbc"])
+    if files.get("alpha"):
+        lines.append("Alphafile %s" % files["alpha"])
     for k, v in keywords.items():
         lines.append("%s %s" % (k, v))
     with open(path, "w") as f:

@@ -70,6 +70,7 @@ typedef struct {
     char *O; long nO;
     char *P; long nP;  /* Positionfile (TransitionDipole / ExtendedDipole) */
     char *B; long nB;  /* PBCfile */
+    char *Al; long nAl; /* Alphafile */
     float *Hc;     /* coupling frame for HamiltonianType Coupling (read_coupling) */
     float *mu_xyz; /* static dipoles for HamiltonianType Coupling */
     int nshift; int *shift_site; float *shift_ab;
@@ -89,7 +90,7 @@ static char *slurp(const char *path, long *bytes) {
 }
 
 static void traj_free(traj_t *t) {
-    free(t->E); free(t->D); free(t->A); free(t->O); free(t->P); free(t->B); free(t->Hc); free(t->mu_xyz);
+    free(t->E); free(t->D); free(t->A); free(t->O); free(t->P); free(t->B); free(t->Al); free(t->Hc); free(t->mu_xyz);
     free(t->shift_site); free(t->shift_ab);
     memset(t, 0, sizeof(*t));
 }
@@ -244,6 +245,15 @@ static int read_over(const traj_t *t, float *over, int pos, int x) {
     return 1;
 }
 
+/* read_alpha (read_trajectory.c:380-399): component x of the polarisability at frame pos. */
+static int read_alpha(const traj_t *t, float *alpha, int pos, int x) {
+    int N = t->p->singles;
+    long off = (long)pos * (4 + 24L * N) + 4 + 4L * x * N;
+    if (pos < 0 || off + 4L * N > t->nAl) return 0;
+    memcpy(alpha, t->Al + off, sizeof(float) * N);
+    return 1;
+}
+
 /* apply_singleshift (hamshift.c:59-66), file format of read_shift (:13-47). */
 static void apply_singleshift(const traj_t *t, float *H) {
     for (int i = 0; i < t->nshift; i++) {
@@ -259,7 +269,17 @@ static int traj_open(traj_t *t, const oracle_params *p, float shifte, int need_a
     int N = p->singles;
     t->E = slurp(p->energy, &t->nE);
     t->D = slurp(p->dipole, &t->nD);
-    if (!t->E || !t->D) return -1;
+    /* calc_DOS and raman.c open no dipole file */
+    const int dipoles = !(p->technique == 12 || p->technique == 14);
+    if (!t->E || (dipoles && !t->D)) return -1;
+    if (p->technique == 12 || p->technique == 13) {
+        t->Al = slurp(p->alpha, &t->nAl);
+        if (!t->Al) return -1;
+    }
+    if (p->technique == 15) {
+        t->P = slurp(p->position, &t->nP);
+        if (!t->P) return -1;
+    }
     if (p->ham_onfly) {
         t->P = slurp(p->position, &t->nP);
         if (!t->P) return -1;
@@ -279,7 +299,7 @@ static int traj_open(traj_t *t, const oracle_params *p, float shifte, int need_a
         free(cb);
         if (!ok) return -1;
         t->mu_xyz = (float *)calloc(3 * (size_t)N, sizeof(float));
-        for (int x = 0; x < 3; x++)
+        for (int x = 0; x < 3 && dipoles; x++)
             if (!read_mue(t, t->D, t->nD, t->mu_xyz + N * x, 0, x)) return -1;
     }
     if (p->shift[0]) {
@@ -978,6 +998,135 @@ int oracle_absorption(const oracle_params *p, double *re_out, double *im_out, in
     for (int i = 0; i < tmax; i++) re_out[i] = re_S[i], im_out[i] = im_S[i];
     *samples_out = samples;
     free(re_S); free(im_S); free(H); free(mu); free(vr); free(vi); free(mu0);
+    traj_free(&t);
+    return rc;
+}
+
+/* Linear techniques besides absorption: the sample loops of LD
+ * (calc_LD.c:149-220, calc_LD :286-296), Raman (raman.c:139-226, :293-310),
+ * SFG (sfg.c:143-205, :281-298), DOS (calc_DOS.c:120-172, :225-234) and CD
+ * (calc_CD.c:172-327, :381-392), each with its own read-outs and channels.
+ * LD, Raman, DOS and CD read frames with read_He (no SingleShift); SFG with
+ * read_Hamiltonian.  SFG's x and y start vectors have no read-out and are not
+ * propagated here. */
+int oracle_linear(const oracle_params *p, double *re_out, double *im_out, int *nch_out, int *samples_out) {
+    const int N = p->singles, tech = p->technique, tmax = p->tmax1;
+    if (tech < 11 || tech > 15) return -6;
+    float shift1 = (p->max1 + p->min1) / 2;
+    traj_t t;
+    if (traj_open(&t, p, shift1, 0) != 0) { traj_free(&t); return -1; }
+    int N_samples = (p->length - p->tmax1 - 1) / p->sample + 1;
+    if (N_samples <= 0) { traj_free(&t); return -2; }
+    int end = p->end == 0 ? N_samples : p->end;
+    if (end > N_samples) { traj_free(&t); return -3; }
+    const int nch = (tech == 12 || tech == 13) ? 2 : 1;
+    const int nvec = tech == 14 ? N : (tech == 15 ? N : 1);  /* vectors propagated together */
+    acc *S = (acc *)calloc(2 * (size_t)nch * tmax, sizeof(acc));   /* [ch][re/im][t1] */
+    acc *Sj = (acc *)calloc(2 * (size_t)N * tmax, sizeof(acc));    /* CD: per initial site */
+    float *H = ham_alloc(&t), *mu = (float *)malloc(sizeof(float) * N), *op = (float *)malloc(sizeof(float) * N);
+    float *pos = (float *)malloc(sizeof(float) * N), *pos0 = (float *)malloc(sizeof(float) * 3 * N);
+    real *vr = (real *)calloc((size_t)nvec * N, sizeof(real)), *vi = (real *)calloc((size_t)nvec * N, sizeof(real));
+    int rc = 0, samples;
+#define SRE(ch, t1) S[(2 * (size_t)(ch)) * tmax + (t1)]
+#define SIM(ch, t1) S[(2 * (size_t)(ch) + 1) * tmax + (t1)]
+    if (tech == 15 && p->ham_coupling)  /* static positions of frame 0 (calc_CD.c:164-170) */
+        for (int x = 0; x < 3; x++)
+            if (!read_mue(&t, t.P, t.nP, pos0 + N * x, 0, x)) rc = -4;
+    const int nx = tech == 12 ? 6 : (tech == 13 || tech == 14 ? 1 : 3);
+    for (samples = p->begin; samples < end && rc == 0; samples++) {
+        const int ti = samples * p->sample;
+        for (int x = 0; x < nx && rc == 0; x++) {
+            /* initial vectors */
+            memset(vr, 0, sizeof(real) * nvec * N);
+            memset(vi, 0, sizeof(real) * nvec * N);
+            if (tech == 11 || tech == 13) {        /* mu_x(ti); SFG: mu_z */
+                if (!mu_read(&t, mu, ti, tech == 13 ? 2 : x)) { rc = -4; break; }
+                for (int i = 0; i < N; i++) vr[i] = mu[i];
+            } else if (tech == 12) {               /* alpha_x(ti) */
+                if (!read_alpha(&t, op, ti, x)) { rc = -4; break; }
+                for (int i = 0; i < N; i++) vr[i] = op[i];
+            } else if (tech == 14) {               /* unitmat */
+                for (int j = 0; j < N; j++) vr[(size_t)j * N + j] = 1;
+            } else {                               /* CD: mu_x(ti)_j on site j */
+                if (!mu_read(&t, mu, ti, x)) { rc = -4; break; }
+                for (int j = 0; j < N; j++) vr[(size_t)j * N + j] = mu[j];
+            }
+            for (int t1 = 0; t1 < tmax; t1++) {
+                const int tj = ti + t1;
+                if (!read_He(&t, H, tj)) { rc = -5; break; }
+                if (tech == 13) apply_singleshift(&t, H);
+                if (tech == 11) {
+                    if (!mu_read(&t, mu, tj, x)) { rc = -4; break; }
+                    float factor = x == 2 ? 1 : -0.5;
+                    for (int i = 0; i < N; i++) {
+                        SRE(0, t1) += mu[i] * vr[i] * factor;
+                        SIM(0, t1) += mu[i] * vi[i] * factor;
+                    }
+                } else if (tech == 12) {
+                    if (!read_alpha(&t, op, tj, x)) { rc = -4; break; }
+                    if (x == 0 || x == 3 || x == 5)
+                        for (int i = 0; i < N; i++) { SRE(0, t1) += op[i] * vr[i]; SIM(0, t1) += op[i] * vi[i]; }
+                    else
+                        for (int i = 0; i < N; i++) { SRE(1, t1) += 2 * op[i] * vr[i]; SIM(1, t1) += 2 * op[i] * vi[i]; }
+                } else if (tech == 13) {
+                    for (int xa = 0; xa < 6; xa++) {
+                        if (!read_alpha(&t, op, tj, xa)) { rc = -4; break; }
+                        if (xa == 5)
+                            for (int i = 0; i < N; i++) { SRE(0, t1) += op[i] * vr[i]; SIM(0, t1) += op[i] * vi[i]; }
+                        if (xa == 0 || xa == 3)
+                            for (int i = 0; i < N; i++) {
+                                SRE(1, t1) += op[i] * vr[i] / 2;
+                                SIM(1, t1) += op[i] * vi[i] / 2;
+                            }
+                    }
+                    if (rc) break;
+                } else if (tech == 14) {
+                    for (int i = 0; i < N; i++) {
+                        SRE(0, t1) += vr[(size_t)i * N + i];
+                        SIM(0, t1) += vi[(size_t)i * N + i];
+                    }
+                } else {
+                    for (int y = 0; y < 3; y++) {
+                        if (y == x) continue;
+                        int z = 3 - x - y, sign = 0;
+                        if (z == 0 && y == 1 && x == 2) sign = 1;
+                        if (z == 0 && y == 2 && x == 1) sign = -1;
+                        if (z == 1 && y == 0 && x == 2) sign = -1;
+                        if (z == 2 && y == 0 && x == 1) sign = 1;
+                        if (z == 2 && y == 1 && x == 0) sign = -1;
+                        if (z == 1 && y == 2 && x == 0) sign = 1;
+                        /* static dipoles: the reference copies component x (calc_CD.c:250) */
+                        if (!mu_read(&t, mu, tj, p->ham_coupling ? x : y)) { rc = -4; break; }
+                        if (p->ham_coupling) memcpy(pos, pos0 + N * z, sizeof(float) * N);
+                        else if (!read_mue(&t, t.P, t.nP, pos, tj, z)) { rc = -4; break; }
+                        for (int j = 0; j < N; j++)
+                            for (int i = 0; i < N; i++) {
+                                Sj[(size_t)j * tmax + t1] += sign * (pos[i] - pos[j]) * mu[i] * vr[(size_t)j * N + i];
+                                Sj[((size_t)N + j) * tmax + t1] += sign * (pos[i] - pos[j]) * mu[i] * vi[(size_t)j * N + i];
+                            }
+                    }
+                    if (rc) break;
+                }
+                for (int v = 0; v < nvec; v++) propagate_vector(p, H, vr + (size_t)v * N, vi + (size_t)v * N, 1);
+            }
+        }
+    }
+    if (tech == 15)  /* sum over the initial sites (calc_CD.c:334-342) */
+        for (int t1 = 0; t1 < tmax; t1++)
+            for (int j = 0; j < N; j++) {
+                SRE(0, t1) += Sj[(size_t)j * tmax + t1];
+                SIM(0, t1) += Sj[((size_t)N + j) * tmax + t1];
+            }
+    for (int ch = 0; ch < nch; ch++)
+        for (int t1 = 0; t1 < tmax; t1++) {
+            re_out[(size_t)ch * tmax + t1] = SRE(ch, t1);
+            im_out[(size_t)ch * tmax + t1] = SIM(ch, t1);
+        }
+#undef SRE
+#undef SIM
+    *nch_out = nch;
+    *samples_out = samples;
+    free(S); free(Sj); free(H); free(mu); free(op); free(pos); free(pos0); free(vr); free(vi);
     traj_free(&t);
     return rc;
 }

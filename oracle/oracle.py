@@ -16,7 +16,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 
 TECHNIQUES = {"Absorption": 0, "2DIR": 1, "GBIR": 2, "SEIR": 3, "EAIR": 4, "noEAIR": 5,
-              "2DUVvis": 6, "GBUVvis": 7, "SEUVvis": 8, "EAUVvis": 9, "noEAUVvis": 10}
+              "2DUVvis": 6, "GBUVvis": 7, "SEUVvis": 8, "EAUVvis": 9, "noEAUVvis": 10,
+              "LD": 11, "Raman": 12, "SFG": 13, "DOS": 14, "CD": 15}
+# output files of the linear techniques per channel (calc_LD.c, raman.c, sfg.c, calc_DOS.c, calc_CD.c)
+LINEAR_FILES = {"LD": [("TD_LD.dat", "LD.dat")],
+                "Raman": [("TD_Raman_VV.dat", "Raman_VV.dat"), ("TD_Raman_VH.dat", "Raman_VH.dat")],
+                "SFG": [("TD_SFG_PPP.dat", "SFG_PPP.dat"), ("TD_SFG_SSP.dat", "SFG_SSP.dat")],
+                "DOS": [("TD_DOS.dat", "DOS.dat")], "CD": [("TD_CD.dat", "CD.dat")]}
 ICM2IFS = np.float32(2.99792458e-5)
 TWOPI = np.float32(2 * 3.14159265359)
 
@@ -36,6 +42,7 @@ class OracleParams(ctypes.Structure):
         ("energy", ctypes.c_char * 256), ("dipole", ctypes.c_char * 256), ("coupling", ctypes.c_char * 256),
         ("anharm", ctypes.c_char * 256), ("overtone", ctypes.c_char * 256), ("shift", ctypes.c_char * 256),
         ("ham_onfly", ctypes.c_int), ("position", ctypes.c_char * 256), ("pbc", ctypes.c_char * 256),
+        ("alpha", ctypes.c_char * 256),
     ]
 
 
@@ -72,14 +79,14 @@ def params(keywords, files):
     prop = kw.get("Propagation", "")
     p.propagation = {"Coupling": 1, "Diagonal": 2, "RK4": 3}.get(prop, 0)
     p.technique = TECHNIQUES[kw.get("Technique", "Absorption")]
-    if p.technique != 0:
+    if 1 <= p.technique <= 10:
         p.tmax3 = p.tmax1  # readinput.c:212
     thres = np.float32(float(kw.get("Threshold", 0)))
     if p.propagation == 0:  # readinput.c:264-267, in float arithmetic
         s = np.float32(np.float32(np.float32(p.deltat) * ICM2IFS) * TWOPI) / np.float32(p.ts)
         thres = np.float32(thres * np.float32(s * s))
     p.thres = float(thres)
-    for key in ("energy", "dipole", "coupling", "anharm", "overtone", "shift", "position", "pbc"):
+    for key in ("energy", "dipole", "coupling", "anharm", "overtone", "shift", "position", "pbc", "alpha"):
         setattr(p, key, (files.get(key) or "").encode())
     return p
 
@@ -97,6 +104,7 @@ def lib(prec="f64"):
         dp = ctypes.POINTER(ctypes.c_double)
         L.oracle_absorption.argtypes = [P, dp, dp, ctypes.POINTER(ctypes.c_int)]
         L.oracle_2dir.argtypes = [P, dp, ctypes.POINTER(ctypes.c_int)]
+        L.oracle_linear.argtypes = [P, dp, dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.oracle_1dfft.argtypes = [P, dp, dp, ctypes.c_int, dp, dp, dp, ctypes.c_int]
         L.oracle_print2d_normalize.argtypes = [P, dp, dp, ctypes.c_int]
         fp = ctypes.POINTER(ctypes.c_float)
@@ -143,6 +151,18 @@ def spectrum(p, re, im, samples, prec="f64"):
                                   _ptr(np.ascontiguousarray(im, dtype=np.float64)), samples, _ptr(w), _ptr(sr),
                                   _ptr(si), fft)
     return w[:rows], sr[:rows], si[:rows]
+
+
+def linear(p, prec="f64"):
+    """LD, Raman, SFG, DOS, CD: raw response sums re, im [channel][tmax1] and the normaliser."""
+    re = np.zeros((4, p.tmax1))
+    im = np.zeros((4, p.tmax1))
+    ch = ctypes.c_int(0)
+    n = ctypes.c_int(0)
+    rc = lib(prec).oracle_linear(ctypes.byref(p), _ptr(re), _ptr(im), ctypes.byref(ch), ctypes.byref(n))
+    if rc != 0:
+        raise RuntimeError("oracle_linear failed (%d)" % rc)
+    return re[:ch.value], im[:ch.value], n.value
 
 
 def twodir(p, prec="f64"):

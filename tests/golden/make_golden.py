@@ -145,6 +145,46 @@ CASES = {
                   dipole_frames=1, mu_jitter=0.0),
         keywords=synth.c2_keywords(Singles=5, Length=300, RunTimes="8 2 8", Samplerate=40,
                                    Technique="noEAUVvis")),
+    # linear techniques besides absorption (calc_LD.c, raman.c, sfg.c, calc_DOS.c, calc_CD.c)
+    "lin_ld": dict(
+        spec=dict(n_sites=10, frames=300, dt_fs=2.0, geometry=synth.CHAIN, seed=51),
+        keywords=synth.c0_keywords(Singles=10, Length=300, RunTimes="40 0 0", Samplerate=30, Technique="LD",
+                                   FFT=256)),
+    "lin_ld_static_sparse": dict(
+        spec=dict(n_sites=12, frames=300, dt_fs=1.0, geometry=L, spacing=8.0, eps0=15000.0, sigma=300.0,
+                  tau_fs=50.0, jcut=2.0, mu_jitter=0.0, ham_type=synth.COUPLING, dipole_frames=1, seed=52),
+        keywords=synth.c1_keywords(Singles=12, Length=300, RunTimes="32 0 0", Samplerate=40, Technique="LD",
+                                   Threshold=0, FFT=256)),
+    "lin_raman_rk4": dict(
+        spec=dict(n_sites=8, frames=300, dt_fs=2.0, geometry=synth.CHAIN, seed=53),
+        keywords=synth.c0_keywords(Singles=8, Length=300, RunTimes="40 0 0", Samplerate=30, Technique="Raman",
+                                   Propagation="RK4", Trotter=2, FFT=256),
+        alpha=dict(seed=54)),
+    "lin_sfg_shift": dict(
+        spec=dict(n_sites=9, frames=300, dt_fs=2.0, geometry=C, spacing=6.0, sigma=12.0, mu_jitter=0.0,
+                  ham_type=synth.COUPLING, dipole_frames=1, seed=55),
+        keywords=synth.c2_keywords(Singles=9, Length=300, RunTimes="40 0 0", Samplerate=30, Technique="SFG",
+                                   FFT=256),
+        shift=[(1, 1.0, 6.0), (4, 0.98, -2.0)], alpha=dict(seed=56)),
+    "lin_dos": dict(
+        spec=dict(n_sites=10, frames=300, dt_fs=2.0, geometry=synth.CHAIN, seed=57),
+        keywords=synth.c0_keywords(Singles=10, Length=300, RunTimes="40 0 0", Samplerate=30, Technique="DOS",
+                                   FFT=256)),
+    "lin_dos_sparse": dict(
+        spec=dict(n_sites=8, frames=300, dt_fs=2.0, geometry=synth.CHAIN, seed=58),
+        keywords=synth.c0_keywords(Singles=8, Length=300, RunTimes="32 0 0", Samplerate=30, Technique="DOS",
+                                   Propagation="Sparse", Threshold=0, FFT=256)),
+    "lin_cd": dict(
+        spec=dict(n_sites=8, frames=300, dt_fs=2.0, geometry=synth.CHAIN, seed=59),
+        keywords=synth.c0_keywords(Singles=8, Length=300, RunTimes="32 0 0", Samplerate=40, Technique="CD",
+                                   FFT=256),
+        cd_positions=dict(seed=60, spacing=4.5)),
+    "lin_cd_static": dict(
+        spec=dict(n_sites=9, frames=300, dt_fs=2.0, geometry=C, spacing=6.0, sigma=12.0, mu_jitter=0.0,
+                  ham_type=synth.COUPLING, dipole_frames=1, seed=61),
+        keywords=synth.c2_keywords(Singles=9, Length=300, RunTimes="32 0 0", Samplerate=40, Technique="CD",
+                                   FFT=256),
+        cd_positions=dict(seed=62, spacing=5.0)),
 }
 
 
@@ -163,6 +203,11 @@ def materialise(case, directory):
         pos = case["positions"]
         files.update(synth.write_positions(directory, case["spec"]["n_sites"], case["spec"]["frames"], **pos))
         files["coupling"] = ""  # couplings come from the positions
+    if case.get("cd_positions"):  # CD: positions only for the rotatory strengths
+        files.update(synth.write_positions(directory, case["spec"]["n_sites"], case["spec"]["frames"],
+                                           **case["cd_positions"]))
+    if case.get("alpha"):
+        files.update(synth.write_alpha(directory, case["spec"]["n_sites"], case["spec"]["frames"], **case["alpha"]))
     return files
 
 
@@ -181,9 +226,15 @@ def main(names=None):
             inp = synth.write_input(os.path.join(work, "input"), case["keywords"], files)
             oracle.run_reference(inp, work)
             out = {}
-            if case["keywords"]["Technique"] == "Absorption":
+            tech = case["keywords"]["Technique"]
+            if tech == "Absorption":
                 out["td"] = np.loadtxt(os.path.join(work, "TD_Absorption.dat"), ndmin=2)
                 out["spec"] = np.loadtxt(os.path.join(work, "Absorption.dat"), ndmin=2)
+            elif tech in oracle.LINEAR_FILES:
+                # per channel: td [tmax1][t, Re, Im], spec [rows][w, Re, Im]
+                out["td"] = np.stack([np.loadtxt(os.path.join(work, td), ndmin=2) for td, _ in oracle.LINEAR_FILES[tech]])
+                out["spec"] = np.stack([np.loadtxt(os.path.join(work, sp), ndmin=2)
+                                        for _, sp in oracle.LINEAR_FILES[tech]])
             else:
                 p = oracle.params(case["keywords"], files)
                 R = np.zeros((6, 2, p.tmax3, p.tmax1))

@@ -10,7 +10,8 @@ import oracle
 
 CASES = helpers.cases()
 ABS = [k for k, c in CASES.items() if c["keywords"]["Technique"] == "Absorption"]
-TWO_D = [k for k in CASES if k not in ABS]
+LIN = [k for k, c in CASES.items() if c["keywords"]["Technique"] in oracle.LINEAR_FILES]
+TWO_D = [k for k in CASES if k not in ABS and k not in LIN]
 # print precision of the reference's %e output, plus float summation order
 PRINT_TOL = 2e-6
 
@@ -42,6 +43,37 @@ def test_absorption_fp64_within_reference_rounding(name, tmp_path):
     re, im, n = oracle.absorption(p, "f64")
     err = helpers.rel(np.stack([re / n, im / n], 1), g["td"][:, 1:])
     assert err < 1e-4
+
+
+@pytest.mark.parametrize("name", LIN)
+def test_linear_restatement_matches_reference(name, tmp_path):
+    """LD, Raman, SFG, DOS, CD: every channel's TD_*.dat and spectrum file."""
+    case = CASES[name]
+    files = helpers.materialise(case, str(tmp_path))
+    g = helpers.golden(name)
+    p = oracle.params(case["keywords"], files)
+    re, im, n = oracle.linear(p, "f32")
+    assert len(re) == len(g["td"])
+    tol = 1e-5 if helpers.uses_eigen(case) else PRINT_TOL
+    for k in range(len(re)):
+        td = g["td"][k]
+        assert helpers.rel(np.stack([re[k] / n, im[k] / n], 1), td[:, 1:]) < tol
+        w, sr, si = oracle.spectrum(p, re[k], im[k], n, "f32")
+        assert len(w) == len(g["spec"][k])
+        assert helpers.rel(np.stack([sr, si], 1), g["spec"][k][:, 1:]) < max(tol, PRINT_TOL)
+
+
+@pytest.mark.parametrize("name", LIN)
+def test_linear_fp64_within_reference_rounding(name, tmp_path):
+    case = CASES[name]
+    files = helpers.materialise(case, str(tmp_path))
+    g = helpers.golden(name)
+    p = oracle.params(case["keywords"], files)
+    re, im, n = oracle.linear(p, "f64")
+    # CD and SSP responses are small differences of large terms: the reference's
+    # single-precision propagation error reaches 3e-4 of them (static CD)
+    for k in range(len(re)):
+        assert helpers.rel(np.stack([re[k] / n, im[k] / n], 1), g["td"][k][:, 1:]) < 5e-4
 
 
 @pytest.mark.parametrize("name", TWO_D)
