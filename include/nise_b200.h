@@ -19,6 +19,7 @@
  *                             (calc_2DES.c:22-586), one GPU instead of MPI ranks
  *   nise_linear            <- LD(), raman(), sfg(), calc_DOS(), calc_CD() (calc_LD.c,
  *                             raman.c, sfg.c, calc_DOS.c, calc_CD.c)
+ *   nise_translate         <- translate's main() (translate.c:25-65)
  *   nise_propagate         <- propagate_vector() (propagate.c:20-39), batched
  *   nise_propagate_doubles <- propagate_vec_coupling_S_doubles / _RK4_doubles /
  *                             propagate_double_sparce (propagate.c:376-1394)
@@ -213,6 +214,15 @@ int nise_set_trajectory_onfly(nise_ctx *ctx, const void *energy, size_t energy_b
                               size_t dipole_bytes, const void *position, size_t position_bytes, const void *pbc,
                               size_t pbc_bytes, const void *anharm, size_t anharm_bytes, const void *overtone,
                               size_t overtone_bytes);
+
+/* Trajectory format translation (the reference's translate program,
+ * translate.c:25-940): reads its keyword file (InputFormat/OutputFormat among
+ * GROBIN, GROASC, MITASC, MITTXT, SPECTRON, SKIBIN; the InputX and OutputX file
+ * names; Singles, Doubles, Length, Anharmonicity, Skip Doubles and the
+ * Modify Select/Label/Shift block) and writes the translated files.  Host
+ * only.  Returns NISE_ERR_IO for a missing file, NISE_ERR_ARG for a bad
+ * keyword file (message in nise_global_error). */
+int nise_translate(const char *keyword_file);
 
 /* Operator records of the linear techniques: alpha the Alphafile (read_alpha,
  * read_trajectory.c:380-399: int32 tag + 6N floats per frame, components

@@ -40,7 +40,7 @@ EXPORTED = [
     "nise_probe_fp32_peak", "nise_absorption_noalloc", "nise_2dfft_files", "nise_absorption_model",
     "nise_backward_absorption", "nise_absorption_tune", "nise_batch_create", "nise_batch_run", "nise_batch_result",
     "nise_batch_spectrum", "nise_batch_timing", "nise_batch_error", "nise_batch_destroy", "nise_set_trajectory_onfly",
-    "nise_set_operators", "nise_linear", "nise_linear_file", "nise_write_td",
+    "nise_set_operators", "nise_linear", "nise_linear_file", "nise_write_td", "nise_translate",
 ]
 
 
@@ -125,12 +125,20 @@ def lib():
         L.nise_linear_file.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.nise_linear_file.restype = ctypes.c_char_p
         L.nise_write_td.argtypes = [ctypes.c_char_p, P, dp, dp, ctypes.c_int, ctypes.c_int]
+        L.nise_translate.argtypes = [ctypes.c_char_p]
         _lib = L
     return _lib
 
 
 def _dp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def translate(keyword_file):
+    """Run a translate keyword file (trajectory format conversion, host only)."""
+    rc = lib().nise_translate(os.fsencode(keyword_file))
+    if rc != 0:
+        raise NiseError(rc, lib().nise_global_error().decode())
 
 
 def linear_files(technique):

@@ -4,6 +4,8 @@ Products (all written next to this file, so they travel with the source tree):
   libnise_b200.so   the engine: CUDA kernels for sm_100a + the C ABI (include/nise_b200.h)
   libnise_synth.so  the seeded synthetic GROBIN trajectory generator
   nise              the NISE-compatible C driver (keyword file in, output files out)
+  nise2dfft         the 2DFFT-compatible driver
+  nise_translate    the translate-compatible trajectory format converter
 
 Usage: python -m nise_2017_b200.build  (or build_all() from Python).
 """
@@ -38,6 +40,7 @@ CPP_SOURCES = [
     "absrun.cpp",
     "input.cpp",
     "singles.cpp",
+    "translate.cpp",
 ]
 
 
@@ -100,8 +103,10 @@ def build_engine(force=False, verbose_ptxas=False):
 
 
 def build_driver(force=False):
-    """The drop-in executables: nise (NISE's propagation path) and nise2dfft (2DFFT)."""
-    for exe, c in (("nise", "nise_main.c"), ("nise2dfft", "nise2dfft_main.c")):
+    """The drop-in executables: nise (NISE's propagation path), nise2dfft (2DFFT)
+    and nise_translate (translate)."""
+    for exe, c in (("nise", "nise_main.c"), ("nise2dfft", "nise2dfft_main.c"),
+                   ("nise_translate", "nise_translate_main.c")):
         out = os.path.join(HERE, exe)
         src = os.path.join(CSRC, c)
         if force or _newer(out, [src, os.path.join(INCLUDE, "nise_b200.h")]):
@@ -118,4 +123,4 @@ def build_all(force=False):
 
 if __name__ == "__main__":
     build_all(force="--force" in sys.argv)
-    print("built:", ", ".join(f for f in os.listdir(HERE) if f.endswith(".so") or f in ("nise", "nise2dfft")))
+    print("built:", ", ".join(f for f in os.listdir(HERE) if f.endswith(".so") or f in ("nise", "nise2dfft", "nise_translate")))
