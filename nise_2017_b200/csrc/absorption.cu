@@ -205,8 +205,17 @@ __global__ void k_abs_rk4(DevTraj T, Rk4Plan P, AbsJob J, double2 *resp, int nve
 }
 
 // ------------------------------------------------------------ sparse Taylor
+// Truncation tolerance of the exact propagator's series per step, relative
+// to the vector's norm: below the unit roundoff of the arithmetic (FP32
+// 6.0e-8, FP64 1.1e-16), so truncation adds less than one rounding of the
+// step it ends.
+constexpr double kSeriesTolF32 = 1e-8, kSeriesTolF64 = 1e-16;
+
 // Order of the Taylor series of exp(-i H f) per frame: the smallest K with
-// b^(K+1)/(K+1)! * e^b <= tol, b = |f| * (max|h_ii| + max row sum |J|) >= ||H f||.
+// b^(K+1)/(K+1)! <= tol, b = |f| * (max|h_ii| + max row sum |J|) >= ||H f||_2.
+// H is Hermitian, so the remainder's 2-norm is the largest remainder of the
+// scalar series of exp(-i x) over the eigenvalues, and |x|^(K+1)/(K+1)!
+// bounds that for real x (Lagrange form).
 template <typename R>
 __global__ void k_prep_taylor(DevTraj T, TaylorPlan P, double rowabs, double f, double tol, int *order) {
     long fi = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -214,7 +223,7 @@ __global__ void k_prep_taylor(DevTraj T, TaylorPlan P, double rowabs, double f, 
     long t = P.f0 + fi;
     double dmax = 0;
     for (int i = 0; i < P.n; i++) dmax = fmax(dmax, fabs((double)traj_diag(T, t, i, P.singleshift != 0)));
-    double b = fabs(f) * (dmax + rowabs), term = exp(b);
+    double b = fabs(f) * (dmax + rowabs), term = 1.0;
     int K = 0;
     for (K = 0; K < 60; K++) {
         term *= b / (K + 1);
@@ -1130,7 +1139,7 @@ int launch_abs_rk4(int prec, const DevTraj &T, const Rk4Plan &P, const AbsJob &J
 
 int launch_prep_taylor(int prec, const DevTraj &T, TaylorPlan &P, double rowabs_max, double f, int *order,
                        cudaStream_t s) {
-    double tol = prec == 0 ? 1e-10 : 1e-17;
+    double tol = prec == 0 ? kSeriesTolF32 : kSeriesTolF64;
     if (P.nf) k_prep_taylor<float><<<(P.nf + 127) / 128, 128, 0, s>>>(T, P, rowabs_max, f, tol, order);
     P.order = order;
     return (int)cudaGetLastError();
@@ -1315,7 +1324,7 @@ int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const Abs
 
 int launch_prep_cheb(const DevTraj &T, TaylorPlan &P, double rowabs_max, double f, int *order, float *inv_r,
                      float2 *coef, cudaStream_t s) {
-    if (P.nf) k_prep_cheb<<<(P.nf + 127) / 128, 128, 0, s>>>(T, P, rowabs_max, f, 1e-10, order, inv_r, coef);
+    if (P.nf) k_prep_cheb<<<(P.nf + 127) / 128, 128, 0, s>>>(T, P, rowabs_max, f, kSeriesTolF32, order, inv_r, coef);
     P.order = order;
     P.cheb_inv_r = inv_r;
     P.cheb_coef = coef;

@@ -161,6 +161,21 @@ def test_taylor_route_large_lattice(n, tmp_path):
     assert helpers.rel(rep + 1j * imp, re32 + 1j * im32) < 1e-6
 
 
+def test_c1_lattice_full_coherence_time(tmp_path):
+    """The benchmark lattice (N = 1024, static couplings, Propagation Sparse)
+    over its full 256-step coherence time: the FP32 series, truncated below
+    the FP32 unit roundoff per step, stays within 1e-5 of the FP64 run."""
+    from nise_2017_b200 import synth
+    s = synth.c1_spec(frames=560, seed=77)
+    files = synth.write(s, str(tmp_path))
+    kw = synth.c1_keywords(Length=560, Samplerate=150)
+    case = dict(keywords=kw)
+    _, re32, im32, n32, _ = run_engine(case, files)
+    _, re64, im64, n64, _ = run_engine(case, files, precision=nise.FP64)
+    assert n32 == n64 == 3
+    assert helpers.rel(re32 + 1j * im32, re64 + 1j * im64) < 1e-5
+
+
 def random_hamiltonians(rng, nvec, n, cut):
     nn2 = n * (n + 1) // 2
     H = np.zeros((nvec, nn2), np.float32)
