@@ -472,26 +472,33 @@ __global__ void __launch_bounds__(512) k_abs_taylor2(DevTraj T, TaylorPlan P, Ab
 }
 
 // Sparse Taylor propagation with the coupling matrix in shared memory as a
-// sliced ELL: slice s = rows 4s..4s+3 (the rows of one warp instruction at
-// G = 8), Ls entries per row (the slice's longest row, shorter rows padded
-// with zero weights), entry = (offset of the neighbour row in the state,
-// weight), stored [slot][row in slice] so a warp instruction reads 4
-// consecutive entries.  The state is single-buffered: the next Taylor term of
-// a thread's rows is kept in registers until every warp has read the current
-// term, then written back.
+// sliced ELL: slice s = rows 4s..4s+3, Ls entries per row (the slice's
+// longest row, shorter rows padded with zero weights), entry = (offset of the
+// neighbour row in a state of NISE_T3_ROW vectors per row, weight), stored
+// [slot][row in slice] so 4 lanes read 4 consecutive entries.  The state is
+// single-buffered: the next Taylor term of a thread's rows is kept in
+// registers until every warp has read the current term, then written back.
+//
+// G vectors per CTA: lane = (vector g, row q of a slice, slice so of the
+// 8 / G slices a warp instruction covers).  G = 8 is the throughput layout
+// (one slice per warp instruction, rows of 8 vectors); G = 1 covers 8 slices
+// per warp instruction, so a CTA finishes its vector several times sooner:
+// the launcher gives it the vectors of a last, partial wave, or every vector
+// when there are fewer than the SMs.  Vectors v0 .. v0+nvec-1.
 template <typename R> struct EllEnt;
 template <> struct EllEnt<float> { int off; float v; };
 template <> struct EllEnt<double> { int off; int pad; double v; };
 
-template <typename R, int IT>
-__global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, AbsJob J, double2 *resp, int nvec,
+template <typename R, int IT, int G>
+__global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, AbsJob J, double2 *resp, int v0, int nvec,
                                                     const EllEnt<R> *__restrict__ ell_g, const int *__restrict__ sptr_g,
                                                     int nslices, int nent, const int *__restrict__ rows_g) {
     typedef typename Vec2<R>::T R2;
-    constexpr int G = 8, QR = 4, RS = NISE_T3_ROW;
+    constexpr int QR = 4, SPW = 8 / G, RS = G == 8 ? NISE_T3_ROW : G;
+    static_assert(G == 8 || G == 1, "G = 8 or 1 vectors per CTA");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = P.n, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, NW = blockDim.x >> 5;
-    const int g = lane % G, q = lane / G;
+    const int g = lane % G, q = (lane / G) % QR, so = lane / (G * QR);
     R2 *cur = (R2 *)smem_raw;
     EllEnt<R> *ell = (EllEnt<R> *)(cur + (size_t)n * RS);
     int *sptr = (int *)(ell + nent);
@@ -502,16 +509,19 @@ __global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, Ab
     for (int e = tid; e < 4 * nslices; e += blockDim.x) rows[e] = rows_g[e];
     __syncthreads();
     auto rowof = [&](int sl) { return sl < nslices ? rows[q + QR * sl] : n; };
+    auto slice = [&](int it) { return (warp + NW * it) * SPW + so; };
+    // a neighbour's state: entry offsets address rows of NISE_T3_ROW
+    auto nbr = [&](int off) { return RS == NISE_T3_ROW ? off + g : (off / NISE_T3_ROW) * RS + g; };
     const int v = blockIdx.x * G + g;
     const bool valid = v < nvec;
-    const int vv = valid ? v : blockIdx.x * G;
+    const int vv = v0 + (valid ? v : blockIdx.x * G);
     const int x = vv % 3;
     const long ti = (long)(J.begin + vv / 3) * J.sample;
     R2 psi[IT], nx[IT];
     float dg[IT];
 #pragma unroll
     for (int it = 0; it < IT; it++) {
-        int i = rowof(warp + NW * it);
+        int i = rowof(slice(it));
         psi[it].x = i < n ? (R)traj_mu(T, ti, x, i) : (R)0;
         psi[it].y = 0;
     }
@@ -521,7 +531,7 @@ __global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, Ab
         double re = 0, im = 0;
 #pragma unroll
         for (int it = 0; it < IT; it++) {
-            int i = rowof(warp + NW * it);
+            int i = rowof(slice(it));
             if (i < n) {
                 R m = (R)traj_mu(T, tj, x, i);
                 re += (double)(m * psi[it].x);
@@ -532,19 +542,19 @@ __global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, Ab
             re += __shfl_xor_sync(0xffffffffu, re, o);
             im += __shfl_xor_sync(0xffffffffu, im, o);
         }
-        if (q == 0) { red[(warp * G + g) * 2] = re; red[(warp * G + g) * 2 + 1] = im; }
+        if (lane < G) { red[(warp * G + g) * 2] = re; red[(warp * G + g) * 2 + 1] = im; }
         __syncthreads();
         if (tid < G && blockIdx.x * G + tid < nvec) {
             double sr = 0, si = 0;
             for (int w = 0; w < NW; w++) { sr += red[(w * G + tid) * 2]; si += red[(w * G + tid) * 2 + 1]; }
-            resp[(size_t)(blockIdx.x * G + tid) * J.tmax + t1] = make_double2(sr, si);
+            resp[(size_t)(v0 + blockIdx.x * G + tid) * J.tmax + t1] = make_double2(sr, si);
         }
         if (t1 == J.tmax - 1) break;
         int K = P.order[tj - P.f0];
         for (int o = 1; o < G; o <<= 1) K = max(K, __shfl_xor_sync(0xffffffffu, K, o));
 #pragma unroll
         for (int it = 0; it < IT; it++) {
-            int i = rowof(warp + NW * it);
+            int i = rowof(slice(it));
             dg[it] = i < n ? traj_diag(T, tj, i, P.singleshift != 0) : 0.0f;
             if (i < n) cur[(size_t)i * RS + g] = psi[it];
         }
@@ -553,14 +563,14 @@ __global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, Ab
             const R c = (R)(J.f / k);
 #pragma unroll
             for (int it = 0; it < IT; it++) {
-                const int sl = warp + NW * it, i = rowof(sl);
+                const int sl = slice(it), i = rowof(sl);
                 if (sl >= nslices) continue;
                 R2 z = cur[(size_t)(i < n ? i : 0) * RS + g];
                 R yr = (R)dg[it] * z.x, yi = (R)dg[it] * z.y;
                 const int b0 = sptr[sl], b1 = sptr[sl + 1];
                 for (int e = b0 + q; e < b1; e += QR) {
                     EllEnt<R> en = ell[e];
-                    R2 zz = cur[en.off + g];
+                    R2 zz = cur[nbr(en.off)];
                     yr += en.v * zz.x;
                     yi += en.v * zz.y;
                 }
@@ -570,7 +580,7 @@ __global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, Ab
             __syncthreads();
 #pragma unroll
             for (int it = 0; it < IT; it++) {
-                const int sl = warp + NW * it, i = rowof(sl);
+                const int sl = slice(it), i = rowof(sl);
                 if (sl >= nslices || i >= n) continue;
                 cur[(size_t)i * RS + g] = nx[it];
                 psi[it].x += nx[it].x;
@@ -1168,10 +1178,10 @@ static int run_taylor2(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, d
     return (int)cudaGetLastError();
 }
 
-size_t taylor3_smem(const TaylorPlan &P, size_t rsz) {
+size_t taylor3_smem(const TaylorPlan &P, size_t rsz, int G = 8) {
     size_t ent = rsz == 4 ? 8 : 16;
-    return (size_t)P.n * NISE_T3_ROW * 2 * rsz + (size_t)P.ell_nent * ent + sizeof(int) * (5 * P.ell_nslices + 1) + 16 +
-           16 * 8 * 2 * sizeof(double);
+    return (size_t)P.n * (G == 8 ? NISE_T3_ROW : G) * 2 * rsz + (size_t)P.ell_nent * ent +
+           sizeof(int) * (5 * P.ell_nslices + 1) + 16 + 16 * 8 * 2 * sizeof(double);
 }
 
 template <int IT>
@@ -1199,21 +1209,46 @@ static int run_cheb3(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, dou
     return (int)cudaGetLastError();
 }
 
-template <typename R, int IT>
-static int run_taylor3(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int nvec,
-                       cudaStream_t s) {
-    const int NT = 512;
-    size_t smem = taylor3_smem(P, sizeof(R));
+template <typename R, int IT, int G>
+static int run_taylor3_g(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int v0, int nvec,
+                         cudaStream_t s) {
+    if (nvec <= 0) return 0;
+    size_t smem = taylor3_smem(P, sizeof(R), G);
     int e;
-    if ((e = set_smem(k_abs_taylor3<R, IT>, smem))) return e;
-    k_abs_taylor3<R, IT><<<(nvec + 7) / 8, NT, smem, s>>>(T, P, J, resp, nvec, (const EllEnt<R> *)P.ell,
-                                                          P.ell_sptr, P.ell_nslices, P.ell_nent, P.ell_rows);
-    (void)NT;
+    if ((e = set_smem(k_abs_taylor3<R, IT, G>, smem))) return e;
+    k_abs_taylor3<R, IT, G><<<(nvec + G - 1) / G, 512, smem, s>>>(T, P, J, resp, v0, nvec, (const EllEnt<R> *)P.ell,
+                                                                  P.ell_sptr, P.ell_nslices, P.ell_nent, P.ell_rows);
     return (int)cudaGetLastError();
 }
 
+// Streaming multiprocessors of the current device (wave sizes).
+int sm_count() {
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 1;
+}
+
+// One CTA per SM at G = 8: whole waves of 8-vector CTAs, and the vectors of a
+// last wave that would be less than half full on 1-vector CTAs (which finish
+// several times sooner); fewer vectors than SMs all on 1-vector CTAs.
+template <typename R, int IT>
+static int run_taylor3(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int nvec,
+                       cudaStream_t s, int *kernels) {
+    constexpr int IT1 = IT <= 8 ? 1 : IT / 8;  // rows per thread at G = 1: 8 slices per warp instruction
+    const int nsm = sm_count(), ctas = (nvec + 7) / 8;
+    int main = nvec;
+    if (nvec <= nsm) main = 0;
+    else if (ctas % nsm != 0 && ctas % nsm < nsm / 2 && ctas >= nsm) main = (ctas / nsm) * nsm * 8;
+    if (kernels) *kernels = (main > 0) + (nvec > main);
+    int e = run_taylor3_g<R, IT, 8>(T, P, J, resp, 0, main, s);
+    if (e) return e;
+    return run_taylor3_g<R, IT1, 1>(T, P, J, resp, main, nvec - main, s);
+}
+
 int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp,
-                      int vec_per_cta, cudaStream_t s) {
+                      int vec_per_cta, cudaStream_t s, int *kernels) {
+    if (kernels) *kernels = 1;
     if (P.use_v4) {  // the 4-vector sliced-ELL kernel (FP32, ELL through L1)
         if (prec != 0 || !P.ell4) return (int)cudaErrorNotSupported;
         int nvec = 3 * J.nsamp;
@@ -1251,12 +1286,12 @@ int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const Abs
         if (it <= 32) {
 #define T3(R)                                                                    \
     switch (IT) {                                                                \
-    case 1: return run_taylor3<R, 1>(T, P, J, resp, nvec, s);                    \
-    case 2: return run_taylor3<R, 2>(T, P, J, resp, nvec, s);                    \
-    case 4: return run_taylor3<R, 4>(T, P, J, resp, nvec, s);                    \
-    case 8: return run_taylor3<R, 8>(T, P, J, resp, nvec, s);                    \
-    case 16: return run_taylor3<R, 16>(T, P, J, resp, nvec, s);                  \
-    default: return run_taylor3<R, 32>(T, P, J, resp, nvec, s);                  \
+    case 1: return run_taylor3<R, 1>(T, P, J, resp, nvec, s, kernels);  \
+    case 2: return run_taylor3<R, 2>(T, P, J, resp, nvec, s, kernels);  \
+    case 4: return run_taylor3<R, 4>(T, P, J, resp, nvec, s, kernels);  \
+    case 8: return run_taylor3<R, 8>(T, P, J, resp, nvec, s, kernels);  \
+    case 16: return run_taylor3<R, 16>(T, P, J, resp, nvec, s, kernels); \
+    default: return run_taylor3<R, 32>(T, P, J, resp, nvec, s, kernels); \
     }
             if (prec == 0) { T3(float) }
             T3(double)

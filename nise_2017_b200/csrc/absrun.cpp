@@ -460,8 +460,9 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
 // The propagation kernel(s) of the job with launch configuration cfg.
 int AbsRun::run_main(cudaStream_t s, int cfg, double2 *dst) {
     const int pr = prec == NISE_FP32 ? 0 : 1;
-    int e = 0;
+    int e = 0, kernels = 1;
     auto one = [&](const AbsJob &Js, double2 *r) -> int {
+        kernels = 1;
         switch (scheme) {
         case SCHEME_TROTTER:
             if (cfg > 0) return launch_abs_trotter_lv(pr, T, TP, Js, r, perm.p, lvptr.p, nlev, cfg, s);
@@ -481,7 +482,7 @@ int AbsRun::run_main(cudaStream_t s, int cfg, double2 *dst) {
                 P.cheb_inv_r = nullptr;
                 P.cheb_coef = nullptr;
             }
-            return launch_abs_taylor(pr, T, P, Js, r, cfg == 10 ? 8 : cfg < 0 ? -cfg : cfg, s);
+            return launch_abs_taylor(pr, T, P, Js, r, cfg == 10 ? 8 : cfg < 0 ? -cfg : cfg, s, &kernels);
         }
         default:
             return launch_abs_dia(pr, T, Ue.p, f0, N, Js, r, s);
@@ -493,11 +494,11 @@ int AbsRun::run_main(cudaStream_t s, int cfg, double2 *dst) {
             Js.begin = begin + q;
             Js.nsamp = 1;
             e = one(Js, dst + (size_t)3 * q * tmax);
-            c->launches++;
+            c->launches += kernels;
         }
     } else {
         e = one(J, dst);
-        c->launches++;
+        c->launches += kernels;
     }
     return e;
 }

@@ -93,8 +93,10 @@ int launch_prep_rk4(int prec, const DevTraj &T, const Rk4Plan &P, double fsub, f
 int launch_abs_rk4(int prec, const DevTraj &T, const Rk4Plan &P, const AbsJob &J, double2 *resp, cudaStream_t s);
 int launch_prep_taylor(int prec, const DevTraj &T, TaylorPlan &P, double rowabs_max, double f, int *order,
                        cudaStream_t s);
+// kernels (optional): the number of kernels launched (the sliced-ELL Taylor
+// kernel runs whole waves of 8-vector CTAs plus 1-vector CTAs for the rest).
 int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp,
-                      int vec_per_cta, cudaStream_t s);
+                      int vec_per_cta, cudaStream_t s, int *kernels = nullptr);
 // Chebyshev coefficients of the exact step per frame (FP32 kernel); sets
 // P.order, P.cheb_inv_r and P.cheb_coef.
 int launch_prep_cheb(const DevTraj &T, TaylorPlan &P, double rowabs_max, double f, int *order, float *inv_r,

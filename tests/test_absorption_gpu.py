@@ -161,6 +161,26 @@ def test_taylor_route_large_lattice(n, tmp_path):
     assert helpers.rel(rep + 1j * imp, re32 + 1j * im32) < 1e-6
 
 
+def test_taylor3_full_waves_and_tail(tmp_path):
+    """More vectors than one wave of 8-vector CTAs: whole waves run on the
+    8-vector layout and the rest on 1-vector CTAs; every start point must
+    match the FP64 oracle, wherever its vectors landed."""
+    from nise_2017_b200 import synth
+    s = synth.c1_spec(n_sites=27, frames=900, seed=78)
+    files = synth.write(s, str(tmp_path))
+    kw = synth.c1_keywords(Singles=27, Length=900, RunTimes="16 0 0", Samplerate=2)
+    case = dict(keywords=kw)
+    p = nise.params_from_keywords(kw, files, kernel_config=8)
+    with nise.Context(p) as c:
+        c.load_files()
+        re, im, n = c.absorption()
+        _, _, launches = c.timing()
+    assert n == 442 and launches >= 3  # 1326 vectors: 148 CTAs of 8, then 142 vectors on 1-vector CTAs
+    ore, oim, on = oracle.absorption(oracle.params(kw, files), "f64")
+    assert n == on
+    assert helpers.rel(re + 1j * im, ore + 1j * oim) < SPARSE_FP32
+
+
 def test_c1_lattice_full_coherence_time(tmp_path):
     """The benchmark lattice (N = 1024, static couplings, Propagation Sparse)
     over its full 256-step coherence time: the FP32 series, truncated below
