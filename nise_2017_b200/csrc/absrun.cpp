@@ -44,7 +44,9 @@ std::mutex g_tune_mu;
 
 int default_config(int scheme, int N, bool plain, bool cheb) {
     if (scheme == SCHEME_TROTTER) return N >= 96 ? 128 : 0;
-    if (plain) return 3;  // one start point per launch: 3 vectors
+    // one start point per launch (3 vectors): the sliced-ELL kernel, which
+    // gives every vector its own CTA when there are fewer vectors than SMs
+    if (plain) return 8;
     (void)cheb;           // the Chebyshev kernel is a tuned alternative: fewer terms, more work per term
     return 8;
 }
