@@ -485,22 +485,29 @@ __global__ void __launch_bounds__(512) k_abs_taylor2(DevTraj T, TaylorPlan P, Ab
 // per warp instruction, so a CTA finishes its vector several times sooner:
 // the launcher gives it the vectors of a last, partial wave, or every vector
 // when there are fewer than the SMs.  Vectors v0 .. v0+nvec-1.
+//
+// NT threads per CTA.  NT = 512 keeps each row's diagonal element in
+// registers; above 512 (fewer registers per thread, more warps to hide the
+// shared-memory latency) the diagonal of every (row, vector) is kept in
+// shared memory instead.
 template <typename R> struct EllEnt;
 template <> struct EllEnt<float> { int off; float v; };
 template <> struct EllEnt<double> { int off; int pad; double v; };
 
-template <typename R, int IT, int G>
-__global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, AbsJob J, double2 *resp, int v0, int nvec,
+template <typename R, int IT, int G, int NT>
+__global__ void __launch_bounds__(NT, 1) k_abs_taylor3(DevTraj T, TaylorPlan P, AbsJob J, double2 *resp, int v0, int nvec,
                                                     const EllEnt<R> *__restrict__ ell_g, const int *__restrict__ sptr_g,
                                                     int nslices, int nent, const int *__restrict__ rows_g) {
     typedef typename Vec2<R>::T R2;
     constexpr int QR = 4, SPW = 8 / G, RS = G == 8 ? NISE_T3_ROW : G;
     static_assert(G == 8 || G == 1, "G = 8 or 1 vectors per CTA");
+    constexpr bool kDgShared = NT > 512;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = P.n, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, NW = blockDim.x >> 5;
     const int g = lane % G, q = (lane / G) % QR, so = lane / (G * QR);
     R2 *cur = (R2 *)smem_raw;
-    EllEnt<R> *ell = (EllEnt<R> *)(cur + (size_t)n * RS);
+    float *dgs = (float *)(cur + (size_t)n * RS);  // [n][G] diagonal of each vector's frame (kDgShared)
+    EllEnt<R> *ell = (EllEnt<R> *)(dgs + (kDgShared ? (size_t)n * G : 0));
     int *sptr = (int *)(ell + nent);
     int *rows = sptr + nslices + 1;  // [nslices][4] site of each slice row (n: padding)
     double *red = (double *)(((uintptr_t)(rows + 4 * nslices) + 15) & ~(uintptr_t)15);
@@ -518,7 +525,7 @@ __global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, Ab
     const int x = vv % 3;
     const long ti = (long)(J.begin + vv / 3) * J.sample;
     R2 psi[IT], nx[IT];
-    float dg[IT];
+    float dg[kDgShared ? 1 : IT];
 #pragma unroll
     for (int it = 0; it < IT; it++) {
         int i = rowof(slice(it));
@@ -555,7 +562,12 @@ __global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, Ab
 #pragma unroll
         for (int it = 0; it < IT; it++) {
             int i = rowof(slice(it));
-            dg[it] = i < n ? traj_diag(T, tj, i, P.singleshift != 0) : 0.0f;
+            const float d = i < n ? traj_diag(T, tj, i, P.singleshift != 0) : 0.0f;
+            if (kDgShared) {
+                if (i < n) dgs[(size_t)i * G + g] = d;
+            } else {
+                dg[it] = d;
+            }
             if (i < n) cur[(size_t)i * RS + g] = psi[it];
         }
         for (int k = 1; k <= K; k++) {
@@ -565,8 +577,10 @@ __global__ void __launch_bounds__(512) k_abs_taylor3(DevTraj T, TaylorPlan P, Ab
             for (int it = 0; it < IT; it++) {
                 const int sl = slice(it), i = rowof(sl);
                 if (sl >= nslices) continue;
-                R2 z = cur[(size_t)(i < n ? i : 0) * RS + g];
-                R yr = (R)dg[it] * z.x, yi = (R)dg[it] * z.y;
+                const int ic = i < n ? i : 0;
+                R2 z = cur[(size_t)ic * RS + g];
+                const R d = kDgShared ? (R)dgs[(size_t)ic * G + g] : (R)dg[kDgShared ? 0 : it];
+                R yr = d * z.x, yi = d * z.y;
                 const int b0 = sptr[sl], b1 = sptr[sl + 1];
                 for (int e = b0 + q; e < b1; e += QR) {
                     EllEnt<R> en = ell[e];
@@ -1178,10 +1192,10 @@ static int run_taylor2(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, d
     return (int)cudaGetLastError();
 }
 
-size_t taylor3_smem(const TaylorPlan &P, size_t rsz, int G = 8) {
+size_t taylor3_smem(const TaylorPlan &P, size_t rsz, int G = 8, int NT = 512) {
     size_t ent = rsz == 4 ? 8 : 16;
-    return (size_t)P.n * (G == 8 ? NISE_T3_ROW : G) * 2 * rsz + (size_t)P.ell_nent * ent +
-           sizeof(int) * (5 * P.ell_nslices + 1) + 16 + 16 * 8 * 2 * sizeof(double);
+    return (size_t)P.n * (G == 8 ? NISE_T3_ROW : G) * 2 * rsz + (NT > 512 ? (size_t)P.n * G * sizeof(float) : 0) +
+           (size_t)P.ell_nent * ent + sizeof(int) * (5 * P.ell_nslices + 1) + 16 + (NT / 32) * 8 * 2 * sizeof(double);
 }
 
 template <int IT>
@@ -1209,14 +1223,14 @@ static int run_cheb3(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, dou
     return (int)cudaGetLastError();
 }
 
-template <typename R, int IT, int G>
+template <typename R, int IT, int G, int NT = 512>
 static int run_taylor3_g(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int v0, int nvec,
                          cudaStream_t s) {
     if (nvec <= 0) return 0;
-    size_t smem = taylor3_smem(P, sizeof(R), G);
+    size_t smem = taylor3_smem(P, sizeof(R), G, NT);
     int e;
-    if ((e = set_smem(k_abs_taylor3<R, IT, G>, smem))) return e;
-    k_abs_taylor3<R, IT, G><<<(nvec + G - 1) / G, 512, smem, s>>>(T, P, J, resp, v0, nvec, (const EllEnt<R> *)P.ell,
+    if ((e = set_smem(k_abs_taylor3<R, IT, G, NT>, smem))) return e;
+    k_abs_taylor3<R, IT, G, NT><<<(nvec + G - 1) / G, NT, smem, s>>>(T, P, J, resp, v0, nvec, (const EllEnt<R> *)P.ell,
                                                                   P.ell_sptr, P.ell_nslices, P.ell_nent, P.ell_rows);
     return (int)cudaGetLastError();
 }
@@ -1231,7 +1245,10 @@ int sm_count() {
 
 // One CTA per SM at G = 8: whole waves of 8-vector CTAs, and the vectors of a
 // last wave that would be less than half full on 1-vector CTAs (which finish
-// several times sooner); fewer vectors than SMs all on 1-vector CTAs.
+// several times sooner); fewer vectors than SMs all on 1-vector CTAs.  FP32
+// lattices of 513..1056 sites (16 rows per thread at 512 threads) run their
+// 8-vector CTAs with 768 threads, 11 rows each (measured on N = 1024: 75.3 ms
+// instead of 81.7 ms per step; 640 threads 76.3 ms, 896 threads spill).
 template <typename R, int IT>
 static int run_taylor3(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int nvec,
                        cudaStream_t s, int *kernels) {
@@ -1241,7 +1258,11 @@ static int run_taylor3(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, d
     if (nvec <= nsm) main = 0;
     else if (ctas % nsm != 0 && ctas % nsm < nsm / 2 && ctas >= nsm) main = (ctas / nsm) * nsm * 8;
     if (kernels) *kernels = (main > 0) + (nvec > main);
-    int e = run_taylor3_g<R, IT, 8>(T, P, J, resp, 0, main, s);
+    int e = -1;
+    if constexpr (sizeof(R) == 4 && IT == 16)
+        if (P.ell_nslices <= 24 * 11 && taylor3_smem(P, 4, 8, 768) <= 220 * 1024)
+            e = run_taylor3_g<R, 11, 8, 768>(T, P, J, resp, 0, main, s);
+    if (e < 0) e = run_taylor3_g<R, IT, 8>(T, P, J, resp, 0, main, s);
     if (e) return e;
     return run_taylor3_g<R, IT1, 1>(T, P, J, resp, main, nvec - main, s);
 }

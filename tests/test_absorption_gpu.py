@@ -181,6 +181,23 @@ def test_taylor3_full_waves_and_tail(tmp_path):
     assert helpers.rel(re + 1j * im, ore + 1j * oim) < SPARSE_FP32
 
 
+def test_taylor3_wide_ctas_on_1024_sites(tmp_path):
+    """The benchmark lattice with more than a wave of vectors: 8-vector CTAs
+    of 768 threads (the FP32 layout for 513..1056 sites) plus 1-vector CTAs,
+    against the FP64 run and against the 4-vector Taylor kernel."""
+    from nise_2017_b200 import synth
+    s = synth.c1_spec(frames=816, seed=79)
+    files = synth.write(s, str(tmp_path))
+    kw = synth.c1_keywords(Length=816, RunTimes="16 0 0", Samplerate=2)
+    case = dict(keywords=kw)
+    _, re32, im32, n32, _ = run_engine(case, files, kernel_config=8)
+    _, re64, im64, n64, _ = run_engine(case, files, precision=nise.FP64)
+    _, ret2, imt2, nt2, _ = run_engine(case, files, kernel_config=3)
+    assert n32 == n64 == nt2 == 400  # 1200 vectors: 148 CTAs of 8, then 16 on 1-vector CTAs
+    assert helpers.rel(re32 + 1j * im32, re64 + 1j * im64) < SPARSE_FP32
+    assert helpers.rel(re32 + 1j * im32, ret2 + 1j * imt2) < SPARSE_FP32
+
+
 def test_c1_lattice_full_coherence_time(tmp_path):
     """The benchmark lattice (N = 1024, static couplings, Propagation Sparse)
     over its full 256-step coherence time: the FP32 series, truncated below
