@@ -582,11 +582,15 @@ __global__ void __launch_bounds__(NT, 1) k_abs_taylor3(DevTraj T, TaylorPlan P, 
                 const R d = kDgShared ? (R)dgs[(size_t)ic * G + g] : (R)dg[kDgShared ? 0 : it];
                 R yr = d * z.x, yi = d * z.y;
                 const int b0 = sptr[sl], b1 = sptr[sl + 1];
+                // the next entry is loaded one iteration ahead (past the slice it
+                // is not used; the read stays inside this CTA's shared memory)
+                EllEnt<R> en = ell[b0 + q];
                 for (int e = b0 + q; e < b1; e += QR) {
-                    EllEnt<R> en = ell[e];
+                    const EllEnt<R> nen = ell[e + QR];
                     R2 zz = cur[nbr(en.off)];
                     yr += en.v * zz.x;
                     yi += en.v * zz.y;
+                    en = nen;
                 }
                 nx[it].x = c * yi;  // (-i)(c)(y)
                 nx[it].y = -c * yr;
