@@ -365,7 +365,7 @@ __device__ __forceinline__ float over_mu(const TwoD &D, long t, int x, int i) {
 
 // CTA = W warps = W doubles vectors of one start point, all at the same t3.
 template <typename R, int CPL>
-__global__ void __launch_bounds__(512) k2d_doubles(TwoD D, int vec_per_sample, Dcoef<R> *cf_static, int use_tab) {
+__global__ void __launch_bounds__(512, 1) k2d_doubles(TwoD D, int vec_per_sample, Dcoef<R> *cf_static, int use_tab) {
     typedef typename Vec2<R>::T R2;
     typedef Ar<R> A;
     extern __shared__ __align__(16) unsigned char smem_raw[];
