@@ -517,8 +517,12 @@ __global__ void __launch_bounds__(NT, 1) k_abs_taylor3(DevTraj T, TaylorPlan P, 
     __syncthreads();
     auto rowof = [&](int sl) { return sl < nslices ? rows[q + QR * sl] : n; };
     auto slice = [&](int it) { return (warp + NW * it) * SPW + so; };
-    // a neighbour's state: entry offsets address rows of NISE_T3_ROW
-    auto nbr = [&](int off) { return RS == NISE_T3_ROW ? off + g : (off / NISE_T3_ROW) * RS + g; };
+    // a neighbour's state: entry offsets are byte offsets of rows of NISE_T3_ROW vectors
+    const R2 *curg = cur + g;
+    auto nbr = [&](int offb) -> R2 {
+        if (RS == NISE_T3_ROW) return *(const R2 *)((const char *)curg + offb);
+        return curg[(offb / (int)(NISE_T3_ROW * sizeof(R2))) * RS];
+    };
     const int v = blockIdx.x * G + g;
     const bool valid = v < nvec;
     const int vv = v0 + (valid ? v : blockIdx.x * G);
@@ -587,7 +591,7 @@ __global__ void __launch_bounds__(NT, 1) k_abs_taylor3(DevTraj T, TaylorPlan P, 
                 EllEnt<R> en = ell[b0 + q];
                 for (int e = b0 + q; e < b1; e += QR) {
                     const EllEnt<R> nen = ell[e + QR];
-                    R2 zz = cur[nbr(en.off)];
+                    R2 zz = nbr(en.off);
                     yr += en.v * zz.x;
                     yi += en.v * zz.y;
                     en = nen;
@@ -793,6 +797,7 @@ __global__ void __launch_bounds__(512) k_abs_cheb3(DevTraj T, TaylorPlan P, AbsJ
     const int n = P.n, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, NW = blockDim.x >> 5;
     const int g = lane % G, q = lane / G;
     float2 *cur = (float2 *)smem_raw;
+    const float2 *curg = cur + g;  // ELL entry offsets are byte offsets of state rows
     float *dgs = (float *)(cur + (size_t)n * RS);  // [row][g]
     EllEnt<float> *ell = (EllEnt<float> *)(dgs + (size_t)n * G);
     int *sptr = (int *)(ell + nent);
@@ -873,7 +878,8 @@ __global__ void __launch_bounds__(512) k_abs_cheb3(DevTraj T, TaylorPlan P, AbsJ
                 float yr2 = 0.f, yi2 = 0.f;
                 for (; e + QR < b1; e += 2 * QR) {
                     EllEnt<float> e0 = ell[e], e1 = ell[e + QR];
-                    float2 z0 = cur[e0.off + g], z1 = cur[e1.off + g];
+                    float2 z0 = *(const float2 *)((const char *)curg + e0.off);
+                    float2 z1 = *(const float2 *)((const char *)curg + e1.off);
                     yr += e0.v * z0.x;
                     yi += e0.v * z0.y;
                     yr2 += e1.v * z1.x;
@@ -881,7 +887,7 @@ __global__ void __launch_bounds__(512) k_abs_cheb3(DevTraj T, TaylorPlan P, AbsJ
                 }
                 if (e < b1) {
                     EllEnt<float> e0 = ell[e];
-                    float2 z0 = cur[e0.off + g];
+                    float2 z0 = *(const float2 *)((const char *)curg + e0.off);
                     yr += e0.v * z0.x;
                     yi += e0.v * z0.y;
                 }

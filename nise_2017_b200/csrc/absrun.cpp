@@ -270,8 +270,8 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
             }
             if ((rc = dorder.alloc(c, (size_t)nf))) return rc;
             // sliced ELL (4-row slices, [slot][row]) of the same couplings for the
-            // shared-memory kernel; entry offsets address rows of NISE_T3_ROW
-            // complex numbers.  Each row lists its neighbours of the other
+            // shared-memory kernel; entry offsets are byte offsets of rows of
+            // NISE_T3_ROW complex numbers.  Each row lists its neighbours of the other
             // parity first: the four rows of a slice alternate in parity, so a
             // slot whose rows all pick the same relative parity gathers two even
             // and two odd rows, which share no shared-memory banks (FP32).
@@ -323,10 +323,11 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
                 for (int slot = 0; slot < L; slot++)
                     for (int r = 0; r < 4; r++) {
                         int row = srow[4 * sl + r], e = sptr[sl] + slot * 4 + r;
-                        int off = (row < N ? row : 0) * NISE_T3_ROW;
+                        const int rowb = NISE_T3_ROW * (prec == NISE_FP32 ? 8 : 16);  // bytes per state row
+                        int off = (row < N ? row : 0) * rowb;
                         double v = 0;
                         if (row < N && slot < rp[row + 1] - rp[row]) {
-                            off = ecol[rp[row] + slot] * NISE_T3_ROW;
+                            off = ecol[rp[row] + slot] * rowb;
                             v = evd[rp[row] + slot];
                         }
                         unsigned char *dst = ell.data() + (size_t)e * esz;
