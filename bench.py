@@ -67,8 +67,9 @@ def parse():
     a.add_argument("--impl", choices=["ours", "reference"], default="ours")
     a.add_argument("--frames", type=int, default=100000, help="trajectory length (default: the full workload)")
     a.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline (profiling runs)")
-    a.add_argument("--config", choices=["c1", "c2", "c4"], default="c1",
-                   help="c1: the headline (batched absorption, N=1024); c2: 2DIR, N=64 cluster; c4: 64-trajectory "
+    a.add_argument("--config", choices=["c1", "c2", "c3", "c4"], default="c1",
+                   help="c1: the headline (batched absorption, N=1024); c2: 2DIR, N=64 cluster; c3: adjoint, N=256 "
+                        "chain; c4: 64-trajectory "
                         "mixed-size batch (secondary workloads)")
     a.add_argument("--t2", type=int, default=0, help="c2 only: waiting-time steps (RunTimes 64 t2 64)")
     a.add_argument("--end", type=int, default=0, help="c2 only: EndPoint (0 = all start points)")
@@ -401,6 +402,91 @@ def run_c2(args):
     return out
 
 
+def run_c3(args):
+    """Adjoint of linear absorption (FP64 Trotter model): N = 256 chain with the c0
+    statistics, 20000 x 2 fs frames, Tmax1 128, Samplerate 20.  The loss is the L2
+    distance to a target spectrum made by the same model with per-site shifts drawn
+    from N(0, 5 cm^-1) and a coupling scale of 1.1; gradients with respect to the 256
+    shifts, the coupling scale and the lifetime, checkpoints every 32 steps.
+
+    value = site-steps per second of one forward model run plus one backward run (the
+    backward sweep recomputes the states from checkpoints); fd_check = the largest
+    disagreement with central differences (h = 1e-3, one Richardson step) over sites 0,
+    85, 170, 255, the scale and the lifetime, relative to the largest gradient component."""
+    import numpy as np
+    import torch
+    import nise_2017_b200 as nise
+    from nise_2017_b200 import synth
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    s = synth.c3_spec()
+    kw = synth.c3_keywords()
+    with tempfile.TemporaryDirectory() as td:
+        files = synth.write(s, td)
+        p = nise.params_from_keywords(kw, files, device=local, precision=nise.FP64)
+        n, lt0 = p.singles, float(p.lifetime)
+        nsamp = (p.length - p.tmax1 - 1) // p.sample + 1
+        site_steps = 3 * nsamp * p.tmax1 * n
+        rng = np.random.default_rng(20173)
+        with nise.Context(p) as c:
+            c.load_files()
+            _, tr, ti = c.absorption_model(rng.normal(0, 5, n), 1.1, lt0)
+
+            def loss(shift, scale, lt):
+                _, sr, si = c.absorption_model(shift, scale, lt)
+                return float(((sr - tr) ** 2).sum() + ((si - ti) ** 2).sum()), 2 * (sr - tr), 2 * (si - ti)
+
+            shift = np.zeros(n)
+            for _ in range(max(args.warmup, 3)):
+                L, dre, dim = loss(shift, 1.0, lt0)
+                c.backward_absorption(shift, 1.0, lt0, dre, dim)
+            clk = ClockSampler(local)
+            clk.start()
+            times, fwd_ms, bwd_ms = [], [], []
+            for _ in range(args.steps):
+                t0 = time.perf_counter()
+                L, dre, dim = loss(shift, 1.0, lt0)
+                f_ms, _, _ = c.timing()
+                g, gs, gl = c.backward_absorption(shift, 1.0, lt0, dre, dim)
+                b_ms, _, launches = c.timing()
+                times.append((time.perf_counter() - t0) * 1e3)
+                fwd_ms.append(f_ms)
+                bwd_ms.append(b_ms)
+            clocks = clk.stop()
+
+            def central(f, x, h=1e-3):
+                d1 = (f(x + h) - f(x - h)) / (2 * h)
+                d2 = (f(x + h / 2) - f(x - h / 2)) / h
+                return (4 * d2 - d1) / 3
+
+            fd, adj = [], []
+            for a in (0, 85, 170, 255):
+                e = np.zeros(n)
+                e[a] = 1.0
+                fd.append(central(lambda x: loss(shift + x * e, 1.0, lt0)[0], 0.0))
+                adj.append(g[a])
+            fd.append(central(lambda x: loss(shift, x, lt0)[0], 1.0))
+            adj.append(gs)
+            fd.append(central(lambda x: loss(shift, 1.0, x)[0], lt0))
+            adj.append(gl)
+            scale = max(np.abs(g).max(), abs(gs), abs(gl))
+            fd_err = float(max(abs(x - y) for x, y in zip(adj, fd)) / scale)
+    dev_ms = statistics.mean(fwd_ms) + statistics.mean(bwd_ms)
+    out = {"metric": "adjoint of linear absorption: forward + backward site-steps/s (secondary workload)",
+           "value": site_steps / (dev_ms / 1e3), "unit": "site-steps/s", "n_gpus": 1, "steps": args.steps,
+           "warmup": max(args.warmup, 3), "ms_per_step": dev_ms, "higher_is_better": True, "dtype": "f64",
+           "config": {"workload": "adjoint, N=256 chain (c0 statistics), 20000 x 2 fs, RunTimes 128 0 0, "
+                                  "Samplerate 20, Trotter 5, checkpoints every 32 steps; loss vs a target with "
+                                  "shifts ~ N(0, 5 cm^-1) and coupling scale 1.1", "start_points": nsamp},
+           "forward_ms": statistics.mean(fwd_ms), "backward_ms": statistics.mean(bwd_ms),
+           "time_to_gradient_s": statistics.mean(times) / 1e3, "gpu_launches": launches,
+           "fd_check": {"max_rel_err": fd_err, "components": "sites 0, 85, 170, 255; scale; lifetime",
+                        "h": 1e-3, "scheme": "central, one Richardson step"},
+           "clocks": clocks}
+    print(json.dumps(out), flush=True)
+    return out
+
+
 def c4_sites():
     """Site counts of the mixed-size batch: round(8 * 256^(i/63)), i = 0..63 (8 ... 2048)."""
     return [int(round(8 * 256 ** (i / 63.0))) for i in range(64)]
@@ -523,6 +609,8 @@ if __name__ == "__main__":
         run_reference(a)
     elif a.config == "c2":
         run_c2(a)
+    elif a.config == "c3":
+        run_c3(a)
     elif a.config == "c4":
         run_c4(a)
     else:

@@ -4,7 +4,7 @@ The workloads mirror the benchmark configurations of the NISE propagation path:
   c0  linear absorption, Trotter "Coupling": 16-site chain, 10000 frames x 2 fs
   c1  linear absorption, "Sparse": 1024 sites on an 8x8x16 lattice, 100000 x 1 fs
   c2  2DIR, "Coupling": 64 oscillators in a random cluster, 20000 x 2 fs
-  c3  absorption for the adjoint: 256-site chain, 20000 frames
+  c3  absorption for the adjoint: 256-site chain, 20000 frames (c3_spec, c3_keywords)
   c4  mixed-size batch: 64 lattice trajectories, 8..2048 sites, 5000 x 1 fs
 Every function takes overrides so tests can shrink sites, frames and times.
 """
@@ -145,6 +145,19 @@ def c0_keywords(**kw):
              MaxFrequencies="1750 1750 1750", Technique="Absorption", HamiltonianType="Full")
     d.update(kw)
     return d
+
+
+def c3_spec(**kw):
+    """Adjoint workload: the c0 chain statistics on 256 sites, 20000 frames."""
+    d = dict(n_sites=256, frames=20000)
+    d.update(kw)
+    return c0_spec(**d)
+
+
+def c3_keywords(**kw):
+    d = dict(Singles=256, Length=20000)
+    d.update(kw)
+    return c0_keywords(**d)
 
 
 def c1_spec(**kw):

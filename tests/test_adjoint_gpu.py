@@ -145,3 +145,34 @@ def test_adjoint_rejects_other_schemes(tmp_path):
         with pytest.raises(nise.NiseError) as e:
             c.absorption_model(np.zeros(p.singles), 1.0, 600.0)
         assert e.value.code == -6
+
+
+def test_adjoint_c3_configuration(tmp_path):
+    """The full adjoint workload: a 256-site chain over 20000 frames (994 start
+    points, 128 steps, checkpoints every 32).  Adjoint gradients of the L2
+    spectrum loss against central differences (h = 1e-3) for sites at both ends
+    and the middle, the coupling scale and the lifetime."""
+    s = synth.c3_spec(seed=53)
+    files = synth.write(s, str(tmp_path))
+    p = nise.params_from_keywords(synth.c3_keywords(), files, precision=nise.FP64)
+    n, lt = p.singles, float(p.lifetime)
+    rng = np.random.default_rng(20173)
+    with nise.Context(p) as c:
+        c.load_files()
+        _, tr, ti = c.absorption_model(rng.normal(0, 5, n), 1.1, lt)
+        target = (tr, ti)
+        shift = np.zeros(n)
+        L, dre, dim = loss_and_grad(c, target, shift, 1.0, lt)
+        g, gs, gl = c.backward_absorption(shift, 1.0, lt, dre, dim)
+        h = 1e-3
+        checks = []
+        for a in (0, 128, 255):
+            e = np.zeros(n)
+            e[a] = 1.0
+            checks.append((g[a], central(lambda x: loss_and_grad(c, target, shift + x * e, 1.0, lt)[0], 0.0, h)))
+        checks.append((gs, central(lambda x: loss_and_grad(c, target, shift, x, lt)[0], 1.0, h)))
+        checks.append((gl, central(lambda x: loss_and_grad(c, target, shift, 1.0, x)[0], lt, h)))
+    scale = max(np.abs(g).max(), abs(gs), abs(gl))
+    assert L > 0 and scale > 0
+    for adj, fd in checks:
+        assert abs(adj - fd) / scale < ADJ_VS_FD, checks
