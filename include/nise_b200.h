@@ -120,10 +120,11 @@ typedef struct {
     int kernel_config;             /* absorption kernel: 0 automatic (autotuned or default);
                                       Trotter: 1 thread per vector, 64/128/256 level-scheduled
                                       rotations with that many threads per start point;
-                                      Sparse (static couplings): 3 or 9 k_abs_taylor2 with 4 or 8
-                                      vectors per CTA, 8 the sliced-ELL Taylor kernel, 10 the
+                                      Sparse/Diagonal (static couplings): 3 or 9 k_abs_taylor2 with
+                                      4 or 8 vectors per CTA, 8 the sliced-ELL Taylor kernel, 10 the
                                       sliced-ELL Chebyshev kernel (FP32), 12 the sliced-ELL
-                                      Taylor kernel with 4 vectors per CTA (FP32) */
+                                      Taylor kernel with 4 vectors per CTA (FP32), 2 the eigen
+                                      route (explicit per-frame propagators, up to 120 sites) */
     char positionFName[256];       /* Positionfile (TransitionDipole / ExtendedDipole; CD) */
     char pbcFName[256];            /* PBCfile: periodic box per frame (optional) */
     char alphaFName[256];          /* Alphafile: polarisabilities (Raman, SFG) */

@@ -119,14 +119,16 @@ def test_diagonal_scheme_matches_reference_sparse(tmp_path):
     assert helpers.rel(re + 1j * im, ore + 1j * oim) < SPARSE_FP32
 
 
-def test_eigen_route_matches_taylor_route(tmp_path):
-    """Two exact propagators of static couplings: the eigen route (Diagonal)
-    and the sparse Taylor series (Sparse, Threshold 0), both in FP64."""
+@pytest.mark.parametrize("prop", ["Sparse", "Diagonal"])
+def test_eigen_route_matches_taylor_route(prop, tmp_path):
+    """Two exact propagators of static couplings: the eigen route (forced by
+    kernel_config 2) and the sparse Taylor series (the default for static
+    couplings), both in FP64."""
     case = CASES["abs_sparse_static"]
     files = helpers.materialise(case, str(tmp_path))
-    _, re_t, im_t, _, _ = run_engine(case, files, precision=nise.FP64)
-    kw = dict(case["keywords"], Propagation="Diagonal")
-    _, re_e, im_e, _, _ = run_engine(dict(case, keywords=kw), files, precision=nise.FP64)
+    kw = dict(case["keywords"], Propagation=prop)
+    _, re_t, im_t, _, _ = run_engine(dict(case, keywords=kw), files, precision=nise.FP64)
+    _, re_e, im_e, _, _ = run_engine(dict(case, keywords=kw), files, precision=nise.FP64, kernel_config=2)
     assert helpers.rel(re_e + 1j * im_e, re_t + 1j * im_t) < 1e-9
 
 
