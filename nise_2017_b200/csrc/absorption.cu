@@ -14,6 +14,7 @@
 // once per frame by a preparation kernel and read by every vector that
 // crosses the frame.  The sparse Taylor scheme is a sparse-matrix product per
 // Taylor order: a CTA owns G vectors and spreads the sites over its threads.
+#include <algorithm>
 #include <cstdio>
 
 #include "common.cuh"
@@ -86,13 +87,14 @@ __global__ void k_abs_trotter(DevTraj T, TrotterPlan P, AbsJob J, double2 *resp,
 // rotation k gets level 1 + the highest level of the earlier rotations that
 // share one of its sites, so the rotations of one level touch disjoint sites
 // and applying a level in parallel reproduces the sequential lexicographic
-// order of propagate.c:876-888 operation for operation.  CTA per start
+// order of propagate.c:876-888 operation for operation.  The coupling pairs
+// are stored in level order: level l is pairs[lvptr[l] .. lvptr[l+1]).  CTA per start
 // point, its three polarisation vectors in shared memory; the response is
-// summed in site order by one thread per polarisation (the order of dot_mu),
-// so every Trotter kernel gives bitwise identical results.
+// summed by one thread per polarisation in the order of dot_mu, so every
+// Trotter kernel gives bitwise identical results.
 template <typename R>
-__global__ void k_abs_trotter_lv(DevTraj T, TrotterPlan P, AbsJob J, double2 *resp, const int *__restrict__ perm,
-                                 const int *__restrict__ lvptr, int nlev) {
+__global__ void k_abs_trotter_lv(DevTraj T, TrotterPlan P, AbsJob J, double2 *resp, const int *__restrict__ lvptr,
+                                 int nlev) {
     typedef typename Vec2<R>::T R2;
     typedef Ar<R> A;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -112,13 +114,18 @@ __global__ void k_abs_trotter_lv(DevTraj T, TrotterPlan P, AbsJob J, double2 *re
         const long t = ti + t1;
         for (int e = tid; e < 3 * n; e += NT) mu[e] = traj_mu(T, t, e / n, e % n);
         __syncthreads();
-        if (tid < 3) {
+        if (tid < 3) {  // the residue order of dot_mu
             double re = 0, im = 0;
-            for (int a = 0; a < n; a++) {
-                R m = (R)mu[tid * n + a];
-                R2 z = C[tid * n + a];
-                re += (double)A::mul(m, z.x);
-                im += (double)A::mul(m, z.y);
+            for (int r = 0; r < 32; r++) {
+                double pr = 0, pi = 0;
+                for (int a = r; a < n; a += 32) {
+                    R m = (R)mu[tid * n + a];
+                    R2 z = C[tid * n + a];
+                    pr += (double)A::mul(m, z.x);
+                    pi += (double)A::mul(m, z.y);
+                }
+                re += pr;
+                im += pi;
             }
             resp[(size_t)(3 * sl + tid) * J.tmax + t1] = make_double2(re, im);
         }
@@ -139,7 +146,7 @@ __global__ void k_abs_trotter_lv(DevTraj T, TrotterPlan P, AbsJob J, double2 *re
                 for (int l = 0; l < nlev; l++) {
                     const int r0 = lvptr[l], cnt = lvptr[l + 1] - r0;
                     for (int e = tid; e < 3 * cnt; e += NT) {
-                        const int k = perm[r0 + e / 3], x = e % 3;
+                        const int k = r0 + e / 3, x = e % 3;
                         const int2 ab = P.pairs[k];
                         const R2 cs = Rf[k];
                         R2 *ca = C + x * n + ab.x, *cb = C + x * n + ab.y;
@@ -154,6 +161,167 @@ __global__ void k_abs_trotter_lv(DevTraj T, TrotterPlan P, AbsJob J, double2 *re
                     __syncthreads();
                 }
             }
+        }
+    }
+}
+
+// Trotter absorption, warp per vector.  The rotations of one level touch
+// disjoint sites (on lattices a level holds ~20 of them and there are ~N/3.6
+// levels, because rotations that share a site keep their lexicographic
+// order); the host splits every level into chunks of at most 32 rotations
+// (chunk c = pairs[chk[c] .. chk[c+1])), the lanes apply one chunk and a
+// __syncwarp separates chunks.  A two-deep register pipeline loads the bounds
+// of chunk c+2 and the pairs and coefficients of chunk c+1 while chunk c is
+// applied, so only the state loads sit on the critical path.  A lane with no
+// rotation in a chunk rotates its own spare site n + lane by the identity
+// (cos 1, sin 0; the spare sites stay zero), so the warp never diverges; in
+// shared memory these identity rotations are table entries K .. K+31.
+// Every vector
+// sees the reference's float operations (propagate.c:868-895); the response
+// is summed in the order of dot_mu (lane r sums the sites r, r+32, ...), so
+// all Trotter kernels give bitwise identical results.  W warps = W vectors
+// per CTA; vector v is polarisation v % 3 of start point v / 3.
+//
+// SM: the rotation table lives in shared memory (pairs packed a | b << 16,
+// coefficients as R2).  Static coefficients are loaded once; per-frame
+// coefficients are reloaded every frame, and then the CTA is the three
+// polarisations of one start point (W = 3, every warp active), which cross
+// the same frames.  ustage: each warp copies the frame's half-step phases
+// into shared memory with the response loads, once per frame instead of
+// reading them twice per sub-step.
+template <typename R, bool SM>
+__global__ void k_abs_trotter_wv(DevTraj T, TrotterPlan P, AbsJob J, double2 *resp, int nvec,
+                                 const int *__restrict__ chk_g, int nchk, int ustage) {
+    typedef typename Vec2<R>::T R2;
+    typedef Ar<R> A;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = P.n, K = P.k, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = blockDim.x >> 5;
+    unsigned char *sp = smem_raw;
+    int *chk = (int *)sp;  // [nchk + 4]: chunk bounds, then K (empty chunks)
+    sp += ((size_t)(nchk + 4) * sizeof(int) + 15) & ~(size_t)15;
+    R2 *tcs = (R2 *)sp;  // SM: [K + 32] coefficients
+    unsigned *tab = (unsigned *)(sp + (SM ? (((size_t)(K + 32) * sizeof(R2) + 15) & ~(size_t)15) : 0));  // SM: pairs
+    if (SM) sp = (unsigned char *)tab + (((size_t)(K + 32) * sizeof(unsigned) + 15) & ~(size_t)15);
+    const int nc = n + 32;  // sites and the 32 spare sites
+    R2 *C = (R2 *)sp + (size_t)warp * nc * (ustage ? 2 : 1);
+    R2 *Us = C + nc;  // ustage: [n] phases of the frame
+    for (int e = threadIdx.x; e < nchk + 4; e += blockDim.x) chk[e] = e <= nchk ? chk_g[e] : K;
+    if (SM) {
+        for (int e = threadIdx.x; e < K + 32; e += blockDim.x) {
+            const int2 ab = e < K ? P.pairs[e] : make_int2(n + e - K, n + e - K);
+            tab[e] = (unsigned)ab.x | ((unsigned)ab.y << 16);
+        }
+        for (int e = threadIdx.x; e < K + 32; e += blockDim.x) {
+            R2 u;
+            u.x = 1;
+            u.y = 0;
+            if (e >= K) tcs[e] = u;
+            else if (P.rot_static) tcs[e] = ((const R2 *)P.rot)[e];
+        }
+    }
+    __syncthreads();
+    const int v = blockIdx.x * W + warp;
+    if (v >= nvec) return;  // never with per-frame coefficients in shared memory (W = 3)
+    const int x = v % 3;
+    const long ti = (long)(J.begin + v / 3) * J.sample;
+    for (int a = lane; a < nc; a += 32) {
+        R2 z;
+        z.x = a < n ? (R)traj_mu(T, ti, x, a) : (R)0;
+        z.y = 0;
+        C[a] = z;
+    }
+    const R2 *U = (const R2 *)P.U, *rot = (const R2 *)P.rot;
+    const int2 spare = make_int2(n + lane, n + lane);
+    R2 unit;
+    unit.x = 1;
+    unit.y = 0;
+    auto pair = [&](int k) -> int2 {
+        if (SM) {
+            const unsigned w = tab[k];
+            return make_int2((int)(w & 0xffffu), (int)(w >> 16));
+        }
+        return P.pairs[k];
+    };
+    for (int t1 = 0; t1 < J.tmax; t1++) {
+        const long t = ti + t1;
+        const bool step = t1 + 1 < J.tmax;  // the frame's phases exist only for propagated frames
+        const R2 *Uf = U + (t - P.f0) * n;
+        double re = 0, im = 0;
+        for (int a = lane; a < n; a += 32) {
+            R m = (R)traj_mu(T, t, x, a);
+            if (ustage && step) Us[a] = Uf[a];
+            R2 z = C[a];
+            re += (double)A::mul(m, z.x);
+            im += (double)A::mul(m, z.y);
+        }
+        const double2 rs = resp_sum_warp(re, im);
+        if (lane == 0) resp[(size_t)v * J.tmax + t1] = rs;
+        if (!step) break;
+        const R2 *Rf;
+        if (SM) {
+            if (!P.rot_static) {
+                __syncthreads();  // every warp is done with the previous frame's coefficients
+                const R2 *src = rot + (t - P.f0) * K;
+                for (int e = threadIdx.x; e < K; e += blockDim.x) tcs[e] = src[e];
+                __syncthreads();
+            }
+            Rf = tcs;
+        } else {
+            Rf = P.rot_static ? rot : rot + (t - P.f0) * K;
+        }
+        const R2 *Uu = ustage ? Us : Uf;  // a lane reads back only the phases it copied
+        for (int sub = 0; sub < J.ts; sub++) {
+            for (int a = lane; a < n; a += 32) {  // propagate.c:870-873
+                R2 z = C[a], u = Uu[a], o;
+                o.x = A::sub(A::mul(z.x, u.x), A::mul(z.y, u.y));
+                o.y = A::add(A::mul(z.y, u.x), A::mul(z.x, u.y));
+                C[a] = o;
+            }
+            __syncwarp();
+            // chunk c = pairs[chk[c] .. e0): this lane's rotation (ab0, cs0);
+            // e1 = end of chunk c+1
+            int e0 = chk[1], e1 = chk[2];
+            int2 ab0;
+            R2 cs0;
+            auto fetch = [&](int k, int end, int2 &ab, R2 &cs) {
+                if (SM) {
+                    k = k < end ? k : K + lane;
+                    ab = pair(k);
+                    cs = Rf[k];
+                } else {
+                    ab = k < end ? pair(k) : spare;
+                    cs = k < end ? Rf[k] : unit;
+                }
+            };
+            fetch(chk[0] + lane, e0, ab0, cs0);
+#pragma unroll 2
+            for (int c = 0; c < nchk; c++) {
+                int2 ab1;
+                R2 cs1;
+                fetch(e0 + lane, e1, ab1, cs1);
+                const int e2 = chk[c + 3];
+                {  // propagate.c:876-888
+                    R2 xa = C[ab0.x], xb = C[ab0.y], ya, yb;
+                    ya.x = A::sub(A::mul(cs0.x, xa.x), A::mul(cs0.y, xb.y));
+                    ya.y = A::add(A::mul(cs0.x, xa.y), A::mul(cs0.y, xb.x));
+                    yb.x = A::sub(A::mul(cs0.x, xb.x), A::mul(cs0.y, xa.y));
+                    yb.y = A::add(A::mul(cs0.x, xb.y), A::mul(cs0.y, xa.x));
+                    C[ab0.x] = ya;
+                    C[ab0.y] = yb;
+                }
+                __syncwarp();
+                e0 = e1;
+                e1 = e2;
+                ab0 = ab1;
+                cs0 = cs1;
+            }
+            for (int a = lane; a < n; a += 32) {  // propagate.c:891-894
+                R2 z = C[a], u = Uu[a], o;
+                o.x = A::sub(A::mul(z.x, u.x), A::mul(z.y, u.y));
+                o.y = A::add(A::mul(z.y, u.x), A::mul(z.x, u.y));
+                C[a] = o;
+            }
+            __syncwarp();
         }
     }
 }
@@ -1132,17 +1300,73 @@ int launch_abs_trotter(int prec, const DevTraj &T, const TrotterPlan &P, const A
 }
 
 int launch_abs_trotter_lv(int prec, const DevTraj &T, const TrotterPlan &P, const AbsJob &J, double2 *resp,
-                          const int *perm, const int *lvptr, int nlev, int threads, cudaStream_t s) {
+                          const int *lvptr, int nlev, int threads, cudaStream_t s) {
     if (J.nsamp <= 0) return 0;
     const size_t smem = (size_t)3 * P.n * ((prec == 0 ? sizeof(float2) : sizeof(double2)) + sizeof(float));
     int e;
     if (prec == 0) {
         if ((e = set_smem(k_abs_trotter_lv<float>, smem))) return e;
-        k_abs_trotter_lv<float><<<J.nsamp, threads, smem, s>>>(T, P, J, resp, perm, lvptr, nlev);
+        k_abs_trotter_lv<float><<<J.nsamp, threads, smem, s>>>(T, P, J, resp, lvptr, nlev);
     } else {
         if ((e = set_smem(k_abs_trotter_lv<double>, smem))) return e;
-        k_abs_trotter_lv<double><<<J.nsamp, threads, smem, s>>>(T, P, J, resp, perm, lvptr, nlev);
+        k_abs_trotter_lv<double><<<J.nsamp, threads, smem, s>>>(T, P, J, resp, lvptr, nlev);
     }
+    return (int)cudaGetLastError();
+}
+
+int sm_count();
+
+// Shared memory of k_abs_trotter_wv: chunk table, rotation table (sm), W
+// vectors (and their phases with ustage).
+static size_t trotter_wv_smem(int prec, const TrotterPlan &P, int nchk, bool sm, bool ustage, int W) {
+    const size_t r2 = prec == 0 ? sizeof(float2) : sizeof(double2);
+    size_t b = ((size_t)(nchk + 4) * sizeof(int) + 15) & ~(size_t)15;
+    if (sm) b += (((size_t)(P.k + 32) * r2 + 15) & ~(size_t)15) + (((size_t)(P.k + 32) * sizeof(unsigned) + 15) & ~(size_t)15);
+    return b + (size_t)W * (P.n + 32) * r2 * (ustage ? 2 : 1);
+}
+
+// tables: 1 = the rotation table in shared memory where it fits (else in
+// global memory), 0 = in global memory.  With static coefficients W vectors
+// share a CTA, W = the vectors per SM (at most 16, as shared memory allows),
+// so that small jobs spread over every SM; the phases are staged where
+// shared memory has room for them at that W.
+int launch_abs_trotter_wv(int prec, const DevTraj &T, const TrotterPlan &P, const AbsJob &J, double2 *resp,
+                          const int *chk, int nchk, int tables, cudaStream_t s) {
+    if (J.nsamp <= 0) return 0;
+    const int nvec = 3 * J.nsamp, nsm = sm_count();
+    bool sm = tables != 0 && P.n + 32 <= 65536, ustage = false;
+    int W = 3;
+    auto fits = [&](bool m, bool u, int w) { return trotter_wv_smem(prec, P, nchk, m, u, w) <= kMaxSmem; };
+    auto widest = [&](bool m) {
+        int w = std::min(16, std::max(1, (nvec + nsm - 1) / nsm));
+        while (w > 1 && !fits(m, false, w)) w--;
+        return w;
+    };
+    if (sm && !P.rot_static) {
+        if (!fits(true, false, 3)) sm = false;
+    } else if (sm && !fits(true, false, widest(true))) {
+        sm = false;
+    }
+    if (sm && P.rot_static) W = widest(true);
+    if (!sm) W = widest(false);
+    if (!fits(sm, false, W)) return (int)cudaErrorNotSupported;
+    ustage = fits(sm, true, W);
+    const size_t smem = trotter_wv_smem(prec, P, nchk, sm, ustage, W);
+    const int grid = (nvec + W - 1) / W, us = ustage ? 1 : 0;
+    int e;
+#define NISE_WV(RT, SMT)                                                                         \
+    do {                                                                                       \
+        if ((e = set_smem(k_abs_trotter_wv<RT, SMT>, smem))) return e;                         \
+        k_abs_trotter_wv<RT, SMT><<<grid, 32 * W, smem, s>>>(T, P, J, resp, nvec, chk, nchk, us); \
+    } while (0)
+    if (prec == 0) {
+        if (sm) NISE_WV(float, true);
+        else NISE_WV(float, false);
+    } else {
+        if (sm) NISE_WV(double, true);
+        else NISE_WV(double, false);
+    }
+#undef NISE_WV
     return (int)cudaGetLastError();
 }
 

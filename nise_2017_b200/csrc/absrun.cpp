@@ -30,9 +30,11 @@ namespace {
 enum Scheme { SCHEME_TROTTER, SCHEME_RK4, SCHEME_TAYLOR, SCHEME_EIGEN };
 
 // Launch configurations the autotuner chooses from.
-//   Trotter: 0 = thread per vector (k_abs_trotter), T > 0 = level-scheduled
-//            rotations with T threads per start point (k_abs_trotter_lv);
-//            all are bitwise identical.
+//   Trotter: 0 = thread per vector (k_abs_trotter), T = 64/128/256 =
+//            level-scheduled rotations with T threads per start point
+//            (k_abs_trotter_lv); 32 / 33 = warp per vector
+//            (k_abs_trotter_wv) with the rotation table in shared / global
+//            memory; all bitwise identical.
 //   Taylor:  3 = k_abs_taylor2 with 4 vectors per CTA, 8 = the sliced-ELL
 //            kernel with 8 (k_abs_taylor2 with 8 where it does not fit),
 //            -8 = k_abs_taylor2 with 8, 10 = the FP32 sliced-ELL kernel with
@@ -42,8 +44,15 @@ typedef std::tuple<int, int, int, int, int> TuneKey;  // scheme, precision, site
 std::map<TuneKey, int> g_tuned;
 std::mutex g_tune_mu;
 
-int default_config(int scheme, int N, bool plain, bool cheb) {
-    if (scheme == SCHEME_TROTTER) return N >= 96 ? 128 : 0;
+// Trotter: the warp-per-vector kernel where the levels are wide (lattices:
+// ~20 rotations per level) or the job has too few vectors to fill warps of
+// threads (a warp per vector then has the shorter critical path); thread per
+// vector for chains (one rotation per level) with many vectors.
+int default_config(int scheme, int N, bool plain, bool cheb, int K, int nchk, int nvec) {
+    if (scheme == SCHEME_TROTTER) {
+        if (K > 0 && (K >= 4 * nchk || nvec < 1024)) return 32;
+        return N >= 96 ? 128 : 0;
+    }
     // one start point per launch (3 vectors): the sliced-ELL kernel, which
     // gives every vector its own CTA when there are fewer vectors than SMs
     if (plain) return 8;
@@ -53,6 +62,10 @@ int default_config(int scheme, int N, bool plain, bool cheb) {
 
 // Rotation levels of the lexicographic coupling list: perm holds the
 // rotation indices ordered by (level, index), lvptr the level boundaries.
+// Two rotations that share a site keep their order (the later one has the
+// higher level), so applying the rotations in perm order performs the same
+// floating-point operations on every site as the lexicographic order of
+// propagate.c:876-888.
 void rotation_levels(const std::vector<int2> &pairs, int n, std::vector<int> &perm, std::vector<int> &lvptr) {
     std::vector<int> last(n, 0), lv(pairs.size());
     int nlev = 0;
@@ -85,8 +98,8 @@ struct AbsRun {
     // Trotter
     DevBuf<int2> dpairs;
     DevBuf<char> U, rot;
-    DevBuf<int> perm, lvptr;
-    int nlev = 0;
+    DevBuf<int> lvptr, lvchk;  // level bounds; the same split into chunks of at most 32
+    int nlev = 0, nchk = 0;
     TrotterPlan TP;
     // RK4
     DevBuf<int2> dent;
@@ -177,14 +190,22 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
         TP.nf = nf;
         TP.rot_static = p.hamiltonian == NISE_HAM_COUPLING;
         TP.singleshift = c->nshift > 0;
+        // the pairs (and so the rotation tables) in level order
         std::vector<int> hperm, hlv;
         rotation_levels(pairs, N, hperm, hlv);
         nlev = (int)hlv.size() - 1;
-        if ((rc = dpairs.upload(c, pairs.empty() ? std::vector<int2>(1) : pairs)) ||
+        std::vector<int2> lpairs(pairs.size());
+        for (size_t q = 0; q < pairs.size(); q++) lpairs[q] = pairs[hperm[q]];
+        if ((rc = dpairs.upload(c, lpairs.empty() ? std::vector<int2>(1) : lpairs)) ||
             (rc = U.alloc(c, r2 * (size_t)nf * N)) ||
             (rc = rot.alloc(c, r2 * (size_t)(TP.rot_static ? 1 : nf) * (TP.k ? TP.k : 1))) ||
-            (rc = perm.upload(c, hperm.empty() ? std::vector<int>(1) : hperm)) || (rc = lvptr.upload(c, hlv)))
+            (rc = lvptr.upload(c, hlv)))
             return rc;
+        std::vector<int> hchk(1, 0);
+        for (int l = 0; l < nlev; l++)
+            for (int q = hlv[l]; q < hlv[l + 1]; q += 32) hchk.push_back(std::min(q + 32, hlv[l + 1]));
+        nchk = (int)hchk.size() - 1;
+        if ((rc = lvchk.upload(c, hchk))) return rc;
         TP.pairs = dpairs.p;
         TP.U = U.p;
         TP.rot = rot.p;
@@ -443,11 +464,11 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
                 return rc;
         }
     }
-    config = default_config(scheme, N, plain, cheb);
+    config = default_config(scheme, N, plain, cheb, TP.k, nchk, plain ? 3 : nvec);
     if (p.kernel_config != 0) {  // forced by the caller
         const int k = p.kernel_config;
         if (scheme == SCHEME_EIGEN && k == 2) return NISE_OK;
-        if (scheme == SCHEME_TROTTER && (k == 1 || k == 64 || k == 128 || k == 256)) config = k == 1 ? 0 : k;
+        if (scheme == SCHEME_TROTTER && (k == 1 || k == 32 || k == 33 || k == 64 || k == 128 || k == 256)) config = k == 1 ? 0 : k;
         else if (scheme == SCHEME_TAYLOR && (k == 3 || k == 8 || k == 9 || (k == 10 && cheb) || (k == 12 && dell4.p)))
             config = k == 9 ? -8 : k;
         else return nise_fail(c, NISE_ERR_ARG, "kernel_config %d does not apply to this scheme", k);
@@ -472,7 +493,8 @@ int AbsRun::run_main(cudaStream_t s, int cfg, double2 *dst) {
         kernels = 1;
         switch (scheme) {
         case SCHEME_TROTTER:
-            if (cfg > 0) return launch_abs_trotter_lv(pr, T, TP, Js, r, perm.p, lvptr.p, nlev, cfg, s);
+            if (cfg == 32 || cfg == 33) return launch_abs_trotter_wv(pr, T, TP, Js, r, lvchk.p, nchk, cfg == 32, s);
+            if (cfg > 0) return launch_abs_trotter_lv(pr, T, TP, Js, r, lvptr.p, nlev, cfg, s);
             return launch_abs_trotter(pr, T, TP, Js, r, s);
         case SCHEME_RK4:
             return launch_abs_rk4(pr, T, RP, Js, r, s);
@@ -515,7 +537,7 @@ int AbsRun::run_main(cudaStream_t s, int cfg, double2 *dst) {
 int AbsRun::tune() {
     std::vector<int> cand;
     if (scheme == SCHEME_TROTTER) {
-        cand = {0, 64, 128, 256};
+        cand = {0, 32, 33, 64, 128, 256};
     } else {
         cand = {3, -8, 8};
         if (cheb) cand.push_back(10);

@@ -85,10 +85,16 @@ int launch_prep_trotter(int prec, const DevTraj &T, const TrotterPlan &P, double
 int launch_abs_trotter(int prec, const DevTraj &T, const TrotterPlan &P, const AbsJob &J, double2 *resp,
                        cudaStream_t s);
 // Trotter absorption with level-scheduled rotations (CTA per start point):
-// perm lists the rotation indices level by level, lvptr[l]..lvptr[l+1] the
+// P.pairs holds the couplings in level order, lvptr[l]..lvptr[l+1] the
 // rotations of level l.  Bitwise identical to launch_abs_trotter.
 int launch_abs_trotter_lv(int prec, const DevTraj &T, const TrotterPlan &P, const AbsJob &J, double2 *resp,
-                          const int *perm, const int *lvptr, int nlev, int threads, cudaStream_t s);
+                          const int *lvptr, int nlev, int threads, cudaStream_t s);
+// The same with a warp per vector (the lanes share a level's rotations),
+// bitwise identical to both.  chk[c]..chk[c+1] are the rotations of
+// chunk c (a level, or at most 32 of its rotations).  tables = 1: the
+// rotation table in shared memory where it fits; 0: read from global memory.
+int launch_abs_trotter_wv(int prec, const DevTraj &T, const TrotterPlan &P, const AbsJob &J, double2 *resp,
+                          const int *chk, int nchk, int tables, cudaStream_t s);
 int launch_prep_rk4(int prec, const DevTraj &T, const Rk4Plan &P, double fsub, float fsub32, cudaStream_t s);
 int launch_abs_rk4(int prec, const DevTraj &T, const Rk4Plan &P, const AbsJob &J, double2 *resp, cudaStream_t s);
 int launch_prep_taylor(int prec, const DevTraj &T, TaylorPlan &P, double rowabs_max, double f, int *order,

@@ -193,16 +193,37 @@ __device__ __forceinline__ void rk4_apply(typename Vec2<R>::T *S, int B, int lan
 
 // Response of one vector at one time: sum_i mu_i * psi_i.  In FP32 the
 // product is rounded to float before the FP64 sum, as calc_S1
-// (absorption.c:205-212) does with a double accumulator.
+// (absorption.c:205-212) does with a double accumulator.  The FP64 sum runs
+// in one fixed order that a thread and a warp can both produce: a partial
+// sum per site residue r = i mod 32 (ascending sites), then the 32 partials
+// in residue order.  It differs from the site order of the reference only by
+// FP64 rounding, and every kernel that uses it (a thread per vector here, a
+// warp per vector in resp_sum_warp) gives bitwise the same responses.
 template <typename R>
 __device__ __forceinline__ double2 dot_mu(const DevTraj &T, long t, int x, const typename Vec2<R>::T *S, int B,
                                           int lane, int n) {
     double re = 0, im = 0;
-    for (int i = 0; i < n; i++) {
-        R m = (R)traj_mu(T, t, x, i);
-        typename Vec2<R>::T z = S[i * B + lane];
-        re += (double)Ar<R>::mul(m, z.x);
-        im += (double)Ar<R>::mul(m, z.y);
+    for (int r = 0; r < 32; r++) {
+        double pr = 0, pi = 0;
+        for (int i = r; i < n; i += 32) {
+            R m = (R)traj_mu(T, t, x, i);
+            typename Vec2<R>::T z = S[i * B + lane];
+            pr += (double)Ar<R>::mul(m, z.x);
+            pi += (double)Ar<R>::mul(m, z.y);
+        }
+        re += pr;
+        im += pi;
+    }
+    return make_double2(re, im);
+}
+
+// The residue-order sum of dot_mu across a warp: lane r holds the partial
+// sum of sites r, r+32, ... (ascending); every lane gets the total.
+__device__ __forceinline__ double2 resp_sum_warp(double pr, double pi) {
+    double re = 0, im = 0;
+    for (int r = 0; r < 32; r++) {
+        re += __shfl_sync(0xffffffffu, pr, r);
+        im += __shfl_sync(0xffffffffu, pi, r);
     }
     return make_double2(re, im);
 }

@@ -1,8 +1,8 @@
 """Level-scheduled Trotter rotations, the launch autotuner and the batch API.
 
-The level-scheduled kernel applies the rotations of one level (disjoint site
-pairs) in parallel; it must reproduce the sequential lexicographic order bit
-for bit.  A batch runs many contexts' jobs as one CUDA graph and must return
+The level-scheduled kernels apply the rotations of one level (disjoint site
+pairs) in parallel, a CTA or a warp per vector; they must reproduce the
+sequential lexicographic order, and the response sum order, bit for bit.  A batch runs many contexts' jobs as one CUDA graph and must return
 exactly what the same contexts return one by one.
 """
 import numpy as np
@@ -25,7 +25,7 @@ def run(kw, files, **engine):
     return re, im, n
 
 
-@pytest.mark.parametrize("cfg", [64, 128, 256])
+@pytest.mark.parametrize("cfg", [32, 33, 64, 128, 256])
 @pytest.mark.parametrize("prec", [nise.FP32, nise.FP64])
 def test_level_kernel_bitwise_equal_to_thread_per_vector(cfg, prec, tmp_path):
     case = CASES["abs_coupling_full"]
@@ -47,6 +47,54 @@ def test_level_kernel_lattice_static_couplings(tmp_path):
     r1 = run(kw, files, kernel_config=128)
     assert np.array_equal(r0[0], r1[0]) and np.array_equal(r0[1], r1[1])
     ore, oim, on = oracle.absorption(oracle.params(kw, files), "f32a64")
+    assert helpers.rel(r1[0] + 1j * r1[1], ore + 1j * oim) < 1e-11
+
+
+def same(r0, r1):
+    return r0[2] == r1[2] and np.array_equal(r0[0], r1[0]) and np.array_equal(r0[1], r1[1])
+
+
+def test_warp_kernel_levels_wider_than_a_warp(tmp_path):
+    """Static couplings whose levels hold 40, 80 and 40 rotations (dimers (2i, 2i+1) and
+    partners (i, i + 80) on 160 sites): lanes take several rotations of one level."""
+    import oracle
+    n = 160
+    s = synth.c1_spec(n_sites=n, frames=260, seed=62)
+    files = synth.write(s, str(tmp_path))
+    rec = np.fromfile(files["coupling"], dtype=np.float32)
+    h = rec[1:]  # int32 tag, then the packed upper triangle (index b + a(2n-a-1)/2)
+    diag = np.array([h[a + a * (2 * n - a - 1) // 2] for a in range(n)])
+    h[:] = 0
+    for a in range(n):
+        h[a + a * (2 * n - a - 1) // 2] = diag[a]
+    for i in range(n // 2):
+        a, b = 2 * i, 2 * i + 1
+        h[b + a * (2 * n - a - 1) // 2] = 12.0
+        h[i + n // 2 + i * (2 * n - i - 1) // 2] = -7.0
+    rec.tofile(files["coupling"])
+    kw = synth.c1_keywords(Singles=n, Length=260, RunTimes="24 0 0", Samplerate=40, Propagation="Coupling",
+                           Trotter=2)
+    r0 = run(kw, files, kernel_config=1)
+    for cfg in (32, 33, 64):
+        assert same(r0, run(kw, files, kernel_config=cfg)), cfg
+    r1 = run(kw, files, kernel_config=32)
+    ore, oim, on = oracle.absorption(oracle.params(kw, files), "f32a64")
+    assert helpers.rel(r1[0] + 1j * r1[1], ore + 1j * oim) < 1e-11
+
+
+@pytest.mark.parametrize("cfg", [32, 33])
+@pytest.mark.parametrize("prec", [nise.FP32, nise.FP64])
+def test_warp_kernel_lattice_static_couplings(cfg, prec, tmp_path):
+    """300-site lattice (levels of ~20 rotations; the phases staged in shared memory)."""
+    import oracle
+    s = synth.c1_spec(n_sites=300, frames=260, seed=63)
+    files = synth.write(s, str(tmp_path))
+    kw = synth.c1_keywords(Singles=300, Length=260, RunTimes="24 0 0", Samplerate=20, Propagation="Coupling",
+                           Trotter=2)
+    r0 = run(kw, files, precision=prec, kernel_config=1)
+    r1 = run(kw, files, precision=prec, kernel_config=cfg)
+    assert same(r0, r1)
+    ore, oim, on = oracle.absorption(oracle.params(kw, files), "f32a64" if prec == nise.FP32 else "f64")
     assert helpers.rel(r1[0] + 1j * r1[1], ore + 1j * oim) < 1e-11
 
 
