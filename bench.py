@@ -73,6 +73,8 @@ def parse():
                         "mixed-size batch (secondary workloads)")
     a.add_argument("--t2", type=int, default=0, help="c2 only: waiting-time steps (RunTimes 64 t2 64)")
     a.add_argument("--end", type=int, default=0, help="c2 only: EndPoint (0 = all start points)")
+    a.add_argument("--c4-job", type=int, default=-1,
+                   help="c4 only: time job I (0..63) of the batch alone, default kernel configuration")
     return a.parse_args()
 
 
@@ -517,6 +519,8 @@ def run_c4(args):
     torch.cuda.set_device(local)
     frames, tmax, sample = 5000, 128, 25
     sizes = c4_sites()
+    if args.c4_job >= 0:
+        return run_c4_job(args, args.c4_job, sizes[args.c4_job], frames, tmax, sample, local)
     nsamp = (frames - tmax - 1) // sample + 1
     site_steps = sum(3 * nsamp * tmax * n for n in sizes)
     ctxs = []
@@ -566,6 +570,34 @@ def run_c4(args):
                           "mode": "the same jobs one context at a time (nise_absorption)",
                           "slowest_job_ms": max(per_job), "slowest_job_sites": sizes[per_job.index(max(per_job))]},
            "batched_over_sequential": seq_ms / ms, "clocks": clocks, "gpu_launches": launches}
+    print(json.dumps(out), flush=True)
+    return out
+
+
+def run_c4_job(args, i, n, frames, tmax, sample, local):
+    """One job of the C4 batch alone (profiling case): the same trajectory and keywords,
+    the default kernel configuration, device time per absorption call."""
+    import nise_2017_b200 as nise
+    from nise_2017_b200 import synth
+    prop = "Coupling" if i % 2 == 0 else "Diagonal"
+    times = []
+    with tempfile.TemporaryDirectory() as td:
+        s = synth.c1_spec(n_sites=n, frames=frames, seed=40000 + i)
+        files = synth.write(s, td)
+        kw = synth.c1_keywords(Singles=n, Length=frames, RunTimes="%d 0 0" % tmax, Samplerate=sample,
+                               Propagation=prop, FFT=1024)
+        with nise.Context(nise.params_from_keywords(kw, files, device=local)) as c:
+            c.load_files()
+            for k in range(max(args.warmup, 1) + args.steps):
+                c.absorption()
+                tot, main, launches = c.timing()
+                if k >= max(args.warmup, 1):
+                    times.append((tot, main))
+    nsamp = (frames - tmax - 1) // sample + 1
+    out = {"metric": "C4 job %d alone: site-steps/s" % i, "value": 3 * nsamp * tmax * n / (statistics.mean(
+        t[0] for t in times) / 1e3), "unit": "site-steps/s", "sites": n, "propagation": prop,
+        "ms_per_job": statistics.mean(t[0] for t in times), "main_kernel_ms": statistics.mean(t[1] for t in times),
+        "steps": args.steps, "gpu_launches": launches}
     print(json.dumps(out), flush=True)
     return out
 

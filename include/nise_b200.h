@@ -119,7 +119,9 @@ typedef struct {
     int device;                    /* CUDA device ordinal */
     int kernel_config;             /* absorption kernel: 0 automatic (autotuned or default);
                                       Trotter: 1 thread per vector, 64/128/256 level-scheduled
-                                      rotations with that many threads per start point;
+                                      rotations with that many threads per start point, 32/33 a
+                                      warp per vector with the rotation table in shared/global
+                                      memory (all bitwise identical);
                                       Sparse/Diagonal (static couplings): 3 or 9 k_abs_taylor2 with
                                       4 or 8 vectors per CTA, 8 the sliced-ELL Taylor kernel, 10 the
                                       sliced-ELL Chebyshev kernel (FP32), 12 the sliced-ELL

@@ -116,7 +116,7 @@ __global__ void k_abs_trotter_lv(DevTraj T, TrotterPlan P, AbsJob J, double2 *re
         __syncthreads();
         if (tid < 3) {  // the residue order of dot_mu
             double re = 0, im = 0;
-            for (int r = 0; r < 32; r++) {
+            for (int r = 0; r < 32 && r < n; r++) {
                 double pr = 0, pi = 0;
                 for (int a = r; a < n; a += 32) {
                     R m = (R)mu[tid * n + a];
@@ -173,9 +173,11 @@ __global__ void k_abs_trotter_lv(DevTraj T, TrotterPlan P, AbsJob J, double2 *re
 // __syncwarp separates chunks.  A two-deep register pipeline loads the bounds
 // of chunk c+2 and the pairs and coefficients of chunk c+1 while chunk c is
 // applied, so only the state loads sit on the critical path.  A lane with no
-// rotation in a chunk rotates its own spare site n + lane by the identity
-// (cos 1, sin 0; the spare sites stay zero), so the warp never diverges; in
-// shared memory these identity rotations are table entries K .. K+31.
+// rotation in a chunk rotates a spare site of its own (n .. n+31) by the
+// identity (cos 1, sin 0; the spare sites stay zero), so the warp never
+// diverges; in
+// shared memory these identity rotations are table entries K .. K+31, and an
+// idle lane reads the one congruent mod 32 to the entry it stands in for.
 // Every vector
 // sees the reference's float operations (propagate.c:868-895); the response
 // is summed in the order of dot_mu (lane r sums the sites r, r+32, ...), so
@@ -231,7 +233,7 @@ __global__ void k_abs_trotter_wv(DevTraj T, TrotterPlan P, AbsJob J, double2 *re
         C[a] = z;
     }
     const R2 *U = (const R2 *)P.U, *rot = (const R2 *)P.rot;
-    const int2 spare = make_int2(n + lane, n + lane);
+    const int2 spare = make_int2(n + lane, n + lane);  // global-table kernel
     R2 unit;
     unit.x = 1;
     unit.y = 0;
@@ -254,7 +256,7 @@ __global__ void k_abs_trotter_wv(DevTraj T, TrotterPlan P, AbsJob J, double2 *re
             re += (double)A::mul(m, z.x);
             im += (double)A::mul(m, z.y);
         }
-        const double2 rs = resp_sum_warp(re, im);
+        const double2 rs = resp_sum_warp(re, im, n);
         if (lane == 0) resp[(size_t)v * J.tmax + t1] = rs;
         if (!step) break;
         const R2 *Rf;
@@ -284,8 +286,8 @@ __global__ void k_abs_trotter_wv(DevTraj T, TrotterPlan P, AbsJob J, double2 *re
             int2 ab0;
             R2 cs0;
             auto fetch = [&](int k, int end, int2 &ab, R2 &cs) {
-                if (SM) {
-                    k = k < end ? k : K + lane;
+                if (SM) {  // identity entry congruent to k mod 32: no bank conflict with the chunk
+                    k = k < end ? k : K + ((k - K) & 31);
                     ab = pair(k);
                     cs = Rf[k];
                 } else {
@@ -1314,8 +1316,6 @@ int launch_abs_trotter_lv(int prec, const DevTraj &T, const TrotterPlan &P, cons
     return (int)cudaGetLastError();
 }
 
-int sm_count();
-
 // Shared memory of k_abs_trotter_wv: chunk table, rotation table (sm), W
 // vectors (and their phases with ustage).
 static size_t trotter_wv_smem(int prec, const TrotterPlan &P, int nchk, bool sm, bool ustage, int W) {
@@ -1325,8 +1325,8 @@ static size_t trotter_wv_smem(int prec, const TrotterPlan &P, int nchk, bool sm,
     return b + (size_t)W * (P.n + 32) * r2 * (ustage ? 2 : 1);
 }
 
-// tables: 1 = the rotation table in shared memory where it fits (else in
-// global memory), 0 = in global memory.  With static coefficients W vectors
+// tables = 1: the rotation table in shared memory where it fits (else in
+// global memory), 0: in global memory.  With static coefficients W vectors
 // share a CTA, W = the vectors per SM (at most 16, as shared memory allows),
 // so that small jobs spread over every SM; the phases are staged where
 // shared memory has room for them at that W.

@@ -89,6 +89,8 @@ int launch_abs_trotter(int prec, const DevTraj &T, const TrotterPlan &P, const A
 // rotations of level l.  Bitwise identical to launch_abs_trotter.
 int launch_abs_trotter_lv(int prec, const DevTraj &T, const TrotterPlan &P, const AbsJob &J, double2 *resp,
                           const int *lvptr, int nlev, int threads, cudaStream_t s);
+// Streaming multiprocessors of the current device.
+int sm_count();
 // The same with a warp per vector (the lanes share a level's rotations),
 // bitwise identical to both.  chk[c]..chk[c+1] are the rotations of
 // chunk c (a level, or at most 32 of its rotations).  tables = 1: the

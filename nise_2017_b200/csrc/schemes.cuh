@@ -199,11 +199,13 @@ __device__ __forceinline__ void rk4_apply(typename Vec2<R>::T *S, int B, int lan
 // in residue order.  It differs from the site order of the reference only by
 // FP64 rounding, and every kernel that uses it (a thread per vector here, a
 // warp per vector in resp_sum_warp) gives bitwise the same responses.
+// Residues r >= n have no sites: their partial is +0, which leaves a sum
+// that starts at +0 unchanged, so they are skipped.
 template <typename R>
 __device__ __forceinline__ double2 dot_mu(const DevTraj &T, long t, int x, const typename Vec2<R>::T *S, int B,
                                           int lane, int n) {
     double re = 0, im = 0;
-    for (int r = 0; r < 32; r++) {
+    for (int r = 0; r < 32 && r < n; r++) {
         double pr = 0, pi = 0;
         for (int i = r; i < n; i += 32) {
             R m = (R)traj_mu(T, t, x, i);
@@ -219,9 +221,9 @@ __device__ __forceinline__ double2 dot_mu(const DevTraj &T, long t, int x, const
 
 // The residue-order sum of dot_mu across a warp: lane r holds the partial
 // sum of sites r, r+32, ... (ascending); every lane gets the total.
-__device__ __forceinline__ double2 resp_sum_warp(double pr, double pi) {
+__device__ __forceinline__ double2 resp_sum_warp(double pr, double pi, int n) {
     double re = 0, im = 0;
-    for (int r = 0; r < 32; r++) {
+    for (int r = 0; r < 32 && r < n; r++) {
         re += __shfl_sync(0xffffffffu, pr, r);
         im += __shfl_sync(0xffffffffu, pi, r);
     }

@@ -163,3 +163,4 @@ def test_batch_with_autotune(tmp_path):
             b.run()
             re, im, n = b.result(0)
     assert np.array_equal(re, ref[0]) and np.array_equal(im, ref[1])
+
