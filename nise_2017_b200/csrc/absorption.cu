@@ -249,6 +249,7 @@ __global__ void k_abs_trotter_wv(DevTraj T, TrotterPlan P, AbsJob J, double2 *re
         const bool step = t1 + 1 < J.tmax;  // the frame's phases exist only for propagated frames
         const R2 *Uf = U + (t - P.f0) * n;
         double re = 0, im = 0;
+#pragma unroll 4
         for (int a = lane; a < n; a += 32) {
             R m = (R)traj_mu(T, t, x, a);
             if (ustage && step) Us[a] = Uf[a];
@@ -271,14 +272,21 @@ __global__ void k_abs_trotter_wv(DevTraj T, TrotterPlan P, AbsJob J, double2 *re
         } else {
             Rf = P.rot_static ? rot : rot + (t - P.f0) * K;
         }
-        const R2 *Uu = ustage ? Us : Uf;  // a lane reads back only the phases it copied
-        for (int sub = 0; sub < J.ts; sub++) {
-            for (int a = lane; a < n; a += 32) {  // propagate.c:870-873
-                R2 z = C[a], u = Uu[a], o;
+        // half-step phases (propagate.c:870-873 / 891-894), from the staged copy (a lane
+        // reads back only the phases it copied) or from global memory: two instances,
+        // so that each reads one address space
+        auto phase = [&](const R2 *uu) {
+#pragma unroll 4
+            for (int a = lane; a < n; a += 32) {
+                R2 z = C[a], u = uu[a], o;
                 o.x = A::sub(A::mul(z.x, u.x), A::mul(z.y, u.y));
                 o.y = A::add(A::mul(z.y, u.x), A::mul(z.x, u.y));
                 C[a] = o;
             }
+        };
+        for (int sub = 0; sub < J.ts; sub++) {
+            if (ustage) phase(Us);
+            else phase(Uf);
             __syncwarp();
             // chunk c = pairs[chk[c] .. e0): this lane's rotation (ab0, cs0);
             // e1 = end of chunk c+1
@@ -317,12 +325,8 @@ __global__ void k_abs_trotter_wv(DevTraj T, TrotterPlan P, AbsJob J, double2 *re
                 ab0 = ab1;
                 cs0 = cs1;
             }
-            for (int a = lane; a < n; a += 32) {  // propagate.c:891-894
-                R2 z = C[a], u = Uu[a], o;
-                o.x = A::sub(A::mul(z.x, u.x), A::mul(z.y, u.y));
-                o.y = A::add(A::mul(z.y, u.x), A::mul(z.x, u.y));
-                C[a] = o;
-            }
+            if (ustage) phase(Us);
+            else phase(Uf);
             __syncwarp();
         }
     }
