@@ -175,14 +175,13 @@ __global__ void k_abs_trotter_lv(DevTraj T, TrotterPlan P, AbsJob J, double2 *re
 // applied, so only the state loads sit on the critical path.  A lane with no
 // rotation in a chunk rotates a spare site of its own (n .. n+31) by the
 // identity (cos 1, sin 0; the spare sites stay zero), so the warp never
-// diverges; in
-// shared memory these identity rotations are table entries K .. K+31, and an
-// idle lane reads the one congruent mod 32 to the entry it stands in for.
-// Every vector
-// sees the reference's float operations (propagate.c:868-895); the response
-// is summed in the order of dot_mu (lane r sums the sites r, r+32, ...), so
-// all Trotter kernels give bitwise identical results.  W warps = W vectors
-// per CTA; vector v is polarisation v % 3 of start point v / 3.
+// diverges; in shared memory these identity rotations are table entries
+// K .. K+31, and an idle lane reads the one congruent mod 32 to the entry it
+// stands in for.  Every vector sees the reference's float operations
+// (propagate.c:868-895); the response is summed in the order of dot_mu (lane
+// r sums the sites r, r+32, ...), so all Trotter kernels give bitwise
+// identical results.  W warps = W vectors per CTA; vector v is polarisation
+// v % 3 of start point v / 3.
 //
 // SM: the rotation table lives in shared memory (pairs packed a | b << 16,
 // coefficients as R2).  Static coefficients are loaded once; per-frame
