@@ -48,7 +48,7 @@ std::mutex g_tune_mu;
 // ~20 rotations per level) or the job has too few vectors to fill warps of
 // threads (a warp per vector then has the shorter critical path); thread per
 // vector for chains (one rotation per level) with many vectors.
-int default_config(int scheme, int N, bool plain, bool cheb, int K, int nchk, int nvec) {
+int default_config(int scheme, int N, bool plain, bool cheb, int K, int nchk, int nvec, bool has4) {
     if (scheme == SCHEME_TROTTER) {
         if (K > 0 && (K >= 4 * nchk || nvec < 1024)) return 32;
         return N >= 96 ? 128 : 0;
@@ -58,9 +58,11 @@ int default_config(int scheme, int N, bool plain, bool cheb, int K, int nchk, in
     if (plain) return 8;
     (void)cheb;           // the Chebyshev kernel is a tuned alternative: fewer terms, more work per term
     // less than one wave of 8-vector CTAs: 4 vectors per CTA reach twice the
-    // SMs (C4 jobs, 585 vectors: 1440 sites 12.1 against 25.0 ms; never slower
-    // from 18 to 2048 sites)
-    if (nvec < 8 * sm_count()) return 3;
+    // SMs.  C4 jobs (585 vectors): the FP32 sliced-ELL kernel with 4 vectors
+    // up to 1024 sites (295 sites 1.96 against 2.31 ms for k_abs_taylor2 and
+    // 2.32 for the default), k_abs_taylor2 with 4 above (1440 sites 12.1
+    // against 15.8 and 25.0 ms)
+    if (nvec < 8 * sm_count()) return has4 && N <= 1024 ? 12 : 3;
     return 8;
 }
 
@@ -468,7 +470,7 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
                 return rc;
         }
     }
-    config = default_config(scheme, N, plain, cheb, TP.k, nchk, plain ? 3 : nvec);
+    config = default_config(scheme, N, plain, cheb, TP.k, nchk, plain ? 3 : nvec, dell4.p != nullptr);
     if (p.kernel_config != 0) {  // forced by the caller
         const int k = p.kernel_config;
         if (scheme == SCHEME_EIGEN && k == 2) return NISE_OK;
