@@ -1,0 +1,100 @@
+"""Level order of the Trotter rotations, on the CPU.
+
+The engine stores the coupling pairs in level order: rotation k gets level
+1 + the highest level of the earlier rotations sharing one of its sites
+(rotation_levels in csrc/absrun.cpp), and the GPU kernels apply the
+rotations level by level, a level (split into chunks of at most 32) in
+parallel.  That is only exact if every site sees the same float operations
+as in the lexicographic order of propagate.c:876-888.  These tests apply
+the reference's float32 rotation both ways on lattice and chain patterns and
+require bitwise equality.
+"""
+import numpy as np
+
+from nise_2017_b200 import synth
+
+
+def lattice_pairs(n, seed):
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        files = synth.write(synth.c1_spec(n_sites=n, frames=2, seed=seed), td)
+        rec = np.fromfile(files["coupling"], dtype=np.float32)[1:]
+    pairs = []
+    for a in range(n):
+        for b in range(a + 1, n):
+            if abs(rec[b + a * (2 * n - a - 1) // 2]) >= 2.0:
+                pairs.append((a, b))
+    return pairs
+
+
+def levels(pairs, n):
+    last = [0] * n
+    lv = []
+    for a, b in pairs:
+        l = max(last[a], last[b]) + 1
+        last[a] = last[b] = l
+        lv.append(l - 1)
+    return lv
+
+
+def rotate(cr, ci, pairs, cs, order):
+    """propagate.c:876-888 in float32, rotations taken in `order`."""
+    cr, ci = cr.copy(), ci.copy()
+    for k in order:
+        a, b = pairs[k]
+        co, si = cs[k]
+        ra, ia, rb, ib = cr[a], ci[a], cr[b], ci[b]
+        cr[a] = co * ra - si * ib
+        ci[a] = co * ia + si * rb
+        cr[b] = co * rb - si * ia
+        ci[b] = co * ib + si * ra
+    return cr, ci
+
+
+def check(pairs, n, seed):
+    rng = np.random.default_rng(seed)
+    cr = rng.normal(size=n).astype(np.float32)
+    ci = rng.normal(size=n).astype(np.float32)
+    ang = rng.uniform(-0.3, 0.3, size=len(pairs)).astype(np.float32)
+    cs = [(np.float32(np.cos(x)), np.float32(-np.sin(x))) for x in ang]
+    lv = levels(pairs, n)
+    by_level = sorted(range(len(pairs)), key=lambda k: (lv[k], k))
+    # every level touches disjoint sites
+    for l in set(lv):
+        sites = [s for k in range(len(pairs)) if lv[k] == l for s in pairs[k]]
+        assert len(sites) == len(set(sites))
+    r0 = rotate(cr, ci, pairs, cs, range(len(pairs)))
+    r1 = rotate(cr, ci, pairs, cs, by_level)
+    assert np.array_equal(r0[0], r1[0]) and np.array_equal(r0[1], r1[1])
+    # within a level any order (any lane assignment) gives the same bits
+    shuffled = sorted(range(len(pairs)), key=lambda k: (lv[k], rng.random()))
+    r2 = rotate(cr, ci, pairs, cs, shuffled)
+    assert np.array_equal(r0[0], r2[0]) and np.array_equal(r0[1], r2[1])
+    return lv
+
+
+def test_lattice_level_order_is_bitwise_lexicographic():
+    n = 120
+    pairs = lattice_pairs(n, seed=7)
+    lv = check(pairs, n, seed=1)
+    widths = np.bincount(lv)
+    assert len(pairs) > 4 * len(widths)  # wide levels: the warp-per-vector case
+    assert widths.max() <= 32
+
+
+def test_chain_level_order_is_bitwise_lexicographic():
+    n = 40
+    pairs = [(a, a + 1) for a in range(n - 1)]
+    lv = check(pairs, n, seed=2)
+    assert len(set(lv)) == n - 1  # a chain: one rotation per level
+
+
+def test_dimer_levels_wider_than_a_warp():
+    """Levels of 40, 80 and 40 rotations, split into chunks of at most 32."""
+    n = 160
+    pairs = sorted([(2 * i, 2 * i + 1) for i in range(n // 2)] + [(i, i + n // 2) for i in range(n // 2)])
+    lv = check(pairs, n, seed=3)
+    widths = np.bincount(lv)
+    assert list(widths) == [40, 80, 40]
+    chunks = [min(32, w - q) for w in widths for q in range(0, w, 32)]
+    assert chunks == [32, 8, 32, 32, 16, 32, 8]
