@@ -309,6 +309,17 @@ int nise_backward_absorption(nise_ctx *ctx, const double *site_shift, double cou
                              const double *dL_dspec_re, const double *dL_dspec_im, int rows, double *g_shift,
                              double *g_scale, double *g_lifetime);
 
+/* Host-only: the order in which the engine applies the Trotter rotations of
+ * a coupling list (propagate.c:876-888 applies them in the list's
+ * lexicographic order, one after another).  ab holds k pairs (a, b), a < b,
+ * in that order.  Rotation q gets level 1 + the highest level of the earlier
+ * rotations sharing one of its sites; perm (k values) lists the rotations by
+ * (level, list index), lvptr (nlev + 1 values, at most k + 1) bounds the
+ * levels in perm, and chkptr (nchk + 1 values, at most k + 1) splits every
+ * level into chunks of at most 32 rotations, one warp step each.  Touches no
+ * GPU. */
+int nise_rotation_schedule(const int *ab, int k, int n, int *perm, int *lvptr, int *nlev, int *chkptr, int *nchk);
+
 /* No counterpart in the reference.  Linear absorption with the Trotter
  * "Coupling" scheme (HamiltonianType Full) for callers whose device memory is
  * owned by their own allocator and who therefore cannot let the library call
@@ -317,8 +328,10 @@ int nise_backward_absorption(nise_ctx *ctx, const double *site_shift, double cou
  * DEVICE buffers, every intermediate table lives in one static device array
  * of 32 MiB that each GPU loading the library keeps until exit, and larger
  * jobs return NISE_ERR_SHAPE.  Work is enqueued on `stream` (a cudaStream_t,
- * NULL = default stream) on the current device and the call returns when it
- * is done.  All calls share the array: calls whose device work overlaps race.
+ * NULL = default stream) on the current device; the call reads a count back
+ * to the host and synchronises `stream` before it returns.  All calls share
+ * the array: calls whose device work overlaps (other streams, other host
+ * threads) race, so the caller serialises them.
  * The first call on a device looks up the array's device address; make it
  * before any stream capture.  Results equal nise_absorption's. */
 int nise_absorption_noalloc(const nise_params *p, const void *d_energy, size_t energy_bytes, const void *d_dipole,

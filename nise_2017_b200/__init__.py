@@ -41,6 +41,7 @@ EXPORTED = [
     "nise_backward_absorption", "nise_absorption_tune", "nise_batch_create", "nise_batch_run", "nise_batch_result",
     "nise_batch_spectrum", "nise_batch_timing", "nise_batch_error", "nise_batch_destroy", "nise_set_trajectory_onfly",
     "nise_set_operators", "nise_linear", "nise_linear_file", "nise_write_td", "nise_translate",
+    "nise_rotation_schedule",
 ]
 
 
@@ -126,12 +127,30 @@ def lib():
         L.nise_linear_file.restype = ctypes.c_char_p
         L.nise_write_td.argtypes = [ctypes.c_char_p, P, dp, dp, ctypes.c_int, ctypes.c_int]
         L.nise_translate.argtypes = [ctypes.c_char_p]
+        L.nise_rotation_schedule.argtypes = [ip, ctypes.c_int, ctypes.c_int, ip, ip, ip, ip, ip]
         _lib = L
     return _lib
 
 
 def _dp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def rotation_schedule(pairs, n):
+    """The engine's Trotter rotation order for a lexicographic coupling list
+    (host only): (perm, level bounds, chunk bounds) as numpy int arrays."""
+    ab = np.ascontiguousarray(np.asarray(pairs, dtype=np.int32).reshape(-1, 2))
+    k = len(ab)
+    perm = np.zeros(max(k, 1), np.int32)
+    lv = np.zeros(k + 1, np.int32)
+    chk = np.zeros(k + 1, np.int32)
+    nlev, nchk = ctypes.c_int(), ctypes.c_int()
+    ip = ctypes.POINTER(ctypes.c_int)
+    rc = lib().nise_rotation_schedule(ab.ctypes.data_as(ip), k, n, perm.ctypes.data_as(ip), lv.ctypes.data_as(ip),
+                                      ctypes.byref(nlev), chk.ctypes.data_as(ip), ctypes.byref(nchk))
+    if rc != 0:
+        raise NiseError(rc, lib().nise_global_error().decode())
+    return perm[:k], lv[:nlev.value + 1], chk[:nchk.value + 1]
 
 
 def translate(keyword_file):

@@ -89,7 +89,40 @@ void rotation_levels(const std::vector<int2> &pairs, int n, std::vector<int> &pe
     for (size_t k = 0; k < pairs.size(); k++) perm[fill[lv[k]]++] = (int)k;
 }
 
+// The levels split into chunks of at most 32 rotations (one warp step of
+// the warp-per-vector kernel each): chk holds the chunk boundaries.
+void rotation_chunks(const std::vector<int> &lvptr, std::vector<int> &chk) {
+    chk.assign(1, 0);
+    for (size_t l = 0; l + 1 < lvptr.size(); l++)
+        for (int q = lvptr[l]; q < lvptr[l + 1]; q += 32) chk.push_back(std::min(q + 32, lvptr[l + 1]));
+}
+
 }  // namespace
+
+extern "C" int nise_rotation_schedule(const int *ab, int k, int n, int *perm, int *lvptr, int *nlev, int *chkptr,
+                                      int *nchk) {
+    if (k < 0 || n < 1 || (k && (!ab || !perm)) || !lvptr || !nlev || !chkptr || !nchk) {
+        nise_set_global_error("bad rotation schedule arguments");
+        return NISE_ERR_ARG;
+    }
+    std::vector<int2> pairs(k);
+    for (int q = 0; q < k; q++) {
+        pairs[q] = make_int2(ab[2 * q], ab[2 * q + 1]);
+        if (pairs[q].x < 0 || pairs[q].x >= n || pairs[q].y < 0 || pairs[q].y >= n || pairs[q].x == pairs[q].y) {
+            nise_set_global_error("rotation pair out of range");
+            return NISE_ERR_ARG;
+        }
+    }
+    std::vector<int> hperm, hlv, hchk;
+    rotation_levels(pairs, n, hperm, hlv);
+    rotation_chunks(hlv, hchk);
+    std::copy(hperm.begin(), hperm.end(), perm);
+    std::copy(hlv.begin(), hlv.end(), lvptr);
+    std::copy(hchk.begin(), hchk.end(), chkptr);
+    *nlev = (int)hlv.size() - 1;
+    *nchk = (int)hchk.size() - 1;
+    return NISE_OK;
+}
 
 struct AbsRun {
     nise_ctx *c = nullptr;
@@ -207,9 +240,8 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
             (rc = rot.alloc(c, r2 * (size_t)(TP.rot_static ? 1 : nf) * (TP.k ? TP.k : 1))) ||
             (rc = lvptr.upload(c, hlv)))
             return rc;
-        std::vector<int> hchk(1, 0);
-        for (int l = 0; l < nlev; l++)
-            for (int q = hlv[l]; q < hlv[l + 1]; q += 32) hchk.push_back(std::min(q + 32, hlv[l + 1]));
+        std::vector<int> hchk;
+        rotation_chunks(hlv, hchk);
         nchk = (int)hchk.size() - 1;
         if ((rc = lvchk.upload(c, hchk))) return rc;
         TP.pairs = dpairs.p;

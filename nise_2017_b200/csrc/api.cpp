@@ -123,13 +123,13 @@ extern "C" int nise_create(const nise_params *p, nise_ctx **out) {
 }
 
 void nise_free_traj(nise_ctx *c) {
-    void *ptrs[] = {c->d_energy, c->d_dipole, c->d_hc, c->d_mu_static, c->d_anh, c->d_over, c->d_shift_site,
+    void *ptrs[] = {c->d_energy, c->d_dipole, c->d_hc, c->d_mu_static, c->d_anh, c->d_over, c->d_shift_ptr,
                     c->d_shift_ab, c->d_alpha, c->d_pos};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     c->d_energy = c->d_dipole = c->d_hc = c->d_mu_static = c->d_anh = c->d_over = c->d_shift_ab = nullptr;
     c->d_alpha = c->d_pos = nullptr;
-    c->d_shift_site = nullptr;
+    c->d_shift_ptr = nullptr;
     c->cap_energy = c->cap_dipole = c->cap_anh = c->cap_over = c->cap_hc = c->cap_mu = c->cap_ab = 0;
     c->cap_alpha = c->cap_pos = 0;
     c->al_frames = c->pos_frames = 0;
@@ -318,20 +318,29 @@ extern "C" int nise_set_operators(nise_ctx *c, const void *alpha, size_t alpha_b
 extern "C" int nise_set_singleshift(nise_ctx *c, int n, const int *sites, const float *a, const float *b) {
     if (!c || n < 0) return nise_fail(c, NISE_ERR_ARG, "bad SingleShift arguments");
     cudaSetDevice(c->p.device);
-    std::vector<float> ab(2 * (size_t)n);
+    // entries grouped by site, each site's in file order (apply_singleshift,
+    // hamshift.c:59-66, applies them one after another)
+    std::vector<int> ptr(c->n + 1, 0);
     for (int i = 0; i < n; i++) {
         if (sites[i] < 0 || sites[i] >= c->n) return nise_fail(c, NISE_ERR_ARG, "SingleShift site out of range");
-        ab[2 * i] = a[i];
-        ab[2 * i + 1] = b[i];
+        ptr[sites[i] + 1]++;
     }
-    if (c->d_shift_site) cudaFree(c->d_shift_site);
-    c->d_shift_site = nullptr;
+    for (int s = 0; s < c->n; s++) ptr[s + 1] += ptr[s];
+    std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+    std::vector<float> ab(2 * (size_t)n);
+    for (int i = 0; i < n; i++) {
+        int e = fill[sites[i]]++;
+        ab[2 * e] = a[i];
+        ab[2 * e + 1] = b[i];
+    }
+    if (c->d_shift_ptr) cudaFree(c->d_shift_ptr);
+    c->d_shift_ptr = nullptr;
     c->nshift = n;
     int rc;
     if (n) {
-        if (cudaMalloc((void **)&c->d_shift_site, sizeof(int) * n))
+        if (cudaMalloc((void **)&c->d_shift_ptr, sizeof(int) * (c->n + 1)))
             return nise_fail(c, NISE_ERR_NOMEM, "device allocation failed");
-        cudaMemcpyAsync(c->d_shift_site, sites, sizeof(int) * n, cudaMemcpyHostToDevice, c->stream);
+        cudaMemcpyAsync(c->d_shift_ptr, ptr.data(), sizeof(int) * (c->n + 1), cudaMemcpyHostToDevice, c->stream);
     }
     if ((rc = upload(c, &c->d_shift_ab, &c->cap_ab, n ? ab.data() : nullptr, sizeof(float) * 2 * n))) return rc;
     return nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "SingleShift upload");
@@ -426,7 +435,7 @@ DevTraj nise_devtraj(const nise_ctx *c) {
     T.a_frames = c->a_frames;
     T.over = c->d_over;
     T.o_frames = c->o_frames;
-    T.shift_site = c->d_shift_site;
+    T.shift_ptr = c->d_shift_ptr;
     T.shift_ab = c->d_shift_ab;
     T.nshift = c->nshift;
     T.n = c->n;

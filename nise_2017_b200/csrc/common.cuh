@@ -42,12 +42,15 @@ __device__ __forceinline__ float traj_diag_raw(const DevTraj &T, long t, int i) 
 }
 
 // Shifted diagonal with SingleShift applied (read_Hamiltonian,
-// read_trajectory.c:73-87 -> apply_singleshift, hamshift.c:59-66).
+// read_trajectory.c:73-87 -> apply_singleshift, hamshift.c:59-66).  The
+// reference applies the file's entries in order; a site's own entries are
+// looked up through shift_ptr and applied in the same order, so a site named
+// twice gets the same two roundings.
 __device__ __forceinline__ float traj_diag(const DevTraj &T, long t, int i, bool singleshift) {
     float h = traj_diag_raw(T, t, i);
     if (singleshift)
-        for (int s = 0; s < T.nshift; s++)
-            if (T.shift_site[s] == i) h = __fadd_rn(__fmul_rn(h, T.shift_ab[2 * s]), T.shift_ab[2 * s + 1]);
+        for (int e = T.shift_ptr[i]; e < T.shift_ptr[i + 1]; e++)
+            h = __fadd_rn(__fmul_rn(h, T.shift_ab[2 * e]), T.shift_ab[2 * e + 1]);
     return h;
 }
 

@@ -19,8 +19,8 @@ struct DevTraj {
     long a_frames;
     const float *over;       // overtone dipole records (3N per frame) or nullptr
     long o_frames;
-    const int *shift_site;   // SingleShift sites
-    const float *shift_ab;   // (a, b) pairs
+    const int *shift_ptr;    // SingleShift entries of site i: shift_ab[2e], e in [shift_ptr[i], shift_ptr[i+1])
+    const float *shift_ab;   // (a, b) pairs, grouped by site in file order
     int nshift;
     int n;                   // singles
     float shifte;            // (min1 + max1) / 2

@@ -278,7 +278,7 @@ extern "C" int nise_linear(nise_ctx *c, double *re_S, double *im_S, int max_chan
     cudaEventRecord(c->ev0, c->stream);
     DevTraj T = nise_devtraj(c);
     if (!L.singleshift) {  // read_He / read_Dia: no SingleShift
-        T.shift_site = nullptr;
+        T.shift_ptr = nullptr;
         T.nshift = 0;
     }
     LinJob J{};

@@ -25,7 +25,7 @@ struct nise_ctx {
     // trajectory in device memory (record images, 4-byte words)
     float *d_energy = nullptr, *d_dipole = nullptr, *d_hc = nullptr, *d_mu_static = nullptr;
     float *d_anh = nullptr, *d_over = nullptr, *d_shift_ab = nullptr;
-    int *d_shift_site = nullptr;
+    int *d_shift_ptr = nullptr;  // [N+1] SingleShift entries per site
     int nshift = 0;
     long e_words = 0, e_frames = 0, d_words = 0, d_frames = 0, a_frames = 0, o_frames = 0;
     size_t cap_energy = 0, cap_dipole = 0, cap_anh = 0, cap_over = 0, cap_hc = 0, cap_mu = 0, cap_ab = 0;

@@ -173,6 +173,7 @@ extern "C" int nise_absorption_noalloc(const nise_params *p, const void *d_energ
         double fsub = (double)p->deltat * (double)2.99792458e-5f * (double)(float)(2 * 3.14159265359) / p->ts;
         if (launch_prep_trotter(prec, T, P, fsub, f32_sub(p), st)) goto dev_fail;
         AbsJob J;
+        memset(&J, 0, sizeof(J));
         J.begin = p->begin;
         J.nsamp = nsamp;
         J.sample = p->sample;

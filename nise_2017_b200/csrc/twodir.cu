@@ -1095,7 +1095,7 @@ extern "C" int nise_2dir(nise_ctx *c, double *R, int *sample_count) {
     cudaMemcpyAsync(dlt.p, lt.data(), sizeof(float) * plane, cudaMemcpyHostToDevice, c->stream);
 
     DevTraj T = nise_devtraj(c);
-    T.shift_site = nullptr;  // calc_2DIR reads frames with read_He: no SingleShift
+    T.shift_ptr = nullptr;  // calc_2DIR reads frames with read_He: no SingleShift
     T.nshift = 0;
     size_t rsz = prec == NISE_FP32 ? sizeof(float) : sizeof(double), r2 = 2 * rsz;
     // singles coefficient tables over all frames of the job

@@ -119,12 +119,23 @@ def lib(prec="f64"):
     return _libs[prec]
 
 
+# Where the reference's sources are read from when the reference programs are
+# compiled (NISE_REFERENCE_SRC overrides the default location).
+REF_SRC = os.environ.get("NISE_REFERENCE_SRC", "/root/reference/src")
+
+
+def reference_present():
+    return os.path.isdir(REF_SRC)
+
+
 def build(ref=True):
     """Compile the restatement and, when the reference sources are present, the reference."""
+    import sysconfig
     targets = ["oracle"]
-    if ref and os.path.isdir("/root/reference/src"):
+    if ref and reference_present():
         targets.append("ref")
-    subprocess.run(["make", "-s"] + targets, cwd=HERE, check=True)
+    subprocess.run(["make", "-s", "REF=" + REF_SRC, "PYLIB=" + sysconfig.get_paths()["purelib"]] + targets,
+                   cwd=HERE, check=True)
 
 
 def _ptr(a, t=ctypes.c_double):

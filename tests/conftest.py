@@ -19,4 +19,4 @@ def native_build():
     from nise_2017_b200 import build
     import oracle
     build.build_all()
-    oracle.build(ref=os.path.isdir("/root/reference/src"))
+    oracle.build(ref=oracle.reference_present())

@@ -51,6 +51,20 @@ def rotate(cr, ci, pairs, cs, order):
     return cr, ci
 
 
+def engine_matches(pairs, n, lv):
+    """The engine's schedule (nise_rotation_schedule, the code the kernels'
+    tables come from) is the (level, index) order of levels() and splits each
+    level into chunks of at most 32."""
+    import nise_2017_b200 as nise
+    perm, lvptr, chk = nise.rotation_schedule(pairs, n)
+    expect = sorted(range(len(pairs)), key=lambda k: (lv[k], k))
+    assert list(perm) == expect
+    widths = np.bincount(lv, minlength=1) if len(lv) else np.zeros(0, int)
+    assert list(np.diff(lvptr)) == list(widths)
+    bounds = [0] + [min(q + 32, e) for s, e in zip(lvptr[:-1], lvptr[1:]) for q in range(s, e, 32)]
+    assert list(chk) == bounds
+
+
 def check(pairs, n, seed):
     rng = np.random.default_rng(seed)
     cr = rng.normal(size=n).astype(np.float32)
@@ -70,6 +84,7 @@ def check(pairs, n, seed):
     shuffled = sorted(range(len(pairs)), key=lambda k: (lv[k], rng.random()))
     r2 = rotate(cr, ci, pairs, cs, shuffled)
     assert np.array_equal(r0[0], r2[0]) and np.array_equal(r0[1], r2[1])
+    engine_matches(pairs, n, lv)
     return lv
 
 
@@ -98,3 +113,14 @@ def test_dimer_levels_wider_than_a_warp():
     assert list(widths) == [40, 80, 40]
     chunks = [min(32, w - q) for w in widths for q in range(0, w, 32)]
     assert chunks == [32, 8, 32, 32, 16, 32, 8]
+    _, _, chk = __import__("nise_2017_b200").rotation_schedule(pairs, n)
+    assert list(np.diff(chk)) == chunks
+
+
+def test_engine_schedule_rejects_bad_pairs():
+    import pytest
+    import nise_2017_b200 as nise
+    with pytest.raises(nise.NiseError):
+        nise.rotation_schedule([(0, 5)], 4)
+    perm, lv, chk = nise.rotation_schedule([], 4)
+    assert len(perm) == 0 and list(lv) == [0] and list(chk) == [0]
