@@ -34,6 +34,7 @@ CU_SOURCES = [
     "adjoint.cu",
     "onfly.cu",
     "linear.cu",
+    "taylor_rv.cu",
 ]
 CPP_SOURCES = [
     "api.cpp",

@@ -1091,16 +1091,31 @@ __global__ void __launch_bounds__(512) k_abs_cheb3(DevTraj T, TaylorPlan P, AbsJ
     }
 }
 
-__global__ void k_reduce_resp(const double2 *resp, int nvec, int tmax, double2 *out) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= tmax) return;
+// Sum of the per-vector responses resp[v][t] over v, in one fixed order: a
+// CTA owns 32 consecutive t (lane = t, coalesced rows); warp w sums the
+// vectors v = w, w + 32, ... in increasing v, then the 32 warp partials are
+// added in warp order.
+__global__ void __launch_bounds__(1024) k_reduce_resp(const double2 *resp, int nvec, int tmax, double2 *out) {
+    __shared__ double2 part[32][33];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, t = blockIdx.x * 32 + lane;
     double re = 0, im = 0;
-    for (int v = 0; v < nvec; v++) {
-        double2 z = resp[(size_t)v * tmax + t];
-        re += z.x;
-        im += z.y;
+    if (t < tmax)
+#pragma unroll 8
+        for (int v = w; v < nvec; v += 32) {
+            const double2 z = resp[(size_t)v * tmax + t];
+            re += z.x;
+            im += z.y;
+        }
+    part[w][lane] = make_double2(re, im);
+    __syncthreads();
+    if (w == 0 && t < tmax) {
+        double sr = 0, si = 0;
+        for (int q = 0; q < 32; q++) {
+            sr += part[q][lane].x;
+            si += part[q][lane].y;
+        }
+        out[t] = make_double2(sr, si);
     }
-    out[t] = make_double2(re, im);
 }
 
 // ------------------------------------------------------------ single steps
@@ -1496,8 +1511,18 @@ static int run_taylor3(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, d
     else if (ctas % nsm != 0 && ctas % nsm < nsm / 2 && ctas >= nsm) main = (ctas / nsm) * nsm * 8;
     if (kernels) *kernels = (main > 0) + (nvec > main);
     int e = -1;
+    if constexpr (sizeof(R) == 4)  // the row-owner kernel for the 8-vector waves
+        if (!P.no_rv && main > 0 && taylor_rv_fits(T, P)) e = launch_abs_taylor_rv(T, P, J, resp, 0, main, s);
+    if (P.rv_cheb) {  // the Chebyshev tables serve the row-owner kernel only; the tail runs the Taylor series
+        if (main > 0 && e) return e < 0 ? (int)cudaErrorNotSupported : e;
+        TaylorPlan Pt = P;
+        Pt.order = P.order_taylor;
+        Pt.cheb_coef = nullptr;
+        Pt.cheb_inv_r = nullptr;
+        return run_taylor3_g<R, IT1, 1>(T, Pt, J, resp, main, nvec - main, s);
+    }
     if constexpr (sizeof(R) == 4 && IT == 16)
-        if (P.ell_nslices <= 24 * 11 && taylor3_smem(P, 4, 8, 768) <= 220 * 1024)
+        if (e < 0 && P.ell_nslices <= 24 * 11 && taylor3_smem(P, 4, 8, 768) <= 220 * 1024)
             e = run_taylor3_g<R, 11, 8, 768>(T, P, J, resp, 0, main, s);
     if (e < 0) e = run_taylor3_g<R, IT, 8>(T, P, J, resp, 0, main, s);
     if (e) return e;
@@ -1520,6 +1545,20 @@ int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const Abs
         case 8: return run_taylor4<8>(T, P, J, resp, nvec, s);
         case 16: return run_taylor4<16>(T, P, J, resp, nvec, s);
         default: return run_taylor4<32>(T, P, J, resp, nvec, s);
+        }
+    }
+    if (P.cheb_coef && P.rv_cheb) {  // the row-owner kernel with the Chebyshev expansion (FP32)
+        if (prec != 0 || !P.order_taylor || !P.ell || !taylor_rv_fits(T, P)) return (int)cudaErrorNotSupported;
+        const int it = (P.ell_nslices + 15) / 16;
+        if (it > 32 || taylor3_smem(P, 4) > 220 * 1024) return (int)cudaErrorNotSupported;
+        const int nvec = 3 * J.nsamp;
+        switch (it <= 1 ? 1 : it <= 2 ? 2 : it <= 4 ? 4 : it <= 8 ? 8 : it <= 16 ? 16 : 32) {
+        case 1: return run_taylor3<float, 1>(T, P, J, resp, nvec, s, kernels);
+        case 2: return run_taylor3<float, 2>(T, P, J, resp, nvec, s, kernels);
+        case 4: return run_taylor3<float, 4>(T, P, J, resp, nvec, s, kernels);
+        case 8: return run_taylor3<float, 8>(T, P, J, resp, nvec, s, kernels);
+        case 16: return run_taylor3<float, 16>(T, P, J, resp, nvec, s, kernels);
+        default: return run_taylor3<float, 32>(T, P, J, resp, nvec, s, kernels);
         }
     }
     if (P.cheb_coef) {  // Chebyshev tables present: the FP32 sliced-ELL Chebyshev kernel
@@ -1631,7 +1670,7 @@ int launch_pattern_scan(const DevTraj &T, long f0, long nf, int *flag, cudaStrea
 }
 
 int launch_reduce_resp(const double2 *resp, int nvec, int tmax, double2 *out, cudaStream_t s) {
-    k_reduce_resp<<<(tmax + 127) / 128, 128, 0, s>>>(resp, nvec, tmax, out);
+    k_reduce_resp<<<(tmax + 31) / 32, 1024, 0, s>>>(resp, nvec, tmax, out);
     return (int)cudaGetLastError();
 }
 

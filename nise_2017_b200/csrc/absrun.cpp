@@ -48,7 +48,7 @@ std::mutex g_tune_mu;
 // ~20 rotations per level) or the job has too few vectors to fill warps of
 // threads (a warp per vector then has the shorter critical path); thread per
 // vector for chains (one rotation per level) with many vectors.
-int default_config(int scheme, int N, bool plain, bool cheb, int K, int nchk, int nvec, bool has4) {
+int default_config(int scheme, int N, bool plain, bool cheb, int K, int nchk, int nvec, bool has4, bool rv) {
     if (scheme == SCHEME_TROTTER) {
         if (K > 0 && (K >= 4 * nchk || nvec < 1024)) return 32;
         return N >= 96 ? 128 : 0;
@@ -63,6 +63,11 @@ int default_config(int scheme, int N, bool plain, bool cheb, int K, int nchk, in
     // 2.32 for the default), k_abs_taylor2 with 4 above (1440 sites 12.1
     // against 15.8 and 25.0 ms)
     if (nvec < 8 * sm_count()) return has4 && N <= 1024 ? 12 : 3;
+    // whole waves of 8-vector CTAs: the row-owner kernel with the Chebyshev
+    // expansion (FP32 lattices up to 1024 sites; on the 1024-site lattice,
+    // 100 000 frames: 52.0 ms against 55.8 with the Taylor series and 69.7 on
+    // the 8-vector sliced-ELL kernel)
+    if (rv && cheb) return 15;
     return 8;
 }
 
@@ -148,6 +153,10 @@ struct AbsRun {
     DevBuf<int> drp, dcol, dorder, dsptr, dcorder, drows, dsptr4, drows4;
     DevBuf<int2> dell4;
     int ell4_nslices = 0, ell4_nent = 0;
+    DevBuf<uint32_t> doffs8;  // row-owner layout (k_abs_taylor_rv)
+    DevBuf<float2> dvals8;
+    DevBuf<int> dpptr8, drows8, dwsl8[2], derr;
+    int ell8_nslices = 0, ell8_npg = 0, ell8_it[2] = {0, 0};
     DevBuf<char> dval, dell;
     DevBuf<float> dinvr;
     DevBuf<float2> dcoef;
@@ -167,6 +176,15 @@ struct AbsRun {
 
     int plan(nise_ctx *ctx, bool autotune);
     int enqueue(cudaStream_t s, bool events);
+    // after the job: a kernel whose bounded wait for a staged frame gave up
+    // leaves its flag set (NISE_ERR_TIMEOUT)
+    int check_err() {
+        if (!derr.p) return NISE_OK;
+        int h = 0;
+        if (cudaMemcpy(&h, derr.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return nise_fail(c, NISE_ERR_DEVICE, "error flag read failed");
+        return h ? nise_fail(c, NISE_ERR_TIMEOUT, "a bounded wait for a staged frame gave up") : NISE_OK;
+    }
     int run_main(cudaStream_t s, int cfg, double2 *dst);
     double flops() const;
     int tune();
@@ -469,6 +487,99 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
                 ell4_nslices = ns4;
                 ell4_nent = sp4[ns4];
             }
+            if (prec == NISE_FP32) {
+                // row-owner layout: 8-row slices whose rows alternate in parity (the
+                // same degree-sorted interleave as above), neighbours other parity
+                // first (ecol), entries (byte offset of the neighbour's 64-byte row,
+                // weight bits) [slot][row]; padding entries point at a row of the
+                // other parity with weight 0
+                const int ns8 = (N + 7) / 8;
+                std::vector<int> r8(8 * (size_t)ns8, N);
+                {
+                    std::vector<int> cls[2];
+                    for (int i = 0; i < N; i++) cls[i & 1].push_back(i);
+                    for (int k = 0; k < 2; k++)
+                        std::stable_sort(cls[k].begin(), cls[k].end(), [&](int a, int b) {
+                            return rp[a + 1] - rp[a] > rp[b + 1] - rp[b];
+                        });
+                    size_t take[2] = {0, 0};
+                    for (int pos = 0; pos < 8 * ns8; pos++) {
+                        int want = pos & 1;
+                        if (take[want] >= cls[want].size()) want ^= 1;
+                        if (take[want] < cls[want].size()) r8[pos] = cls[want][take[want]++];
+                    }
+                }
+                std::vector<int> sp8(ns8 + 1, 0);
+                for (int sl = 0; sl < ns8; sl++) {
+                    int Lm = 0;
+                    for (int r = 0; r < 8; r++) {
+                        int row = r8[8 * sl + r];
+                        if (row < N) Lm = std::max(Lm, rp[row + 1] - rp[row]);
+                    }
+                    sp8[sl + 1] = sp8[sl] + 8 * Lm;
+                }
+                // slot pairs: [group][row] words of two 16-bit neighbour row byte
+                // offsets and float2 weights (an odd slot count padded by one slot)
+                std::vector<int> pp8(ns8 + 1, 0);
+                for (int sl = 0; sl < ns8; sl++) pp8[sl + 1] = pp8[sl] + ((sp8[sl + 1] - sp8[sl]) / 8 + 1) / 2;
+                const int npg = pp8[ns8];
+                std::vector<uint32_t> o8(8 * (size_t)std::max(npg, 1), 0);
+                std::vector<float2> v8(8 * (size_t)std::max(npg, 1), make_float2(0.f, 0.f));
+                for (int sl = 0; sl < ns8; sl++) {
+                    const int Lm = (sp8[sl + 1] - sp8[sl]) / 8;
+                    for (int slot = 0; slot < 2 * (pp8[sl + 1] - pp8[sl]); slot++)
+                        for (int r = 0; r < 8; r++) {
+                            int row = r8[8 * sl + r];
+                            int pad = row < N ? (row ^ 1) : 1;
+                            if (pad >= N) pad = N > 1 ? N - 2 : 0;
+                            uint32_t off = (uint32_t)pad * 64;
+                            float v = 0.f;
+                            if (row < N && slot < Lm && slot < rp[row + 1] - rp[row]) {
+                                off = (uint32_t)ecol[rp[row] + slot] * 64;
+                                v = (float)evd[rp[row] + slot];
+                            }
+                            const size_t e = 8 * (size_t)(pp8[sl] + slot / 2) + r;
+                            if (slot & 1) {
+                                o8[e] |= off << 16;
+                                v8[e].y = v;
+                            } else {
+                                o8[e] |= off;
+                                v8[e].x = v;
+                            }
+                        }
+                }
+                // slices dealt to the warps longest first, each to the warp with
+                // the fewest slots so far (24 and 32 warps)
+                const int shapes[2] = {24, 32};
+                for (int sh = 0; sh < 2; sh++) {
+                    const int nw = shapes[sh];
+                    std::vector<int> order(ns8), load(nw, 0), cnt(nw, 0), wl(nw * 8, -1);
+                    for (int sl = 0; sl < ns8; sl++) order[sl] = sl;
+                    std::stable_sort(order.begin(), order.end(),
+                                     [&](int a, int b) { return pp8[a + 1] - pp8[a] > pp8[b + 1] - pp8[b]; });
+                    bool ok = true;
+                    for (int sl : order) {
+                        int w = 0;
+                        for (int q = 1; q < nw; q++)
+                            if (load[q] < load[w] || (load[q] == load[w] && cnt[q] < cnt[w])) w = q;
+                        if (cnt[w] >= 8) { ok = false; break; }
+                        wl[w * 8 + cnt[w]++] = sl;
+                        load[w] += pp8[sl + 1] - pp8[sl];
+                    }
+                    if (!ok) continue;
+                    // each warp's slices in slice order (neighbouring rows together)
+                    for (int w = 0; w < nw; w++) std::sort(wl.begin() + w * 8, wl.begin() + w * 8 + cnt[w]);
+                    ell8_it[sh] = *std::max_element(cnt.begin(), cnt.end());
+                    if ((rc = dwsl8[sh].upload(c, wl))) return rc;
+                }
+                if ((rc = doffs8.upload(c, o8)) || (rc = dvals8.upload(c, v8)) || (rc = dpptr8.upload(c, pp8)) ||
+                    (rc = drows8.upload(c, r8)))
+                    return rc;
+                ell8_nslices = ns8;
+                ell8_npg = npg;
+            }
+            if ((rc = derr.alloc(c, 1))) return rc;
+            cudaMemsetAsync(derr.p, 0, sizeof(int), c->stream);
             if ((rc = dell.alloc(c, ell.size()))) return rc;
             cudaMemcpyAsync(dell.p, ell.data(), ell.size(), cudaMemcpyHostToDevice, c->stream);
             if ((rc = dsptr.upload(c, sptr))) return rc;
@@ -491,23 +602,39 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
             }
             XP.ell_nslices = nsl;
             XP.ell_nent = nent;
+            if (doffs8.p) {
+                XP.ell8_offs = doffs8.p;
+                XP.ell8_vals = dvals8.p;
+                XP.ell8_pptr = dpptr8.p;
+                XP.ell8_rows = drows8.p;
+                XP.ell8_nslices = ell8_nslices;
+                XP.ell8_npg = ell8_npg;
+                for (int sh = 0; sh < 2; sh++) {
+                    XP.ell8_wsl[sh] = dwsl8[sh].p;
+                    XP.ell8_it[sh] = ell8_it[sh];
+                }
+            }
+            XP.err = derr.p;
             XP.f0 = f0;
             XP.nf = nf;
             XP.singleshift = c->nshift > 0;
             // Chebyshev kernel: FP32, its shared-memory footprint (state, diagonal, ELL)
             const size_t csm = (size_t)N * NISE_T3_ROW * 8 + (size_t)N * 32 + (size_t)nent * 8 + 4 * (5 * nsl + 1) + 4096;
-            cheb = prec == NISE_FP32 && csm <= 227 * 1024 && (nsl + 15) / 16 <= 32;
+            cheb = prec == NISE_FP32 && ((csm <= 227 * 1024 && (nsl + 15) / 16 <= 32) || doffs8.p);
             if (cheb && ((rc = dcorder.alloc(c, (size_t)nf)) || (rc = dinvr.alloc(c, (size_t)nf)) ||
                          (rc = dcoef.alloc(c, (size_t)nf * (NISE_CHEB_KMAX + 1)))))
                 return rc;
         }
     }
-    config = default_config(scheme, N, plain, cheb, TP.k, nchk, plain ? 3 : nvec, dell4.p != nullptr);
+    config = default_config(scheme, N, plain, cheb, TP.k, nchk, plain ? 3 : nvec, dell4.p != nullptr,
+                            scheme == SCHEME_TAYLOR && taylor_rv_fits(T, XP));
     if (p.kernel_config != 0) {  // forced by the caller
         const int k = p.kernel_config;
         if (scheme == SCHEME_EIGEN && k == 2) return NISE_OK;
         if (scheme == SCHEME_TROTTER && (k == 1 || k == 32 || k == 33 || k == 64 || k == 128 || k == 256)) config = k == 1 ? 0 : k;
-        else if (scheme == SCHEME_TAYLOR && (k == 3 || k == 8 || k == 9 || (k == 10 && cheb) || (k == 12 && dell4.p)))
+        else if (scheme == SCHEME_TAYLOR &&
+                 (k == 3 || k == 8 || k == 9 || (k == 10 && cheb) || (k == 12 && dell4.p) || k == 13 || k == 14 ||
+                  (k == 15 && cheb && doffs8.p)))
             config = k == 9 ? -8 : k;
         else return nise_fail(c, NISE_ERR_ARG, "kernel_config %d does not apply to this scheme", k);
         return NISE_OK;
@@ -540,16 +667,20 @@ int AbsRun::run_main(cudaStream_t s, int cfg, double2 *dst) {
             TaylorPlan P = XP;
             P.only_v2 = cfg < 0;
             P.use_v4 = cfg == 12;
-            if (cfg == 10) {
+            P.no_rv = cfg == 13;
+            if (cfg == 10 || cfg == 15) {
                 P.order = dcorder.p;
                 P.cheb_inv_r = dinvr.p;
                 P.cheb_coef = dcoef.p;
+                P.rv_cheb = cfg == 15;
+                P.order_taylor = dorder.p;
             } else {
                 P.order = dorder.p;
                 P.cheb_inv_r = nullptr;
                 P.cheb_coef = nullptr;
             }
-            return launch_abs_taylor(pr, T, P, Js, r, cfg == 10 ? 8 : cfg < 0 ? -cfg : cfg, s, &kernels);
+            P.rv_shape = cfg == 14 ? 1 : 0;
+            return launch_abs_taylor(pr, T, P, Js, r, cfg == 10 || cfg >= 13 ? 8 : cfg < 0 ? -cfg : cfg, s, &kernels);
         }
         default:
             return launch_abs_dia(pr, T, Ue.p, f0, N, Js, r, s);
@@ -577,8 +708,9 @@ int AbsRun::tune() {
     if (scheme == SCHEME_TROTTER) {
         cand = {0, 32, 33, 64, 128, 256};
     } else {
-        cand = {3, -8, 8};
+        cand = {3, -8, 8, 13, 14};
         if (cheb) cand.push_back(10);
+        if (cheb && doffs8.p) cand.push_back(15);
         if (dell4.p) cand.push_back(12);
     }
     // the tables the kernels read (both series for the Taylor route)
@@ -636,12 +768,15 @@ int AbsRun::enqueue(cudaStream_t s, bool events) {
         break;
     case SCHEME_TAYLOR: {
         TaylorPlan P = XP;
-        if (config == 10)
+        if (config == 10 || config == 15) {
             rc = nise_cuda(c, launch_prep_cheb(T, P, rowabs, J.f, dcorder.p, dinvr.p, dcoef.p, s), "Chebyshev prep");
-        else
+            c->launches++;
+        }
+        if (!rc && config != 10) {
             rc = nise_cuda(c, launch_prep_taylor(prec, T, P, rowabs, J.f, dorder.p, s), "Taylor prep");
+            c->launches++;
+        }
         if (rc) return rc;
-        c->launches++;
         break;
     }
     default: {
@@ -684,10 +819,11 @@ double AbsRun::flops() const {
         // and the diagonal, scaling and accumulation (6 flops per site)
         // (Chebyshev: the same products per term plus the recurrence, 10 flops per site)
         std::vector<int> order(nf);
-        cudaMemcpy(order.data(), config == 10 ? dcorder.p : dorder.p, sizeof(int) * nf, cudaMemcpyDeviceToHost);
+        const bool ch = config == 10 || config == 15;
+        cudaMemcpy(order.data(), ch ? dcorder.p : dorder.p, sizeof(int) * nf, cudaMemcpyDeviceToHost);
         double orders = 0;
         for (long t = 0; t < nf; t++) orders += (double)order[t] * cross[t];
-        return orders * (4.0 * XP.nnz + (config == 10 ? 10.0 : 6.0) * N);
+        return orders * (4.0 * XP.nnz + (ch ? 10.0 : 6.0) * N);
     }
     default:
         return (double)nf * 6.7 * N * (double)N * N + (double)vec_steps * 8.0 * N * N;
@@ -708,6 +844,7 @@ extern "C" int nise_absorption(nise_ctx *c, double *re_S, double *im_S, int *sam
     std::vector<double2> h(R.tmax);
     cudaMemcpyAsync(h.data(), R.out.p, sizeof(double2) * R.tmax, cudaMemcpyDeviceToHost, c->stream);
     if ((rc = nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "absorption"))) return rc;
+    if ((rc = R.check_err())) return rc;
     nise_collect_timing(c);
     c->last_flops = R.flops();
     for (int t = 0; t < R.tmax; t++) {
@@ -880,6 +1017,9 @@ extern "C" int nise_batch_run(nise_batch *b) {
     }
     cudaError_t e = cudaStreamSynchronize(b->master);
     if (e != cudaSuccess) return batch_fail(b, NISE_ERR_DEVICE, std::string("nise_batch_run: ") + cudaGetErrorString(e));
+    for (int i = 0; i < n; i++)
+        if (b->runs[i]->check_err())
+            return batch_fail(b, NISE_ERR_TIMEOUT, "nise_batch_run: a bounded wait for a staged frame gave up");
     float ms = 0;
     cudaEventElapsedTime(&ms, b->start, b->stop);
     b->last_ms = ms;

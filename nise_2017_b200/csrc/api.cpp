@@ -154,6 +154,11 @@ extern "C" const char *nise_last_error(const nise_ctx *c) { return c ? c->err.c_
 // Copy host bytes to a context buffer, keeping the allocation when it is
 // already large enough (repeated uploads of same-sized trajectories allocate
 // nothing).
+// Every device trajectory image carries kImageSlack bytes past its last
+// record: bulk copies of a record, widened to 16-byte boundaries, stay inside
+// the allocation.
+static const size_t kImageSlack = 256;
+
 static int upload(nise_ctx *c, float **dst, size_t *cap, const void *src, size_t bytes) {
     if (!src || !bytes) {
         if (*dst) cudaFree(*dst);
@@ -165,8 +170,9 @@ static int upload(nise_ctx *c, float **dst, size_t *cap, const void *src, size_t
         if (*dst) cudaFree(*dst);
         *dst = nullptr;
         *cap = 0;
-        if (cudaMalloc((void **)dst, bytes) != cudaSuccess)
+        if (cudaMalloc((void **)dst, bytes + kImageSlack) != cudaSuccess)
             return nise_fail(c, NISE_ERR_NOMEM, "device allocation of %zu bytes failed", bytes);
+        cudaMemsetAsync((char *)*dst + bytes, 0, kImageSlack, c->stream);
         *cap = bytes;
     }
     int e = (int)cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, c->stream);

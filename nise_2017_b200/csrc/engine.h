@@ -3,6 +3,7 @@
 // cast to int (0 = success) and only enqueues work on the given stream.
 #pragma once
 #include <cuda_runtime.h>
+#include <stdint.h>
 
 #include "devtypes.h"
 
@@ -67,6 +68,24 @@ struct TaylorPlan {
     const void *ell4;
     const int *ell4_sptr, *ell4_rows;
     int ell4_nslices, ell4_nent;
+    // row-owner layout (k_abs_taylor_rv, FP32): 8-row slices of alternating
+    // parity, couplings in slot pairs [group][row]: offs = the two neighbours'
+    // row byte offsets (column * 64, 16 bits each), vals = the two weights;
+    // pptr [nslices + 1] first group of each slice, rows [nslices][8]; wsl[s]
+    // the slices of each warp of launch shape s (24 or 32 warps, [warp][8],
+    // -1 = none), it[s] the most slices of a warp; no_rv keeps the 8-vector
+    // waves on k_abs_taylor3
+    const uint32_t *ell8_offs;
+    const float2 *ell8_vals;
+    const int *ell8_pptr, *ell8_rows;
+    const int *ell8_wsl[2];
+    int ell8_it[2];
+    int ell8_nslices, ell8_npg;
+    int rv_shape;
+    int no_rv;
+    int rv_cheb;           // with the Chebyshev tables: the row-owner kernel's Chebyshev form
+    const int *order_taylor;  // rv_cheb: Taylor orders for the 1-vector tail CTAs
+    int *err;              // device flag: 1 = a bounded wait for a staged frame gave up
 };
 #define NISE_CHEB_KMAX 40
 
@@ -103,6 +122,12 @@ int launch_prep_taylor(int prec, const DevTraj &T, TaylorPlan &P, double rowabs_
                        cudaStream_t s);
 // kernels (optional): the number of kernels launched (the sliced-ELL Taylor
 // kernel runs whole waves of 8-vector CTAs plus 1-vector CTAs for the rest).
+// The row-owner Taylor kernel (FP32, static couplings, 8 vectors per CTA)
+// for vectors v0 .. v0+nvec-1; cudaErrorNotSupported when the job does not
+// fit its layout (shared memory, dipoles not static).
+int launch_abs_taylor_rv(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int v0, int nvec,
+                         cudaStream_t s);
+bool taylor_rv_fits(const DevTraj &T, const TaylorPlan &P);
 int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp,
                       int vec_per_cta, cudaStream_t s, int *kernels = nullptr);
 // Chebyshev coefficients of the exact step per frame (FP32 kernel); sets

@@ -153,6 +153,93 @@ def absorption(p, prec="f64"):
     return re, im, n.value
 
 
+def _f32(x):
+    return float(np.float32(x))
+
+
+def exact_step_factor(deltat):
+    """f = deltat * icm2ifs * twoPi (propagate.c:67) from the float constants of types.h."""
+    return _f32(deltat) * _f32(2.99792458e-5) * _f32(2 * 3.14159265359)
+
+
+def read_frames(keywords, files, frames):
+    """Shifted, cut Hamiltonians (FP64 copies of the float32 values the
+    reference's readers produce, read_trajectory.c:73-314) of the given frames,
+    and the dipole reader for HamiltonianType Coupling (static dipoles of frame
+    0, read_trajectory.c:61-67) or Full (per-frame, :357-377)."""
+    n = int(keywords["Singles"])
+    mins = [float(v) for v in str(keywords["MinFrequencies"]).split()]
+    maxs = [float(v) for v in str(keywords["MaxFrequencies"]).split()]
+    shift = np.float32((np.float32(maxs[0]) + np.float32(mins[0])) / np.float32(2))
+    cut = np.float32(keywords.get("Couplingcut", 0))
+    coupling = keywords.get("HamiltonianType", "Full") == "Coupling"
+    iu = np.triu_indices(n)
+    e = np.fromfile(files["energy"], dtype=np.float32)
+    d = np.fromfile(files["dipole"], dtype=np.float32)
+    if coupling:
+        hc = np.fromfile(files["coupling"], dtype=np.float32)[1:1 + n * (n + 1) // 2]
+    H = {}
+    for t in frames:
+        if coupling:
+            packed = hc.copy()
+            rec = e[t * (1 + n) + 1:(t + 1) * (1 + n)]
+            diag = rec
+        else:
+            w = 1 + n * (n + 1) // 2
+            packed = e[t * w + 1:(t + 1) * w].copy()
+            diag = packed[[a * n + a - a * (a + 1) // 2 for a in range(n)]]
+        M = np.zeros((n, n), np.float32)
+        M[iu] = packed
+        off = np.abs(M) < cut
+        M[off] = 0
+        M = np.triu(M, 1)
+        M = M + M.T
+        M[np.arange(n), np.arange(n)] = (diag.astype(np.float32) - shift).astype(np.float32)
+        H[t] = M.astype(np.float64)
+
+    def mu(t, x):
+        tt = 0 if coupling else t
+        return d[tt * (1 + 3 * n) + 1 + x * n:tt * (1 + 3 * n) + 1 + (x + 1) * n].astype(np.float64)
+    return H, mu
+
+
+def exact_propagators(H, f):
+    """U = V exp(-i e f) V^T of every frame (propagate_vec_DIA,
+    propagate.c:60-125, in FP64; the eigendecomposition is numpy's)."""
+    U = {}
+    for t, M in H.items():
+        e, V = np.linalg.eigh(M)
+        U[t] = (V * np.exp(-1j * e * f)) @ V.T
+    return U
+
+
+def absorption_exact(keywords, files):
+    """FP64 linear absorption with the exact propagator (Sparse, Threshold 0):
+    the sample loop of absorption.c:92-192 (response before propagation,
+    :119-145) with one U per frame shared by every vector that crosses it.
+    Returns (re_S, im_S, samples) like absorption()."""
+    n = int(keywords["Singles"])
+    length = int(keywords["Length"])
+    sample = int(keywords["Samplerate"])
+    tmax = int(str(keywords["RunTimes"]).split()[0])
+    begin = int(keywords.get("BeginPoint", 0))
+    nsamp = (length - tmax - 1) // sample + 1  # NISE_subs.c:197-221
+    end = int(keywords.get("EndPoint", 0)) or nsamp
+    assert 0 < end <= nsamp and not keywords.get("SingleShift")
+    frames = sorted({s * sample + t1 for s in range(begin, end) for t1 in range(tmax)})
+    H, mu = read_frames(keywords, files, frames)
+    U = exact_propagators(H, exact_step_factor(float(keywords["Timestep"])))
+    S = np.zeros(tmax, np.complex128)
+    for s in range(begin, end):
+        ti = s * sample
+        for x in range(3):
+            c = mu(ti, x).astype(np.complex128)
+            for t1 in range(tmax):
+                S[t1] += mu(ti + t1, x) @ c
+                c = U[ti + t1] @ c
+    return S.real.copy(), S.imag.copy(), end
+
+
 def spectrum(p, re, im, samples, prec="f64"):
     fft = max(p.fft, p.tmax1)
     w = np.zeros(fft)

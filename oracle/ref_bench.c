@@ -9,9 +9,12 @@
  * one JSON line.  Site-steps = threads * steps * N.
  *
  * usage: ref_bench energy.bin coupling.bin|- N propagation couplingcut deltat
- *                  trotter threshold min1 max1 threads steps
+ *                  trotter threshold min1 max1 threads steps [in.bin out.bin]
  *   energy.bin holds diagonal-only records (HamiltonianType Coupling) when a
  *   coupling file is given, else Full records; frame 0 is used.
+ *   With in.bin and out.bin the starting vectors are read from in.bin and the
+ *   propagated ones written to out.bin (float32 [threads][re N, im N]): the
+ *   reference's own propagated states, for the parity fixtures.
  */
 #include <omp.h>
 #include <stdio.h>
@@ -71,11 +74,32 @@ int main(int argc, char **argv) {
     float *vr = (float *)calloc((size_t)threads * N, sizeof(float));
     float *vi = (float *)calloc((size_t)threads * N, sizeof(float));
     for (long i = 0; i < (long)threads * N; i++) vr[i] = (float)((i * 7919 % 1000) / 1000.0 - 0.5);
+    const char *in_path = argc >= 15 ? argv[13] : NULL, *out_path = argc >= 15 ? argv[14] : NULL;
+    if (in_path) {
+        FILE *f = fopen(in_path, "rb");
+        if (!f) return 4;
+        for (int v = 0; v < threads; v++)
+            if (fread(vr + (size_t)v * N, sizeof(float), N, f) != (size_t)N ||
+                fread(vi + (size_t)v * N, sizeof(float), N, f) != (size_t)N) {
+                fclose(f);
+                return 4;
+            }
+        fclose(f);
+    }
     double t0 = omp_get_wtime();
 #pragma omp parallel for num_threads(threads) schedule(static, 1)
     for (int v = 0; v < threads; v++)
         for (int s = 0; s < steps; s++) propagate_vector(non, H, vr + (size_t)v * N, vi + (size_t)v * N, 1, 1, 1);
     double t1 = omp_get_wtime();
+    if (out_path) {
+        FILE *f = fopen(out_path, "wb");
+        if (!f) return 5;
+        for (int v = 0; v < threads; v++) {
+            fwrite(vr + (size_t)v * N, sizeof(float), N, f);
+            fwrite(vi + (size_t)v * N, sizeof(float), N, f);
+        }
+        fclose(f);
+    }
     double chk = 0;
     for (long i = 0; i < (long)threads * N; i++) chk += vr[i] * vr[i] + vi[i] * vi[i];
     printf("{\"seconds\": %.6f, \"threads\": %d, \"steps\": %d, \"sites\": %d, \"site_steps\": %ld, \"norm\": %.6e}\n",
