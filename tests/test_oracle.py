@@ -142,3 +142,23 @@ def test_fft_restatement_matches_numpy():
     order = list(range(128, 256)) + list(range(0, 128))
     assert np.allclose(sr, X.imag[order], rtol=0, atol=1e-12 * np.abs(X).max())
     assert np.allclose(si, X.real[order], rtol=0, atol=1e-12 * np.abs(X).max())
+
+
+@pytest.mark.parametrize("case", ["t2_0", "t2_4"])
+def test_restatement_reproduces_reference_at_2dir_benchmark_size(case, tmp_path):
+    """The FP32 restatement (float response sums, the reference's arithmetic)
+    against the reference program's R*.dat files on the 64-site cluster of
+    the 2DIR benchmark (tests/golden/make_golden_large.py): print precision
+    for t2 = 0; with t2 > 0 the t2 step's eigenvectors (ssyev_ vs Jacobi)
+    differ by rounding that the GB + SE + EA cancellation amplifies."""
+    import json
+    import os
+    from nise_2017_b200 import synth
+    d = np.load(os.path.join(helpers.GOLDEN, "large_c2_2dir.npz"))
+    spec = json.loads(str(d["meta"]))[case]
+    files = synth.write(synth.c2_spec(**spec["spec"]), str(tmp_path))
+    po = oracle.params(spec["keywords"], files)
+    R, n = oracle.twodir(po, "f32")
+    Rn = helpers.R12_to_files(oracle.normalize_2d(po, R, n, "f64"))
+    t2 = int(str(spec["keywords"]["RunTimes"]).split()[1])
+    assert helpers.rel2d(Rn, d[case]) < (5e-4 if t2 > 0 else 2e-6)
