@@ -35,6 +35,7 @@ CU_SOURCES = [
     "onfly.cu",
     "linear.cu",
     "taylor_rv.cu",
+    "eigen_large.cu",
 ]
 CPP_SOURCES = [
     "api.cpp",

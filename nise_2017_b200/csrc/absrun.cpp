@@ -166,7 +166,8 @@ struct AbsRun {
     // eigen route
     DevBuf<char> Ue;
     DevBuf<long> efr;
-    DevBuf<double> eV, ew;
+    DevBuf<double> eV, ew, eA;  // eigenvectors, eigenvalues, QR workspace (above the Jacobi's size)
+    DevBuf<int> estatus;
     long FC = 1;
     bool truncated = false;
     double fe = 0;
@@ -179,11 +180,18 @@ struct AbsRun {
     // after the job: a kernel whose bounded wait for a staged frame gave up
     // leaves its flag set (NISE_ERR_TIMEOUT)
     int check_err() {
-        if (!derr.p) return NISE_OK;
         int h = 0;
-        if (cudaMemcpy(&h, derr.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
-            return nise_fail(c, NISE_ERR_DEVICE, "error flag read failed");
-        return h ? nise_fail(c, NISE_ERR_TIMEOUT, "a bounded wait for a staged frame gave up") : NISE_OK;
+        if (derr.p) {
+            if (cudaMemcpy(&h, derr.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+                return nise_fail(c, NISE_ERR_DEVICE, "error flag read failed");
+            if (h) return nise_fail(c, NISE_ERR_TIMEOUT, "a bounded wait for a staged frame gave up");
+        }
+        if (estatus.p) {
+            if (cudaMemcpy(&h, estatus.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+                return nise_fail(c, NISE_ERR_DEVICE, "eigensolver status read failed");
+            if (h) return nise_fail(c, NISE_ERR_DEVICE, "the eigensolver did not converge on a frame");
+        }
+        return NISE_OK;
     }
     int run_main(cudaStream_t s, int cfg, double2 *dst);
     double flops() const;
@@ -296,13 +304,10 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
         const bool eigen_route = truncated || p.hamiltonian != NISE_HAM_COUPLING || p.kernel_config == 2;
         if (eigen_route) {
             scheme = SCHEME_EIGEN;
-            if (N > NISE_EIG_MAX_N)
+            if (N > 1024)
                 return nise_fail(c, NISE_ERR_UNSUPPORTED,
-                                 truncated ? "Sparse with Threshold > 0 is limited to 120 sites (eigen route)"
-                                 : p.hamiltonian == NISE_HAM_COUPLING
-                                     ? "kernel_config 2 (the eigen route) is limited to 120 sites"
-                                     : "exact propagation of per-frame couplings (HamiltonianType Full) is "
-                                       "limited to 120 sites (eigen route)");
+                                 "the eigen route (Threshold > 0, per-frame couplings, kernel_config 2) is limited to "
+                                 "1024 sites");
             const size_t ubytes = r2 * (size_t)nf * N * N;
             if (ubytes > ((size_t)64 << 30))
                 return nise_fail(c, NISE_ERR_NOMEM,
@@ -311,8 +316,10 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
             for (long t = 0; t < nf; t++) frames[t] = f0 + t;
             FC = std::max(1L, std::min(nf, (long)(((size_t)512 << 20) / (sizeof(double) * (size_t)N * N))));
             if ((rc = Ue.alloc(c, ubytes)) || (rc = efr.upload(c, frames)) || (rc = eV.alloc(c, (size_t)FC * N * N)) ||
-                (rc = ew.alloc(c, (size_t)FC * N)))
+                (rc = ew.alloc(c, (size_t)FC * N)) || (rc = eA.alloc(c, eig_any_ws_doubles(N, FC))) ||
+                (rc = estatus.alloc(c, 1)))
                 return rc;
+            cudaMemsetAsync(estatus.p, 0, sizeof(int), c->stream);
             // propagate_vec_DIA: f = deltat*icm2ifs*twoPi*sign in float, one full step
             fe = prec == NISE_FP32 ? (double)J.f32_full : J.f;
         } else {
@@ -787,8 +794,9 @@ int AbsRun::enqueue(cudaStream_t s, bool events) {
         const size_t r2 = prec == NISE_FP32 ? sizeof(float2) : sizeof(double2);
         for (long q = 0; q < nf; q += FC) {
             long m = std::min(FC, nf - q);
-            if ((rc = nise_cuda(c, launch_eig(EJ, efr.p + q, m, eV.p, ew.p, s), "eigensolver"))) return rc;
-            if ((rc = nise_cuda(c, launch_build_u(pr, eV.p, ew.p, m, N, fe, c->thres, truncated,
+            if ((rc = nise_cuda(c, launch_eig_any(EJ, efr.p + q, m, eV.p, ew.p, eA.p, estatus.p, s), "eigensolver")))
+                return rc;
+            if ((rc = nise_cuda(c, launch_build_u_any(pr, eV.p, ew.p, m, N, fe, c->thres, truncated,
                                                   Ue.p + r2 * (size_t)q * N * N, s),
                                 "propagator build")))
                 return rc;

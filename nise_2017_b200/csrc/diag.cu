@@ -166,11 +166,16 @@ int launch_abs_dia(int prec, const DevTraj &T, const void *U, long f0, int n, co
     if (J.nsamp <= 0) return 0;
     const int threads = ((n + 31) / 32) * 32;
     const int nw = threads / 32;
+    if (threads > 1024) return (int)cudaErrorNotSupported;
     if (prec == 0) {
         size_t sm = sizeof(float2) * 3 * n + sizeof(double2) * 3 * nw;
+        cudaError_t e = cudaFuncSetAttribute(k_abs_dia<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return (int)e;
         k_abs_dia<float><<<J.nsamp, threads, sm, s>>>(T, (const float2 *)U, f0, n, J, resp);
     } else {
         size_t sm = sizeof(double2) * 3 * n + sizeof(double2) * 3 * nw;
+        cudaError_t e = cudaFuncSetAttribute(k_abs_dia<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return (int)e;
         k_abs_dia<double><<<J.nsamp, threads, sm, s>>>(T, (const double2 *)U, f0, n, J, resp);
     }
     return (int)cudaGetLastError();

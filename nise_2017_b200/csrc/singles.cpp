@@ -56,19 +56,22 @@ int nise_singles_tables(nise_ctx *c, const DevTraj &T, long fmin, long nf, int s
         // <= 1) and time_evolution_mat's truncated sub-step propagator for the
         // doubles (Threshold always applied); Diagonal is the untruncated
         // exact propagator.
-        if (N > NISE_EIG_MAX_N)
-            return nise_fail(c, NISE_ERR_UNSUPPORTED, "Propagation Sparse/Diagonal on per-frame tables is limited to %d sites",
-                             NISE_EIG_MAX_N);
+        if (N > 1024)
+            return nise_fail(c, NISE_ERR_UNSUPPORTED, "Propagation Sparse/Diagonal on per-frame tables is limited to "
+                             "1024 sites");
         const float thr = p.propagation == NISE_PROP_DIAGONAL ? 0.0f : c->thres;
         const bool trunc_singles = thr != 0 && !(thr > 1);
         const long FC = std::max(1L, std::min(nf, (long)(((size_t)512 << 20) / (sizeof(double) * (size_t)N * N))));
         std::vector<long> frs(nf);
         for (long t = 0; t < nf; t++) frs[t] = fmin + t;
         DevBuf<long> dfr;
-        DevBuf<double> V, w;
+        DevBuf<double> V, w, Aws;
+        DevBuf<int> st;
         if ((rc = dfr.upload(c, frs)) || (rc = V.alloc(c, (size_t)FC * N * N)) || (rc = w.alloc(c, (size_t)FC * N)) ||
+            (rc = Aws.alloc(c, eig_any_ws_doubles(N, FC))) || (rc = st.alloc(c, 1)) ||
             (rc = B.U.alloc(c, r2 * (size_t)nf * N * N)))
             return rc;
+        cudaMemsetAsync(st.p, 0, sizeof(int), c->stream);
         if (doubles_u && (rc = B.rot.alloc(c, r2 * (size_t)nf * N * N))) return rc;
         EigJob EJ;
         EJ.T = T; EJ.n = N; EJ.singleshift = singleshift;
@@ -77,18 +80,25 @@ int nise_singles_tables(nise_ctx *c, const DevTraj &T, long fmin, long nf, int s
         const double fsub = prec == NISE_FP32 ? (double)nise_f32(p, 1, p.ts) : nise_f64(p, 1, p.ts);
         for (long q = 0; q < nf; q += FC) {
             long m = std::min(FC, nf - q);
-            if ((rc = nise_cuda(c, launch_eig(EJ, dfr.p + q, m, V.p, w.p, c->stream), "eigensolver"))) return rc;
-            if ((rc = nise_cuda(c, launch_build_u(pr, V.p, w.p, m, N, ffull, thr, trunc_singles,
+            if ((rc = nise_cuda(c, launch_eig_any(EJ, dfr.p + q, m, V.p, w.p, Aws.p, st.p, c->stream), "eigensolver")))
+                return rc;
+            if ((rc = nise_cuda(c, launch_build_u_any(pr, V.p, w.p, m, N, ffull, thr, trunc_singles,
                                                   B.U.p + r2 * (size_t)q * N * N, c->stream), "propagator build")))
                 return rc;
             c->launches += 2;
             if (doubles_u) {
-                if ((rc = nise_cuda(c, launch_build_u(pr, V.p, w.p, m, N, fsub, thr, 1, B.rot.p + r2 * (size_t)q * N * N,
+                if ((rc = nise_cuda(c, launch_build_u_any(pr, V.p, w.p, m, N, fsub, thr, 1, B.rot.p + r2 * (size_t)q * N * N,
                                                       c->stream), "doubles propagator build")))
                     return rc;
                 c->launches++;
             }
         }
+        int hst = 0;
+        if ((rc = nise_cuda(c, (int)cudaMemcpyAsync(&hst, st.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream),
+                            "eigensolver status")) ||
+            (rc = nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "eigensolver")))
+            return rc;
+        if (hst) return nise_fail(c, NISE_ERR_DEVICE, "the eigensolver did not converge on a frame");
         S.Ud = B.U.p;
         if (doubles_u) B.Us = B.rot.p;
     } else {

@@ -203,13 +203,19 @@ def read_frames(keywords, files, frames):
     return H, mu
 
 
-def exact_propagators(H, f):
+def exact_propagators(H, f, thres=0.0):
     """U = V exp(-i e f) V^T of every frame (propagate_vec_DIA,
-    propagate.c:60-125, in FP64; the eigendecomposition is numpy's)."""
+    propagate.c:60-125, in FP64; the eigendecomposition is numpy's); with
+    0 < thres <= 1 only the elements with |U_ab|^2 > thres are kept
+    (propagate_vec_DIA_S, propagate.c:185-258; propagate_vector's dispatch,
+    propagate.c:24-28)."""
     U = {}
     for t, M in H.items():
         e, V = np.linalg.eigh(M)
-        U[t] = (V * np.exp(-1j * e * f)) @ V.T
+        Ut = (V * np.exp(-1j * e * f)) @ V.T
+        if thres != 0 and not thres > 1:
+            Ut[np.abs(Ut) ** 2 <= thres] = 0
+        U[t] = Ut
     return U
 
 
@@ -228,7 +234,10 @@ def absorption_exact(keywords, files):
     assert 0 < end <= nsamp and not keywords.get("SingleShift")
     frames = sorted({s * sample + t1 for s in range(begin, end) for t1 in range(tmax)})
     H, mu = read_frames(keywords, files, frames)
-    U = exact_propagators(H, exact_step_factor(float(keywords["Timestep"])))
+    thres = 0.0
+    if keywords.get("Propagation", "Sparse") not in ("Coupling", "RK4", "Diagonal"):
+        thres = float(params(keywords, files).thres)  # Threshold scaled by (f/ts)^2 as readinput.c:264-267
+    U = exact_propagators(H, exact_step_factor(float(keywords["Timestep"])), thres)
     S = np.zeros(tmax, np.complex128)
     for s in range(begin, end):
         ti = s * sample

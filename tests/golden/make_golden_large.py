@@ -20,7 +20,12 @@ these fixtures are generated once, here, and the GPU tests only read them.
 The trajectories are regenerated by the tests from the stored generator
 arguments (nise_2017_b200.synth, seeded).
 
-Run from the repository root:  python tests/golden/make_golden_large.py [c1v] [c1a] [c2]
+  large_eig.npz           absorption with per-frame couplings on a 256-site chain
+                          (Propagation Sparse, Threshold 0 and truncating), the
+                          reference program's TD_Absorption.dat and the FP64
+                          exact responses
+
+Run from the repository root:  python tests/golden/make_golden_large.py [c1v] [c1a] [c2] [eig]
 """
 import json
 import os
@@ -45,6 +50,16 @@ C1_WIDE = dict(spec=dict(frames=408, seed=92),
                keywords=synth.c1_keywords(Length=408, RunTimes="8 0 0", Samplerate=1))
 C1_REF = dict(spec=C1_WIDE["spec"],
               keywords=synth.c1_keywords(Length=408, RunTimes="8 0 0", Samplerate=1, EndPoint=1))
+# the eigen route above the shared-memory Jacobi's 120 sites: per-frame
+# couplings (HamiltonianType Full), exact and truncated
+EIG_CASES = {
+    "full_256": dict(spec=dict(n_sites=256, frames=60, dt_fs=2.0, geometry=synth.CHAIN, seed=95),
+                     keywords=synth.c0_keywords(Singles=256, Length=60, RunTimes="8 0 0", Samplerate=20,
+                                                Propagation="Sparse", Threshold=0, EndPoint=1)),
+    "trunc_256": dict(spec=dict(n_sites=256, frames=60, dt_fs=2.0, geometry=synth.CHAIN, j_nn=-12.0, seed=96),
+                      keywords=synth.c0_keywords(Singles=256, Length=60, RunTimes="8 0 0", Samplerate=20,
+                                                 Propagation="Sparse", Threshold=100000, EndPoint=1)),
+}
 C2_CASES = {
     "t2_0": dict(spec=dict(frames=220, seed=93),
                  keywords=synth.c2_keywords(Length=220, RunTimes="8 0 8", Samplerate=100, EndPoint=2)),
@@ -115,6 +130,25 @@ def c1_absorption():
         shutil.rmtree(work, ignore_errors=True)
 
 
+def eig_large():
+    out = {}
+    for name, case in EIG_CASES.items():
+        work = tempfile.mkdtemp(prefix="golden_eig_")
+        try:
+            files = synth.write(synth.spec(**case["spec"]), work)
+            inp = synth.write_input(os.path.join(work, "input"), case["keywords"], files)
+            t0 = time.time()
+            oracle.run_reference(inp, work, timeout=4 * 3600)
+            print("reference NISE_acc %s: %.0f s" % (name, time.time() - t0))
+            out[name + "_td"] = np.loadtxt(os.path.join(work, "TD_Absorption.dat"), ndmin=2)
+            re, im, n = oracle.absorption_exact(case["keywords"], files)
+            out[name + "_exact"] = np.stack([re, im])
+            out[name + "_samples"] = n
+        finally:
+            shutil.rmtree(work, ignore_errors=True)
+    np.savez_compressed(os.path.join(HERE, "large_eig.npz"), meta=json.dumps(EIG_CASES), **out)
+
+
 def c2_2dir():
     out = {}
     for name, case in C2_CASES.items():
@@ -136,10 +170,12 @@ def c2_2dir():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["c1v", "c1a", "c2"]
+    which = sys.argv[1:] or ["c1v", "c1a", "c2", "eig"]
     if "c1v" in which:
         c1_vectors()
     if "c1a" in which:
         c1_absorption()
     if "c2" in which:
         c2_2dir()
+    if "eig" in which:
+        eig_large()

@@ -162,3 +162,18 @@ def test_restatement_reproduces_reference_at_2dir_benchmark_size(case, tmp_path)
     Rn = helpers.R12_to_files(oracle.normalize_2d(po, R, n, "f64"))
     t2 = int(str(spec["keywords"]["RunTimes"]).split()[1])
     assert helpers.rel2d(Rn, d[case]) < (5e-4 if t2 > 0 else 2e-6)
+
+
+@pytest.mark.parametrize("name", ["abs_sparse_static", "abs_sparse_full", "abs_sparse_trunc", "abs_sparse_trunc_static"])
+def test_exact_restatement_matches_c_restatement(name, tmp_path):
+    """oracle.absorption_exact (numpy FP64: one eigendecomposition per frame,
+    shared by every vector crossing it; truncation as propagate_vec_DIA_S)
+    against the C restatement's FP64 build and the reference's output: the
+    checker of the large-site tests."""
+    case = CASES[name]
+    files = helpers.materialise(case, str(tmp_path))
+    re, im, n = oracle.absorption_exact(case["keywords"], files)
+    ore, oim, on = oracle.absorption(oracle.params(case["keywords"], files), "f64")
+    assert n == on
+    assert helpers.rel(re + 1j * im, ore + 1j * oim) < 1e-12
+    assert helpers.rel(np.stack([re / n, im / n], 1), helpers.golden(name)["td"][:, 1:]) < 1e-5
