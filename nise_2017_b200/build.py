@@ -36,6 +36,7 @@ CU_SOURCES = [
     "linear.cu",
     "taylor_rv.cu",
     "eigen_large.cu",
+    "dia_tc.cu",
 ]
 CPP_SOURCES = [
     "api.cpp",

@@ -168,6 +168,8 @@ struct AbsRun {
     DevBuf<long> efr;
     DevBuf<double> eV, ew, eA;  // eigenvectors, eigenvalues, QR workspace (above the Jacobi's size)
     DevBuf<int> estatus;
+    DevBuf<float> tcX;           // state columns of the tensor-core apply
+    bool use_tc = false;
     long FC = 1;
     bool truncated = false;
     double fe = 0;
@@ -322,6 +324,16 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
             cudaMemsetAsync(estatus.p, 0, sizeof(int), c->stream);
             // propagate_vec_DIA: f = deltat*icm2ifs*twoPi*sign in float, one full step
             fe = prec == NISE_FP32 ? (double)J.f32_full : J.f;
+            // FP32 above the Jacobi's size: U applied on the tensor cores
+            // (kernel_config 16: the per-start-point kernel, 17: the tensor
+            // cores at any size)
+            AbsJob Jt = J;
+            if (plain) Jt.nsamp = 1;
+            use_tc = prec == NISE_FP32 && tc_dia_fits(Jt, N) &&
+                     (p.kernel_config == 17 || (N > NISE_EIG_MAX_N && p.kernel_config != 16));
+            if (use_tc && ((rc = tcX.alloc(c, (size_t)4 * tc_dia_columns(Jt) * N)) || (rc = derr.alloc(c, 1))))
+                return rc;
+            if (use_tc) cudaMemsetAsync(derr.p, 0, sizeof(int), c->stream);
         } else {
             scheme = SCHEME_TAYLOR;
             // CSR of the static couplings (read cut applied, |J| >= cut kept)
@@ -637,7 +649,7 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
                             scheme == SCHEME_TAYLOR && taylor_rv_fits(T, XP));
     if (p.kernel_config != 0) {  // forced by the caller
         const int k = p.kernel_config;
-        if (scheme == SCHEME_EIGEN && k == 2) return NISE_OK;
+        if (scheme == SCHEME_EIGEN && (k == 2 || k == 16 || k == 17)) return NISE_OK;
         if (scheme == SCHEME_TROTTER && (k == 1 || k == 32 || k == 33 || k == 64 || k == 128 || k == 256)) config = k == 1 ? 0 : k;
         else if (scheme == SCHEME_TAYLOR &&
                  (k == 3 || k == 8 || k == 9 || (k == 10 && cheb) || (k == 12 && dell4.p) || k == 13 || k == 14 ||
@@ -690,6 +702,7 @@ int AbsRun::run_main(cudaStream_t s, int cfg, double2 *dst) {
             return launch_abs_taylor(pr, T, P, Js, r, cfg == 10 || cfg >= 13 ? 8 : cfg < 0 ? -cfg : cfg, s, &kernels);
         }
         default:
+            if (use_tc) return launch_abs_dia_tc(T, Ue.p, f0, N, Js, r, tcX.p, derr.p, s);
             return launch_abs_dia(pr, T, Ue.p, f0, N, Js, r, s);
         }
     };

@@ -162,6 +162,13 @@ int launch_build_u(int prec, const double *V, const double *w, long nfr, int n, 
                    void *U, cudaStream_t s);
 // Linear absorption of the start points of J with the per-frame propagators
 // U (frames from f0): one CTA per start point, n <= 1024.
+// The eigen-route absorption with the propagators applied on the tensor cores
+// (FP32, time-major; dia_tc.cu): X is 4 * tc_dia_columns(J) * n floats of
+// workspace, err a device flag set when a bounded wait gives up.
+int tc_dia_columns(const AbsJob &J);
+bool tc_dia_fits(const AbsJob &J, int n);
+int launch_abs_dia_tc(const DevTraj &T, const void *U, long f0, int n, const AbsJob &J, double2 *resp, float *X,
+                      int *err, cudaStream_t s);
 int launch_abs_dia(int prec, const DevTraj &T, const void *U, long f0, int n, const AbsJob &J, double2 *resp,
                    cudaStream_t s);
 

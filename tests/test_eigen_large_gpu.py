@@ -23,6 +23,9 @@ from nise_2017_b200 import synth
 pytestmark = pytest.mark.gpu
 
 SPARSE_FP32 = 3e-6
+# the tensor-core apply against the per-start-point FP32 kernel: the tensor
+# core's product alignment rounds toward zero (measured 1.2e-6 over 48 steps)
+TC_VS_SCALAR = 2e-6
 
 
 def absorb(kw, files, **engine):
@@ -121,3 +124,39 @@ def test_linear_technique_above_120_sites(tmp_path):
     ore, oim, on = oracle.linear(oracle.params(kw, files), "f64")
     assert n == on
     assert helpers.rel(np.asarray(re) + 1j * np.asarray(im), ore + 1j * oim) < 1e-9
+
+
+@pytest.mark.parametrize("name", ["abs_sparse_full", "abs_sparse_trunc"])
+def test_tensor_core_apply_matches_scalar_apply(name, tmp_path):
+    """kernel_config 17 applies the propagators on the tensor cores (3xTF32,
+    time-major) even below 120 sites; 16 keeps the per-start-point kernel with
+    the reference's float accumulation.  Both against each other and against
+    the FP64 restatement."""
+    case = helpers.cases()[name]
+    files = helpers.materialise(case, str(tmp_path))
+    tc, n1 = absorb(case["keywords"], files, kernel_config=17)
+    sc, n2 = absorb(case["keywords"], files, kernel_config=16)
+    ore, oim, on = oracle.absorption(oracle.params(case["keywords"], files), "f64")
+    assert n1 == n2 == on
+    print("%s: tensor cores vs per-start-point kernel %.2e; vs FP64 %.2e (per-start-point %.2e)"
+          % (name, helpers.rel(tc, sc), helpers.rel(tc, ore + 1j * oim), helpers.rel(sc, ore + 1j * oim)))
+    assert helpers.rel(tc, sc) < TC_VS_SCALAR
+    assert helpers.rel(tc, ore + 1j * oim) < SPARSE_FP32
+
+
+def test_tensor_core_apply_wide_state(tmp_path):
+    """64 state columns (20 start points in flight, 3 polarisations), 160
+    sites (a partial 128-row tile and 32-site chunk), against the FP64
+    restatement."""
+    s = synth.spec(n_sites=160, frames=120, dt_fs=2.0, geometry=synth.CHAIN, seed=440)
+    files = synth.write(s, str(tmp_path))
+    kw = synth.c0_keywords(Singles=160, Length=120, RunTimes="40 0 0", Samplerate=2, Propagation="Sparse",
+                           Threshold=0)
+    ex_re, ex_im, en = oracle.absorption_exact(kw, files)
+    r32, n = absorb(kw, files)
+    sc, _ = absorb(kw, files, kernel_config=16)
+    assert n == en == 40
+    print("wide state: tensor cores vs FP64 %.2e, per-start-point kernel vs FP64 %.2e"
+          % (helpers.rel(r32, ex_re + 1j * ex_im), helpers.rel(sc, ex_re + 1j * ex_im)))
+    assert helpers.rel(r32, ex_re + 1j * ex_im) < SPARSE_FP32
+    assert helpers.rel(r32, sc) < TC_VS_SCALAR
