@@ -1529,6 +1529,26 @@ static int run_taylor3(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, d
     return run_taylor3_g<R, IT1, 1>(T, P, J, resp, main, nvec - main, s);
 }
 
+int launch_abs_taylor_part(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int v0, int nvec,
+                           bool one, cudaStream_t s) {
+    if (nvec <= 0) return 0;
+    if (!one) return launch_abs_taylor_rv(T, P, J, resp, v0, nvec, s);
+    TaylorPlan Pt = P;  // 1-vector CTAs run the Taylor series
+    if (P.rv_cheb) {
+        Pt.order = P.order_taylor;
+        Pt.cheb_coef = nullptr;
+        Pt.cheb_inv_r = nullptr;
+    }
+    const int it = (P.ell_nslices + 15) / 16;
+    if (!P.ell || it > 32) return (int)cudaErrorNotSupported;
+    const int IT = it <= 1 ? 1 : it <= 2 ? 2 : it <= 4 ? 4 : it <= 8 ? 8 : it <= 16 ? 16 : 32;
+    switch (IT <= 8 ? 1 : IT / 8) {
+    case 1: return run_taylor3_g<float, 1, 1>(T, Pt, J, resp, v0, nvec, s);
+    case 2: return run_taylor3_g<float, 2, 1>(T, Pt, J, resp, v0, nvec, s);
+    default: return run_taylor3_g<float, 4, 1>(T, Pt, J, resp, v0, nvec, s);
+    }
+}
+
 int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp,
                       int vec_per_cta, cudaStream_t s, int *kernels) {
     if (kernels) *kernels = 1;

@@ -179,6 +179,18 @@ struct AbsRun {
 
     int plan(nise_ctx *ctx, bool autotune);
     int enqueue(cudaStream_t s, bool events);
+    // The static-coupling series kernels wave by wave, each wave after the
+    // energy chunk holding its last frame (and the series tables of the
+    // frames up to there): the copy from the host overlaps the propagation.
+    int enqueue_waves(cudaStream_t s);
+    bool waves_apply() const;
+    // A plan reused by a later call: the trajectory pointers may have moved
+    // and the error flags start clear.
+    void refresh() {
+        T = nise_devtraj(c);
+        if (derr.p) cudaMemsetAsync(derr.p, 0, sizeof(int), c->stream);
+        if (estatus.p) cudaMemsetAsync(estatus.p, 0, sizeof(int), c->stream);
+    }
     // after the job: a kernel whose bounded wait for a staged frame gave up
     // leaves its flag set (NISE_ERR_TIMEOUT)
     int check_err() {
@@ -773,10 +785,75 @@ int AbsRun::tune() {
 }
 
 // Kernels of the job on stream s: tables, propagation, response sum.
+bool AbsRun::waves_apply() const {
+    return c->nchunks > 0 && scheme == SCHEME_TAYLOR && !plain && (config == 15 || config == 8) &&
+           prec == NISE_FP32 && taylor_rv_fits(T, XP) && nvec > sm_count();
+}
+
+int AbsRun::enqueue_waves(cudaStream_t s) {
+    TaylorPlan P = XP;
+    P.rv_shape = 0;
+    if (config == 15) {
+        P.order = dcorder.p;
+        P.cheb_inv_r = dinvr.p;
+        P.cheb_coef = dcoef.p;
+        P.rv_cheb = 1;
+        P.order_taylor = dorder.p;
+    } else {
+        P.order = dorder.p;
+    }
+    // whole waves of 8-vector CTAs, the rest on 1-vector CTAs (as launch_abs_taylor)
+    const int nsm = sm_count(), ctas = (nvec + 7) / 8;
+    int main = nvec;
+    if (ctas % nsm != 0 && ctas % nsm < nsm / 2 && ctas >= nsm) main = (ctas / nsm) * nsm * 8;
+    long prepped = f0;  // frames [f0, prepped) have their series tables
+    int rc = 0;
+    auto prep_to = [&](long last) -> int {
+        if (last < prepped) return 0;
+        nise_wait_frames(c, s, last);
+        TaylorPlan Q = XP;
+        Q.f0 = prepped;
+        Q.nf = last + 1 - prepped;
+        const long o = prepped - f0;
+        int e = 0;
+        if (config == 15) {
+            e = nise_cuda(c, launch_prep_cheb(T, Q, rowabs, J.f, dcorder.p + o, dinvr.p + o,
+                                              dcoef.p + o * (NISE_CHEB_KMAX + 1), s), "Chebyshev prep");
+            c->launches++;
+        }
+        if (!e) e = nise_cuda(c, launch_prep_taylor(prec, T, Q, rowabs, J.f, dorder.p + o, s), "Taylor prep");
+        c->launches++;
+        prepped = last + 1;
+        return e;
+    };
+    for (int v = 0; v < main && !rc; v += 8 * nsm) {
+        const int ve = std::min(v + 8 * nsm, main);
+        // the last frame any vector of the wave steps through
+        if ((rc = prep_to((long)(J.begin + (ve - 1) / 3) * J.sample + J.tmax - 2))) return rc;
+        rc = nise_cuda(c, launch_abs_taylor_part(T, P, J, resp.p, v, ve - v, false, s), "propagation");
+        c->launches++;
+    }
+    if (!rc && main < nvec) {
+        if ((rc = prep_to(f0 + nf - 1))) return rc;
+        rc = nise_cuda(c, launch_abs_taylor_part(T, P, J, resp.p, main, nvec - main, true, s), "propagation");
+        c->launches++;
+    }
+    return rc;
+}
+
 int AbsRun::enqueue(cudaStream_t s, bool events) {
     const int pr = prec == NISE_FP32 ? 0 : 1;
     int rc;
+    const bool waves = waves_apply();
+    if (c->nchunks > 0 && !waves) nise_wait_all_frames(c, s);
     if (events) cudaEventRecord(c->evk0, s);
+    if (waves) {
+        if ((rc = enqueue_waves(s))) return rc;
+        if (events) cudaEventRecord(c->evk1, s);
+        if ((rc = nise_cuda(c, launch_reduce_resp(resp.p, nvec, tmax, out.p, s), "response reduction"))) return rc;
+        c->launches++;
+        return NISE_OK;
+    }
     switch (scheme) {
     case SCHEME_TROTTER:
         if ((rc = nise_cuda(c, launch_prep_trotter(prec, T, TP, J.f64_sub, J.f32_sub, s), "Trotter prep"))) return rc;
@@ -854,11 +931,23 @@ double AbsRun::flops() const {
 extern "C" int nise_absorption(nise_ctx *c, double *re_S, double *im_S, int *samples) {
     if (!c || !re_S || !im_S || !samples) return nise_fail(c, NISE_ERR_ARG, "null argument");
     cudaSetDevice(c->p.device);
-    AbsRun R;
     c->launches = 0;
     c->last_flops = c->last_bytes = 0;
     int rc;
-    if ((rc = R.plan(c, false))) return rc;
+    AbsRun *Rp = nullptr;
+    if (c->abs_plan && c->abs_plan_epoch == c->plan_epoch) {
+        Rp = (AbsRun *)c->abs_plan.get();  // same layout, couplings, SingleShift and stream
+        Rp->refresh();
+    } else {
+        c->abs_plan.reset();
+        if (c->p.hamiltonian != NISE_HAM_COUPLING) nise_wait_all_frames(c, c->stream);  // the pattern scan reads frames
+        std::unique_ptr<AbsRun> fresh(new AbsRun);
+        if ((rc = fresh->plan(c, false))) return rc;
+        Rp = fresh.release();
+        c->abs_plan = std::shared_ptr<void>(Rp, [](void *q) { delete (AbsRun *)q; });
+        c->abs_plan_epoch = c->plan_epoch;
+    }
+    AbsRun &R = *Rp;
     cudaEventRecord(c->ev0, c->stream);
     if ((rc = R.enqueue(c->stream, true))) return rc;
     cudaEventRecord(c->ev1, c->stream);
@@ -879,6 +968,9 @@ extern "C" int nise_absorption(nise_ctx *c, double *re_S, double *im_S, int *sam
 extern "C" int nise_absorption_tune(nise_ctx *c) {
     if (!c) return nise_fail(nullptr, NISE_ERR_ARG, "null context");
     cudaSetDevice(c->p.device);
+    c->abs_plan.reset();
+    c->plan_epoch++;
+    nise_wait_all_frames(c, c->stream);
     AbsRun R;
     c->launches = 0;
     return R.plan(c, true);
@@ -941,6 +1033,10 @@ extern "C" int nise_batch_create(nise_ctx *const *ctxs, int n, int autotune, nis
         b->ctx.push_back(c);
         b->runs.emplace_back(new AbsRun());
         c->launches = 0;
+        // the graph below captures kernels only: energy records still in
+        // flight from the host land first
+        if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+        c->nchunks = 0;
         int rc = b->runs.back()->plan(c, autotune != 0);
         if (rc) {
             std::string m = "job " + std::to_string(i) + ": " + c->err;

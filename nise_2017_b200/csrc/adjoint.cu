@@ -379,6 +379,7 @@ extern "C" int nise_absorption_model(nise_ctx *c, const double *site_shift, doub
                                      double *freq, double *spec_re, double *spec_im, int max_rows, int *rows) {
     if (!c || !freq || !spec_re || !spec_im || !rows) return nise_fail(c, NISE_ERR_ARG, "null argument");
     cudaSetDevice(c->p.device);
+    nise_wait_all_frames(c, c->stream);  // energy records still in flight from the host
     AdjRun R;
     DevBuf<double> dshift, jf;
     DevBuf<int2> dpairs;
@@ -412,6 +413,7 @@ extern "C" int nise_backward_absorption(nise_ctx *c, const double *site_shift, d
     if (!c || !dL_dspec_re || !dL_dspec_im || !g_shift || !g_scale || !g_lifetime)
         return nise_fail(c, NISE_ERR_ARG, "null argument");
     cudaSetDevice(c->p.device);
+    nise_wait_all_frames(c, c->stream);  // energy records still in flight from the host
     const nise_params &p = c->p;
     const int fft = p.fft < p.tmax1 ? p.tmax1 : p.fft, tmax = p.tmax1, N = c->n;
     std::vector<int> idx;

@@ -123,6 +123,9 @@ extern "C" int nise_create(const nise_params *p, nise_ctx **out) {
 }
 
 void nise_free_traj(nise_ctx *c) {
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+    c->nchunks = 0;
+    c->plan_epoch++;
     void *ptrs[] = {c->d_energy, c->d_dipole, c->d_hc, c->d_mu_static, c->d_anh, c->d_over, c->d_shift_ptr,
                     c->d_shift_ab, c->d_alpha, c->d_pos};
     for (void *q : ptrs)
@@ -136,17 +139,90 @@ void nise_free_traj(nise_ctx *c) {
     c->loaded = false;
 }
 
+// Every device trajectory image carries kImageSlack bytes past its last
+// record: bulk copies of a record, widened to 16-byte boundaries, stay inside
+// the allocation.
+static const size_t kImageSlack = 256;
+
 extern "C" void nise_destroy(nise_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->p.device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+    c->abs_plan.reset();  // its buffers are freed on the stream they were allocated on
+    if (c->stream) cudaStreamSynchronize(c->stream);
     c->stream = c->own_stream;
     nise_free_traj(c);
-    cudaEvent_t evs[] = {c->ev0, c->ev1, c->evk0, c->evk1};
+    cudaEvent_t evs[] = {c->ev0, c->ev1, c->evk0, c->evk1, c->copy_ready};
     for (cudaEvent_t ev : evs)
         if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : c->chunk_ev) cudaEventDestroy(ev);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
+}
+
+void nise_wait_frames(nise_ctx *c, cudaStream_t s, long last_frame) {
+    for (int k = 0; k < c->nchunks; k++)
+        if (c->chunk_end[k] > last_frame || k == c->nchunks - 1) {
+            cudaStreamWaitEvent(s, c->chunk_ev[k], 0);
+            return;
+        }
+}
+
+void nise_wait_all_frames(nise_ctx *c, cudaStream_t s) {
+    if (c->nchunks) cudaStreamWaitEvent(s, c->chunk_ev[c->nchunks - 1], 0);
+}
+
+// Energy image from pinned host memory in chunks of about 16 MB on the copy
+// stream, after the work already enqueued on the context's stream (which may
+// still read the old image); the copies complete the chunk events.
+static int upload_energy_chunked(nise_ctx *c, const void *src, size_t bytes) {
+    if (bytes > c->cap_energy) {
+        cudaStreamSynchronize(c->stream);
+        if (c->d_energy) cudaFree(c->d_energy);
+        c->d_energy = nullptr;
+        c->cap_energy = 0;
+        if (cudaMalloc((void **)&c->d_energy, bytes + kImageSlack) != cudaSuccess)
+            return nise_fail(c, NISE_ERR_NOMEM, "device allocation of %zu bytes failed", bytes);
+        cudaMemsetAsync((char *)c->d_energy + bytes, 0, kImageSlack, c->stream);
+        c->cap_energy = bytes;
+    }
+    if (!c->copy_stream && cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return nise_fail(c, NISE_ERR_DEVICE, "copy stream creation failed");
+    if (!c->copy_ready && cudaEventCreateWithFlags(&c->copy_ready, cudaEventDisableTiming) != cudaSuccess)
+        return nise_fail(c, NISE_ERR_DEVICE, "event creation failed");
+    cudaEventRecord(c->copy_ready, c->stream);
+    cudaStreamWaitEvent(c->copy_stream, c->copy_ready, 0);
+    const size_t rec = 4 * (size_t)c->e_words;
+    const long per = std::max(1L, (long)(((size_t)16 << 20) / rec));
+    c->nchunks = 0;
+    c->chunk_end.clear();
+    for (long f0 = 0; f0 < c->e_frames; f0 += per) {
+        const long f1 = std::min(c->e_frames, f0 + per);
+        if ((int)c->chunk_ev.size() <= c->nchunks) {
+            cudaEvent_t ev;
+            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+                return nise_fail(c, NISE_ERR_DEVICE, "event creation failed");
+            c->chunk_ev.push_back(ev);
+        }
+        int e = (int)cudaMemcpyAsync((char *)c->d_energy + (size_t)f0 * rec, (const char *)src + (size_t)f0 * rec,
+                                     (size_t)(f1 - f0) * rec, cudaMemcpyHostToDevice, c->copy_stream);
+        if (e) return nise_cuda(c, e, "trajectory upload");
+        cudaEventRecord(c->chunk_ev[c->nchunks], c->copy_stream);
+        c->chunk_end.push_back(f1);
+        c->nchunks++;
+    }
+    return NISE_OK;
+}
+
+static bool pinned_host(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
 }
 
 extern "C" const char *nise_last_error(const nise_ctx *c) { return c ? c->err.c_str() : g_error.c_str(); }
@@ -154,11 +230,6 @@ extern "C" const char *nise_last_error(const nise_ctx *c) { return c ? c->err.c_
 // Copy host bytes to a context buffer, keeping the allocation when it is
 // already large enough (repeated uploads of same-sized trajectories allocate
 // nothing).
-// Every device trajectory image carries kImageSlack bytes past its last
-// record: bulk copies of a record, widened to 16-byte boundaries, stay inside
-// the allocation.
-static const size_t kImageSlack = 256;
-
 static int upload(nise_ctx *c, float **dst, size_t *cap, const void *src, size_t bytes) {
     if (!src || !bytes) {
         if (*dst) cudaFree(*dst);
@@ -197,36 +268,66 @@ extern "C" int nise_set_trajectory(nise_ctx *c, const void *energy, size_t energ
     if (c->e_frames < 1) return nise_fail(c, NISE_ERR_IO, "Hamiltonian trajectory file to short");
     if (c->d_frames < 1) return nise_fail(c, NISE_ERR_IO, "Dipole trajectory file to short");
     int rc;
-    if ((rc = upload(c, &c->d_energy, &c->cap_energy, energy, (size_t)c->e_frames * 4 * c->e_words))) return rc;
+    const size_t ebytes = (size_t)c->e_frames * 4 * c->e_words;
+    // the plan of the previous call stays valid for the same layout and the
+    // same couplings (the diagonal records are read by the kernels, not the plan)
+    const long old_frames = c->e_frames, old_words = c->e_words;
+    std::vector<float> old_hc;
+    old_hc.swap(c->h_hc);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);  // an earlier chunked copy
+    c->nchunks = 0;
+    // the small records first: a pageable copy queued behind the chunked
+    // energy copy on the copy engine would hold the host until it is done
     if ((rc = upload(c, &c->d_dipole, &c->cap_dipole, dipole, (size_t)c->d_frames * 4 * c->d_words))) return rc;
     c->a_frames = anharm ? (long)(anharm_bytes / (4 * (size_t)(1 + N))) : 0;
     c->o_frames = overtone ? (long)(overtone_bytes / (4 * (size_t)(1 + 3L * N))) : 0;
     if ((rc = upload(c, &c->d_anh, &c->cap_anh, anharm, (size_t)c->a_frames * 4 * (1 + N)))) return rc;
     if ((rc = upload(c, &c->d_over, &c->cap_over, overtone, (size_t)c->o_frames * 4 * (1 + 3L * N)))) return rc;
-    c->h_hc.clear();
+    const std::vector<float> old_mu = c->h_mu_static;
     c->h_mu_static.clear();
+    bool hc_changed = true;
     if (coupling_type) {
         // read_coupling (read_trajectory.c:47-70): one Full record at position 0
         // with the read cut, and the dipoles of frame 0.
         if (!coupling || coupling_bytes < 4 * (size_t)full_words)
             return nise_fail(c, NISE_ERR_IO, "Coupling trajectory file to short");
-        c->h_hc.assign((const float *)coupling + 1, (const float *)coupling + 1 + c->nn2);
-        for (int i = 0; i < N; i++) c->h_hc[(size_t)i * N + i - (size_t)i * (i + 1) / 2] -= c->shifte;
-        for (int i = 0; i < N; i++)
-            for (int j = i + 1; j < N; j++) {
-                long idx = j + (long)i * ((N << 1) - i - 1) / 2;
-                if (fabs(c->h_hc[idx]) < p.couplingcut) c->h_hc[idx] = 0;
-            }
+        const float *raw = (const float *)coupling + 1;
+        const bool same = c->d_hc && old_hc.size() == (size_t)c->nn2 && c->h_hc_raw.size() == (size_t)c->nn2 &&
+                          memcmp(c->h_hc_raw.data(), raw, sizeof(float) * c->nn2) == 0;
+        hc_changed = !same;
+        if (same) {
+            c->h_hc.swap(old_hc);  // processed and on the device already
+        } else {
+            c->h_hc_raw.assign(raw, raw + c->nn2);
+            c->h_hc.assign(raw, raw + c->nn2);
+            for (int i = 0; i < N; i++) c->h_hc[(size_t)i * N + i - (size_t)i * (i + 1) / 2] -= c->shifte;
+            for (int i = 0; i < N; i++)
+                for (int j = i + 1; j < N; j++) {
+                    long idx = j + (long)i * ((N << 1) - i - 1) / 2;
+                    if (fabs(c->h_hc[idx]) < p.couplingcut) c->h_hc[idx] = 0;
+                }
+            if ((rc = upload(c, &c->d_hc, &c->cap_hc, c->h_hc.data(), sizeof(float) * c->nn2))) return rc;
+        }
         const float *m = (const float *)dipole + 1;
         c->h_mu_static.assign(m, m + 3L * N);
-        if ((rc = upload(c, &c->d_hc, &c->cap_hc, c->h_hc.data(), sizeof(float) * c->nn2))) return rc;
-        if ((rc = upload(c, &c->d_mu_static, &c->cap_mu, c->h_mu_static.data(), sizeof(float) * 3 * N))) return rc;
+        if (!(c->d_mu_static && c->h_mu_static == old_mu) &&
+            (rc = upload(c, &c->d_mu_static, &c->cap_mu, c->h_mu_static.data(), sizeof(float) * 3 * N)))
+            return rc;
     } else {
+        c->h_hc.clear();
+        c->h_hc_raw.clear();
         if ((rc = upload(c, &c->d_hc, &c->cap_hc, nullptr, 0))) return rc;
         if ((rc = upload(c, &c->d_mu_static, &c->cap_mu, nullptr, 0))) return rc;
     }
+    if (ebytes >= ((size_t)64 << 20) && pinned_host(energy)) {
+        if ((rc = upload_energy_chunked(c, energy, ebytes))) return rc;
+    } else if ((rc = upload(c, &c->d_energy, &c->cap_energy, energy, ebytes))) {
+        return rc;
+    }
     int e = (int)cudaStreamSynchronize(c->stream);
     if (e) return nise_cuda(c, e, "trajectory upload");
+    if (!coupling_type || c->e_frames != old_frames || c->e_words != old_words || hc_changed || !c->loaded)
+        c->plan_epoch++;
     c->loaded = true;
     return NISE_OK;
 }
@@ -268,11 +369,14 @@ extern "C" int nise_set_trajectory_onfly(nise_ctx *c, const void *energy, size_t
     c->h_mu_static.clear();
     // inputs of the frame builder (freed when it is done) and the built records
     const size_t rec_bytes = (size_t)frames * 4 * full_words;
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+    c->nchunks = 0;
+    c->plan_epoch++;
     if (rec_bytes > c->cap_energy) {
         if (c->d_energy) cudaFree(c->d_energy);
         c->d_energy = nullptr;
         c->cap_energy = 0;
-        if (cudaMalloc((void **)&c->d_energy, rec_bytes) != cudaSuccess)
+        if (cudaMalloc((void **)&c->d_energy, rec_bytes + kImageSlack) != cudaSuccess)
             return nise_fail(c, NISE_ERR_NOMEM, "couplings on the fly: %zu bytes of frame records do not fit", rec_bytes);
         c->cap_energy = rec_bytes;
     }
@@ -342,6 +446,7 @@ extern "C" int nise_set_singleshift(nise_ctx *c, int n, const int *sites, const 
     if (c->d_shift_ptr) cudaFree(c->d_shift_ptr);
     c->d_shift_ptr = nullptr;
     c->nshift = n;
+    c->plan_epoch++;
     int rc;
     if (n) {
         if (cudaMalloc((void **)&c->d_shift_ptr, sizeof(int) * (c->n + 1)))
@@ -567,6 +672,7 @@ extern "C" int nise_set_stream(nise_ctx *c, void *stream) {
     if (!c) return nise_fail(nullptr, NISE_ERR_ARG, "null context");
     cudaStreamSynchronize(c->stream);
     c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    c->plan_epoch++;
     return NISE_OK;
 }
 

@@ -128,6 +128,11 @@ int launch_prep_taylor(int prec, const DevTraj &T, TaylorPlan &P, double rowabs_
 int launch_abs_taylor_rv(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int v0, int nvec,
                          cudaStream_t s);
 bool taylor_rv_fits(const DevTraj &T, const TaylorPlan &P);
+// Vectors [v0, v0 + nvec) of an FP32 static-coupling job: on the row-owner
+// kernel (whole CTAs of 8), or on 1-vector CTAs of the sliced-ELL Taylor
+// kernel (one).
+int launch_abs_taylor_part(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int v0, int nvec,
+                           bool one, cudaStream_t s);
 int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp,
                       int vec_per_cta, cudaStream_t s, int *kernels = nullptr);
 // Chebyshev coefficients of the exact step per frame (FP32 kernel); sets

@@ -247,6 +247,7 @@ extern "C" int nise_linear(nise_ctx *c, double *re_S, double *im_S, int max_chan
     if (!c || !re_S || !im_S || !channels || !samples) return nise_fail(c, NISE_ERR_ARG, "null argument");
     if (!c->loaded) return nise_fail(c, NISE_ERR_STATE, "no trajectory loaded");
     cudaSetDevice(c->p.device);
+    nise_wait_all_frames(c, c->stream);  // energy records still in flight from the host
     const nise_params &p = c->p;
     const int tech = p.technique, N = c->n, tmax = p.tmax1;
     const LinSpec L = lin_spec(tech);

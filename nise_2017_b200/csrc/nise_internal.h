@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -35,8 +36,28 @@ struct nise_ctx {
     long al_frames = 0, pos_frames = 0;
     size_t cap_alpha = 0, cap_pos = 0;
     std::vector<float> h_hc;        // coupling frame (HamiltonianType Coupling), shifted, cut
+    std::vector<float> h_hc_raw;    // the coupling record as given (an unchanged one is not processed again)
     std::vector<float> h_mu_static; // dipoles of frame 0 (HamiltonianType Coupling)
+    // Energy records copied from pinned host memory in frame chunks on
+    // copy_stream: chunk k holds frames [chunk_end[k-1], chunk_end[k]) and
+    // completes chunk_ev[k].  Kernels wait for the chunks they read
+    // (nise_wait_frames), so the copy overlaps the propagation.
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t copy_ready = nullptr;
+    std::vector<cudaEvent_t> chunk_ev;
+    std::vector<long> chunk_end;
+    int nchunks = 0;
+    // The linear-absorption plan of the last call (tables, sliced ELL, work
+    // buffers), reused while plan_epoch is unchanged: every change of the
+    // trajectory layout, couplings, SingleShift or stream advances it.
+    long plan_epoch = 0;
+    long abs_plan_epoch = -1;
+    std::shared_ptr<void> abs_plan;
 };
+
+// Make stream s wait until energy frames [0, last_frame] are on the device.
+void nise_wait_frames(nise_ctx *c, cudaStream_t s, long last_frame);
+void nise_wait_all_frames(nise_ctx *c, cudaStream_t s);
 
 int nise_fail(nise_ctx *c, int code, const char *fmt, ...);
 int nise_cuda(nise_ctx *c, int e, const char *what);

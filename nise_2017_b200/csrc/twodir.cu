@@ -1034,6 +1034,7 @@ extern "C" int nise_2dir(nise_ctx *c, double *R, int *sample_count) {
     if (!c || !R || !sample_count) return nise_fail(c, NISE_ERR_ARG, "null argument");
     if (!c->loaded) return nise_fail(c, NISE_ERR_STATE, "no trajectory loaded");
     cudaSetDevice(c->p.device);
+    nise_wait_all_frames(c, c->stream);  // energy records still in flight from the host
     const nise_params &p = c->p;
     const int N = c->n, T1 = p.tmax1, T2 = p.tmax2, T3 = p.tmax3, prec = p.precision;
     int tech = p.technique;
