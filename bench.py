@@ -67,10 +67,11 @@ def parse():
     a.add_argument("--impl", choices=["ours", "reference"], default="ours")
     a.add_argument("--frames", type=int, default=100000, help="trajectory length (default: the full workload)")
     a.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline (profiling runs)")
-    a.add_argument("--config", choices=["c1", "c2", "c3", "c4"], default="c1",
-                   help="c1: the headline (batched absorption, N=1024); c2: 2DIR, N=64 cluster; c3: adjoint, N=256 "
-                        "chain; c4: 64-trajectory "
-                        "mixed-size batch (secondary workloads)")
+    a.add_argument("--no-secondary", action="store_true", help="c1: skip the 2DIR secondary block")
+    a.add_argument("--config", choices=["c0", "c1", "c2", "c3", "c4"], default="c1",
+                   help="c1: the headline (batched absorption, N=1024); c0: plain absorption, N=16 chain; c2: 2DIR, "
+                        "N=64 cluster; c3: adjoint, N=256 chain; c4: 64-trajectory mixed-size batch (secondary "
+                        "workloads)")
     a.add_argument("--t2", type=int, default=0, help="c2 only: waiting-time steps (RunTimes 64 t2 64)")
     a.add_argument("--end", type=int, default=0, help="c2 only: EndPoint (0 = all start points)")
     a.add_argument("--c4-job", type=int, default=-1,
@@ -301,7 +302,17 @@ def run_ours(args):
     main_ms = statistics.mean(mains)
     achieved = flops / (main_ms / 1e3) / 1e12
     peak = nise.fp32_peak(local)
-    traffic = read_traffic().get("k_abs_taylor3_fp32_per_launch")
+    traffic = read_traffic().get("k_abs_taylor_rv_fp32_per_launch")
+    # shared-memory side of the same kernels: every Chebyshev term gathers each
+    # coupling's neighbour state (8 bytes per vector); their rate against the
+    # SM shared-memory bandwidth, 128 bytes per clock per SM at the sampled clock
+    cf = np.frombuffer(C.numpy().tobytes(), dtype=np.float32)[1:]
+    iu = np.triu_indices(n)
+    nnz = 2 * int(np.count_nonzero((np.abs(cf) >= float(kw["Couplingcut"])) & (iu[0] != iu[1])))
+    orders_cross = flops / (4.0 * nnz + 10.0 * n)
+    smem_bytes = orders_cross * nnz * 8.0
+    nsm = torch.cuda.get_device_properties(local).multi_processor_count
+    smem_peak = nsm * 128.0 * (clk.get("sm_mhz") or 1965.0) * 1e6 / 1e9
     # the HBM side of the same kernel, against the measured copy bandwidth
     try:
         with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")) as f:
@@ -338,11 +349,21 @@ def run_ours(args):
             "batched_over_plain": value / plain_value,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_ms / args.steps},
-            "roofline": {"bound": "fp32", "kernel": "k_abs_taylor3", "achieved": achieved, "peak": peak,
-                         "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": traffic,
+            "roofline": {"bound": "fp32",
+                         "kernel": "k_abs_taylor_rv (row-owner Chebyshev series, whole waves) + k_abs_taylor3 "
+                                   "(1-vector tail) + series prep",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak if peak else None, "traffic": traffic,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of k_abs_taylor_rv on "
+                                           "the 40 000-frame case, scaled by start points (profiles/dram_traffic.txt)",
                          "peak_source": "measured in-process FP32 FMA throughput (nise_probe_fp32_peak)",
                          "algorithmic_flops_per_launch": flops, "algorithmic_hbm_bytes_per_launch": hbm,
                          "kernel_ms": main_ms,
+                         "smem": {"achieved": smem_bytes / (main_ms / 1e3) / 1e9, "peak": smem_peak, "unit": "GB/s",
+                                  "frac": smem_bytes / (main_ms / 1e3) / 1e9 / smem_peak,
+                                  "algorithmic_bytes_per_launch": smem_bytes,
+                                  "peak_source": "%d SMs x 128 B/clock at the median sampled SM clock" % nsm,
+                                  "note": "the binding resource: the neighbour-state gathers of every series term"},
                          "hbm": {"achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
                                  "frac": hbm_achieved / hbm_peak, "peak_source": hbm_src,
                                  "note": "each frame is read once and shared by every vector in flight: "
@@ -351,16 +372,67 @@ def run_ours(args):
             "clocks": clk,
             "gpu_launches": launches,
         }
-        print(json.dumps(out), flush=True)
     c.close()
+    if rank == 0 and world == 1 and not args.no_secondary:
+        # the 2DIR workload on its first 20 start points, with its own clock record
+        sec = argparse.Namespace(**vars(args))
+        sec.end, sec.t2, sec.steps, sec.warmup = 20, 0, 2, 1
+        out["secondary"] = {"c2": run_c2(sec, emit=False)}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     return out
 
 
+# ---------------------------------------------------------------- C0 (secondary)
+def run_c0(args):
+    """Linear absorption, Propagation Coupling (Trotter), N = 16 chain (c0 statistics), 10000 x 2 fs
+    frames, RunTimes 128, Samplerate 20 (494 start points), Couplingcut 0.1, Trotter 5.
+
+    value = site-steps per second of the batched job (all start points in one launch); plain =
+    the same job with one start point (3 polarisations) per launch."""
+    import torch
+    import nise_2017_b200 as nise
+    from nise_2017_b200 import synth
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    kw = synth.c0_keywords()
+    out = {}
+    with tempfile.TemporaryDirectory() as td:
+        files = synth.write(synth.c0_spec(), td)
+        for mode in (nise.BATCHED, nise.PLAIN):
+            with nise.Context(nise.params_from_keywords(kw, files, device=local, launch_mode=mode)) as c:
+                c.load_files()
+                for _ in range(max(args.warmup, 3)):
+                    c.absorption()
+                clk = ClockSampler(local)
+                clk.start()
+                times = []
+                for _ in range(args.steps):
+                    re, im, ns = c.absorption()
+                    tot, main, launches = c.timing()
+                    times.append(tot)
+                out[mode] = (statistics.mean(times), launches, clk.stop(), ns)
+    ms, launches, clocks, ns = out[nise.BATCHED]
+    pms = out[nise.PLAIN][0]
+    site_steps = 3 * ns * 128 * 16
+    res = {"metric": "C0 linear absorption, Trotter scheme: site-steps/s, batched vs plain (secondary workload)",
+           "value": site_steps / (ms / 1e3), "unit": "site-steps/s", "n_gpus": 1, "steps": args.steps,
+           "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
+           "dtype": "f32 (propagation), f64 (response sums)",
+           "config": {"workload": "plain linear absorption, Propagation Coupling, N=16 chain, 10000 x 2 fs, "
+                                  "RunTimes 128, Samplerate 20, Couplingcut 0.1, Trotter 5", "start_points": ns},
+           "plain": {"value": site_steps / (pms / 1e3), "unit": "site-steps/s", "ms": pms,
+                     "mode": "one start point (3 polarisations) per launch", "launches": out[nise.PLAIN][1]},
+           "batched_over_plain": pms / ms, "clocks": clocks, "gpu_launches": launches}
+    print(json.dumps(res), flush=True)
+    return res
+
+
 # ---------------------------------------------------------------- 2DIR (secondary)
-def run_c2(args):
+def run_c2(args, emit=True):
     """2DIR, N = 64 random cluster, Tmax1 = Tmax3 = 64, Samplerate 100, 20000 x 2 fs frames.
 
     value = reference-equivalent doubles site-steps per second: the reference
@@ -383,11 +455,14 @@ def run_c2(args):
             for _ in range(max(args.warmup, 1)):
                 c.twodir()
             times, mains = [], []
+            clk = ClockSampler(local)
+            clk.start()
             for _ in range(args.steps):
                 R, n = c.twodir()
                 tot, main, launches = c.timing()
                 times.append(tot)
                 mains.append(main)
+            clocks = clk.stop()
             flops, _ = c.work()
         # plain: one start point per launch of every kernel, over the first 4 start points
         plain_samples = 4
@@ -410,8 +485,9 @@ def run_c2(args):
            "doubles_fp32_tflops": flops / (statistics.mean(mains) / 1e3) / 1e12, "gpu_launches": launches,
            "plain": {"value": plain_value, "unit": "site-steps/s", "ms": plain_ms, "start_points": plain_samples,
                      "mode": "one start point per launch of every kernel"},
-           "batched_over_plain": (site_steps / (ms / 1e3)) / plain_value}
-    print(json.dumps(out), flush=True)
+           "batched_over_plain": (site_steps / (ms / 1e3)) / plain_value, "clocks": clocks}
+    if emit:
+        print(json.dumps(out), flush=True)
     return out
 
 
@@ -603,7 +679,140 @@ def run_c4_job(args, i, n, frames, tmax, sample, local):
 
 
 # ---------------------------------------------------------------- reference arm
+def ref_exe(name):
+    exe = os.path.join(ROOT, "oracle", "_ref", name)
+    return exe if os.path.exists(exe) else None
+
+
+def run_program(exe, inp, cwd, threads):
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS="1")
+    t0 = time.perf_counter()
+    r = subprocess.run([exe, inp], cwd=cwd, env=env, stdout=subprocess.DEVNULL, stderr=subprocess.STDOUT)
+    return time.perf_counter() - t0, r.returncode
+
+
+def run_reference_c0(args):
+    """The reference program (oracle/_ref/NISE_acc, absorption.c) on the whole C0 job: one process,
+    and P processes over disjoint BeginPoint/EndPoint ranges (absorption is serial in the
+    reference; its response sums are additive over start points)."""
+    from nise_2017_b200 import synth
+    exe = ref_exe("NISE_acc")
+    if not exe:
+        return {"impl": "reference", "unavailable": "oracle/_ref/NISE_acc was not built"}
+    kw = synth.c0_keywords()
+    nsamp = (10000 - 128 - 1) // 20 + 1
+    site_steps = 3 * nsamp * 128 * 16
+    procs = max(1, min(host_threads(), 8))
+    with tempfile.TemporaryDirectory() as td:
+        files = synth.write(synth.c0_spec(), td)
+        inp = synth.write_input(os.path.join(td, "input"), kw, files)
+        run_program(exe, inp, td, 1)  # untimed: pages in the binary
+        one, rc = run_program(exe, inp, td, 1)
+        if rc:
+            return {"impl": "reference", "unavailable": "NISE_acc failed on the C0 input"}
+        jobs, t0 = [], time.perf_counter()
+        for k in range(procs):
+            d = os.path.join(td, "p%d" % k)
+            os.makedirs(d)
+            b, e = k * nsamp // procs, (k + 1) * nsamp // procs
+            ip = synth.write_input(os.path.join(d, "input"), dict(kw, BeginPoint=b, EndPoint=e), files)
+            jobs.append(subprocess.Popen([exe, ip], cwd=d, env=dict(os.environ, OMP_NUM_THREADS="1"),
+                                         stdout=subprocess.DEVNULL, stderr=subprocess.STDOUT))
+        for j in jobs:
+            j.wait()
+        multi = time.perf_counter() - t0
+    return {"impl": "reference", "config": "c0", "value": site_steps / multi, "unit": UNIT,
+            "time_to_spectrum_s": multi, "one_process": {"value": site_steps / one, "seconds": one, "cores": 1},
+            "cpu_baseline": {"value": site_steps / multi, "unit": UNIT, "cores": procs, "kind": "reference",
+                             "sample": "the whole C0 job (%d start points) in %d processes over disjoint "
+                                       "BeginPoint/EndPoint ranges" % (nsamp, procs)}}
+
+
+def run_reference_c2(args):
+    """The reference program (calc_2DIR.c, OpenMP over t1 in propagate.c:1541) on the first
+    start points of the C2 job, extrapolated linearly to all 199."""
+    from nise_2017_b200 import synth
+    exe = ref_exe("NISE_acc")
+    if not exe:
+        return {"impl": "reference", "unavailable": "oracle/_ref/NISE_acc was not built"}
+    threads = host_threads()
+    sample_points = 2
+    kw = synth.c2_keywords(EndPoint=sample_points)
+    nsamp = (20000 - 64 - 0 - 64 - 1) // 100 + 1
+    with tempfile.TemporaryDirectory() as td:
+        files = synth.write(synth.c2_spec(), td)
+        inp = synth.write_input(os.path.join(td, "input"), kw, files)
+        secs, rc = run_program(exe, inp, td, threads)
+        if rc:
+            return {"impl": "reference", "unavailable": "NISE_acc failed on the C2 input"}
+    n2 = 64 * 65 // 2
+    per_point = secs / sample_points
+    return {"impl": "reference", "config": "c2", "value": 21 * 65 * 64 * n2 / per_point, "unit": "site-steps/s",
+            "time_to_spectrum_s": per_point * nsamp, "extrapolated": True,
+            "cpu_baseline": {"value": 21 * 65 * 64 * n2 / per_point, "unit": "site-steps/s", "cores": threads,
+                             "kind": "reference",
+                             "sample": "%d of %d start points (%.1f s), extrapolated linearly" % (
+                                 sample_points, nsamp, secs)}}
+
+
+def run_reference_c4(args):
+    """The reference's propagate_vector (oracle/_ref/ref_bench) per C4 job: the Coupling (Trotter)
+    jobs timed on a few concurrent vector steps each; the Diagonal jobs (the reference runs them as
+    Sparse, Threshold 0: ssyev_ plus N^3 per vector step) timed up to 300 sites and extrapolated
+    with the measured N^3 law above.  Job time = vector steps x time per vector step."""
+    from nise_2017_b200 import synth
+    exe = ref_exe("ref_bench")
+    if not exe:
+        return {"impl": "reference", "unavailable": "oracle/_ref/ref_bench was not built"}
+    threads = max(1, min(host_threads(), 16))
+    frames, tmax, sample = 5000, 128, 25
+    nsamp = (frames - tmax - 1) // sample + 1
+    vec_steps = 3 * nsamp * (tmax - 1)
+    per_step, measured = {}, {}
+    with tempfile.TemporaryDirectory() as td:
+        for i, n in enumerate(c4_sites()):
+            diag = i % 2 == 1
+            if diag and n > 300:
+                continue
+            d = os.path.join(td, "t%02d" % i)
+            synth.write(synth.c1_spec(n_sites=n, frames=2, seed=40000 + i), d)
+            reps = 1 if diag else 8
+            env = dict(os.environ, OPENBLAS_NUM_THREADS="1", OMP_NUM_THREADS=str(threads))
+            cmd = [exe, os.path.join(d, "Energy.bin"), os.path.join(d, "Coupling.bin"), str(n), "0" if diag else "1",
+                   "2", "1", "5", "0", "13500", "16500", str(threads), str(reps)]
+            r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True, env=env)
+            if r.returncode:
+                return {"impl": "reference", "unavailable": "ref_bench failed on C4 job %d" % i}
+            dd = json.loads(r.stdout.strip().splitlines()[-1])
+            per_step[i] = dd["seconds"] / reps  # wall time of one round of `threads` concurrent vector steps
+            measured[i] = True
+    # Diagonal jobs above 300 sites: a * N^3 fitted on the measured Diagonal jobs above 100 sites
+    pts = [(c4_sites()[i], t) for i, t in per_step.items() if i % 2 == 1 and c4_sites()[i] > 100]
+    a = statistics.mean(t / n ** 3 for n, t in pts) if pts else None
+    total, job_s = 0.0, []
+    for i, n in enumerate(c4_sites()):
+        t = per_step.get(i, a * n ** 3 if a else float("nan"))
+        secs = vec_steps * t / threads  # `threads` vectors propagated concurrently
+        job_s.append(secs)
+        total += secs
+    site_steps = sum(3 * nsamp * tmax * n for n in c4_sites())
+    return {"impl": "reference", "config": "c4", "value": site_steps / total, "unit": "site-steps/s",
+            "time_to_all_spectra_s": total, "slowest_job_s": max(job_s), "extrapolated": True,
+            "cpu_baseline": {"value": site_steps / total, "unit": "site-steps/s", "cores": threads,
+                             "kind": "reference",
+                             "sample": "per job: %d concurrent vector steps (8 each for Coupling jobs, 1 for "
+                                       "Diagonal jobs up to 300 sites; larger Diagonal jobs from the fitted N^3 "
+                                       "law), scaled to the job's %d vector steps" % (threads, vec_steps)}}
+
+
 def run_reference(args):
+    if args.config in ("c0", "c2", "c4"):
+        if int(os.environ.get("RANK", "0")) != 0:
+            return None
+        fn = {"c0": run_reference_c0, "c2": run_reference_c2, "c4": run_reference_c4}[args.config]
+        out = fn(args)
+        print(json.dumps(out), flush=True)
+        return out
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
@@ -650,6 +859,8 @@ if __name__ == "__main__":
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.config == "c0":
+        run_c0(a)
     elif a.config == "c2":
         run_c2(a)
     elif a.config == "c3":
