@@ -1487,6 +1487,16 @@ static int run_taylor3_g(const DevTraj &T, const TaylorPlan &P, const AbsJob &J,
     return (int)cudaGetLastError();
 }
 
+// Vectors of a job's last partial wave on 1-vector CTAs (k_abs_taylor3 with
+// G = 1), 512 threads with IT1 rows per lane (1024 threads with one row per
+// lane measured slower on the 1024-site lattice: 52.3 against 51.0 ms per
+// job; the per-term barriers, not the lanes' gather chains, set its pace).
+template <typename R, int IT1>
+static int run_taylor3_tail(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int v0, int nvec,
+                            cudaStream_t s) {
+    return run_taylor3_g<R, IT1, 1>(T, P, J, resp, v0, nvec, s);
+}
+
 // Streaming multiprocessors of the current device (wave sizes).
 int sm_count() {
     int dev = 0, n = 0;
@@ -1519,14 +1529,14 @@ static int run_taylor3(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, d
         Pt.order = P.order_taylor;
         Pt.cheb_coef = nullptr;
         Pt.cheb_inv_r = nullptr;
-        return run_taylor3_g<R, IT1, 1>(T, Pt, J, resp, main, nvec - main, s);
+        return run_taylor3_tail<R, IT1>(T, Pt, J, resp, main, nvec - main, s);
     }
     if constexpr (sizeof(R) == 4 && IT == 16)
         if (e < 0 && P.ell_nslices <= 24 * 11 && taylor3_smem(P, 4, 8, 768) <= 220 * 1024)
             e = run_taylor3_g<R, 11, 8, 768>(T, P, J, resp, 0, main, s);
     if (e < 0) e = run_taylor3_g<R, IT, 8>(T, P, J, resp, 0, main, s);
     if (e) return e;
-    return run_taylor3_g<R, IT1, 1>(T, P, J, resp, main, nvec - main, s);
+    return run_taylor3_tail<R, IT1>(T, P, J, resp, main, nvec - main, s);
 }
 
 int launch_abs_taylor_part(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int v0, int nvec,
@@ -1543,9 +1553,9 @@ int launch_abs_taylor_part(const DevTraj &T, const TaylorPlan &P, const AbsJob &
     if (!P.ell || it > 32) return (int)cudaErrorNotSupported;
     const int IT = it <= 1 ? 1 : it <= 2 ? 2 : it <= 4 ? 4 : it <= 8 ? 8 : it <= 16 ? 16 : 32;
     switch (IT <= 8 ? 1 : IT / 8) {
-    case 1: return run_taylor3_g<float, 1, 1>(T, Pt, J, resp, v0, nvec, s);
-    case 2: return run_taylor3_g<float, 2, 1>(T, Pt, J, resp, v0, nvec, s);
-    default: return run_taylor3_g<float, 4, 1>(T, Pt, J, resp, v0, nvec, s);
+    case 1: return run_taylor3_tail<float, 1>(T, Pt, J, resp, v0, nvec, s);
+    case 2: return run_taylor3_tail<float, 2>(T, Pt, J, resp, v0, nvec, s);
+    default: return run_taylor3_tail<float, 4>(T, Pt, J, resp, v0, nvec, s);
     }
 }
 

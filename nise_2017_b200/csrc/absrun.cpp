@@ -153,10 +153,9 @@ struct AbsRun {
     DevBuf<int> drp, dcol, dorder, dsptr, dcorder, drows, dsptr4, drows4;
     DevBuf<int2> dell4;
     int ell4_nslices = 0, ell4_nent = 0;
-    DevBuf<uint32_t> doffs8;  // row-owner layout (k_abs_taylor_rv)
-    DevBuf<float2> dvals8;
-    DevBuf<int> dpptr8, drows8, dwsl8[2], derr;
-    int ell8_nslices = 0, ell8_npg = 0, ell8_it[2] = {0, 0};
+    DevBuf<float4> dtri8;  // row-owner layout (k_abs_taylor_rv)
+    DevBuf<int> dtptr8, drows8, dwsl8[2], derr;
+    int ell8_nslices = 0, ell8_ntg = 0, ell8_it[2] = {0, 0};
     DevBuf<char> dval, dell;
     DevBuf<float> dinvr;
     DevBuf<float2> dcoef;
@@ -521,9 +520,8 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
             if (prec == NISE_FP32) {
                 // row-owner layout: 8-row slices whose rows alternate in parity (the
                 // same degree-sorted interleave as above), neighbours other parity
-                // first (ecol), entries (byte offset of the neighbour's 64-byte row,
-                // weight bits) [slot][row]; padding entries point at a row of the
-                // other parity with weight 0
+                // first (ecol); padding slots point at a row of the other parity
+                // with weight 0
                 const int ns8 = (N + 7) / 8;
                 std::vector<int> r8(8 * (size_t)ns8, N);
                 {
@@ -549,36 +547,33 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
                     }
                     sp8[sl + 1] = sp8[sl] + 8 * Lm;
                 }
-                // slot pairs: [group][row] words of two 16-bit neighbour row byte
-                // offsets and float2 weights (an odd slot count padded by one slot)
+                // slot triples: [group][row] float4 of three weights and the
+                // three neighbours' row indices (10 bits each; a slot count not
+                // divisible by 3 padded with weight-0 slots)
                 std::vector<int> pp8(ns8 + 1, 0);
-                for (int sl = 0; sl < ns8; sl++) pp8[sl + 1] = pp8[sl] + ((sp8[sl + 1] - sp8[sl]) / 8 + 1) / 2;
-                const int npg = pp8[ns8];
-                std::vector<uint32_t> o8(8 * (size_t)std::max(npg, 1), 0);
-                std::vector<float2> v8(8 * (size_t)std::max(npg, 1), make_float2(0.f, 0.f));
+                for (int sl = 0; sl < ns8; sl++) pp8[sl + 1] = pp8[sl] + ((sp8[sl + 1] - sp8[sl]) / 8 + 2) / 3;
+                const int ntg = pp8[ns8];
+                std::vector<float4> t8(8 * (size_t)std::max(ntg, 1), make_float4(0.f, 0.f, 0.f, 0.f));
+                std::vector<uint32_t> tix(t8.size(), 0);
                 for (int sl = 0; sl < ns8; sl++) {
                     const int Lm = (sp8[sl + 1] - sp8[sl]) / 8;
-                    for (int slot = 0; slot < 2 * (pp8[sl + 1] - pp8[sl]); slot++)
+                    for (int slot = 0; slot < 3 * (pp8[sl + 1] - pp8[sl]); slot++)
                         for (int r = 0; r < 8; r++) {
                             int row = r8[8 * sl + r];
                             int pad = row < N ? (row ^ 1) : 1;
                             if (pad >= N) pad = N > 1 ? N - 2 : 0;
-                            uint32_t off = (uint32_t)pad * 64;
+                            uint32_t col = (uint32_t)pad;
                             float v = 0.f;
                             if (row < N && slot < Lm && slot < rp[row + 1] - rp[row]) {
-                                off = (uint32_t)ecol[rp[row] + slot] * 64;
+                                col = (uint32_t)ecol[rp[row] + slot];
                                 v = (float)evd[rp[row] + slot];
                             }
-                            const size_t e = 8 * (size_t)(pp8[sl] + slot / 2) + r;
-                            if (slot & 1) {
-                                o8[e] |= off << 16;
-                                v8[e].y = v;
-                            } else {
-                                o8[e] |= off;
-                                v8[e].x = v;
-                            }
+                            const size_t e = 8 * (size_t)(pp8[sl] + slot / 3) + r;
+                            (slot % 3 == 0 ? t8[e].x : slot % 3 == 1 ? t8[e].y : t8[e].z) = v;
+                            tix[e] |= col << (10 * (slot % 3));
                         }
                 }
+                for (size_t e = 0; e < t8.size(); e++) memcpy(&t8[e].w, &tix[e], 4);
                 // slices dealt to the warps longest first, each to the warp with
                 // the fewest slots so far (24 and 32 warps)
                 const int shapes[2] = {24, 32};
@@ -603,11 +598,9 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
                     ell8_it[sh] = *std::max_element(cnt.begin(), cnt.end());
                     if ((rc = dwsl8[sh].upload(c, wl))) return rc;
                 }
-                if ((rc = doffs8.upload(c, o8)) || (rc = dvals8.upload(c, v8)) || (rc = dpptr8.upload(c, pp8)) ||
-                    (rc = drows8.upload(c, r8)))
-                    return rc;
+                if ((rc = dtri8.upload(c, t8)) || (rc = dtptr8.upload(c, pp8)) || (rc = drows8.upload(c, r8))) return rc;
                 ell8_nslices = ns8;
-                ell8_npg = npg;
+                ell8_ntg = ntg;
             }
             if ((rc = derr.alloc(c, 1))) return rc;
             cudaMemsetAsync(derr.p, 0, sizeof(int), c->stream);
@@ -633,13 +626,12 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
             }
             XP.ell_nslices = nsl;
             XP.ell_nent = nent;
-            if (doffs8.p) {
-                XP.ell8_offs = doffs8.p;
-                XP.ell8_vals = dvals8.p;
-                XP.ell8_pptr = dpptr8.p;
+            if (dtri8.p) {
+                XP.ell8_tri = dtri8.p;
+                XP.ell8_tptr = dtptr8.p;
                 XP.ell8_rows = drows8.p;
                 XP.ell8_nslices = ell8_nslices;
-                XP.ell8_npg = ell8_npg;
+                XP.ell8_ntg = ell8_ntg;
                 for (int sh = 0; sh < 2; sh++) {
                     XP.ell8_wsl[sh] = dwsl8[sh].p;
                     XP.ell8_it[sh] = ell8_it[sh];
@@ -651,7 +643,7 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
             XP.singleshift = c->nshift > 0;
             // Chebyshev kernel: FP32, its shared-memory footprint (state, diagonal, ELL)
             const size_t csm = (size_t)N * NISE_T3_ROW * 8 + (size_t)N * 32 + (size_t)nent * 8 + 4 * (5 * nsl + 1) + 4096;
-            cheb = prec == NISE_FP32 && ((csm <= 227 * 1024 && (nsl + 15) / 16 <= 32) || doffs8.p);
+            cheb = prec == NISE_FP32 && ((csm <= 227 * 1024 && (nsl + 15) / 16 <= 32) || dtri8.p);
             if (cheb && ((rc = dcorder.alloc(c, (size_t)nf)) || (rc = dinvr.alloc(c, (size_t)nf)) ||
                          (rc = dcoef.alloc(c, (size_t)nf * (NISE_CHEB_KMAX + 1)))))
                 return rc;
@@ -665,7 +657,7 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
         if (scheme == SCHEME_TROTTER && (k == 1 || k == 32 || k == 33 || k == 64 || k == 128 || k == 256)) config = k == 1 ? 0 : k;
         else if (scheme == SCHEME_TAYLOR &&
                  (k == 3 || k == 8 || k == 9 || (k == 10 && cheb) || (k == 12 && dell4.p) || k == 13 || k == 14 ||
-                  (k == 15 && cheb && doffs8.p)))
+                  (k == 15 && cheb && dtri8.p)))
             config = k == 9 ? -8 : k;
         else return nise_fail(c, NISE_ERR_ARG, "kernel_config %d does not apply to this scheme", k);
         return NISE_OK;
@@ -742,7 +734,7 @@ int AbsRun::tune() {
     } else {
         cand = {3, -8, 8, 13, 14};
         if (cheb) cand.push_back(10);
-        if (cheb && doffs8.p) cand.push_back(15);
+        if (cheb && dtri8.p) cand.push_back(15);
         if (dell4.p) cand.push_back(12);
     }
     // the tables the kernels read (both series for the Taylor route)

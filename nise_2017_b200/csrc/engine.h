@@ -69,18 +69,17 @@ struct TaylorPlan {
     const int *ell4_sptr, *ell4_rows;
     int ell4_nslices, ell4_nent;
     // row-owner layout (k_abs_taylor_rv, FP32): 8-row slices of alternating
-    // parity, couplings in slot pairs [group][row]: offs = the two neighbours'
-    // row byte offsets (column * 64, 16 bits each), vals = the two weights;
-    // pptr [nslices + 1] first group of each slice, rows [nslices][8]; wsl[s]
-    // the slices of each warp of launch shape s (24 or 32 warps, [warp][8],
-    // -1 = none), it[s] the most slices of a warp; no_rv keeps the 8-vector
-    // waves on k_abs_taylor3
-    const uint32_t *ell8_offs;
-    const float2 *ell8_vals;
-    const int *ell8_pptr, *ell8_rows;
+    // parity, couplings in slot triples [group][row]: float4 of the three
+    // weights and the bits of the three neighbours' row indices (10 bits
+    // each); tptr [nslices + 1] first group of each slice, rows [nslices][8];
+    // wsl[s] the slices of each warp of launch shape s (24 or 32 warps,
+    // [warp][8], -1 = none), it[s] the most slices of a warp; no_rv keeps the
+    // 8-vector waves on k_abs_taylor3
+    const float4 *ell8_tri;
+    const int *ell8_tptr, *ell8_rows;
     const int *ell8_wsl[2];
     int ell8_it[2];
-    int ell8_nslices, ell8_npg;
+    int ell8_nslices, ell8_ntg;
     int rv_shape;
     int no_rv;
     int rv_cheb;           // with the Chebyshev tables: the row-owner kernel's Chebyshev form

@@ -15,8 +15,9 @@
 //  - the 8 rows of a slice alternate in parity and every row lists its
 //    other-parity neighbours first, so the two rows of a quarter-warp gather
 //    rows of opposite parity, which sit on opposite halves of the banks;
-//  - couplings are stored in slot pairs: one word with the two neighbours'
-//    16-bit row byte offsets and one float2 with the two weights;
+//  - couplings are stored in slot triples, one 16-byte entry per row: the
+//    three weights and the three neighbours' 10-bit row indices, so one
+//    load (8 rows: one shared-memory wavefront) serves three slots;
 //  - the slices are dealt to the warps longest first (each warp's total
 //    slot count nearly equal: the CTA barrier waits for the slowest warp);
 //  - the diagonal records of the frames the CTA's vectors need next are
@@ -39,24 +40,22 @@ constexpr int kRvMaxIT = 8;       // slices per warp
 constexpr unsigned kRvSpin = 1u << 20;  // bound on the mbarrier waits
 
 struct RvLayout {
-    size_t cur, offs, vals, pptr, rows, wsl, dg, red, mbar, total;
+    size_t cur, tri, tptr, rows, wsl, dg, red, mbar, total;
     int dgw;  // words per staged diagonal record (16-byte multiple)
 };
 
 __host__ __device__ inline size_t rv_al(size_t x) { return (x + 15) & ~(size_t)15; }
 
-// Shared-memory layout for n sites, npg slot-pair groups (8 rows each), nsl
+// Shared-memory layout for n sites, ntg slot-triple groups (8 rows each), nsl
 // slices and nw warps.
-__host__ __device__ inline RvLayout rv_layout(int n, int npg, int nsl, int nw) {
+__host__ __device__ inline RvLayout rv_layout(int n, int ntg, int nsl, int nw) {
     RvLayout L;
     size_t o = 0;
     L.cur = o;
     o = rv_al(o + (size_t)2 * n * 64);
-    L.offs = o;
-    o = rv_al(o + (size_t)(npg + 1) * 8 * 4);  // + one group of slack for the prefetch
-    L.vals = o;
-    o = rv_al(o + (size_t)(npg + 1) * 8 * 8);
-    L.pptr = o;
+    L.tri = o;
+    o = rv_al(o + (size_t)(ntg + 1) * 8 * 16);  // + one group of slack for the prefetch
+    L.tptr = o;
     o = rv_al(o + (size_t)(nsl + 1) * 4);
     L.rows = o;
     o = rv_al(o + (size_t)nsl * 8 * 4);
@@ -150,12 +149,11 @@ __global__ void __launch_bounds__(NT, 1)
     k_abs_taylor_rv(DevTraj T, TaylorPlan P, AbsJob J, double2 *resp, int v0, int nvec, const int *__restrict__ wsl_g) {
     constexpr int NW = NT / 32;
     extern __shared__ __align__(16) unsigned char sm[];
-    const int n = P.n, nsl = P.ell8_nslices, npg = P.ell8_npg;
-    const RvLayout L = rv_layout(n, npg, nsl, NW);
+    const int n = P.n, nsl = P.ell8_nslices, ntg = P.ell8_ntg;
+    const RvLayout L = rv_layout(n, ntg, nsl, NW);
     float4 *cur = (float4 *)(sm + L.cur);  // [2][n][4]
-    uint32_t *offs = (uint32_t *)(sm + L.offs);
-    float2 *vals = (float2 *)(sm + L.vals);
-    int *pptr = (int *)(sm + L.pptr);
+    float4 *tri = (float4 *)(sm + L.tri);
+    int *tptr = (int *)(sm + L.tptr);
     int *rows = (int *)(sm + L.rows);
     int *wsl = (int *)(sm + L.wsl);
     float *dg = (float *)(sm + L.dg);
@@ -164,15 +162,9 @@ __global__ void __launch_bounds__(NT, 1)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int r = lane >> 2, c = lane & 3;
 
-    for (int e = tid; e < 8 * npg; e += NT) {
-        offs[e] = P.ell8_offs[e];
-        vals[e] = P.ell8_vals[e];
-    }
-    for (int e = tid; e < 8; e += NT) {
-        offs[8 * npg + e] = 0;
-        vals[8 * npg + e] = make_float2(0.f, 0.f);
-    }
-    for (int e = tid; e <= nsl; e += NT) pptr[e] = P.ell8_pptr[e];
+    for (int e = tid; e < 8 * ntg; e += NT) tri[e] = P.ell8_tri[e];
+    for (int e = tid; e < 8; e += NT) tri[8 * ntg + e] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int e = tid; e <= nsl; e += NT) tptr[e] = P.ell8_tptr[e];
     for (int e = tid; e < 8 * nsl; e += NT) rows[e] = P.ell8_rows[e];
     for (int e = tid; e < NW * kRvMaxIT; e += NT) wsl[e] = wsl_g[e];
     if (tid == 0) {
@@ -322,17 +314,17 @@ __global__ void __launch_bounds__(NT, 1)
                 const float4 own = i < n ? src[(size_t)i * 4 + c] : make_float4(0.f, 0.f, 0.f, 0.f);
                 float a0 = d0[it] * own.x, b0 = d0[it] * own.y;
                 float a1 = d1[it] * own.z, b1 = d1[it] * own.w;
-                // slot pairs; the next pair's entries are loaded one iteration
-                // ahead (past the slice they are unused; one group of slack)
-                const int p1 = pptr[sl + 1];
-                int p = pptr[sl];
-                uint32_t o = offs[8 * p + r];
-                float2 w = vals[8 * p + r];
+                // slot triples; the next triple is loaded one iteration ahead
+                // (past the slice it is unused; one group of slack)
+                const int p1 = tptr[sl + 1];
+                int p = tptr[sl];
+                float4 w = tri[8 * p + r];
                 for (; p < p1; p++) {
-                    const uint32_t no = offs[8 * (p + 1) + r];
-                    const float2 nw = vals[8 * (p + 1) + r];
-                    const float4 za = *(const float4 *)(srcc + (o & 0xffffu));
-                    const float4 zb = *(const float4 *)(srcc + (o >> 16));
+                    const float4 nw = tri[8 * (p + 1) + r];
+                    const uint32_t ix = __float_as_uint(w.w);
+                    const float4 za = *(const float4 *)(srcc + ((ix & 0x3ffu) << 6));
+                    const float4 zb = *(const float4 *)(srcc + (((ix >> 10) & 0x3ffu) << 6));
+                    const float4 zc = *(const float4 *)(srcc + ((ix >> 20) << 6));
                     a0 += w.x * za.x;
                     b0 += w.x * za.y;
                     a1 += w.x * za.z;
@@ -341,7 +333,10 @@ __global__ void __launch_bounds__(NT, 1)
                     b0 += w.y * zb.y;
                     a1 += w.y * zb.z;
                     b1 += w.y * zb.w;
-                    o = no;
+                    a0 += w.z * zc.x;
+                    b0 += w.z * zc.y;
+                    a1 += w.z * zc.z;
+                    b1 += w.z * zc.w;
                     w = nw;
                 }
                 if (i < n) {
@@ -380,7 +375,7 @@ __global__ void __launch_bounds__(NT, 1)
 template <int IT, int NT, bool CHEB>
 int run_rv1(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int v0, int nvec, const int *wsl,
             cudaStream_t s) {
-    const size_t smem = rv_layout(P.n, P.ell8_npg, P.ell8_nslices, NT / 32).total;
+    const size_t smem = rv_layout(P.n, P.ell8_ntg, P.ell8_nslices, NT / 32).total;
     cudaError_t e =
         cudaFuncSetAttribute(k_abs_taylor_rv<IT, NT, CHEB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
@@ -402,10 +397,10 @@ int run_rv(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp
 const int kRvWarps[2] = {24, 32};
 
 bool taylor_rv_fits(const DevTraj &T, const TaylorPlan &P) {
-    if (!P.ell8_offs || !P.err || !T.mu_static || T.full || !P.static_j || P.n > 1024) return false;
+    if (!P.ell8_tri || !P.err || !T.mu_static || T.full || !P.static_j || P.n > 1024) return false;
     const int sh = P.rv_shape;
     if (sh < 0 || sh > 1 || !P.ell8_wsl[sh] || P.ell8_it[sh] > kRvMaxIT) return false;
-    return rv_layout(P.n, P.ell8_npg, P.ell8_nslices, kRvWarps[sh]).total <= 227 * 1024;
+    return rv_layout(P.n, P.ell8_ntg, P.ell8_nslices, kRvWarps[sh]).total <= 227 * 1024;
 }
 
 int launch_abs_taylor_rv(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int v0, int nvec,
