@@ -175,6 +175,7 @@ struct AbsRun {
     // work accounting
     std::vector<long> cross;
     long vec_steps = 0;
+    double alg_bytes = 0;  // every frame read once (diagonal or full record) and the dipoles
 
     int plan(nise_ctx *ctx, bool autotune);
     int enqueue(cudaStream_t s, bool events);
@@ -252,8 +253,7 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
         for (int t = 0; t < tmax - 1; t++) cross[a + t] += 3;
     }
     vec_steps = 3L * nsamp * (tmax - 1);
-    // bytes: every frame read once (diagonal or full record) and the dipoles
-    c->last_bytes = (double)nf * 4 * (p.hamiltonian == NISE_HAM_COUPLING ? N : c->nn2) +
+    alg_bytes = (double)nf * 4 * (p.hamiltonian == NISE_HAM_COUPLING ? N : c->nn2) +
                     (double)(p.hamiltonian == NISE_HAM_COUPLING ? 3 * N : (nf + 1) * 3L * N) * 4;
     const size_t rsz = prec == NISE_FP32 ? sizeof(float) : sizeof(double), r2 = 2 * rsz;
 
@@ -949,6 +949,7 @@ extern "C" int nise_absorption(nise_ctx *c, double *re_S, double *im_S, int *sam
     if ((rc = R.check_err())) return rc;
     nise_collect_timing(c);
     c->last_flops = R.flops();
+    c->last_bytes = R.alg_bytes;
     for (int t = 0; t < R.tmax; t++) {
         re_S[t] = h[t].x;
         im_S[t] = h[t].y;

@@ -43,8 +43,12 @@ def test_chunked_upload_equals_resident(tmp_path):
     with nise.Context(p) as c:
         keep = pinned_set(c, files)
         r1, i1, n1 = c.absorption()
+        w1 = c.work()
         r2, i2, n2 = c.absorption()  # the cached plan
+        w2 = c.work()
         del keep
+    # the algorithmic counts are the plan's, reported again when it is reused
+    assert w1 == w2 and w1[0] > 0 and w1[1] >= 16400 * 1024 * 4
     assert n0 == n1 == n2 == 1615
     assert np.array_equal(r0, r1) and np.array_equal(i0, i1)
     assert np.array_equal(r1, r2) and np.array_equal(i1, i2)
