@@ -123,10 +123,18 @@ typedef struct {
                                       warp per vector with the rotation table in shared/global
                                       memory (all bitwise identical);
                                       Sparse/Diagonal (static couplings): 3 or 9 k_abs_taylor2 with
-                                      4 or 8 vectors per CTA, 8 the sliced-ELL Taylor kernel, 10 the
-                                      sliced-ELL Chebyshev kernel (FP32), 12 the sliced-ELL
-                                      Taylor kernel with 4 vectors per CTA (FP32), 2 the eigen
-                                      route (explicit per-frame propagators, up to 120 sites) */
+                                      4 or 8 vectors per CTA, 8 the Taylor series (row-owner
+                                      layout where it fits, else sliced ELL), 13 the sliced-ELL
+                                      Taylor kernel, 14 the row-owner Taylor kernel with 32 warps
+                                      per CTA, 10 the sliced-ELL Chebyshev kernel (FP32), 15 the
+                                      row-owner Chebyshev kernel (FP32), 12 the sliced-ELL Taylor
+                                      kernel with 4 vectors per CTA (FP32);
+                                      2 the eigen route (explicit per-frame propagators, up to
+                                      1024 sites), 16 / 17 its propagators applied per start
+                                      point / on the tensor cores;
+                                      2D techniques, Trotter doubles: 1 one warp per doubles
+                                      vector (else two warps per vector for 32 < N <= 64,
+                                      bitwise the same result) */
     char positionFName[256];       /* Positionfile (TransitionDipole / ExtendedDipole; CD) */
     char pbcFName[256];            /* PBCfile: periodic box per frame (optional) */
     char alphaFName[256];          /* Alphafile: polarisabilities (Raman, SFG) */

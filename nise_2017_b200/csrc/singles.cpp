@@ -24,13 +24,15 @@ int nise_singles_tables(nise_ctx *c, const DevTraj &T, long fmin, long nf, int s
     int rc;
     std::vector<int2> pairs;
     if ((rc = nise_pattern(c, fmin, nf, pairs))) return rc;
+    const int K = (int)pairs.size();
+    pairs.push_back(make_int2(0, 0));  // one record past the last: read ahead without a bound check
     if ((rc = B.pairs.upload(c, pairs))) return rc;
     S.n = N;
     S.ts = p.ts;
     S.prop = p.propagation;
     S.f0 = fmin;
     S.pairs = B.pairs.p;
-    S.K = (int)pairs.size();
+    S.K = K;
     S.U = S.rot = S.rkval = S.Ud = nullptr;
     S.ent = nullptr;
     S.Kr = 0;
@@ -106,7 +108,7 @@ int nise_singles_tables(nise_ctx *c, const DevTraj &T, long fmin, long nf, int s
         size_t q = 0;
         for (int a = 0; a < N; a++) {
             ent.push_back(make_int2(a, a));
-            while (q < pairs.size() && pairs[q].x == a) ent.push_back(pairs[q++]);
+            while (q < (size_t)K && pairs[q].x == a) ent.push_back(pairs[q++]);
         }
         if ((rc = B.ent.upload(c, ent))) return rc;
         Rk4Plan P;

@@ -250,7 +250,8 @@ __device__ __forceinline__ void rot2(typename Vec2<R>::T &x1, typename Vec2<R>::
     x2 = y2;
 }
 
-template <typename R> struct Dcoef { R co, si, co2, si2; };
+// 16-byte (FP32) / 32-byte (FP64) records, one vector load each
+template <typename R> struct alignas(4 * sizeof(R)) Dcoef { R co, si, co2, si2; };
 
 template <typename R>
 __device__ __forceinline__ typename Vec2<R>::T make_vec2(R x, R y) {
@@ -363,6 +364,66 @@ __device__ __forceinline__ float over_mu(const TwoD &D, long t, int x, int i) {
     return D.T.over[t * (1 + 3L * D.n) + 1 + x * D.n + i];
 }
 
+// Initial doubles vector: dipole_double (NISE_subs.c:485-509) of the SE
+// vector src at frame tk, component p2, into the circulant layout; element e
+// of the packed order by thread tid, stride `stride`.
+template <typename R>
+__device__ __forceinline__ void doubles_init(const TwoD &D, typename Vec2<R>::T *F, const typename Vec2<R>::T *src,
+                                             long tk, int p2, int n, int Wd, int tid, int stride) {
+    typedef typename Vec2<R>::T R2;
+    typedef Ar<R> A;
+    const int N2 = n * (n + 1) / 2;
+    for (int e = tid; e < N2; e += stride) {
+        // e -> (i, j) with i <= j in the packed order
+        int i = 0, rem = e;
+        while (rem >= n - i) { rem -= n - i; i++; }
+        int j = i + rem;
+        R2 f;
+        if (i == j) {
+            R o = (R)over_mu(D, tk, p2, i);
+            R2 c = src[i];
+            f.x = A::mul(o, c.x);
+            f.y = A::mul(o, c.y);
+        } else {
+            R mi = (R)traj_mu(D.T, tk, p2, i), mj = (R)traj_mu(D.T, tk, p2, j);
+            R2 ci = src[i], cj = src[j];
+            f.x = A::add(A::mul(mi, cj.x), A::mul(mj, ci.x));
+            f.y = A::add(A::mul(mi, cj.y), A::mul(mj, ci.y));
+        }
+        F[circ(i, j, n, Wd)] = f;
+    }
+}
+
+// Half-step phases of frame tl (propagate.c:918-954): exp(-i (e_a+e_b-Delta)
+// f/2) for every packed pair, from the frame's diagonal dg; all threads of
+// the CTA.
+template <typename R>
+__device__ __forceinline__ void doubles_half_phases(const TwoD &D, typename Vec2<R>::T *Uh, const float *dg, long tl,
+                                                    int n, int Wd) {
+    typedef typename Vec2<R>::T R2;
+    const int N2 = n * (n + 1) / 2;
+    for (int e = threadIdx.x; e < N2; e += blockDim.x) {
+        int i = 0, rem = e;
+        while (rem >= n - i) { rem -= n - i; i++; }
+        int j = i + rem;
+        R2 u;
+        if (sizeof(R) == 4) {
+            float hf = __fadd_rn(dg[i], dg[j]);
+            if (i == j && !D.es) hf = __fsub_rn(hf, D.anh != 0.0f ? D.anh : D.T.anh[tl * (1L + n) + 1 + i]);
+            float arg = __fmul_rn(__fmul_rn(0.5f, hf), D.f32_dsub);
+            u.x = (R)(float)cos((double)arg);
+            u.y = (R)(-(float)sin((double)arg));
+        } else {
+            double hd = (double)dg[i] + (double)dg[j];
+            if (i == j && !D.es) hd -= D.anh != 0.0f ? (double)D.anh : (double)D.T.anh[tl * (1L + n) + 1 + i];
+            double arg = 0.5 * hd * D.f64_dsub;
+            u.x = (R)cos(arg);
+            u.y = (R)(-sin(arg));
+        }
+        Uh[circ(i, j, n, Wd)] = u;
+    }
+}
+
 // CTA = W warps = W doubles vectors of one start point, all at the same t3.
 template <typename R, int CPL>
 __global__ void __launch_bounds__(512, 1) k2d_doubles(TwoD D, int vec_per_sample, Dcoef<R> *cf_static, int use_tab) {
@@ -396,29 +457,10 @@ __global__ void __launch_bounds__(512, 1) k2d_doubles(TwoD D, int vec_per_sample
         for (int e = threadIdx.x; e < n * n; e += blockDim.x) cidx[e] = (short)circ(e / n, e % n, n, Wd);
     for (int e = lane; e < slots; e += 32) F[e] = make_vec2<R>(0, 0);
     __syncthreads();
-    // initial vector: dipole_double (NISE_subs.c:485-509) of the SE vector at tk
-    if (active) {
-        const R2 *src = (const R2 *)D.SE + ((size_t)s * D.T3 * NV + (kind == 0 ? pa : 3 + pa * D.T1 + t1)) * n;
-        for (int e = lane; e < N2; e += 32) {
-            // e -> (i, j) with i <= j in the packed order
-            int i = 0, rem = e;
-            while (rem >= n - i) { rem -= n - i; i++; }
-            int j = i + rem;
-            R2 f;
-            if (i == j) {
-                R o = (R)over_mu(D, tk, p2, i);
-                R2 c = src[i];
-                f.x = A::mul(o, c.x);
-                f.y = A::mul(o, c.y);
-            } else {
-                R mi = (R)traj_mu(D.T, tk, p2, i), mj = (R)traj_mu(D.T, tk, p2, j);
-                R2 ci = src[i], cj = src[j];
-                f.x = A::add(A::mul(mi, cj.x), A::mul(mj, ci.x));
-                f.y = A::add(A::mul(mi, cj.y), A::mul(mj, ci.y));
-            }
-            F[circ(i, j, n, Wd)] = f;
-        }
-    }
+    // initial vector: dipole_double of the SE vector at tk
+    if (active)
+        doubles_init<R>(D, F, (const R2 *)D.SE + ((size_t)s * D.T3 * NV + (kind == 0 ? pa : 3 + pa * D.T1 + t1)) * n,
+                        tk, p2, n, Wd, lane, 32);
     for (int t3 = 0; t3 < D.T3; t3++) {
         const long tl = tk + t3;
         __syncthreads();
@@ -495,37 +537,241 @@ __global__ void __launch_bounds__(512, 1) k2d_doubles(TwoD D, int vec_per_sample
             }
         }
         if (t3 == D.T3 - 1) break;
-        // half-step phases of the frame (propagate.c:918-954): exp(-i (e_a+e_b-Delta) f/2)
+        // half-step phases of the frame
         for (int i = threadIdx.x; i < n; i += blockDim.x) dg[i] = traj_diag(D.T, tl, i, false);
         __syncthreads();
-        for (int e = threadIdx.x; e < N2; e += blockDim.x) {
-            int i = 0, rem = e;
-            while (rem >= n - i) { rem -= n - i; i++; }
-            int j = i + rem;
-            R h;
-            if (sizeof(R) == 4) {
-                float hf = __fadd_rn(dg[i], dg[j]);
-                if (i == j && !D.es) hf = __fsub_rn(hf, D.anh != 0.0f ? D.anh : D.T.anh[tl * (1L + n) + 1 + i]);
-                float arg = __fmul_rn(__fmul_rn(0.5f, hf), D.f32_dsub);
-                R2 u;
-                u.x = (R)(float)cos((double)arg);
-                u.y = (R)(-(float)sin((double)arg));
-                Uh[circ(i, j, n, Wd)] = u;
-                (void)h;
-            } else {
-                double hd = (double)dg[i] + (double)dg[j];
-                if (i == j && !D.es) hd -= D.anh != 0.0f ? (double)D.anh : (double)D.T.anh[tl * (1L + n) + 1 + i];
-                double arg = 0.5 * hd * D.f64_dsub;
-                R2 u;
-                u.x = (R)cos(arg);
-                u.y = (R)(-sin(arg));
-                Uh[circ(i, j, n, Wd)] = u;
-            }
-        }
+        doubles_half_phases<R>(D, Uh, dg, tl, n, Wd);
         __syncthreads();
         const Dcoef<R> *cf = D.rot_static ? cf_static : cf_static + (tl - D.f0) * D.K;
         if (active)
             for (int sub = 0; sub < D.ts; sub++) doubles_substep<R, CPL>(F, Uh, cf, D.pairs, D.K, n, Wd, lane, cidx, D.es != 0);
+    }
+}
+
+// ------------------------------------------------ doubles, two warps per vector
+// For 32 < n <= 64 a doubles vector is shared by two warps: thread c of the
+// pair (c = 32 * half + lane) owns column c of |ac>, so a CTA runs twice the
+// warps of k2d_doubles on the same shared memory.  Each thread performs the
+// float operations k2d_doubles performs for that column, in the same order,
+// so the results are bitwise those of k2d_doubles.
+//
+// Ordering.  Within one run of couplings (a, b) with the same first site a,
+// coupling (a, b) touches |bc> (thread c, every c != a) and |aa> (thread b),
+// coupling (a, b') touches |b'c> and |aa>; the only shared elements are |bb'>
+// (threads b' then b) and |aa> (threads b then b').  Two couplings of a run
+// therefore only need ordering across the pair when b and b' belong to
+// different warps: a __syncwarp orders every coupling, and the pair's named
+// barrier is taken when the warp owning b changes within a run, and around
+// the pivot change (row a stored back by every column, the next row loaded;
+// thread c loads |a c>, which thread a stored).
+__device__ __forceinline__ void duo_sync(int id) { asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory"); }
+
+template <typename R, bool ES>
+__device__ void doubles_substep_duo(typename Vec2<R>::T *F, const typename Vec2<R>::T *Uh, const Dcoef<R> *cf,
+                                    const int2 *pairs, int K, int n, int W, int t64, const short *__restrict__ ci,
+                                    int bar) {
+    typedef typename Vec2<R>::T R2;
+    typedef Ar<R> A;
+    const int slots = n * W, c = t64;
+    const bool col = c < n;
+    const short *cic = ci ? ci + c : nullptr;  // column c of the slot table
+    for (int e = t64; e < slots; e += 64) {  // propagate.c:959-962
+        R2 z = F[e], u = Uh[e], o;
+        o.x = A::sub(A::mul(z.x, u.x), A::mul(z.y, u.y));
+        o.y = A::add(A::mul(z.x, u.y), A::mul(z.y, u.x));
+        F[e] = o;
+    }
+    duo_sync(bar);
+    int cur_a = -1, cur_w = -1, ix_aa = 0;
+    R2 piv = make_vec2<R>(0, 0);
+    // the pair and coefficient arrays hold one record past K, so the next
+    // record is loaded without a bound check
+    int2 ab_next = pairs[0];
+    Dcoef<R> q_next = cf[0];
+    for (int k = 0; k < K; k++) {
+        const int a = ab_next.x, b = ab_next.y;
+        const Dcoef<R> q = q_next;
+        ab_next = pairs[k + 1];
+        q_next = cf[k + 1];
+        if (a != cur_a) {
+            if (cur_a >= 0 && col && c != cur_a) F[cic ? cic[cur_a * n] : circ(cur_a, c, n, W)] = piv;
+            duo_sync(bar);
+            if (col && c != a) piv = F[cic ? cic[a * n] : circ(a, c, n, W)];
+            ix_aa = ci ? ci[a * n + a] : circ(a, a, n, W);
+            cur_a = a;
+            cur_w = b >> 5;
+        } else if ((b >> 5) != cur_w) {
+            duo_sync(bar);
+            cur_w = b >> 5;
+        }
+        // c == a case: (|aa>,|ab>) with the sqrt(2) angle, by the thread owning c = b
+        if (!ES && c == b) {
+            R2 X = F[ix_aa];
+            rot2<R>(X, piv, q.co2, q.si2);
+            F[ix_aa] = X;
+        }
+        // every other column c != a: (|ac>,|bc>); for c == b that is (|ab>,|bb>) at sqrt(2)
+        if (col && c != a && !(ES && c == b)) {
+            const bool sp = c == b;
+            const int iq = cic ? cic[b * n] : circ(b, c, n, W);
+            R2 Q = F[iq];
+            rot2<R>(piv, Q, sp ? q.co2 : q.co, sp ? q.si2 : q.si);
+            F[iq] = Q;
+        }
+        __syncwarp();
+    }
+    if (cur_a >= 0 && col && c != cur_a) F[cic ? cic[cur_a * n] : circ(cur_a, c, n, W)] = piv;
+    duo_sync(bar);
+    for (int e = t64; e < slots; e += 64) {  // propagate.c:1041-1044
+        R2 z = F[e], u = Uh[e], o;
+        o.x = A::sub(A::mul(z.x, u.x), A::mul(z.y, u.y));
+        o.y = A::add(A::mul(z.x, u.y), A::mul(z.y, u.x));
+        F[e] = o;
+    }
+    duo_sync(bar);
+}
+
+// The pair's part of one EA dot product: thread c holds the float terms of
+// column c; the second warp hands its terms to the first through `red`
+// (two buffers, so one barrier per product), which adds them in k2d_doubles'
+// order (column c, then c + 32) and reduces over the lanes.  Returns the sums
+// in lane 0 of the first warp.
+template <typename R>
+__device__ __forceinline__ double2 duo_dot(typename Vec2<R>::T term, typename Vec2<R>::T *red, int &par, int half,
+                                           int lane, int n, int bar) {
+    typedef typename Vec2<R>::T R2;
+    R2 *buf = red + par * 32;
+    if (half == 1) buf[lane] = term;
+    duo_sync(bar);
+    par ^= 1;
+    double a1 = 0, a2 = 0;
+    if (half == 0) {  // column lane < 32 < n always exists
+        a1 += (double)term.x;
+        a2 += (double)term.y;
+        if (lane + 32 < n) {
+            const R2 o = buf[lane];
+            a1 += (double)o.x;
+            a2 += (double)o.y;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        }
+    }
+    return make_double2(a1, a2);
+}
+
+// CTA = P pairs of warps = P doubles vectors of one start point, all at the
+// same t3 (32 < n <= 64).
+template <typename R>
+__global__ void __launch_bounds__(768, 1) k2d_doubles_duo(TwoD D, int vec_per_sample, Dcoef<R> *cf_static,
+                                                          int use_tab) {
+    typedef typename Vec2<R>::T R2;
+    typedef Ar<R> A;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = D.n, Wd = n / 2 + 2, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int pair = warp >> 1, half = warp & 1, t64 = threadIdx.x & 63, npairs = blockDim.x >> 6;
+    const int bar = 1 + pair;  // named barrier of the pair (0 is __syncthreads)
+    const int slots = n * Wd;  // circulant storage (>= N2)
+    R2 *Uh = (R2 *)smem_raw;                            // [N2] half phases, circulant order
+    R2 *F = Uh + slots + (size_t)pair * slots;          // this pair's vector
+    R2 *red = Uh + slots * (1 + npairs) + pair * 64;    // [2][32] the second warp's dot-product terms
+    float *mu = (float *)(Uh + slots * (1 + npairs) + 64 * npairs);  // [3][n] mu(tl), then [3][n] overtone
+    float *ov = mu + 3 * n;
+    float *dg = ov + 3 * n;                             // [n] diagonal energies of the frame
+    short *cidx = use_tab ? (short *)(dg + n) : nullptr;  // [n][n] circ(x, y), where it fits
+    const int cta_per_sample = (vec_per_sample + npairs - 1) / npairs;
+    const int s = blockIdx.x / cta_per_sample;
+    const int u = (blockIdx.x % cta_per_sample) * npairs + pair;
+    const bool active = u < vec_per_sample;
+    const long tk = tk_of(D, s);
+    const int NV = nvec_se(D);
+    const int q = t64;  // this thread's column
+    const bool qv = q < n;
+    int par = 0;
+    // which vector: u < 9 -> fr for (p1,p2) = (u/3, u%3); else ft1[t1] for (p0,p2)
+    int kind = u < 9 ? 0 : 1, pa = 0, p2 = 0, t1 = 0;
+    if (active) {
+        if (kind == 0) { pa = u / 3; p2 = u % 3; }
+        else { int w = u - 9, cmb = w / D.T1; t1 = w % D.T1; pa = cmb / 3; p2 = cmb % 3; }
+    }
+    for (int e = threadIdx.x; e < slots; e += blockDim.x) Uh[e] = make_vec2<R>(1, 0);
+    if (cidx)
+        for (int e = threadIdx.x; e < n * n; e += blockDim.x) cidx[e] = (short)circ(e / n, e % n, n, Wd);
+    for (int e = t64; e < slots; e += 64) F[e] = make_vec2<R>(0, 0);
+    duo_sync(bar);
+    if (active)
+        doubles_init<R>(D, F, (const R2 *)D.SE + ((size_t)s * D.T3 * NV + (kind == 0 ? pa : 3 + pa * D.T1 + t1)) * n,
+                        tk, p2, n, Wd, t64, 64);
+    for (int t3 = 0; t3 < D.T3; t3++) {
+        const long tl = tk + t3;
+        __syncthreads();
+        for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) {
+            mu[i] = traj_mu(D.T, tl, i / n, i % n);
+            ov[i] = over_mu(D, tl, i / n, i % n);
+        }
+        __syncthreads();
+        // EA projections and dot products (calc_2DIR.c:456-488), as k2d_doubles
+        if (active && D.ea) {
+            for (int p3 = 0; p3 < 3; p3++) {
+                R2 gq;
+                {
+                    R gr = 0, gi = 0;
+                    if (qv)
+                        for (int j = 0; j < n; j++) {
+                            R m = (R)(j == q ? ov[p3 * n + q] : mu[p3 * n + j]);
+                            R2 f = F[cidx ? cidx[j * n + q] : circ(j, q, n, Wd)];
+                            gr = A::add(gr, A::mul(m, f.x));
+                            gi = A::add(gi, A::mul(m, f.y));
+                        }
+                    gq.x = gr;
+                    gq.y = gi;
+                }
+                for (int m = 0; m < 21; m++) {
+                    if (c_px[m][3] != p3 || c_px[m][2] != p2) continue;
+                    if (kind == 0 && c_px[m][1] != pa) continue;
+                    if (kind == 1 && c_px[m][0] != pa) continue;
+                    if (kind == 0) {
+                        int p0 = c_px[m][0];
+                        for (int tt = 0; tt < D.T1; tt++) {
+                            const R2 *rv = (const R2 *)D.SE + (((size_t)s * D.T3 + t3) * NV + 3 + p0 * D.T1 + tt) * n;
+                            R2 term = make_vec2<R>(0, 0);
+                            if (qv) {
+                                R2 r = rv[q];
+                                R Rr = r.x, Ri = -r.y;
+                                term.x = A::add(A::mul(gq.y, Rr), A::mul(gq.x, Ri));
+                                term.y = A::sub(A::mul(gq.x, Rr), A::mul(Ri, gq.y));
+                            }
+                            double2 d = duo_dot<R>(term, red, par, half, lane, n, bar);
+                            if (half == 0 && lane == 0) D.eaI[(((size_t)s * D.T3 + t3) * 21 + m) * D.T1 + tt] = d;
+                        }
+                    } else {
+                        int p1 = c_px[m][1];
+                        const R2 *rv = (const R2 *)D.SE + (((size_t)s * D.T3 + t3) * NV + p1) * n;
+                        R2 term = make_vec2<R>(0, 0);
+                        if (qv) {
+                            R2 r = rv[q];
+                            R nr = r.x, ni = -r.y;
+                            term.x = A::add(A::mul(nr, gq.y), A::mul(ni, gq.x));
+                            term.y = A::sub(A::mul(nr, gq.x), A::mul(ni, gq.y));
+                        }
+                        double2 d = duo_dot<R>(term, red, par, half, lane, n, bar);
+                        if (half == 0 && lane == 0) D.eaII[(((size_t)s * D.T3 + t3) * 21 + m) * D.T1 + t1] = d;
+                    }
+                }
+            }
+        }
+        if (t3 == D.T3 - 1) break;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) dg[i] = traj_diag(D.T, tl, i, false);
+        __syncthreads();
+        doubles_half_phases<R>(D, Uh, dg, tl, n, Wd);
+        __syncthreads();
+        const Dcoef<R> *cf = D.rot_static ? cf_static : cf_static + (tl - D.f0) * D.K;
+        if (active)
+            for (int sub = 0; sub < D.ts; sub++) {
+                if (D.es) doubles_substep_duo<R, true>(F, Uh, cf, D.pairs, D.K, n, Wd, t64, cidx, bar);
+                else doubles_substep_duo<R, false>(F, Uh, cf, D.pairs, D.K, n, Wd, t64, cidx, bar);
+            }
     }
 }
 
@@ -1010,7 +1256,22 @@ int run_chunk(nise_ctx *c, TwoD &D, Dcoef<R> *cf) {
         size_t dsm = bytes(nwarps, use_tab);
         if (dsm > 220 * 1024) return (int)cudaErrorNotSupported;
         int vps = 9 + 9 * D.T1, cps = (vps + nwarps - 1) / nwarps;
-        if (D.n <= 32) {
+        // two warps per vector (k2d_doubles_duo, the same float operations)
+        // unless kernel_config 1 asks for one
+        auto bytes_duo = [&](int pairs, bool tab) {
+            return sizeof(R2) * ((size_t)slots * (1 + pairs) + 64 * (size_t)pairs) + sizeof(float) * 7 * D.n +
+                   (tab ? sizeof(short) * D.n * D.n : 0);
+        };
+        if (D.n > 32 && D.n <= 64 && c->p.kernel_config != 1) {
+            int np = 11;  // 704 threads at most; named barriers 1..11
+            while (np > 1 && bytes_duo(np, false) > 220 * 1024) np--;
+            const int tab = bytes_duo(np, true) <= 220 * 1024;
+            const size_t dsm2 = bytes_duo(np, tab);
+            if (dsm2 > 220 * 1024) return (int)cudaErrorNotSupported;
+            const int cps2 = (vps + np - 1) / np;
+            if ((e = smem_attr(k2d_doubles_duo<R>, dsm2))) return e;
+            k2d_doubles_duo<R><<<D.S * cps2, 64 * np, dsm2, st>>>(D, vps, cf, tab);
+        } else if (D.n <= 32) {
             if ((e = smem_attr(k2d_doubles<R, 1>, dsm))) return e;
             k2d_doubles<R, 1><<<D.S * cps, 32 * nwarps, dsm, st>>>(D, vps, cf, use_tab);
         } else if (D.n <= 64) {
@@ -1118,7 +1379,7 @@ extern "C" int nise_2dir(nise_ctx *c, double *R, int *sample_count) {
     D.rot_static = p.hamiltonian == NISE_HAM_COUPLING;
     if (ea) {  // doubles coupling coefficients: once (static couplings) or per frame
         long ncf = D.rot_static ? 1 : nf;
-        if ((rc = dcoef.alloc(c, 4 * rsz * (size_t)ncf * (D.K ? D.K : 1)))) return rc;
+        if ((rc = dcoef.alloc(c, 4 * rsz * ((size_t)ncf * D.K + 1)))) return rc;  // one record past the last
         long tot = ncf * D.K;
         if (tot > 0) {
             if (prec == NISE_FP32)

@@ -181,3 +181,27 @@ def test_driver_writes_reference_files(tmp_path):
     for k, fn in enumerate(oracle.R2D_FILES):
         got[k, 0], got[k, 1] = oracle.read_2d(str(tmp_path / fn), T1, T1)
     assert helpers.rel2d(got, g) < REF_FP32_SUMS
+
+
+@pytest.mark.parametrize("n_sites, tech, prec", [(40, "2DIR", "fp32"), (64, "2DIR", "fp32"), (64, "2DIR", "fp64"),
+                                                 (48, "2DUVvis", "fp32")])
+def test_two_warp_doubles_kernel_is_bitwise_the_one_warp_kernel(n_sites, tech, prec, tmp_path):
+    """For 32 < N <= 64 the doubles vectors run on two warps each (one
+    column per thread, named barriers where the rotations cross warps);
+    kernel_config 1 keeps one warp per vector.  Same float operations in the
+    same order: in FP32, whose operations are all separately rounded, the
+    responses are bitwise equal; FP64 lets the compiler fuse multiply-adds,
+    differently in the two kernels."""
+    s = synth.c2_spec(n_sites=n_sites, frames=240, seed=60 + n_sites)
+    files = synth.write(s, str(tmp_path))
+    extra = dict(Anharmonicity=0) if tech == "2DUVvis" else {}
+    kw = synth.c2_keywords(Singles=n_sites, Length=240, RunTimes="6 0 6", Samplerate=70, Technique=tech, **extra)
+    precision = nise.FP64 if prec == "fp64" else nise.FP32
+    _, R2w, n2 = run(kw, files, precision=precision)
+    _, R1w, n1 = run(kw, files, precision=precision, kernel_config=1)
+    assert n1 == n2 > 0
+    if prec == "fp32":
+        assert np.array_equal(R2w, R1w)
+    else:
+        assert helpers.rel2d(R2w, R1w) < 1e-12
+    assert np.abs(R2w).max() > 0
