@@ -37,6 +37,8 @@ struct SinglesTab {
     long f0;                  // first frame of the tables
     const int2 *pairs;        // Trotter pattern (a < b, lexicographic)
     int K;
+    const int4 *segs;         // the pattern in segments of one first site a and one warp of
+    int nsegs;                // second sites (b >> 5): (a, first, end, b >> 5)
     const void *U, *rot;      // Trotter tables
     int rot_static;
     const int2 *ent;          // RK4 entries (a <= b)

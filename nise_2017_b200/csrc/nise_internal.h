@@ -105,6 +105,7 @@ template <typename T> struct DevBuf {
 // propagators Us[t][n][n] when requested).
 struct SinglesBufs {
     DevBuf<int2> pairs, ent;
+    DevBuf<int4> segs;
     DevBuf<char> U, rot, rkval;
     const void *Us = nullptr;
 };

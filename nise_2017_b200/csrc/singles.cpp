@@ -25,14 +25,25 @@ int nise_singles_tables(nise_ctx *c, const DevTraj &T, long fmin, long nf, int s
     std::vector<int2> pairs;
     if ((rc = nise_pattern(c, fmin, nf, pairs))) return rc;
     const int K = (int)pairs.size();
+    // segments of one first site and one warp (b >> 5) of second sites, for
+    // the doubles kernel that shares a vector between two warps
+    std::vector<int4> segs;
+    for (int k = 0; k < K;) {
+        const int a = pairs[k].x, w = pairs[k].y >> 5, k0 = k;
+        while (k < K && pairs[k].x == a && (pairs[k].y >> 5) == w) k++;
+        segs.push_back(make_int4(a, k0, k, w));
+    }
+    if (segs.empty()) segs.push_back(make_int4(0, 0, 0, 0));
     pairs.push_back(make_int2(0, 0));  // one record past the last: read ahead without a bound check
-    if ((rc = B.pairs.upload(c, pairs))) return rc;
+    if ((rc = B.pairs.upload(c, pairs)) || (rc = B.segs.upload(c, segs))) return rc;
     S.n = N;
     S.ts = p.ts;
     S.prop = p.propagation;
     S.f0 = fmin;
     S.pairs = B.pairs.p;
     S.K = K;
+    S.segs = B.segs.p;
+    S.nsegs = K ? (int)segs.size() : 0;
     S.U = S.rot = S.rkval = S.Ud = nullptr;
     S.ent = nullptr;
     S.Kr = 0;

@@ -553,23 +553,94 @@ __global__ void __launch_bounds__(512, 1) k2d_doubles(TwoD D, int vec_per_sample
 // pair (c = 32 * half + lane) owns column c of |ac>, so a CTA runs twice the
 // warps of k2d_doubles on the same shared memory.  Each thread performs the
 // float operations k2d_doubles performs for that column, in the same order,
-// so the results are bitwise those of k2d_doubles.
+// so the results are bitwise those of k2d_doubles in FP32.
 //
-// Ordering.  Within one run of couplings (a, b) with the same first site a,
-// coupling (a, b) touches |bc> (thread c, every c != a) and |aa> (thread b),
-// coupling (a, b') touches |b'c> and |aa>; the only shared elements are |bb'>
-// (threads b' then b) and |aa> (threads b then b').  Two couplings of a run
-// therefore only need ordering across the pair when b and b' belong to
-// different warps: a __syncwarp orders every coupling, and the pair's named
-// barrier is taken when the warp owning b changes within a run, and around
-// the pivot change (row a stored back by every column, the next row loaded;
-// thread c loads |a c>, which thread a stored).
+// Ordering.  The couplings run in segments of one first site a and one warp
+// of second sites b (the "owner" warp: b >> 5).  Coupling (a, b) touches
+// |bc> (thread c, every c != a) and |aa> (thread b).  Within a segment:
+//  * two couplings (a, b), (a, b') share only |bb'> (threads b' then b) and
+//    |aa> (threads b then b'), all in the owner warp: a __syncwarp per
+//    coupling orders them there;
+//  * a thread c of the other warp touches only |bc> with b in the owner
+//    warp, elements no other thread touches in the segment: it runs its
+//    rotations with no synchronisation, and loads the elements of several
+//    couplings ahead of its stores.
+// The pair's named barrier separates segments (and the pivot change, where
+// row a is stored back by every column and the next row loaded: thread c
+// loads |a c>, which thread a stored).
 __device__ __forceinline__ void duo_sync(int id) { asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory"); }
+
+// The owner warp's couplings [k0, k1) of a segment: the sqrt(2) rotation
+// (|aa>,|ab>) by thread b, then (|ac>,|bc>) for every c != a ((|ab>,|bb>) at
+// sqrt(2) for c == b; absent for c == b with two-level sites).
+template <typename R, bool ES>
+__device__ __forceinline__ void duo_owner(typename Vec2<R>::T *F, typename Vec2<R>::T &piv, const Dcoef<R> *cf,
+                                          const int2 *pairs, int k0, int k1, int ix_aa, bool act, int c,
+                                          const short *cic, int n, int W) {
+    typedef typename Vec2<R>::T R2;
+    if (k0 >= k1) return;
+    int b_next = pairs[k0].y;  // the arrays hold one record past the last coupling
+    Dcoef<R> q_next = cf[k0];
+    for (int k = k0; k < k1; k++) {
+        const int b = b_next;
+        const Dcoef<R> q = q_next;
+        b_next = pairs[k + 1].y;
+        q_next = cf[k + 1];
+        if (!ES && c == b) {
+            R2 X = F[ix_aa];
+            rot2<R>(X, piv, q.co2, q.si2);
+            F[ix_aa] = X;
+        }
+        if (act && !(ES && c == b)) {
+            const bool sp = c == b;
+            const int iq = cic ? cic[b * n] : circ(b, c, n, W);
+            R2 Q = F[iq];
+            rot2<R>(piv, Q, sp ? q.co2 : q.co, sp ? q.si2 : q.si);
+            F[iq] = Q;
+        }
+        __syncwarp();
+    }
+}
+
+// The other warp's couplings [k0, k1): (|ac>,|bc>) on private elements, four
+// couplings' loads ahead of their rotations.
+template <typename R>
+__device__ __forceinline__ void duo_free(typename Vec2<R>::T *F, typename Vec2<R>::T &piv, const Dcoef<R> *cf,
+                                         const int2 *pairs, int k0, int k1, int c, const short *cic, int n, int W) {
+    typedef typename Vec2<R>::T R2;
+    int k = k0;
+    for (; k + 4 <= k1; k += 4) {
+        int iq[4];
+        R2 Q[4];
+        Dcoef<R> q[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int b = pairs[k + u].y;
+            q[u] = cf[k + u];
+            iq[u] = cic ? cic[b * n] : circ(b, c, n, W);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) Q[u] = F[iq[u]];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            rot2<R>(piv, Q[u], q[u].co, q[u].si);
+            F[iq[u]] = Q[u];
+        }
+    }
+    for (; k < k1; k++) {
+        const int b = pairs[k].y;
+        const Dcoef<R> q = cf[k];
+        const int iq = cic ? cic[b * n] : circ(b, c, n, W);
+        R2 Q = F[iq];
+        rot2<R>(piv, Q, q.co, q.si);
+        F[iq] = Q;
+    }
+}
 
 template <typename R, bool ES>
 __device__ void doubles_substep_duo(typename Vec2<R>::T *F, const typename Vec2<R>::T *Uh, const Dcoef<R> *cf,
-                                    const int2 *pairs, int K, int n, int W, int t64, const short *__restrict__ ci,
-                                    int bar) {
+                                    const int2 *pairs, const int4 *segs, int nsegs, int n, int W, int t64, int half,
+                                    const short *__restrict__ ci, int bar) {
     typedef typename Vec2<R>::T R2;
     typedef Ar<R> A;
     const int slots = n * W, c = t64;
@@ -582,43 +653,23 @@ __device__ void doubles_substep_duo(typename Vec2<R>::T *F, const typename Vec2<
         F[e] = o;
     }
     duo_sync(bar);
-    int cur_a = -1, cur_w = -1, ix_aa = 0;
+    int cur_a = -1, ix_aa = 0;
     R2 piv = make_vec2<R>(0, 0);
-    // the pair and coefficient arrays hold one record past K, so the next
-    // record is loaded without a bound check
-    int2 ab_next = pairs[0];
-    Dcoef<R> q_next = cf[0];
-    for (int k = 0; k < K; k++) {
-        const int a = ab_next.x, b = ab_next.y;
-        const Dcoef<R> q = q_next;
-        ab_next = pairs[k + 1];
-        q_next = cf[k + 1];
+    for (int g = 0; g < nsegs; g++) {
+        const int4 sg = segs[g];  // (a, first coupling, end, owner warp)
+        const int a = sg.x;
         if (a != cur_a) {
             if (cur_a >= 0 && col && c != cur_a) F[cic ? cic[cur_a * n] : circ(cur_a, c, n, W)] = piv;
             duo_sync(bar);
             if (col && c != a) piv = F[cic ? cic[a * n] : circ(a, c, n, W)];
             ix_aa = ci ? ci[a * n + a] : circ(a, a, n, W);
             cur_a = a;
-            cur_w = b >> 5;
-        } else if ((b >> 5) != cur_w) {
+        } else {
             duo_sync(bar);
-            cur_w = b >> 5;
         }
-        // c == a case: (|aa>,|ab>) with the sqrt(2) angle, by the thread owning c = b
-        if (!ES && c == b) {
-            R2 X = F[ix_aa];
-            rot2<R>(X, piv, q.co2, q.si2);
-            F[ix_aa] = X;
-        }
-        // every other column c != a: (|ac>,|bc>); for c == b that is (|ab>,|bb>) at sqrt(2)
-        if (col && c != a && !(ES && c == b)) {
-            const bool sp = c == b;
-            const int iq = cic ? cic[b * n] : circ(b, c, n, W);
-            R2 Q = F[iq];
-            rot2<R>(piv, Q, sp ? q.co2 : q.co, sp ? q.si2 : q.si);
-            F[iq] = Q;
-        }
-        __syncwarp();
+        const bool act = col && c != a;
+        if (half == sg.w) duo_owner<R, ES>(F, piv, cf, pairs, sg.y, sg.z, ix_aa, act, c, cic, n, W);
+        else if (act) duo_free<R>(F, piv, cf, pairs, sg.y, sg.z, c, cic, n, W);
     }
     if (cur_a >= 0 && col && c != cur_a) F[cic ? cic[cur_a * n] : circ(cur_a, c, n, W)] = piv;
     duo_sync(bar);
@@ -769,8 +820,8 @@ __global__ void __launch_bounds__(768, 1) k2d_doubles_duo(TwoD D, int vec_per_sa
         const Dcoef<R> *cf = D.rot_static ? cf_static : cf_static + (tl - D.f0) * D.K;
         if (active)
             for (int sub = 0; sub < D.ts; sub++) {
-                if (D.es) doubles_substep_duo<R, true>(F, Uh, cf, D.pairs, D.K, n, Wd, t64, cidx, bar);
-                else doubles_substep_duo<R, false>(F, Uh, cf, D.pairs, D.K, n, Wd, t64, cidx, bar);
+                if (D.es) doubles_substep_duo<R, true>(F, Uh, cf, D.pairs, D.segs, D.nsegs, n, Wd, t64, half, cidx, bar);
+                else doubles_substep_duo<R, false>(F, Uh, cf, D.pairs, D.segs, D.nsegs, n, Wd, t64, half, cidx, bar);
             }
     }
 }
