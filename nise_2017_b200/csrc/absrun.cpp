@@ -169,6 +169,7 @@ struct AbsRun {
     DevBuf<int> estatus;
     DevBuf<float> tcX;           // state columns of the tensor-core apply
     bool use_tc = false;
+    bool stream_u = false;  // propagators built and applied chunk by chunk (tensor cores, batched)
     long FC = 1;
     bool truncated = false;
     double fe = 0;
@@ -317,17 +318,35 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
         const bool eigen_route = truncated || p.hamiltonian != NISE_HAM_COUPLING || p.kernel_config == 2;
         if (eigen_route) {
             scheme = SCHEME_EIGEN;
-            if (N > 1024)
+            // FP32 above the Jacobi's size: U applied on the tensor cores
+            // (kernel_config 16: the per-start-point kernel, 17: the tensor
+            // cores at any size).  Batched, the tensor-core apply runs frame
+            // by frame, so the propagators are built and applied in chunks
+            // and only a chunk of them is held: up to 2048 sites (the
+            // eigensolver's shared memory), else every frame's U is held.
+            AbsJob Jt = J;
+            if (plain) Jt.nsamp = 1;
+            use_tc = prec == NISE_FP32 && tc_dia_fits(Jt, N) &&
+                     (p.kernel_config == 17 || (N > NISE_EIG_MAX_N && p.kernel_config != 16));
+            stream_u = use_tc && !plain;
+            if (N > (stream_u ? 2048 : 1024))
                 return nise_fail(c, NISE_ERR_UNSUPPORTED,
                                  "the eigen route (Threshold > 0, per-frame couplings, kernel_config 2) is limited to "
-                                 "1024 sites");
-            const size_t ubytes = r2 * (size_t)nf * N * N;
+                                 "%d sites here (2048 with the tensor-core apply of a batched FP32 job)",
+                                 stream_u ? 2048 : 1024);
+            // frames per eigensolver launch (one CTA per frame): a wave of
+            // the 148 SMs, or as many as 1 GB of eigenvectors, QR workspace
+            // (and streamed U) holds, at most 16 GB
+            const size_t per_frame = sizeof(double) * (size_t)N * N * (N > NISE_EIG_MAX_N ? 2 : 1) +
+                                     (stream_u ? r2 * (size_t)N * N : 0);
+            FC = std::max(148L, (long)(((size_t)1 << 30) / per_frame));
+            FC = std::max(1L, std::min(std::min(nf, FC), (long)(((size_t)16 << 30) / per_frame)));
+            const size_t ubytes = r2 * (size_t)(stream_u ? FC : nf) * N * N;
             if (ubytes > ((size_t)64 << 30))
                 return nise_fail(c, NISE_ERR_NOMEM,
                                  "eigen route: %ld frames of %d sites need more than 64 GB of propagators", nf, N);
             std::vector<long> frames(nf);
             for (long t = 0; t < nf; t++) frames[t] = f0 + t;
-            FC = std::max(1L, std::min(nf, (long)(((size_t)512 << 20) / (sizeof(double) * (size_t)N * N))));
             if ((rc = Ue.alloc(c, ubytes)) || (rc = efr.upload(c, frames)) || (rc = eV.alloc(c, (size_t)FC * N * N)) ||
                 (rc = ew.alloc(c, (size_t)FC * N)) || (rc = eA.alloc(c, eig_any_ws_doubles(N, FC))) ||
                 (rc = estatus.alloc(c, 1)))
@@ -335,13 +354,6 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
             cudaMemsetAsync(estatus.p, 0, sizeof(int), c->stream);
             // propagate_vec_DIA: f = deltat*icm2ifs*twoPi*sign in float, one full step
             fe = prec == NISE_FP32 ? (double)J.f32_full : J.f;
-            // FP32 above the Jacobi's size: U applied on the tensor cores
-            // (kernel_config 16: the per-start-point kernel, 17: the tensor
-            // cores at any size)
-            AbsJob Jt = J;
-            if (plain) Jt.nsamp = 1;
-            use_tc = prec == NISE_FP32 && tc_dia_fits(Jt, N) &&
-                     (p.kernel_config == 17 || (N > NISE_EIG_MAX_N && p.kernel_config != 16));
             if (use_tc && ((rc = tcX.alloc(c, (size_t)4 * tc_dia_columns(Jt) * N)) || (rc = derr.alloc(c, 1))))
                 return rc;
             if (use_tc) cudaMemsetAsync(derr.p, 0, sizeof(int), c->stream);
@@ -706,6 +718,25 @@ int AbsRun::run_main(cudaStream_t s, int cfg, double2 *dst) {
             return launch_abs_taylor(pr, T, P, Js, r, cfg == 10 || cfg >= 13 ? 8 : cfg < 0 ? -cfg : cfg, s, &kernels);
         }
         default:
+            if (stream_u) {
+                // chunks of FC frames: eigendecompositions, propagators, then
+                // the tensor-core steps of those frames
+                EigJob EJ;
+                EJ.T = T;
+                EJ.n = N;
+                EJ.singleshift = c->nshift > 0;
+                int er = 0;
+                for (long q = 0; q < nf && !er; q += FC) {
+                    const long m = std::min(FC, nf - q);
+                    if ((er = launch_eig_any(EJ, efr.p + q, m, eV.p, ew.p, eA.p, estatus.p, s))) break;
+                    if ((er = launch_build_u_any(pr, eV.p, ew.p, m, N, fe, c->thres, truncated, Ue.p, s))) break;
+                    // the last chunk runs on to the last response frame, which needs no propagator
+                    const long tb = q + m >= nf ? tc_dia_last_frame(Js) : f0 + q + m - 1;
+                    er = launch_abs_dia_tc_frames(T, Ue.p, f0 + q, N, Js, r, tcX.p, derr.p, f0 + q, tb, s);
+                    kernels += 2;
+                }
+                return er;
+            }
             if (use_tc) return launch_abs_dia_tc(T, Ue.p, f0, N, Js, r, tcX.p, derr.p, s);
             return launch_abs_dia(pr, T, Ue.p, f0, N, Js, r, s);
         }
@@ -874,7 +905,7 @@ int AbsRun::enqueue(cudaStream_t s, bool events) {
         EJ.n = N;
         EJ.singleshift = c->nshift > 0;
         const size_t r2 = prec == NISE_FP32 ? sizeof(float2) : sizeof(double2);
-        for (long q = 0; q < nf; q += FC) {
+        for (long q = 0; q < nf && !stream_u; q += FC) {  // streamed: built inside the propagation
             long m = std::min(FC, nf - q);
             if ((rc = nise_cuda(c, launch_eig_any(EJ, efr.p + q, m, eV.p, ew.p, eA.p, estatus.p, s), "eigensolver")))
                 return rc;

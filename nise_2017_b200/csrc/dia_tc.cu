@@ -352,25 +352,39 @@ int tc_dia_columns(const AbsJob &J) {
 
 bool tc_dia_fits(const AbsJob &J, int n) { return n >= 1 && tc_dia_columns(J) <= 64; }
 
-// The job's frames in order: starts and responses on frame t, then the step
-// with U_t for every frame some vector still propagates through.  X holds
-// 4 planes of cols x n floats (two ping-pong state buffers, real and imaginary).
-int launch_abs_dia_tc(const DevTraj &T, const void *U, long f0, int n, const AbsJob &J, double2 *resp, float *X,
-                      int *err, cudaStream_t s) {
+long tc_dia_first_frame(const AbsJob &J) { return (long)J.begin * J.sample; }
+long tc_dia_last_frame(const AbsJob &J) { return (long)(J.begin + J.nsamp - 1) * J.sample + J.tmax - 1; }
+
+// Frames ta..tb of the job in order: starts and responses on frame t, then the
+// step with U_t (at U + (t - ufirst) n^2) for every frame some vector still
+// propagates through.  X holds 4 planes of cols x n floats (two ping-pong
+// state buffers, real and imaginary); it is cleared when ta is the job's
+// first frame, and frame t's state is in the first pair of planes when
+// t - first frame is even.
+int launch_abs_dia_tc_frames(const DevTraj &T, const void *U, long ufirst, int n, const AbsJob &J, double2 *resp,
+                             float *X, int *err, long ta, long tb, cudaStream_t s) {
     if (J.nsamp <= 0) return 0;
     const int cols = tc_dia_columns(J);
     if (cols > 64) return (int)cudaErrorNotSupported;
     const int slots = (J.tmax - 1) / J.sample + 1;
-    cudaError_t e = cudaMemsetAsync(X, 0, sizeof(float) * 4 * (size_t)cols * n, s);
-    if (e != cudaSuccess) return (int)e;
+    const long tfirst = tc_dia_first_frame(J), tlast = tc_dia_last_frame(J);
+    ta = std::max(ta, tfirst);
+    tb = std::min(tb, tlast);
+    if (ta > tb) return 0;
+    if (ta == tfirst) {
+        cudaError_t e = cudaMemsetAsync(X, 0, sizeof(float) * 4 * (size_t)cols * n, s);
+        if (e != cudaSuccess) return (int)e;
+    }
     float *cr = X, *ci = X + (size_t)cols * n, *nr = ci + (size_t)cols * n, *ni = nr + (size_t)cols * n;
-    const long tfirst = (long)J.begin * J.sample;
-    const long tlast = (long)(J.begin + J.nsamp - 1) * J.sample + J.tmax - 1;  // last response
+    if ((ta - tfirst) & 1) {
+        std::swap(cr, nr);
+        std::swap(ci, ni);
+    }
     const int ncol = 3 * std::min(slots, J.nsamp);
-    for (long t = tfirst; t <= tlast; t++) {
+    for (long t = ta; t <= tb; t++) {
         k_tc_resp<<<ncol, 256, 0, s>>>(T, J, n, t, slots, cr, ci, resp);
         if (t == tlast) break;
-        const float2 *Ut = (const float2 *)U + (size_t)(t - f0) * n * n;
+        const float2 *Ut = (const float2 *)U + (size_t)(t - ufirst) * n * n;
         int rc;
         switch (cols) {
         case 16: rc = run_tc_apply<16>(Ut, n, cr, ci, nr, ni, err, s); break;
@@ -383,4 +397,10 @@ int launch_abs_dia_tc(const DevTraj &T, const void *U, long f0, int n, const Abs
         std::swap(ci, ni);
     }
     return (int)cudaGetLastError();
+}
+
+// Every frame of the job, the propagators of frames f0.. all in U.
+int launch_abs_dia_tc(const DevTraj &T, const void *U, long f0, int n, const AbsJob &J, double2 *resp, float *X,
+                      int *err, cudaStream_t s) {
+    return launch_abs_dia_tc_frames(T, U, f0, n, J, resp, X, err, tc_dia_first_frame(J), tc_dia_last_frame(J), s);
 }

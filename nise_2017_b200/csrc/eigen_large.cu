@@ -61,14 +61,14 @@ __global__ void __launch_bounds__(kEgNT) k_eig_large(EigJob J, const long *frame
     const DevTraj &T = J.T;
 
     // the frame's shifted, cut Hamiltonian (read_He / read_Hamiltonian)
-    for (size_t q = tid; q < (size_t)n * n; q += kEgNT) {
-        const int i = (int)(q / n), j = (int)(q % n);
-        double h;
-        if (i == j) h = (double)traj_diag(T, t, i, J.singleshift != 0);
-        else h = (double)traj_coupling(T, t, min(i, j), max(i, j));
-        A[q] = h;
-        Z[q] = i == j ? 1.0 : 0.0;
-    }
+    for (int i = warp; i < n; i += kEgNW)
+        for (int j = lane; j < n; j += 32) {
+            double h;
+            if (i == j) h = (double)traj_diag(T, t, i, J.singleshift != 0);
+            else h = (double)traj_coupling(T, t, min(i, j), max(i, j));
+            A[(size_t)i * n + j] = h;
+            Z[(size_t)i * n + j] = i == j ? 1.0 : 0.0;
+        }
     __syncthreads();
 
     // 1. tridiagonalisation
@@ -114,9 +114,10 @@ __global__ void __launch_bounds__(kEgNT) k_eig_large(EigJob J, const long *frame
         for (int i = tid; i < m; i += kEgNT) p[i] -= K * v[i];  // w
         __syncthreads();
         // A[k+1:, k+1:] -= v w^T + w v^T
-        for (size_t q = tid; q < (size_t)m * m; q += kEgNT) {
-            const int i = (int)(q / m), j = (int)(q % m);
-            A[(size_t)(k + 1 + i) * n + k + 1 + j] -= v[i] * p[j] + p[i] * v[j];
+        for (int i = warp; i < m; i += kEgNW) {
+            double *ar = A + (size_t)(k + 1 + i) * n + k + 1;
+            const double vi = v[i], pi = p[i];
+            for (int j = lane; j < m; j += 32) ar[j] -= vi * p[j] + pi * v[j];
         }
         // keep v_k in row k right of the diagonal (its first entry, 1, implied)
         for (int i = tid; i < m; i += kEgNT) A[(size_t)k * n + k + 1 + i] = v[i];
@@ -164,24 +165,40 @@ __global__ void __launch_bounds__(kEgNT) k_eig_large(EigJob J, const long *frame
                 // Wilkinson shift from the trailing 2x2 of the block
                 const double dd = 0.5 * (d[m - 1] - d[m]), bm = e[m - 1];
                 const double mu = d[m] - bm * bm / (dd + copysign(hyp(dd, bm), dd == 0.0 ? 1.0 : dd));
+                // the active 2x2 (a, bb; bb, cc) and the bulge travel in
+                // registers; d[k+2] and e[k+1] are read one rotation ahead
                 double x = d[l] - mu, z = e[l];
+                double a = d[l], bb = e[l], cc = d[l + 1];
                 for (int k = l; k < m; k++) {
-                    const double r = hyp(x, z);
-                    const double c = r == 0.0 ? 1.0 : x / r, s = r == 0.0 ? 0.0 : z / r;
-                    if (k > l) e[k - 1] = r;
-                    // T <- G T G^T on rows/columns k, k+1 (G = [c s; -s c])
-                    const double a = d[k], bb = e[k], cc = d[k + 1];
-                    d[k] = c * c * a + 2.0 * c * s * bb + s * s * cc;
-                    d[k + 1] = s * s * a - 2.0 * c * s * bb + c * c * cc;
-                    e[k] = c * s * (cc - a) + (c * c - s * s) * bb;
-                    if (k + 1 < m) {
-                        const double bn = e[k + 1];
-                        x = e[k];
-                        z = s * bn;  // the bulge at (k, k+2)
-                        e[k + 1] = c * bn;
+                    const double bn = k + 1 < m ? e[k + 1] : 0.0, dn = k + 1 < m ? d[k + 2] : 0.0;
+                    // G = [c s; -s c] with c = x / r, s = z / r, r = sqrt(x^2 + z^2)
+                    const double rr = x * x + z * z;
+                    double c = 1.0, s = 0.0, r = 0.0;
+                    if (rr > 0.0) {
+                        const double ri = rsqrt(rr);
+                        c = x * ri;
+                        s = z * ri;
+                        r = rr * ri;
                     }
+                    if (k > l) e[k - 1] = r;
+                    // T <- G T G^T on rows/columns k, k+1
+                    const double c2 = c * c, s2 = s * s, c2s = 2.0 * c * s;
+                    const double dk = c2 * a + c2s * bb + s2 * cc;
+                    const double dk1 = s2 * a - c2s * bb + c2 * cc;
+                    const double ek = c * s * (cc - a) + (c2 - s2) * bb;
+                    d[k] = dk;
                     cs[2 * k] = c;
                     cs[2 * k + 1] = s;
+                    if (k + 1 < m) {
+                        x = ek;
+                        z = s * bn;  // the bulge at (k, k+2)
+                        a = dk1;
+                        bb = c * bn;
+                        cc = dn;
+                    } else {
+                        d[k + 1] = dk1;
+                        e[k] = ek;
+                    }
                 }
             }
         }
@@ -193,27 +210,43 @@ __global__ void __launch_bounds__(kEgNT) k_eig_large(EigJob J, const long *frame
             break;
         }
         // Z <- Z G^T for the step's rotations: component i of eigenvectors k, k+1
-        for (int i = tid; i < n; i += kEgNT) {
-            double zk = Z[(size_t)l * n + i];
+        // two components per thread at a time (independent chains), eight
+        // rows ahead of the rotations
+        for (int i0 = tid; i0 < n; i0 += 2 * kEgNT) {
+            const int i1 = i0 + kEgNT;
+            const bool two = i1 < n;
+            const int j1 = two ? i1 : i0;  // a second chain on the same column when there is none
+            double *z0p = Z + i0, *z1p = Z + j1;
+            double zk0 = z0p[(size_t)l * n], zk1 = z1p[(size_t)l * n];
             int k = l;
-            for (; k + 4 <= m; k += 4) {
-                const double z1 = Z[(size_t)(k + 1) * n + i], z2 = Z[(size_t)(k + 2) * n + i];
-                const double z3 = Z[(size_t)(k + 3) * n + i], z4 = Z[(size_t)(k + 4) * n + i];
-                const double zz[4] = {z1, z2, z3, z4};
+            for (; k + 8 <= m; k += 8) {
+                double a0[8], a1[8];
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
+                for (int q = 0; q < 8; q++) {
+                    a0[q] = z0p[(size_t)(k + 1 + q) * n];
+                    a1[q] = z1p[(size_t)(k + 1 + q) * n];
+                }
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
                     const double c = cs[2 * (k + q)], s = cs[2 * (k + q) + 1];
-                    Z[(size_t)(k + q) * n + i] = c * zk + s * zz[q];
-                    zk = -s * zk + c * zz[q];
+                    const double o0 = c * zk0 + s * a0[q], o1 = c * zk1 + s * a1[q];
+                    zk0 = -s * zk0 + c * a0[q];
+                    zk1 = -s * zk1 + c * a1[q];
+                    z0p[(size_t)(k + q) * n] = o0;
+                    if (two) z1p[(size_t)(k + q) * n] = o1;
                 }
             }
             for (; k < m; k++) {
                 const double c = cs[2 * k], s = cs[2 * k + 1];
-                const double z1 = Z[(size_t)(k + 1) * n + i];
-                Z[(size_t)k * n + i] = c * zk + s * z1;
-                zk = -s * zk + c * z1;
+                const double a0 = z0p[(size_t)(k + 1) * n], a1 = z1p[(size_t)(k + 1) * n];
+                const double o0 = c * zk0 + s * a0, o1 = c * zk1 + s * a1;
+                zk0 = -s * zk0 + c * a0;
+                zk1 = -s * zk1 + c * a1;
+                z0p[(size_t)k * n] = o0;
+                if (two) z1p[(size_t)k * n] = o1;
             }
-            Z[(size_t)m * n + i] = zk;
+            z0p[(size_t)m * n] = zk0;
+            if (two) z1p[(size_t)m * n] = zk1;
         }
         __syncthreads();
     }

@@ -164,15 +164,22 @@ int launch_step_taylor(int prec, int n, const float *H, void *re, void *im, int 
 // when `truncate`, zeroed where |U_ac|^2 <= thres (propagate_vec_DIA_S).
 int launch_build_u(int prec, const double *V, const double *w, long nfr, int n, double f, float thres, int truncate,
                    void *U, cudaStream_t s);
-// Linear absorption of the start points of J with the per-frame propagators
-// U (frames from f0): one CTA per start point, n <= 1024.
 // The eigen-route absorption with the propagators applied on the tensor cores
 // (FP32, time-major; dia_tc.cu): X is 4 * tc_dia_columns(J) * n floats of
-// workspace, err a device flag set when a bounded wait gives up.
+// workspace, err a device flag set when a bounded wait gives up.  The
+// _frames form runs frames ta..tb (clipped to the job's first and last
+// frames) with the propagator of frame t at U + (t - ufirst) n^2, so the
+// propagators can be built and applied chunk by chunk.
 int tc_dia_columns(const AbsJob &J);
 bool tc_dia_fits(const AbsJob &J, int n);
+long tc_dia_first_frame(const AbsJob &J);
+long tc_dia_last_frame(const AbsJob &J);
 int launch_abs_dia_tc(const DevTraj &T, const void *U, long f0, int n, const AbsJob &J, double2 *resp, float *X,
                       int *err, cudaStream_t s);
+int launch_abs_dia_tc_frames(const DevTraj &T, const void *U, long ufirst, int n, const AbsJob &J, double2 *resp,
+                             float *X, int *err, long ta, long tb, cudaStream_t s);
+// Linear absorption of the start points of J with the per-frame propagators
+// U (frames from f0): one CTA per start point, n <= 1024.
 int launch_abs_dia(int prec, const DevTraj &T, const void *U, long f0, int n, const AbsJob &J, double2 *resp,
                    cudaStream_t s);
 

@@ -160,3 +160,25 @@ def test_tensor_core_apply_wide_state(tmp_path):
           % (helpers.rel(r32, ex_re + 1j * ex_im), helpers.rel(sc, ex_re + 1j * ex_im)))
     assert helpers.rel(r32, ex_re + 1j * ex_im) < SPARSE_FP32
     assert helpers.rel(r32, sc) < TC_VS_SCALAR
+
+
+def test_streamed_propagators_above_1024_sites(tmp_path):
+    """A batched FP32 eigen-route job builds and applies the propagators in
+    chunks of frames (only a chunk of U is held), which takes it past 1024
+    sites: 1100 sites, per-frame couplings, against the FP64 exact
+    restatement."""
+    s = synth.spec(n_sites=1100, frames=24, geometry=synth.LATTICE, spacing=8.0, eps0=15000.0, sigma=300.0,
+                   tau_fs=50.0, jcut=2.0, dt_fs=1.0, seed=450)
+    files = synth.write(s, str(tmp_path))
+    kw = synth.c1_keywords(Singles=1100, Length=24, RunTimes="4 0 0", Samplerate=10, HamiltonianType="Full")
+    ex_re, ex_im, en = oracle.absorption_exact(kw, files)
+    r32, n = absorb(kw, files)
+    assert n == en > 0
+    print("1100 sites, streamed propagators: FP32 vs FP64 exact %.2e" % helpers.rel(r32, ex_re + 1j * ex_im))
+    assert helpers.rel(r32, ex_re + 1j * ex_im) < SPARSE_FP32
+    # FP64 has no tensor-core apply, so it keeps every frame's U: 1024 sites at most
+    p = nise.params_from_keywords(kw, files, precision=nise.FP64)
+    with nise.Context(p) as c:
+        c.load_files()
+        with pytest.raises(nise.NiseError):
+            c.absorption()
