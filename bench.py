@@ -26,6 +26,7 @@ import argparse
 import ctypes
 import json
 import os
+import shutil
 import statistics
 import subprocess
 import sys
@@ -74,6 +75,10 @@ def parse():
                         "workloads)")
     a.add_argument("--t2", type=int, default=0, help="c2 only: waiting-time steps (RunTimes 64 t2 64)")
     a.add_argument("--end", type=int, default=0, help="c2 only: EndPoint (0 = all start points)")
+    a.add_argument("--c4-true-diag", action="store_true",
+                   help="c4 only: the 32 Diagonal jobs with every frame diagonalised (kernel_config 2), one "
+                        "context at a time, on the first --c4-frames frames, extrapolated to 5000")
+    a.add_argument("--c4-frames", type=int, default=500, help="c4 --c4-true-diag: frames per job sampled")
     a.add_argument("--c4-job", type=int, default=-1,
                    help="c4 only: time job I (0..63) of the batch alone, default kernel configuration")
     return a.parse_args()
@@ -597,6 +602,8 @@ def run_c4(args):
     sizes = c4_sites()
     if args.c4_job >= 0:
         return run_c4_job(args, args.c4_job, sizes[args.c4_job], frames, tmax, sample, local)
+    if args.c4_true_diag:
+        return run_c4_true_diag(args, sizes, frames, tmax, sample, local)
     nsamp = (frames - tmax - 1) // sample + 1
     site_steps = sum(3 * nsamp * tmax * n for n in sizes)
     ctxs = []
@@ -646,6 +653,47 @@ def run_c4(args):
                           "mode": "the same jobs one context at a time (nise_absorption)",
                           "slowest_job_ms": max(per_job), "slowest_job_sites": sizes[per_job.index(max(per_job))]},
            "batched_over_sequential": seq_ms / ms, "clocks": clocks, "gpu_launches": launches}
+    print(json.dumps(out), flush=True)
+    return out
+
+
+def run_c4_true_diag(args, sizes, frames, tmax, sample, local):
+    """The Diagonal half of C4 (odd i, 9..2048 sites) with every frame diagonalised: the eigen
+    route (kernel_config 2: per-frame FP64 eigendecomposition, U = V exp(-i e f) V^T, applied on
+    the tensor cores above 120 sites with the propagators built chunk by chunk), one context at a
+    time on the first F frames of each trajectory; device time per job, summed, and scaled by
+    5000 / F (the route's cost is per frame).  Beside it the default route (the Chebyshev series
+    for static couplings) on the same sample."""
+    import nise_2017_b200 as nise
+    from nise_2017_b200 import synth
+    F = max(tmax + sample, min(args.c4_frames, frames))
+    jobs = []
+    with tempfile.TemporaryDirectory() as td:
+        for i in range(1, 64, 2):
+            n = sizes[i]
+            s = synth.c1_spec(n_sites=n, frames=F, seed=40000 + i)
+            files = synth.write(s, os.path.join(td, "t%02d" % i))
+            kw = synth.c1_keywords(Singles=n, Length=F, RunTimes="%d 0 0" % tmax, Samplerate=sample,
+                                   Propagation="Diagonal", FFT=1024)
+            row = {"i": i, "sites": n}
+            for label, cfg in (("eigen_ms", 2), ("series_ms", 0)):
+                with nise.Context(nise.params_from_keywords(kw, files, device=local, kernel_config=cfg)) as c:
+                    c.load_files()
+                    c.absorption()
+                    tot, _, _ = c.timing()
+                row[label] = tot
+            jobs.append(row)
+            shutil.rmtree(os.path.join(td, "t%02d" % i), ignore_errors=True)
+    eig = sum(j["eigen_ms"] for j in jobs)
+    ser = sum(j["series_ms"] for j in jobs)
+    out = {"metric": "C4 Diagonal half with true diagonalisation (eigen route) vs the series route",
+           "unit": "ms", "frames_sampled": F, "frames_full": frames,
+           "eigen_ms_sample": eig, "series_ms_sample": ser,
+           "eigen_ms_extrapolated": eig * frames / F, "series_ms_extrapolated": ser * frames / F,
+           "eigen_over_series": eig / ser if ser else None,
+           "note": "one context at a time, device time of one absorption call each (the plan's allocations "
+                   "outside); extrapolated linearly in frames",
+           "jobs": jobs}
     print(json.dumps(out), flush=True)
     return out
 
