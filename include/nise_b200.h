@@ -130,8 +130,8 @@ typedef struct {
                                       row-owner Chebyshev kernel (FP32), 12 the sliced-ELL Taylor
                                       kernel with 4 vectors per CTA (FP32);
                                       2 the eigen route (explicit per-frame propagators, up to
-                                      1024 sites), 16 / 17 its propagators applied per start
-                                      point / on the tensor cores;
+                                      2048 sites batched in FP32, else 1024), 16 / 17 its
+                                      propagators applied per start point / on the tensor cores;
                                       2D techniques, Trotter doubles: 1 one warp per doubles
                                       vector (else two warps per vector for 32 < N <= 64,
                                       bitwise the same result) */
