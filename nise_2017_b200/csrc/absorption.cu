@@ -667,13 +667,18 @@ template <typename R> struct EllEnt;
 template <> struct EllEnt<float> { int off; float v; };
 template <> struct EllEnt<double> { int off; int pad; double v; };
 
-template <typename R, int IT, int G, int NT>
+// CHEB: the Chebyshev form of the same exact step (FP32; P.order holds the
+// Chebyshev orders, P.cheb_inv_r and P.cheb_coef the frame's 1/R and
+// coefficients, as k_prep_cheb writes them): per own row T_(k-2) stays in a
+// register next to the accumulated result.
+template <typename R, int IT, int G, int NT, bool CHEB = false>
 __global__ void __launch_bounds__(NT, 1) k_abs_taylor3(DevTraj T, TaylorPlan P, AbsJob J, double2 *resp, int v0, int nvec,
                                                     const EllEnt<R> *__restrict__ ell_g, const int *__restrict__ sptr_g,
                                                     int nslices, int nent, const int *__restrict__ rows_g) {
     typedef typename Vec2<R>::T R2;
-    constexpr int QR = 4, SPW = 8 / G, RS = G == 8 ? NISE_T3_ROW : G;
+    constexpr int QR = 4, SPW = 8 / G, RS = G == 8 ? NISE_T3_ROW : G, KC = NISE_CHEB_KMAX + 1;
     static_assert(G == 8 || G == 1, "G = 8 or 1 vectors per CTA");
+    static_assert(!CHEB || sizeof(R) == 4, "the Chebyshev tables are FP32");
     constexpr bool kDgShared = NT > 512;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = P.n, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, NW = blockDim.x >> 5;
@@ -701,7 +706,7 @@ __global__ void __launch_bounds__(NT, 1) k_abs_taylor3(DevTraj T, TaylorPlan P, 
     const int vv = v0 + (valid ? v : blockIdx.x * G);
     const int x = vv % 3;
     const long ti = (long)(J.begin + vv / 3) * J.sample;
-    R2 psi[IT], nx[IT];
+    R2 psi[IT], nx[IT], prev[CHEB ? IT : 1];
     float dg[kDgShared ? 1 : IT];
 #pragma unroll
     for (int it = 0; it < IT; it++) {
@@ -734,8 +739,16 @@ __global__ void __launch_bounds__(NT, 1) k_abs_taylor3(DevTraj T, TaylorPlan P, 
             resp[(size_t)(v0 + blockIdx.x * G + tid) * J.tmax + t1] = make_double2(sr, si);
         }
         if (t1 == J.tmax - 1) break;
-        int K = P.order[tj - P.f0];
+        const long fl = tj - P.f0;
+        int K = P.order[fl];
         for (int o = 1; o < G; o <<= 1) K = max(K, __shfl_xor_sync(0xffffffffu, K, o));
+        R ir = 0, ir2 = 0;
+        const float2 *cf = nullptr;
+        if constexpr (CHEB) {
+            ir = (R)P.cheb_inv_r[fl];
+            ir2 = 2 * ir;
+            cf = P.cheb_coef + fl * KC;
+        }
 #pragma unroll
         for (int it = 0; it < IT; it++) {
             int i = rowof(slice(it));
@@ -746,6 +759,12 @@ __global__ void __launch_bounds__(NT, 1) k_abs_taylor3(DevTraj T, TaylorPlan P, 
                 dg[it] = d;
             }
             if (i < n) cur[(size_t)i * RS + g] = psi[it];
+            if constexpr (CHEB) {  // psi becomes a_0 T_0; T_0 is kept
+                const R a0 = (R)cf[0].x;
+                prev[it] = psi[it];
+                psi[it].x *= a0;
+                psi[it].y *= a0;
+            }
         }
         for (int k = 1; k <= K; k++) {
             __syncthreads();
@@ -769,17 +788,39 @@ __global__ void __launch_bounds__(NT, 1) k_abs_taylor3(DevTraj T, TaylorPlan P, 
                     yi += en.v * zz.y;
                     en = nen;
                 }
-                nx[it].x = c * yi;  // (-i)(c)(y)
-                nx[it].y = -c * yr;
+                if constexpr (CHEB) {  // T_1 = (H/R) T_0, T_k = 2 (H/R) T_(k-1) - T_(k-2)
+                    if (k == 1) {
+                        nx[it].x = ir * yr;
+                        nx[it].y = ir * yi;
+                    } else {
+                        nx[it].x = ir2 * yr - prev[it].x;
+                        nx[it].y = ir2 * yi - prev[it].y;
+                    }
+                    prev[it] = z;
+                } else {
+                    nx[it].x = c * yi;  // (-i)(c)(y)
+                    nx[it].y = -c * yr;
+                }
             }
             __syncthreads();
+            R2 a;
+            if constexpr (CHEB) {
+                const float2 ak = cf[k];
+                a.x = (R)ak.x;
+                a.y = (R)ak.y;
+            }
 #pragma unroll
             for (int it = 0; it < IT; it++) {
                 const int sl = slice(it), i = rowof(sl);
                 if (sl >= nslices || i >= n) continue;
                 cur[(size_t)i * RS + g] = nx[it];
-                psi[it].x += nx[it].x;
-                psi[it].y += nx[it].y;
+                if constexpr (CHEB) {
+                    psi[it].x += a.x * nx[it].x - a.y * nx[it].y;
+                    psi[it].y += a.x * nx[it].y + a.y * nx[it].x;
+                } else {
+                    psi[it].x += nx[it].x;
+                    psi[it].y += nx[it].y;
+                }
             }
         }
         __syncthreads();
@@ -1475,15 +1516,15 @@ static int run_cheb3(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, dou
     return (int)cudaGetLastError();
 }
 
-template <typename R, int IT, int G, int NT = 512>
+template <typename R, int IT, int G, int NT = 512, bool CHEB = false>
 static int run_taylor3_g(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int v0, int nvec,
                          cudaStream_t s) {
     if (nvec <= 0) return 0;
     size_t smem = taylor3_smem(P, sizeof(R), G, NT);
     int e;
-    if ((e = set_smem(k_abs_taylor3<R, IT, G, NT>, smem))) return e;
-    k_abs_taylor3<R, IT, G, NT><<<(nvec + G - 1) / G, NT, smem, s>>>(T, P, J, resp, v0, nvec, (const EllEnt<R> *)P.ell,
-                                                                  P.ell_sptr, P.ell_nslices, P.ell_nent, P.ell_rows);
+    if ((e = set_smem(k_abs_taylor3<R, IT, G, NT, CHEB>, smem))) return e;
+    k_abs_taylor3<R, IT, G, NT, CHEB><<<(nvec + G - 1) / G, NT, smem, s>>>(
+        T, P, J, resp, v0, nvec, (const EllEnt<R> *)P.ell, P.ell_sptr, P.ell_nslices, P.ell_nent, P.ell_rows);
     return (int)cudaGetLastError();
 }
 
@@ -1491,9 +1532,13 @@ static int run_taylor3_g(const DevTraj &T, const TaylorPlan &P, const AbsJob &J,
 // G = 1), 512 threads with IT1 rows per lane (1024 threads with one row per
 // lane measured slower on the 1024-site lattice: 52.3 against 51.0 ms per
 // job; the per-term barriers, not the lanes' gather chains, set its pace).
+// With the Chebyshev tables of the row-owner waves (P.rv_cheb) the tail runs
+// the same Chebyshev series.
 template <typename R, int IT1>
 static int run_taylor3_tail(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, double2 *resp, int v0, int nvec,
                             cudaStream_t s) {
+    if constexpr (sizeof(R) == 4)
+        if (P.rv_cheb && P.cheb_coef) return run_taylor3_g<R, IT1, 1, 512, true>(T, P, J, resp, v0, nvec, s);
     return run_taylor3_g<R, IT1, 1>(T, P, J, resp, v0, nvec, s);
 }
 
@@ -1523,13 +1568,9 @@ static int run_taylor3(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, d
     int e = -1;
     if constexpr (sizeof(R) == 4)  // the row-owner kernel for the 8-vector waves
         if (!P.no_rv && main > 0 && taylor_rv_fits(T, P)) e = launch_abs_taylor_rv(T, P, J, resp, 0, main, s);
-    if (P.rv_cheb) {  // the Chebyshev tables serve the row-owner kernel only; the tail runs the Taylor series
+    if (P.rv_cheb) {  // the Chebyshev series for the row-owner waves and the 1-vector tail
         if (main > 0 && e) return e < 0 ? (int)cudaErrorNotSupported : e;
-        TaylorPlan Pt = P;
-        Pt.order = P.order_taylor;
-        Pt.cheb_coef = nullptr;
-        Pt.cheb_inv_r = nullptr;
-        return run_taylor3_tail<R, IT1>(T, Pt, J, resp, main, nvec - main, s);
+        return run_taylor3_tail<R, IT1>(T, P, J, resp, main, nvec - main, s);
     }
     if constexpr (sizeof(R) == 4 && IT == 16)
         if (e < 0 && P.ell_nslices <= 24 * 11 && taylor3_smem(P, 4, 8, 768) <= 220 * 1024)
@@ -1543,12 +1584,7 @@ int launch_abs_taylor_part(const DevTraj &T, const TaylorPlan &P, const AbsJob &
                            bool one, cudaStream_t s) {
     if (nvec <= 0) return 0;
     if (!one) return launch_abs_taylor_rv(T, P, J, resp, v0, nvec, s);
-    TaylorPlan Pt = P;  // 1-vector CTAs run the Taylor series
-    if (P.rv_cheb) {
-        Pt.order = P.order_taylor;
-        Pt.cheb_coef = nullptr;
-        Pt.cheb_inv_r = nullptr;
-    }
+    const TaylorPlan &Pt = P;  // 1-vector CTAs: the same series as the waves
     const int it = (P.ell_nslices + 15) / 16;
     if (!P.ell || it > 32) return (int)cudaErrorNotSupported;
     const int IT = it <= 1 ? 1 : it <= 2 ? 2 : it <= 4 ? 4 : it <= 8 ? 8 : it <= 16 ? 16 : 32;
@@ -1578,7 +1614,7 @@ int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const Abs
         }
     }
     if (P.cheb_coef && P.rv_cheb) {  // the row-owner kernel with the Chebyshev expansion (FP32)
-        if (prec != 0 || !P.order_taylor || !P.ell || !taylor_rv_fits(T, P)) return (int)cudaErrorNotSupported;
+        if (prec != 0 || !P.ell || !taylor_rv_fits(T, P)) return (int)cudaErrorNotSupported;
         const int it = (P.ell_nslices + 15) / 16;
         if (it > 32 || taylor3_smem(P, 4) > 220 * 1024) return (int)cudaErrorNotSupported;
         const int nvec = 3 * J.nsamp;

@@ -844,8 +844,10 @@ int AbsRun::enqueue_waves(cudaStream_t s) {
                                               dcoef.p + o * (NISE_CHEB_KMAX + 1), s), "Chebyshev prep");
             c->launches++;
         }
-        if (!e) e = nise_cuda(c, launch_prep_taylor(prec, T, Q, rowabs, J.f, dorder.p + o, s), "Taylor prep");
-        c->launches++;
+        if (!e && config != 15) {  // config 15 runs the Chebyshev series on every CTA
+            e = nise_cuda(c, launch_prep_taylor(prec, T, Q, rowabs, J.f, dorder.p + o, s), "Taylor prep");
+            c->launches++;
+        }
         prepped = last + 1;
         return e;
     };
@@ -892,7 +894,7 @@ int AbsRun::enqueue(cudaStream_t s, bool events) {
             rc = nise_cuda(c, launch_prep_cheb(T, P, rowabs, J.f, dcorder.p, dinvr.p, dcoef.p, s), "Chebyshev prep");
             c->launches++;
         }
-        if (!rc && config != 10) {
+        if (!rc && config != 10 && config != 15) {
             rc = nise_cuda(c, launch_prep_taylor(prec, T, P, rowabs, J.f, dorder.p, s), "Taylor prep");
             c->launches++;
         }

@@ -83,7 +83,7 @@ struct TaylorPlan {
     int rv_shape;
     int no_rv;
     int rv_cheb;           // with the Chebyshev tables: the row-owner kernel's Chebyshev form
-    const int *order_taylor;  // rv_cheb: Taylor orders for the 1-vector tail CTAs
+    const int *order_taylor;  // the Taylor orders next to the Chebyshev ones (10, 15)
     int *err;              // device flag: 1 = a bounded wait for a staged frame gave up
 };
 #define NISE_CHEB_KMAX 40
