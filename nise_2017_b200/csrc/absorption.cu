@@ -1567,10 +1567,16 @@ static int run_taylor3(const DevTraj &T, const TaylorPlan &P, const AbsJob &J, d
     if (kernels) *kernels = (main > 0) + (nvec > main);
     int e = -1;
     if constexpr (sizeof(R) == 4)  // the row-owner kernel for the 8-vector waves
-        if (!P.no_rv && main > 0 && taylor_rv_fits(T, P)) e = launch_abs_taylor_rv(T, P, J, resp, 0, main, s);
-    if (P.rv_cheb) {  // the Chebyshev series for the row-owner waves and the 1-vector tail
-        if (main > 0 && e) return e < 0 ? (int)cudaErrorNotSupported : e;
-        return run_taylor3_tail<R, IT1>(T, P, J, resp, main, nvec - main, s);
+        if (!P.no_rv && main > 0 && taylor_rv_fits(T, P)) {
+            // the 1-vector CTAs take the first vectors, the waves the rest: the
+            // order in which a trajectory copied in frame chunks arrives (the
+            // chunked path runs the same split), at the same job length
+            if ((e = run_taylor3_tail<R, IT1>(T, P, J, resp, 0, nvec - main, s))) return e;
+            return launch_abs_taylor_rv(T, P, J, resp, nvec - main, main, s);
+        }
+    if (P.rv_cheb) {  // the Chebyshev series on 1-vector CTAs only (no whole wave)
+        if (main > 0) return (int)cudaErrorNotSupported;
+        return run_taylor3_tail<R, IT1>(T, P, J, resp, 0, nvec, s);
     }
     if constexpr (sizeof(R) == 4 && IT == 16)
         if (e < 0 && P.ell_nslices <= 24 * 11 && taylor3_smem(P, 4, 8, 768) <= 220 * 1024)

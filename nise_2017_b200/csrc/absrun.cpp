@@ -185,6 +185,14 @@ struct AbsRun {
     // frames up to there): the copy from the host overlaps the propagation.
     int enqueue_waves(cudaStream_t s);
     bool waves_apply() const;
+    // the side stream of enqueue_waves' 1-vector CTAs, created on first use
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    ~AbsRun() {
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (side) cudaStreamDestroy(side);
+    }
     // A plan reused by a later call: the trajectory pointers may have moved
     // and the error flags start clear.
     void refresh() {
@@ -825,10 +833,15 @@ int AbsRun::enqueue_waves(cudaStream_t s) {
     } else {
         P.order = dorder.p;
     }
-    // whole waves of 8-vector CTAs, the rest on 1-vector CTAs (as launch_abs_taylor)
+    // whole waves of 8-vector CTAs, the rest on 1-vector CTAs (as launch_abs_taylor).
+    // Here the 1-vector CTAs take the FIRST vectors, whose frames arrive first:
+    // they run on a side stream while the rest of the trajectory is copied, and
+    // the waves (the job's length either way: 1-vector CTAs then five waves on
+    // their SMs) start as their frames land.
     const int nsm = sm_count(), ctas = (nvec + 7) / 8;
     int main = nvec;
     if (ctas % nsm != 0 && ctas % nsm < nsm / 2 && ctas >= nsm) main = (ctas / nsm) * nsm * 8;
+    const int ntail = nvec - main;
     long prepped = f0;  // frames [f0, prepped) have their series tables
     int rc = 0;
     auto prep_to = [&](long last) -> int {
@@ -851,18 +864,29 @@ int AbsRun::enqueue_waves(cudaStream_t s) {
         prepped = last + 1;
         return e;
     };
-    for (int v = 0; v < main && !rc; v += 8 * nsm) {
-        const int ve = std::min(v + 8 * nsm, main);
-        // the last frame any vector of the wave steps through
-        if ((rc = prep_to((long)(J.begin + (ve - 1) / 3) * J.sample + J.tmax - 2))) return rc;
+    // the last frame any of vectors [.., ve) steps through
+    auto last_frame = [&](int ve) { return (long)(J.begin + (ve - 1) / 3) * J.sample + J.tmax - 2; };
+    if (ntail > 0) {
+        if (!side) {
+            if ((rc = nise_cuda(c, (int)cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking), "side stream")) ||
+                (rc = nise_cuda(c, (int)cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming), "event")) ||
+                (rc = nise_cuda(c, (int)cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming), "event")))
+                return rc;
+        }
+        if ((rc = prep_to(last_frame(ntail)))) return rc;
+        cudaEventRecord(ev_fork, s);
+        cudaStreamWaitEvent(side, ev_fork, 0);
+        rc = nise_cuda(c, launch_abs_taylor_part(T, P, J, resp.p, 0, ntail, true, side), "propagation");
+        c->launches++;
+        cudaEventRecord(ev_join, side);
+    }
+    for (int v = ntail; v < nvec && !rc; v += 8 * nsm) {
+        const int ve = std::min(v + 8 * nsm, nvec);
+        if ((rc = prep_to(last_frame(ve)))) break;
         rc = nise_cuda(c, launch_abs_taylor_part(T, P, J, resp.p, v, ve - v, false, s), "propagation");
         c->launches++;
     }
-    if (!rc && main < nvec) {
-        if ((rc = prep_to(f0 + nf - 1))) return rc;
-        rc = nise_cuda(c, launch_abs_taylor_part(T, P, J, resp.p, main, nvec - main, true, s), "propagation");
-        c->launches++;
-    }
+    if (ntail > 0) cudaStreamWaitEvent(s, ev_join, 0);  // joined on every path
     return rc;
 }
 
