@@ -1009,9 +1009,72 @@ int oracle_absorption(const oracle_params *p, double *re_out, double *im_out, in
  * LD, Raman, DOS and CD read frames with read_He (no SingleShift); SFG with
  * read_Hamiltonian.  SFG's x and y start vectors have no read-out and are not
  * propagated here. */
+/* Boltzmann weighting of a luminescence initial vector by the equilibrium
+ * density matrix of the packed Hamiltonian H (luminescence.c:246-314,
+ * bltz_weight): v <- rho v, rho = V exp(-E/kT) V^T / Q, the products in the
+ * reference's loop order.  Q is summed from zero (the reference leaves it
+ * uninitialised, luminescence.c:262,277).  FP64 eigendecomposition in place
+ * of ssyev_. */
+static void lum_weight_exact(const oracle_params *p, const float *H, real *v) {
+    const int N = p->singles;
+    real *Hv = (real *)malloc(sizeof(real) * N * N), *e = (real *)malloc(sizeof(real) * N);
+    real *c2 = (real *)malloc(sizeof(real) * N), *c1 = (real *)calloc(N, sizeof(real));
+    real *cnr = (real *)calloc((size_t)N * N, sizeof(real)), *crr = (real *)calloc((size_t)N * N, sizeof(real));
+    diag_packed(H, N, Hv, e);
+    const float kBT = p->temperature * 0.695;  /* Kelvin to cm^-1 */
+    real Q = 0;
+    for (int a = 0; a < N; a++) {
+        c2[a] = (real)exp(-e[a] / kBT);
+        Q = Q + c2[a];
+    }
+    const real iQ = (real)(1.0 / Q);
+    for (int a = 0; a < N; a++)
+        for (int b = 0; b < N; b++) cnr[b + a * N] += Hv[b + a * N] * c2[b] * iQ;
+    for (int a = 0; a < N; a++)
+        for (int b = 0; b < N; b++)
+            for (int c = 0; c < N; c++) crr[a + c * N] += Hv[b + a * N] * cnr[b + c * N];
+    for (int a = 0; a < N; a++)
+        for (int b = 0; b < N; b++) c1[a] += crr[a + b * N] * v[b];
+    for (int a = 0; a < N; a++) v[a] = c1[a];
+    free(Hv); free(e); free(c2); free(c1); free(cnr); free(crr);
+}
+
+/* The same weighting by m imaginary-time Trotter steps (luminescence.c:318-
+ * 409, bltz_weight_itime): per step the diagonal half-factors
+ * exp(-H_aa f/2), the couplings |J| > Couplingcut in lexicographic order as
+ * (cosh, -sinh) pairs of J f, the half-factors again; f = 1/(m kT); then
+ * the vector is scaled back to its initial norm. */
+static void lum_weight_itime(const oracle_params *p, const float *H, real *cr) {
+    const int N = p->singles, m = p->imag_steps;
+    const float kBT = p->temperature * 0.695;
+    const float f = 1.0 / (m * kBT);
+    real *reU = (real *)malloc(sizeof(real) * N), *ocr = (real *)malloc(sizeof(real) * N);
+    real norm = 0, Q = 0;
+    for (int a = 0; a < N; a++) norm += cr[a] * cr[a];
+    for (int a = 0; a < N; a++) reU[a] = (real)exp(-0.5 * H[Sindex(a, a, N)] * f);
+    for (int i = 0; i < m; i++) {
+        for (int a = 0; a < N; a++) ocr[a] = cr[a] * reU[a];
+        for (int a = 0; a < N; a++)
+            for (int b = a + 1; b < N; b++) {
+                float J = H[Sindex(a, b, N)];
+                if (!(fabs(J) > p->couplingcut)) continue;
+                J = -J * f;
+                const real eJ = (real)(exp(J) * 0.5), emJ = (real)(exp(-J) * 0.5);
+                const real sih = eJ - emJ, coh = eJ + emJ;
+                const real r1 = coh * ocr[a] + sih * ocr[b], r2 = coh * ocr[b] + sih * ocr[a];
+                ocr[a] = r1, ocr[b] = r2;
+            }
+        for (int a = 0; a < N; a++) cr[a] = ocr[a] * reU[a];
+    }
+    for (int a = 0; a < N; a++) Q += cr[a] * cr[a];
+    const real iQ = (real)sqrt(norm / Q);
+    for (int a = 0; a < N; a++) cr[a] = cr[a] * iQ;
+    free(reU); free(ocr);
+}
+
 int oracle_linear(const oracle_params *p, double *re_out, double *im_out, int *nch_out, int *samples_out) {
     const int N = p->singles, tech = p->technique, tmax = p->tmax1;
-    if (tech < 11 || tech > 15) return -6;
+    if (tech < 11 || tech > 16) return -6;
     float shift1 = (p->max1 + p->min1) / 2;
     traj_t t;
     if (traj_open(&t, p, shift1, 0) != 0) { traj_free(&t); return -1; }
@@ -1019,7 +1082,7 @@ int oracle_linear(const oracle_params *p, double *re_out, double *im_out, int *n
     if (N_samples <= 0) { traj_free(&t); return -2; }
     int end = p->end == 0 ? N_samples : p->end;
     if (end > N_samples) { traj_free(&t); return -3; }
-    const int nch = (tech == 12 || tech == 13) ? 2 : 1;
+    const int nch = (tech == 12 || tech == 13) ? 2 : (tech == 16 ? 4 : 1);  /* Luminescence: total, x, y, z */
     const int nvec = tech == 14 ? N : (tech == 15 ? N : 1);  /* vectors propagated together */
     acc *S = (acc *)calloc(2 * (size_t)nch * tmax, sizeof(acc));   /* [ch][re/im][t1] */
     acc *Sj = (acc *)calloc(2 * (size_t)N * tmax, sizeof(acc));    /* CD: per initial site */
@@ -1045,6 +1108,11 @@ int oracle_linear(const oracle_params *p, double *re_out, double *im_out, int *n
             } else if (tech == 12) {               /* alpha_x(ti) */
                 if (!read_alpha(&t, op, ti, x)) { rc = -4; break; }
                 for (int i = 0; i < N; i++) vr[i] = op[i];
+            } else if (tech == 16) {               /* mu_x(ti) weighted by the Hamiltonian read last */
+                if (!mu_read(&t, mu, ti, x)) { rc = -4; break; }
+                for (int i = 0; i < N; i++) vr[i] = mu[i];
+                if (p->imag_steps == 0) lum_weight_exact(p, H, vr);
+                else lum_weight_itime(p, H, vr);
             } else if (tech == 14) {               /* unitmat */
                 for (int j = 0; j < N; j++) vr[(size_t)j * N + j] = 1;
             } else {                               /* CD: mu_x(ti)_j on site j */
@@ -1054,7 +1122,7 @@ int oracle_linear(const oracle_params *p, double *re_out, double *im_out, int *n
             for (int t1 = 0; t1 < tmax; t1++) {
                 const int tj = ti + t1;
                 if (!read_He(&t, H, tj)) { rc = -5; break; }
-                if (tech == 13) apply_singleshift(&t, H);
+                if (tech == 13 || tech == 16) apply_singleshift(&t, H);  /* read_Hamiltonian */
                 if (tech == 11) {
                     if (!mu_read(&t, mu, tj, x)) { rc = -4; break; }
                     float factor = x == 2 ? 1 : -0.5;
@@ -1080,6 +1148,16 @@ int oracle_linear(const oracle_params *p, double *re_out, double *im_out, int *n
                             }
                     }
                     if (rc) break;
+                } else if (tech == 16) {  /* calc_LUM: the total and component x's channel */
+                    if (!mu_read(&t, mu, tj, x)) { rc = -4; break; }
+                    for (int i = 0; i < N; i++) {
+                        SRE(0, t1) += mu[i] * vr[i];
+                        SIM(0, t1) += mu[i] * vi[i];
+                    }
+                    for (int i = 0; i < N; i++) {
+                        SRE(1 + x, t1) += mu[i] * vr[i];
+                        SIM(1 + x, t1) += mu[i] * vi[i];
+                    }
                 } else if (tech == 14) {
                     for (int i = 0; i < N; i++) {
                         SRE(0, t1) += vr[(size_t)i * N + i];

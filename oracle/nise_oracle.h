@@ -32,11 +32,13 @@ typedef struct {
     int ham_coupling;    /* 1: HamiltonianType Coupling, 0: Full */
     int propagation;     /* 0 Sparse, 1 Coupling, 2 Diagonal, 3 RK4 */
     int technique;       /* 0 Absorption, 1 2DIR, 2 GBIR, 3 SEIR, 4 EAIR, 5 noEAIR, 6-10 the UVvis names,
-                            11 LD, 12 Raman, 13 SFG, 14 DOS, 15 CD */
+                            11 LD, 12 Raman, 13 SFG, 14 DOS, 15 CD, 16 Luminescence */
     char energy[256], dipole[256], coupling[256], anharm[256], overtone[256], shift[256];
     int ham_onfly;       /* 1: TransitionDipole, 2: ExtendedDipole (couplings from positions) */
     char position[256], pbc[256];
     char alpha[256];     /* Alphafile (Raman, SFG) */
+    float temperature;   /* Temperature (K), Luminescence */
+    int imag_steps;      /* ImaginaryTimesteps: 0 exact Boltzmann weights, else imaginary-time steps */
 } oracle_params;
 
 int oracle_real_size(void);
@@ -45,7 +47,7 @@ int oracle_absorption(const oracle_params *p, double *re_S, double *im_S, int *s
 /* Raw 2D response sums, 12 arrays of tmax3*tmax1 ([t3][t1]) in the order
  * rrIpar riIpar rrIIpar riIIpar rrIper riIper rrIIper riIIper rrIcro riIcro rrIIcro riIIcro. */
 int oracle_2dir(const oracle_params *p, double *R, int *sample_count);
-/* LD, Raman, SFG, DOS, CD (calc_LD.c, raman.c, sfg.c, calc_DOS.c, calc_CD.c):
+/* LD, Raman, SFG, DOS, CD, Luminescence (calc_LD.c, raman.c, sfg.c, calc_DOS.c, calc_CD.c, luminescence.c):
  * raw response sums of each output channel, re/im[channel][tmax1]; *samples = end. */
 int oracle_linear(const oracle_params *p, double *re_S, double *im_S, int *channels, int *samples);
 /* print2D normalisation (MPI_subs.c:20-34) applied in place to one array pair. */

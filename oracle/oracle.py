@@ -17,12 +17,17 @@ REF_DIR = os.path.join(HERE, "_ref")
 
 TECHNIQUES = {"Absorption": 0, "2DIR": 1, "GBIR": 2, "SEIR": 3, "EAIR": 4, "noEAIR": 5,
               "2DUVvis": 6, "GBUVvis": 7, "SEUVvis": 8, "EAUVvis": 9, "noEAUVvis": 10,
-              "LD": 11, "Raman": 12, "SFG": 13, "DOS": 14, "CD": 15}
+              "LD": 11, "Raman": 12, "SFG": 13, "DOS": 14, "CD": 15,
+              "Luminescence": 16, "PL": 16, "Fluorescence": 16}
 # output files of the linear techniques per channel (calc_LD.c, raman.c, sfg.c, calc_DOS.c, calc_CD.c)
 LINEAR_FILES = {"LD": [("TD_LD.dat", "LD.dat")],
                 "Raman": [("TD_Raman_VV.dat", "Raman_VV.dat"), ("TD_Raman_VH.dat", "Raman_VH.dat")],
                 "SFG": [("TD_SFG_PPP.dat", "SFG_PPP.dat"), ("TD_SFG_SSP.dat", "SFG_SSP.dat")],
-                "DOS": [("TD_DOS.dat", "DOS.dat")], "CD": [("TD_CD.dat", "CD.dat")]}
+                "DOS": [("TD_DOS.dat", "DOS.dat")], "CD": [("TD_CD.dat", "CD.dat")],
+                # luminescence.c:223-234: the time-domain file of the total only
+                "Luminescence": [("TD_Lum.dat", "Luminescence.dat"), (None, "Luminescence_x.dat"),
+                                 (None, "Luminescence_y.dat"), (None, "Luminescence_z.dat")]}
+LINEAR_FILES["PL"] = LINEAR_FILES["Fluorescence"] = LINEAR_FILES["Luminescence"]
 ICM2IFS = np.float32(2.99792458e-5)
 TWOPI = np.float32(2 * 3.14159265359)
 
@@ -42,7 +47,7 @@ class OracleParams(ctypes.Structure):
         ("energy", ctypes.c_char * 256), ("dipole", ctypes.c_char * 256), ("coupling", ctypes.c_char * 256),
         ("anharm", ctypes.c_char * 256), ("overtone", ctypes.c_char * 256), ("shift", ctypes.c_char * 256),
         ("ham_onfly", ctypes.c_int), ("position", ctypes.c_char * 256), ("pbc", ctypes.c_char * 256),
-        ("alpha", ctypes.c_char * 256),
+        ("alpha", ctypes.c_char * 256), ("temperature", ctypes.c_float), ("imag_steps", ctypes.c_int),
     ]
 
 
@@ -79,6 +84,8 @@ def params(keywords, files):
     prop = kw.get("Propagation", "")
     p.propagation = {"Coupling": 1, "Diagonal": 2, "RK4": 3}.get(prop, 0)
     p.technique = TECHNIQUES[kw.get("Technique", "Absorption")]
+    p.temperature = float(kw.get("Temperature", 300))  # readinput.c:32
+    p.imag_steps = int(kw.get("ImaginaryTimesteps", 0))  # readinput.c:28
     if 1 <= p.technique <= 10:
         p.tmax3 = p.tmax1  # readinput.c:212
     thres = np.float32(float(kw.get("Threshold", 0)))
@@ -261,7 +268,7 @@ def spectrum(p, re, im, samples, prec="f64"):
 
 
 def linear(p, prec="f64"):
-    """LD, Raman, SFG, DOS, CD: raw response sums re, im [channel][tmax1] and the normaliser."""
+    """LD, Raman, SFG, DOS, CD, Luminescence: raw response sums re, im [channel][tmax1] and the normaliser."""
     re = np.zeros((4, p.tmax1))
     im = np.zeros((4, p.tmax1))
     ch = ctypes.c_int(0)

@@ -185,6 +185,22 @@ CASES = {
         keywords=synth.c2_keywords(Singles=9, Length=300, RunTimes="32 0 0", Samplerate=40, Technique="CD",
                                    FFT=256),
         cd_positions=dict(seed=62, spacing=5.0)),
+    # luminescence (luminescence.c), from the reference built with zero-initialised
+    # automatic variables (oracle/_ref/NISE_lum; its partition function Q is otherwise
+    # summed from an uninitialised float)
+    "lum_exact": dict(
+        spec=dict(n_sites=8, frames=300, dt_fs=2.0, geometry=synth.CHAIN, seed=71),
+        keywords=synth.c0_keywords(Singles=8, Length=300, RunTimes="32 0 0", Samplerate=30,
+                                   Technique="Luminescence", FFT=256, Temperature=300)),
+    "lum_itime": dict(
+        spec=dict(n_sites=8, frames=300, dt_fs=2.0, geometry=synth.CHAIN, seed=72),
+        keywords=synth.c0_keywords(Singles=8, Length=300, RunTimes="32 0 0", Samplerate=30, Technique="PL",
+                                   FFT=256, Temperature=200, ImaginaryTimesteps=20)),
+    "lum_static": dict(
+        spec=dict(n_sites=9, frames=300, dt_fs=2.0, geometry=C, spacing=6.0, sigma=12.0, mu_jitter=0.0,
+                  ham_type=synth.COUPLING, dipole_frames=1, seed=73),
+        keywords=synth.c2_keywords(Singles=9, Length=300, RunTimes="32 0 0", Samplerate=30,
+                                   Technique="Luminescence", FFT=256)),
 }
 
 
@@ -224,15 +240,16 @@ def main(names=None):
         try:
             files = materialise(case, work)
             inp = synth.write_input(os.path.join(work, "input"), case["keywords"], files)
-            oracle.run_reference(inp, work)
-            out = {}
             tech = case["keywords"]["Technique"]
+            oracle.run_reference(inp, work, binary="NISE_lum" if oracle.TECHNIQUES.get(tech) == 16 else "NISE_acc")
+            out = {}
             if tech == "Absorption":
                 out["td"] = np.loadtxt(os.path.join(work, "TD_Absorption.dat"), ndmin=2)
                 out["spec"] = np.loadtxt(os.path.join(work, "Absorption.dat"), ndmin=2)
             elif tech in oracle.LINEAR_FILES:
                 # per channel: td [tmax1][t, Re, Im], spec [rows][w, Re, Im]
-                out["td"] = np.stack([np.loadtxt(os.path.join(work, td), ndmin=2) for td, _ in oracle.LINEAR_FILES[tech]])
+                out["td"] = np.stack([np.loadtxt(os.path.join(work, td), ndmin=2) for td, _ in oracle.LINEAR_FILES[tech]
+                                      if td])
                 out["spec"] = np.stack([np.loadtxt(os.path.join(work, sp), ndmin=2)
                                         for _, sp in oracle.LINEAR_FILES[tech]])
             else:

@@ -41,9 +41,19 @@ def R12_to_files(R):
 
 
 def uses_eigen(case):
+    """Whether the case goes through an eigendecomposition (FP64 here, the
+    reference's ssyev_ in FP32): Sparse/Diagonal propagation, the 2D t2 step,
+    the exact Boltzmann weights of luminescence."""
     kw = case["keywords"]
     t2 = int(str(kw.get("RunTimes", "0 0 0")).split()[1])
-    return kw.get("Propagation") in ("Sparse", "Diagonal") or (kw["Technique"] != "Absorption" and t2 > 0)
+    lum = kw["Technique"] in ("Luminescence", "PL", "Fluorescence") and int(kw.get("ImaginaryTimesteps", 0)) == 0
+    return kw.get("Propagation") in ("Sparse", "Diagonal") or (kw["Technique"] != "Absorption" and t2 > 0) or lum
+
+
+def td_channels(technique, linear_files):
+    """Channels of a linear technique that have a time-domain file, in the
+    order of the golden td arrays (luminescence writes the total's only)."""
+    return [k for k, (td, _) in enumerate(linear_files[technique]) if td]
 
 
 def fft2d_case(name):

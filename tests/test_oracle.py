@@ -47,17 +47,18 @@ def test_absorption_fp64_within_reference_rounding(name, tmp_path):
 
 @pytest.mark.parametrize("name", LIN)
 def test_linear_restatement_matches_reference(name, tmp_path):
-    """LD, Raman, SFG, DOS, CD: every channel's TD_*.dat and spectrum file."""
+    """LD, Raman, SFG, DOS, CD, Luminescence: every TD_*.dat and spectrum file."""
     case = CASES[name]
     files = helpers.materialise(case, str(tmp_path))
     g = helpers.golden(name)
     p = oracle.params(case["keywords"], files)
     re, im, n = oracle.linear(p, "f32")
-    assert len(re) == len(g["td"])
+    tdk = helpers.td_channels(case["keywords"]["Technique"], oracle.LINEAR_FILES)
+    assert len(re) == len(oracle.LINEAR_FILES[case["keywords"]["Technique"]]) and len(tdk) == len(g["td"])
     tol = 1e-5 if helpers.uses_eigen(case) else PRINT_TOL
+    for j, k in enumerate(tdk):
+        assert helpers.rel(np.stack([re[k] / n, im[k] / n], 1), g["td"][j][:, 1:]) < tol
     for k in range(len(re)):
-        td = g["td"][k]
-        assert helpers.rel(np.stack([re[k] / n, im[k] / n], 1), td[:, 1:]) < tol
         w, sr, si = oracle.spectrum(p, re[k], im[k], n, "f32")
         assert len(w) == len(g["spec"][k])
         assert helpers.rel(np.stack([sr, si], 1), g["spec"][k][:, 1:]) < max(tol, PRINT_TOL)
@@ -72,8 +73,8 @@ def test_linear_fp64_within_reference_rounding(name, tmp_path):
     re, im, n = oracle.linear(p, "f64")
     # CD and SSP responses are small differences of large terms: the reference's
     # single-precision propagation error reaches 3e-4 of them (static CD)
-    for k in range(len(re)):
-        assert helpers.rel(np.stack([re[k] / n, im[k] / n], 1), g["td"][k][:, 1:]) < 5e-4
+    for j, k in enumerate(helpers.td_channels(case["keywords"]["Technique"], oracle.LINEAR_FILES)):
+        assert helpers.rel(np.stack([re[k] / n, im[k] / n], 1), g["td"][j][:, 1:]) < 5e-4
 
 
 @pytest.mark.parametrize("name", TWO_D)
