@@ -17,8 +17,8 @@
  *   nise_absorption_fft    <- do_1DFFT() (1DFFT.c:144-228)
  *   nise_2dir              <- calc_2DIR() (calc_2DIR.c:22-629) and calc_2DES()
  *                             (calc_2DES.c:22-586), one GPU instead of MPI ranks
- *   nise_linear            <- LD(), raman(), sfg(), calc_DOS(), calc_CD() (calc_LD.c,
- *                             raman.c, sfg.c, calc_DOS.c, calc_CD.c)
+ *   nise_linear            <- LD(), raman(), sfg(), calc_DOS(), calc_CD(), luminescence()
+ *                             (calc_LD.c, raman.c, sfg.c, calc_DOS.c, calc_CD.c, luminescence.c)
  *   nise_translate         <- translate's main() (translate.c:25-65)
  *   nise_propagate         <- propagate_vector() (propagate.c:20-39), batched
  *   nise_propagate_doubles <- propagate_vec_coupling_S_doubles / _RK4_doubles /
@@ -77,6 +77,7 @@ enum {
     NISE_TECH_SFG = 13,
     NISE_TECH_DOS = 14,
     NISE_TECH_CD = 15,
+    NISE_TECH_LUM = 16,            /* Luminescence, PL, Fluorescence (luminescence.c) */
     NISE_TECH_OTHER = 99
 };
 /* Arithmetic of the propagation.  FP32 reproduces the reference's single
@@ -138,6 +139,9 @@ typedef struct {
     char positionFName[256];       /* Positionfile (TransitionDipole / ExtendedDipole; CD) */
     char pbcFName[256];            /* PBCfile: periodic box per frame (optional) */
     char alphaFName[256];          /* Alphafile: polarisabilities (Raman, SFG) */
+    float temperature;             /* Temperature (K; default 300), Luminescence */
+    int imag_steps;                /* ImaginaryTimesteps: 0 (default) exact Boltzmann weights from an
+                                      eigendecomposition, m > 0 m imaginary-time Trotter steps */
 } nise_params;
 
 typedef struct nise_ctx nise_ctx;
@@ -244,12 +248,14 @@ int nise_set_operators(nise_ctx *ctx, const void *alpha, size_t alpha_bytes, con
                        size_t position_bytes);
 
 /* Linear techniques besides absorption: LD (calc_LD.c:15-290), Raman
- * (raman.c:15-307), SFG (sfg.c:15-297), DOS (calc_DOS.c:15-234) and CD
- * (calc_CD.c:15-392), chosen by the context's technique.  Writes the raw
- * response sums of each output channel, re_S/im_S[channel][tmax1] (LD, DOS,
- * CD: one channel; Raman: VV, VH; SFG: PPP, SSP), the channel count and the
- * sample count the reference divides by.  Each channel's spectrum is
- * nise_absorption_fft of its response. */
+ * (raman.c:15-307), SFG (sfg.c:15-297), DOS (calc_DOS.c:15-234), CD
+ * (calc_CD.c:15-392) and Luminescence (luminescence.c:17-409), chosen by the
+ * context's technique.  Writes the raw response sums of each output channel,
+ * re_S/im_S[channel][tmax1] (LD, DOS, CD: one channel; Raman: VV, VH; SFG:
+ * PPP, SSP; Luminescence: total, x, y, z), the channel count and the sample
+ * count the reference divides by.  Each channel's spectrum is
+ * nise_absorption_fft of its response.  Luminescence sums the partition
+ * function from zero (the reference starts it uninitialised). */
 int nise_linear(nise_ctx *ctx, double *re_S, double *im_S, int max_channels, int *channels, int *samples);
 /* Output file of channel k of a linear technique: the time-domain file
  * (td != 0, e.g. TD_Raman_VV.dat) or the spectrum (Raman_VV.dat); NULL past

@@ -27,7 +27,7 @@ PROP = {"Sparse": 0, "Coupling": 1, "Diagonal": 2, "RK4": 3}
 HAM = {"Full": 0, "Coupling": 1}
 TECH = {"Absorption": 0, "2DIR": 1, "GBIR": 2, "SEIR": 3, "EAIR": 4, "noEAIR": 5,
         "2DUVvis": 6, "GBUVvis": 7, "SEUVvis": 8, "EAUVvis": 9, "noEAUVvis": 10,
-        "LD": 11, "Raman": 12, "SFG": 13, "DOS": 14, "CD": 15}
+        "LD": 11, "Raman": 12, "SFG": 13, "DOS": 14, "CD": 15, "Luminescence": 16, "PL": 16, "Fluorescence": 16}
 FP32, FP64 = 0, 1
 BATCHED, PLAIN = 0, 1
 R2D_NAMES = ["RparI.dat", "RparII.dat", "RperI.dat", "RperII.dat", "RcroI.dat", "RcroII.dat"]
@@ -67,7 +67,7 @@ class Params(ctypes.Structure):
         ("overdipFName", ctypes.c_char * 256), ("singleShiftFName", ctypes.c_char * 256),
         ("precision", ctypes.c_int), ("launch_mode", ctypes.c_int), ("device", ctypes.c_int),
         ("kernel_config", ctypes.c_int), ("positionFName", ctypes.c_char * 256), ("pbcFName", ctypes.c_char * 256),
-        ("alphaFName", ctypes.c_char * 256),
+        ("alphaFName", ctypes.c_char * 256), ("temperature", ctypes.c_float), ("imag_steps", ctypes.c_int),
     ]
 
 
@@ -165,10 +165,11 @@ def linear_files(technique):
     code = TECH[technique] if isinstance(technique, str) else technique
     out = []
     while True:
-        td = lib().nise_linear_file(code, len(out), 1)
-        if td is None:
+        sp = lib().nise_linear_file(code, len(out), 0)
+        if sp is None:
             return out
-        out.append((td.decode(), lib().nise_linear_file(code, len(out), 0).decode()))
+        td = lib().nise_linear_file(code, len(out), 1)  # None: the channel has no time-domain file
+        out.append((td.decode() if td else None, sp.decode()))
 
 
 def default_params():

@@ -52,6 +52,8 @@ extern "C" int nise_params_default(nise_params *p) {
     p->hamiltonian = NISE_HAM_FULL;
     p->propagation = NISE_PROP_SPARSE;
     p->technique = NISE_TECH_OTHER;
+    p->temperature = 300;  // readinput.c:32
+    p->imag_steps = 0;     // readinput.c:28
     p->precision = NISE_FP32;
     p->launch_mode = NISE_BATCHED;
     p->device = 0;
@@ -75,6 +77,8 @@ static int technique_code(const char *t) {
     if (!strcmp(t, "SFG")) return NISE_TECH_SFG;
     if (!strcmp(t, "DOS")) return NISE_TECH_DOS;
     if (!strcmp(t, "CD")) return NISE_TECH_CD;
+    // NISE.c:236 (string_in_array)
+    if (!strcmp(t, "Luminescence") || !strcmp(t, "PL") || !strcmp(t, "Fluorescence")) return NISE_TECH_LUM;
     return NISE_TECH_OTHER;
 }
 
@@ -116,12 +120,12 @@ extern "C" int nise_read_input(const char *path, nise_params *p) {
         if (match(buf, "FFT", L)) { p->fft = atoi(value_start(buf, L)); continue; }
         if (match(buf, "Threshold", L)) { p->thres = (float)atof(value_start(buf, L)); continue; }
         if (match(buf, "Couplingcut", L)) { p->couplingcut = (float)atof(value_start(buf, L)); continue; }
-        if (match(buf, "Temperature", L)) continue;
+        if (match(buf, "Temperature", L)) { p->temperature = (float)atof(value_start(buf, L)); continue; }
         if (match(buf, "RunTimes", L)) {
             sscanf(buf, "%255s %d %d %d", dummy, &p->tmax1, &p->tmax2, &p->tmax3);
             continue;
         }
-        if (match(buf, "ImaginaryTimesteps", L)) continue;
+        if (match(buf, "ImaginaryTimesteps", L)) { p->imag_steps = atoi(value_start(buf, L)); continue; }
         if (match(buf, "Trotter", L)) { p->ts = atoi(value_start(buf, L)); continue; }
         if (match(buf, "Interpolation", L)) continue;
         if (match(buf, "Cluster", L)) continue;

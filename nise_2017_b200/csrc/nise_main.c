@@ -74,7 +74,7 @@ int main(int argc, char *argv[]) {
         printf("----------------------------------------\n");
         printf(" %s calculation succesfully completed\n", p.technique >= NISE_TECH_2DUVVIS ? "2DES" : "2DIR");
         printf("----------------------------------------\n\n");
-    } else if (p.technique >= NISE_TECH_LD && p.technique <= NISE_TECH_CD) {
+    } else if (p.technique >= NISE_TECH_LD && p.technique <= NISE_TECH_LUM) {
         double *re = calloc(4 * (size_t)p.tmax1, sizeof(double)), *im = calloc(4 * (size_t)p.tmax1, sizeof(double));
         int channels = 0, samples = 0;
         if ((rc = nise_linear(c, re, im, 4, &channels, &samples)) != NISE_OK) return fail(c, p.technique_name, rc);
@@ -82,19 +82,21 @@ int main(int argc, char *argv[]) {
         double *w = calloc(fft, sizeof(double)), *sr = calloc(fft, sizeof(double)), *si = calloc(fft, sizeof(double));
         for (int k = 0; k < channels; k++) {
             const double *rk = re + (size_t)k * p.tmax1, *ik = im + (size_t)k * p.tmax1;
-            /* TD_DOS.dat has no trailing blank (calc_DOS.c:209), the others do */
-            nise_write_td(nise_linear_file(p.technique, k, 1), &p, rk, ik, samples, p.technique != NISE_TECH_DOS);
+            /* TD_DOS.dat and TD_Lum.dat have no trailing blank (calc_DOS.c:209, luminescence.c:224), the
+               others do; luminescence writes the total's time-domain file only */
+            const char *td = nise_linear_file(p.technique, k, 1);
+            if (td) nise_write_td(td, &p, rk, ik, samples, p.technique != NISE_TECH_DOS && p.technique != NISE_TECH_LUM);
             if ((rc = nise_absorption_fft(c, rk, ik, samples, w, sr, si, fft, &rows)) != NISE_OK)
                 return fail(c, "1D FFT", rc);
             nise_write_spectrum(nise_linear_file(p.technique, k, 0), w, sr, si, rows);
         }
         free(re); free(im); free(w); free(sr); free(si);
-        static const char *done[] = {"Linear Dichroism", "Raman", "SFG", "DOS", "CD"};
+        static const char *done[] = {"Linear Dichroism", "Raman", "SFG", "DOS", "CD", "Luminescence"};
         printf("----------------------------------------------\n");
         printf(" %s calculation succesfully completed\n", done[p.technique - NISE_TECH_LD]);
         printf("----------------------------------------------\n\n");
     } else {
-        fprintf(stderr, "Technique '%s' is not on this engine's path (Absorption, LD, Raman, SFG, DOS, CD, "
+        fprintf(stderr, "Technique '%s' is not on this engine's path (Absorption, LD, Raman, SFG, DOS, CD, Luminescence, "
                 "2DIR, GBIR, SEIR, EAIR, noEAIR, "
                 "2DUVvis, GBUVvis, SEUVvis, EAUVvis, noEAUVvis)\n",
                 p.technique_name);

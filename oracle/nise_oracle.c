@@ -1047,7 +1047,7 @@ static void lum_weight_exact(const oracle_params *p, const float *H, real *v) {
 static void lum_weight_itime(const oracle_params *p, const float *H, real *cr) {
     const int N = p->singles, m = p->imag_steps;
     const float kBT = p->temperature * 0.695;
-    const float f = 1.0 / (m * kBT);
+    const real f = (real)(1.0 / (m * kBT));  /* float in the reference, real here */
     real *reU = (real *)malloc(sizeof(real) * N), *ocr = (real *)malloc(sizeof(real) * N);
     real norm = 0, Q = 0;
     for (int a = 0; a < N; a++) norm += cr[a] * cr[a];
@@ -1056,7 +1056,7 @@ static void lum_weight_itime(const oracle_params *p, const float *H, real *cr) {
         for (int a = 0; a < N; a++) ocr[a] = cr[a] * reU[a];
         for (int a = 0; a < N; a++)
             for (int b = a + 1; b < N; b++) {
-                float J = H[Sindex(a, b, N)];
+                real J = H[Sindex(a, b, N)];
                 if (!(fabs(J) > p->couplingcut)) continue;
                 J = -J * f;
                 const real eJ = (real)(exp(J) * 0.5), emJ = (real)(exp(-J) * 0.5);
