@@ -122,7 +122,8 @@ typedef struct {
                                       Trotter: 1 thread per vector, 64/128/256 level-scheduled
                                       rotations with that many threads per start point, 32/33 a
                                       warp per vector with the rotation table in shared/global
-                                      memory (all bitwise identical);
+                                      memory, 34 a warp per two vectors (static couplings) (all
+                                      bitwise identical);
                                       Sparse/Diagonal (static couplings): 3 or 9 k_abs_taylor2 with
                                       4 or 8 vectors per CTA, 8 the Taylor series (row-owner
                                       layout where it fits, else sliced ELL), 13 the sliced-ELL

@@ -331,6 +331,145 @@ __global__ void k_abs_trotter_wv(DevTraj T, TrotterPlan P, AbsJob J, double2 *re
     }
 }
 
+// Two vectors per warp (static coefficients): both follow the same rotation
+// schedule with the same coefficients, so a lane fetches its chunk's pair and
+// coefficients once and rotates the pair in both vectors; a site's amplitudes
+// of the two vectors sit next to each other (one 16-byte shared load in FP32).
+// Each vector keeps its own start frame, half-step phases and response, and
+// sees the float operations of k_abs_trotter_wv, so the results are bitwise
+// those of that kernel.
+template <typename R> struct TPair {
+    typename Vec2<R>::T a, b;
+};
+
+template <typename R, bool SM>
+__global__ void k_abs_trotter_wv2(DevTraj T, TrotterPlan P, AbsJob J, double2 *resp, int nvec,
+                                  const int *__restrict__ chk_g, int nchk) {
+    typedef typename Vec2<R>::T R2;
+    typedef TPair<R> P2;
+    typedef Ar<R> A;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = P.n, K = P.k, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = blockDim.x >> 5;
+    unsigned char *sp = smem_raw;
+    int *chk = (int *)sp;  // [nchk + 4]: chunk bounds, then K (empty chunks)
+    sp += ((size_t)(nchk + 4) * sizeof(int) + 15) & ~(size_t)15;
+    R2 *tcs = (R2 *)sp;  // SM: [K + 32] coefficients
+    unsigned *tab = (unsigned *)(sp + (SM ? (((size_t)(K + 32) * sizeof(R2) + 15) & ~(size_t)15) : 0));  // SM: pairs
+    if (SM) sp = (unsigned char *)tab + (((size_t)(K + 32) * sizeof(unsigned) + 15) & ~(size_t)15);
+    const int nc = n + 32;  // sites and the 32 spare sites
+    P2 *C = (P2 *)sp + (size_t)warp * nc;
+    for (int e = threadIdx.x; e < nchk + 4; e += blockDim.x) chk[e] = e <= nchk ? chk_g[e] : K;
+    R2 unit;
+    unit.x = 1;
+    unit.y = 0;
+    if (SM) {
+        for (int e = threadIdx.x; e < K + 32; e += blockDim.x) {
+            const int2 ab = e < K ? P.pairs[e] : make_int2(n + e - K, n + e - K);
+            tab[e] = (unsigned)ab.x | ((unsigned)ab.y << 16);
+            tcs[e] = e < K ? ((const R2 *)P.rot)[e] : unit;
+        }
+    }
+    __syncthreads();
+    const int v0 = (blockIdx.x * W + warp) * 2, v1 = v0 + 1;
+    if (v0 >= nvec) return;
+    const bool has1 = v1 < nvec;
+    const int x0 = v0 % 3, x1 = v1 % 3;
+    const long ti0 = (long)(J.begin + v0 / 3) * J.sample, ti1 = (long)(J.begin + (has1 ? v1 : v0) / 3) * J.sample;
+    for (int a = lane; a < nc; a += 32) {
+        P2 z;
+        z.a.x = a < n ? (R)traj_mu(T, ti0, x0, a) : (R)0;
+        z.b.x = a < n && has1 ? (R)traj_mu(T, ti1, x1, a) : (R)0;
+        z.a.y = z.b.y = 0;
+        C[a] = z;
+    }
+    const R2 *U = (const R2 *)P.U;
+    const R2 *Rf = SM ? tcs : (const R2 *)P.rot;
+    const int2 spare = make_int2(n + lane, n + lane);
+    auto rot1 = [&](R2 &xa, R2 &xb, const R2 cs) {  // propagate.c:876-888
+        R2 ya, yb;
+        ya.x = A::sub(A::mul(cs.x, xa.x), A::mul(cs.y, xb.y));
+        ya.y = A::add(A::mul(cs.x, xa.y), A::mul(cs.y, xb.x));
+        yb.x = A::sub(A::mul(cs.x, xb.x), A::mul(cs.y, xa.y));
+        yb.y = A::add(A::mul(cs.x, xb.y), A::mul(cs.y, xa.x));
+        xa = ya;
+        xb = yb;
+    };
+    auto mulu = [&](R2 z, R2 u) {
+        R2 o;
+        o.x = A::sub(A::mul(z.x, u.x), A::mul(z.y, u.y));
+        o.y = A::add(A::mul(z.y, u.x), A::mul(z.x, u.y));
+        return o;
+    };
+    for (int t1 = 0; t1 < J.tmax; t1++) {
+        const long ta = ti0 + t1, tb = ti1 + t1;
+        const bool step = t1 + 1 < J.tmax;
+        const R2 *Ua = U + (ta - P.f0) * n, *Ub = U + (tb - P.f0) * n;
+        double re0 = 0, im0 = 0, re1 = 0, im1 = 0;
+#pragma unroll 4
+        for (int a = lane; a < n; a += 32) {
+            const P2 z = C[a];
+            const R m0 = (R)traj_mu(T, ta, x0, a), m1 = (R)traj_mu(T, tb, x1, a);
+            re0 += (double)A::mul(m0, z.a.x);
+            im0 += (double)A::mul(m0, z.a.y);
+            re1 += (double)A::mul(m1, z.b.x);
+            im1 += (double)A::mul(m1, z.b.y);
+        }
+        const double2 rs0 = resp_sum_warp(re0, im0, n), rs1 = resp_sum_warp(re1, im1, n);
+        if (lane == 0) {
+            resp[(size_t)v0 * J.tmax + t1] = rs0;
+            if (has1) resp[(size_t)v1 * J.tmax + t1] = rs1;
+        }
+        if (!step) break;
+        auto phase = [&]() {  // propagate.c:870-873 / 891-894, each vector with its frame's phases
+#pragma unroll 4
+            for (int a = lane; a < n; a += 32) {
+                P2 z = C[a];
+                z.a = mulu(z.a, Ua[a]);
+                z.b = mulu(z.b, Ub[a]);
+                C[a] = z;
+            }
+        };
+        for (int sub = 0; sub < J.ts; sub++) {
+            phase();
+            __syncwarp();
+            int e0 = chk[1], e1 = chk[2];
+            int2 ab0;
+            R2 cs0;
+            auto fetch = [&](int k, int end, int2 &ab, R2 &cs) {
+                if (SM) {  // identity entry congruent to k mod 32: no bank conflict with the chunk
+                    k = k < end ? k : K + ((k - K) & 31);
+                    const unsigned w = tab[k];
+                    ab = make_int2((int)(w & 0xffffu), (int)(w >> 16));
+                    cs = Rf[k];
+                } else {
+                    ab = k < end ? P.pairs[k] : spare;
+                    cs = k < end ? Rf[k] : unit;
+                }
+            };
+            fetch(chk[0] + lane, e0, ab0, cs0);
+#pragma unroll 2
+            for (int c = 0; c < nchk; c++) {
+                int2 ab1;
+                R2 cs1;
+                fetch(e0 + lane, e1, ab1, cs1);
+                const int e2 = chk[c + 3];
+                P2 pa = C[ab0.x], pb = C[ab0.y];
+                rot1(pa.a, pb.a, cs0);
+                rot1(pa.b, pb.b, cs0);
+                C[ab0.x] = pa;
+                C[ab0.y] = pb;
+                __syncwarp();
+                e0 = e1;
+                e1 = e2;
+                ab0 = ab1;
+                cs0 = cs1;
+            }
+            phase();
+            __syncwarp();
+        }
+    }
+}
+
 // ------------------------------------------------------------ RK4
 template <typename R>
 __global__ void k_prep_rk4(DevTraj T, Rk4Plan P, R fsub) {
@@ -1426,6 +1565,48 @@ int launch_abs_trotter_wv(int prec, const DevTraj &T, const TrotterPlan &P, cons
         else NISE_WV(double, false);
     }
 #undef NISE_WV
+    return (int)cudaGetLastError();
+}
+
+// Two vectors per warp (static coefficients only): W warps of 2 vectors per
+// CTA, W = half the vectors per SM (at most 16, as shared memory allows), the
+// rotation table in shared memory where it fits.
+int launch_abs_trotter_wv2(int prec, const DevTraj &T, const TrotterPlan &P, const AbsJob &J, double2 *resp,
+                           const int *chk, int nchk, cudaStream_t s) {
+    if (J.nsamp <= 0) return 0;
+    if (!P.rot_static) return (int)cudaErrorNotSupported;
+    const int nvec = 3 * J.nsamp, nsm = sm_count(), npair = (nvec + 1) / 2;
+    const size_t r2 = prec == 0 ? sizeof(float2) : sizeof(double2);
+    auto bytes = [&](bool m, int w) {
+        size_t b = ((size_t)(nchk + 4) * sizeof(int) + 15) & ~(size_t)15;
+        if (m) b += (((size_t)(P.k + 32) * r2 + 15) & ~(size_t)15) + (((size_t)(P.k + 32) * sizeof(unsigned) + 15) & ~(size_t)15);
+        return b + (size_t)w * (P.n + 32) * 2 * r2;
+    };
+    bool sm = P.n + 32 <= 65536;
+    int W = std::min(16, std::max(1, (npair + nsm - 1) / nsm));
+    while (W > 1 && bytes(sm, W) > kMaxSmem) W--;
+    if (sm && bytes(sm, W) > kMaxSmem) sm = false;
+    if (!sm) {
+        W = std::min(16, std::max(1, (npair + nsm - 1) / nsm));
+        while (W > 1 && bytes(false, W) > kMaxSmem) W--;
+    }
+    if (bytes(sm, W) > kMaxSmem) return (int)cudaErrorNotSupported;
+    const size_t smem = bytes(sm, W);
+    const int grid = (npair + W - 1) / W;
+    int e;
+#define NISE_WV2(RT, SMT)                                                                    \
+    do {                                                                                   \
+        if ((e = set_smem(k_abs_trotter_wv2<RT, SMT>, smem))) return e;                    \
+        k_abs_trotter_wv2<RT, SMT><<<grid, 32 * W, smem, s>>>(T, P, J, resp, nvec, chk, nchk); \
+    } while (0)
+    if (prec == 0) {
+        if (sm) NISE_WV2(float, true);
+        else NISE_WV2(float, false);
+    } else {
+        if (sm) NISE_WV2(double, true);
+        else NISE_WV2(double, false);
+    }
+#undef NISE_WV2
     return (int)cudaGetLastError();
 }
 

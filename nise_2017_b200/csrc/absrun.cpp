@@ -48,8 +48,14 @@ std::mutex g_tune_mu;
 // ~20 rotations per level) or the job has too few vectors to fill warps of
 // threads (a warp per vector then has the shorter critical path); thread per
 // vector for chains (one rotation per level) with many vectors.
-int default_config(int scheme, int N, bool plain, bool cheb, int K, int nchk, int nvec, bool has4, bool rv) {
+int default_config(int scheme, int N, bool plain, bool cheb, int K, int nchk, int nvec, bool has4, bool rv,
+                   bool rot_static) {
     if (scheme == SCHEME_TROTTER) {
+        // a warp per two vectors once there are 8 or more vectors per SM (static
+        // couplings; 1024-site lattice, 1185 vectors: 39.3 against 43.9 ms),
+        // else a warp per vector (C4's 585-vector jobs: 18.6 against 25.5 ms at
+        // 1875 sites)
+        if (K > 0 && rot_static && nvec >= 8 * sm_count()) return 34;
         if (K > 0 && (K >= 4 * nchk || nvec < 1024)) return 32;
         return N >= 96 ? 128 : 0;
     }
@@ -670,11 +676,14 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
         }
     }
     config = default_config(scheme, N, plain, cheb, TP.k, nchk, plain ? 3 : nvec, dell4.p != nullptr,
-                            scheme == SCHEME_TAYLOR && taylor_rv_fits(T, XP));
+                            scheme == SCHEME_TAYLOR && taylor_rv_fits(T, XP),
+                            scheme == SCHEME_TROTTER && TP.rot_static);
     if (p.kernel_config != 0) {  // forced by the caller
         const int k = p.kernel_config;
         if (scheme == SCHEME_EIGEN && (k == 2 || k == 16 || k == 17)) return NISE_OK;
-        if (scheme == SCHEME_TROTTER && (k == 1 || k == 32 || k == 33 || k == 64 || k == 128 || k == 256)) config = k == 1 ? 0 : k;
+        if (scheme == SCHEME_TROTTER &&
+            (k == 1 || k == 32 || k == 33 || (k == 34 && TP.rot_static) || k == 64 || k == 128 || k == 256))
+            config = k == 1 ? 0 : k;
         else if (scheme == SCHEME_TAYLOR &&
                  (k == 3 || k == 8 || k == 9 || (k == 10 && cheb) || (k == 12 && dell4.p) || k == 13 || k == 14 ||
                   (k == 15 && cheb && dtri8.p)))
@@ -702,6 +711,7 @@ int AbsRun::run_main(cudaStream_t s, int cfg, double2 *dst) {
         switch (scheme) {
         case SCHEME_TROTTER:
             if (cfg == 32 || cfg == 33) return launch_abs_trotter_wv(pr, T, TP, Js, r, lvchk.p, nchk, cfg == 32, s);
+            if (cfg == 34) return launch_abs_trotter_wv2(pr, T, TP, Js, r, lvchk.p, nchk, s);
             if (cfg > 0) return launch_abs_trotter_lv(pr, T, TP, Js, r, lvptr.p, nlev, cfg, s);
             return launch_abs_trotter(pr, T, TP, Js, r, s);
         case SCHEME_RK4:
@@ -770,6 +780,7 @@ int AbsRun::tune() {
     std::vector<int> cand;
     if (scheme == SCHEME_TROTTER) {
         cand = {0, 32, 33, 64, 128, 256};
+        if (TP.rot_static) cand.push_back(34);
     } else {
         cand = {3, -8, 8, 13, 14};
         if (cheb) cand.push_back(10);

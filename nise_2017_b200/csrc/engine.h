@@ -115,6 +115,10 @@ int sm_count();
 // rotation table in shared memory where it fits; 0: read from global memory.
 int launch_abs_trotter_wv(int prec, const DevTraj &T, const TrotterPlan &P, const AbsJob &J, double2 *resp,
                           const int *chk, int nchk, int tables, cudaStream_t s);
+// Two vectors per warp sharing the schedule (static coefficients only),
+// bitwise identical to launch_abs_trotter_wv.
+int launch_abs_trotter_wv2(int prec, const DevTraj &T, const TrotterPlan &P, const AbsJob &J, double2 *resp,
+                           const int *chk, int nchk, cudaStream_t s);
 int launch_prep_rk4(int prec, const DevTraj &T, const Rk4Plan &P, double fsub, float fsub32, cudaStream_t s);
 int launch_abs_rk4(int prec, const DevTraj &T, const Rk4Plan &P, const AbsJob &J, double2 *resp, cudaStream_t s);
 int launch_prep_taylor(int prec, const DevTraj &T, TaylorPlan &P, double rowabs_max, double f, int *order,
