@@ -1,7 +1,8 @@
 // Adjoint of linear absorption (no reference counterpart; the reference has
 // no derivatives).  The differentiable model is the Trotter "Coupling"
 // absorption of propagate_vec_coupling_S (propagate.c:821-899) and
-// absorption.c:119-145 in FP64, with three parameters:
+// absorption.c:119-145 in FP64 (and, further below, the RK4 scheme of
+// propagate_vec_RK4), with three parameters:
 //   b_a  per-site energy shifts added to the shifted diagonal (the b of a
 //        SingleShift with a = 1, hamshift.c:59-66),
 //   s    a global scale of every coupling (after the read cut),
@@ -198,6 +199,260 @@ int lanes_adj(size_t lane_bytes) {
     return B;
 }
 
+// ------------------------------------------------------------------ RK4
+// The RK4 scheme of propagate_vec_RK4 (propagate.c:261-373) as the model:
+// per frame m = Trotter sub-steps of y = P(A) x, P(A) = I + A + A^2/2 + A^3/6
+// + A^4/24 (RK4 for a constant H is its fourth-order Taylor polynomial),
+// A = -i H f/m, then x' = y |x| / |y| (re_normalize to the pre-step norm).
+// H = diag(h + b) + s J over every nonzero coupling of the pattern (as the
+// Trotter model, so that it is smooth in s).  Vectors live in global scratch,
+// slot q of vector v at base + (q n + a) nvec + v (a warp's lanes read
+// consecutive addresses).
+//
+// Adjoint of one sub-step, l the gradient with respect to x':
+//   c = Re(l . y), l_y = r l - c |x| y / |y|^3 (r = |x|/|y|), and the norm's
+//   own term c x / (|x| |y|) goes to l_x;
+//   l_x += P(A)^+ l_y = sum_p w_p / p!, w_p = (A^+)^p l_y, A^+ = +i H f/m;
+//   dL = Re sum_{p+q<=3} w_p^+ dA u_q / (p+q+1)!, u_q = A^q x, dA = -i dH f/m:
+//   the shift b_a gets (f/m) sum Im(conj(v_q,a) u_q,a) and the scale s gets
+//   (f/m) sum_k J_k [Im(conj(v_q,a) u_q,b) + Im(conj(v_q,b) u_q,a)], with
+//   v_q = sum_{p<=3-q} w_p / (p+q+1)!.
+// The backward sweep recomputes the frame states of each checkpoint block,
+// then each frame's sub-step inputs, from the forward checkpoints.
+struct Rk4Adj {
+    int n, k, m, K, nck, nvec;
+    const int2 *pairs;
+    long f0, nf;
+    const double *D, *Jc, *jf;  // [nf][n] (h + b) f/m, [nf][k] s J f/m, [nf][k] J f/m
+    double2 *scr;               // [slots][n][nvec]
+    double fm;
+};
+
+__global__ void k_adj_rk4_prep(DevTraj T, AdjPlan P, double fm, double *D, double *Jc, double *jf) {
+    long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const long nU = P.nf * P.n, nR = P.nf * P.k;
+    if (g < nU) {
+        long t = g / P.n;
+        int a = (int)(g % P.n);
+        D[g] = ((double)traj_diag_raw(T, P.f0 + t, a) + P.shift[a]) * fm;
+        return;
+    }
+    g -= nU;
+    if (g < nR) {
+        long t = g / P.k;
+        int k = (int)(g % P.k);
+        int2 ab = P.pairs[k];
+        const double J = (double)traj_coupling(T, P.f0 + t, ab.x, ab.y) * fm;
+        jf[g] = J;
+        Jc[g] = P.scale * J;
+    }
+}
+
+struct Slot {
+    double2 *p;
+    int nvec;
+    __device__ double2 &operator[](int a) const { return p[(size_t)a * nvec]; }
+};
+
+__device__ __forceinline__ Slot slot(const Rk4Adj &R, int q, int v) {
+    return Slot{R.scr + (size_t)q * R.n * R.nvec + v, R.nvec};
+}
+
+// y = H0 x (H0 = H f/m, real symmetric), frame row fi.
+__device__ void rk4_h(const Rk4Adj &R, long fi, Slot x, Slot y) {
+    const double *D = R.D + fi * R.n, *Jc = R.Jc + fi * R.k;
+    for (int a = 0; a < R.n; a++) {
+        const double2 z = x[a];
+        y[a] = make_double2(D[a] * z.x, D[a] * z.y);
+    }
+    for (int k = 0; k < R.k; k++) {
+        const int2 ab = R.pairs[k];
+        const double j = Jc[k];
+        const double2 xa = x[ab.x], xb = x[ab.y], ya = y[ab.x], yb = y[ab.y];
+        y[ab.x] = make_double2(ya.x + j * xb.x, ya.y + j * xb.y);
+        y[ab.y] = make_double2(yb.x + j * xa.x, yb.y + j * xa.y);
+    }
+}
+
+// y = A x (adj = false, A = -i H0) or y = A^+ x (adj = true, +i H0).
+__device__ void rk4_a(const Rk4Adj &R, long fi, Slot x, Slot y, bool adj) {
+    rk4_h(R, fi, x, y);
+    for (int a = 0; a < R.n; a++) {
+        const double2 h = y[a];
+        y[a] = adj ? make_double2(-h.y, h.x) : make_double2(h.y, -h.x);
+    }
+}
+
+__device__ double rk4_norm2(const Rk4Adj &R, Slot x) {
+    double s = 0;
+    for (int a = 0; a < R.n; a++) {
+        const double2 z = x[a];
+        s += z.x * z.x + z.y * z.y;
+    }
+    return s;
+}
+
+// y = P(A) x by Horner's rule (t <- x + A t / j, j = 4, 3, 2, 1); tmp is scratch.
+__device__ void rk4_poly(const Rk4Adj &R, long fi, Slot x, Slot y, Slot tmp) {
+    for (int a = 0; a < R.n; a++) y[a] = x[a];
+    for (int j = 4; j >= 1; j--) {
+        rk4_a(R, fi, y, tmp, false);
+        const double c = 1.0 / j;
+        for (int a = 0; a < R.n; a++) {
+            const double2 z = x[a], u = tmp[a];
+            y[a] = make_double2(z.x + c * u.x, z.y + c * u.y);
+        }
+    }
+}
+
+// One frame: m sub-steps x <- P(A) x |x| / |P(A) x|, in place (y, tmp scratch).
+__device__ void rk4_frame(const Rk4Adj &R, long fi, Slot x, Slot y, Slot tmp) {
+    for (int sub = 0; sub < R.m; sub++) {
+        const double n0 = rk4_norm2(R, x);
+        rk4_poly(R, fi, x, y, tmp);
+        const double sc = sqrt(n0 / rk4_norm2(R, y));
+        for (int a = 0; a < R.n; a++) {
+            const double2 z = y[a];
+            x[a] = make_double2(z.x * sc, z.y * sc);
+        }
+    }
+}
+
+// slots of the forward kernel: 0 state, 1 y, 2 tmp
+__global__ void k_adj_rk4_fwd(DevTraj T, Rk4Adj R, AbsJob J, double2 *resp, double2 *ckpt) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= R.nvec) return;
+    const int x = v % 3, n = R.n;
+    const long ti = (long)(J.begin + v / 3) * J.sample;
+    Slot X = slot(R, 0, v), Y = slot(R, 1, v), Tm = slot(R, 2, v);
+    for (int a = 0; a < n; a++) X[a] = make_double2((double)traj_mu(T, ti, x, a), 0.0);
+    for (int t1 = 0; t1 < J.tmax; t1++) {
+        const long t = ti + t1;
+        double re = 0, im = 0;
+        for (int a = 0; a < n; a++) {
+            const double mu = (double)traj_mu(T, t, x, a);
+            const double2 z = X[a];
+            re += mu * z.x;
+            im += mu * z.y;
+        }
+        resp[(size_t)v * J.tmax + t1] = make_double2(re, im);
+        if (t1 == J.tmax - 1) break;
+        if (t1 % R.K == 0)
+            for (int a = 0; a < n; a++) ckpt[((size_t)v * R.nck + t1 / R.K) * n + a] = X[a];
+        rk4_frame(R, t - R.f0, X, Y, Tm);
+    }
+}
+
+// slots of the backward kernel: 0 l, 1 y, 2 tmp, 3 l_new, 4 w, 5 w', 6..9 u_q,
+// 10..13 v_q, 14.. the block's frame states (K), then the frame's sub-step
+// inputs (m)
+__global__ void k_adj_rk4_bwd(DevTraj T, Rk4Adj R, AbsJob J, const double2 *G, const double2 *ckpt, double *gshift,
+                              double *gscale) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= R.nvec) return;
+    const int x = v % 3, n = R.n;
+    const long ti = (long)(J.begin + v / 3) * J.sample;
+    Slot L = slot(R, 0, v), Y = slot(R, 1, v), Tm = slot(R, 2, v), Ln = slot(R, 3, v), W = slot(R, 4, v),
+         W2 = slot(R, 5, v);
+    double *gs = gshift + (size_t)v * n;
+    for (int a = 0; a < n; a++) gs[a] = 0;
+    double gsc = 0;
+    {
+        const double2 g = G[J.tmax - 1];
+        for (int a = 0; a < n; a++) {
+            const double mu = (double)traj_mu(T, ti + J.tmax - 1, x, a);
+            L[a] = make_double2(mu * g.x, mu * g.y);
+        }
+    }
+    const double c_pq[7] = {1.0, 1.0, 1.0 / 2, 1.0 / 6, 1.0 / 24, 1.0 / 120, 1.0 / 720};  // 1/j!
+    for (int cb = R.nck - 1; cb >= 0; cb--) {
+        const int tb0 = cb * R.K, tb1 = min(tb0 + R.K, J.tmax - 1);  // frames [tb0, tb1) propagate
+        // the block's frame states from its checkpoint
+        Slot S0 = slot(R, 14, v);
+        for (int a = 0; a < n; a++) S0[a] = ckpt[((size_t)v * R.nck + cb) * n + a];
+        for (int j = 1; j < tb1 - tb0; j++) {
+            Slot Sp = slot(R, 14 + j - 1, v), Sj = slot(R, 14 + j, v);
+            for (int a = 0; a < n; a++) Sj[a] = Sp[a];
+            rk4_frame(R, ti + tb0 + j - 1 - R.f0, Sj, Y, Tm);
+        }
+        for (int t1 = tb1 - 1; t1 >= tb0; t1--) {
+            const long fi = ti + t1 - R.f0;
+            // the frame's sub-step inputs
+            for (int a = 0; a < n; a++) slot(R, 14 + R.K, v)[a] = slot(R, 14 + t1 - tb0, v)[a];
+            for (int s = 1; s < R.m; s++) {
+                Slot Ip = slot(R, 14 + R.K + s - 1, v), Is = slot(R, 14 + R.K + s, v);
+                for (int a = 0; a < n; a++) Is[a] = Ip[a];
+                const double n0 = rk4_norm2(R, Is);
+                rk4_poly(R, fi, Is, Y, Tm);
+                const double sc = sqrt(n0 / rk4_norm2(R, Y));
+                for (int a = 0; a < n; a++) {
+                    const double2 z = Y[a];
+                    Is[a] = make_double2(z.x * sc, z.y * sc);
+                }
+            }
+            for (int s = R.m - 1; s >= 0; s--) {
+                Slot X = slot(R, 14 + R.K + s, v);
+                // forward powers u_q = A^q x (u_0 = x)
+                for (int a = 0; a < n; a++) slot(R, 6, v)[a] = X[a];
+                for (int q = 1; q < 4; q++) rk4_a(R, fi, slot(R, 6 + q - 1, v), slot(R, 6 + q, v), false);
+                // y = P(A) x and the renormalisation
+                rk4_poly(R, fi, X, Y, Tm);
+                const double nx = sqrt(rk4_norm2(R, X)), ny = sqrt(rk4_norm2(R, Y)), r = nx / ny;
+                double c = 0;
+                for (int a = 0; a < n; a++) {
+                    const double2 l = L[a], y = Y[a];
+                    c += l.x * y.x + l.y * y.y;
+                }
+                const double cy = c * nx / (ny * ny * ny), cx = c / (nx * ny);
+                // w_0 = l_y; l_new = norm term + w_0; v_q = w_0 / (q+1)!
+                for (int a = 0; a < n; a++) {
+                    const double2 l = L[a], y = Y[a], z = X[a];
+                    const double2 w = make_double2(r * l.x - cy * y.x, r * l.y - cy * y.y);
+                    W[a] = w;
+                    Ln[a] = make_double2(cx * z.x + w.x, cx * z.y + w.y);
+                    for (int q = 0; q < 4; q++) slot(R, 10 + q, v)[a] = make_double2(w.x * c_pq[q + 1], w.y * c_pq[q + 1]);
+                }
+                for (int p = 1; p <= 4; p++) {  // w_p = A^+ w_(p-1)
+                    rk4_a(R, fi, p % 2 ? W : W2, p % 2 ? W2 : W, true);
+                    Slot Wp = p % 2 ? W2 : W;
+                    for (int a = 0; a < n; a++) {
+                        const double2 w = Wp[a];
+                        const double2 ln = Ln[a];
+                        Ln[a] = make_double2(ln.x + c_pq[p] * w.x, ln.y + c_pq[p] * w.y);
+                        for (int q = 0; q + p <= 3; q++) {
+                            const double2 vq = slot(R, 10 + q, v)[a];
+                            const double cf = c_pq[p + q + 1];
+                            slot(R, 10 + q, v)[a] = make_double2(vq.x + cf * w.x, vq.y + cf * w.y);
+                        }
+                    }
+                }
+                // parameter gradients: Im(conj(v) u) = v.x u.y - v.y u.x
+                const double *jf = R.jf + fi * R.k;
+                for (int q = 0; q < 4; q++) {
+                    Slot Vq = slot(R, 10 + q, v), Uq = slot(R, 6 + q, v);
+                    for (int a = 0; a < n; a++) {
+                        const double2 vv = Vq[a], uu = Uq[a];
+                        gs[a] += R.fm * (vv.x * uu.y - vv.y * uu.x);
+                    }
+                    for (int k = 0; k < R.k; k++) {
+                        const int2 ab = R.pairs[k];
+                        const double2 va = Vq[ab.x], vb = Vq[ab.y], ua = Uq[ab.x], ub = Uq[ab.y];
+                        gsc += jf[k] * ((va.x * ub.y - va.y * ub.x) + (vb.x * ua.y - vb.y * ua.x));
+                    }
+                }
+                for (int a = 0; a < n; a++) L[a] = Ln[a];
+            }
+            const double2 g = G[t1];
+            for (int a = 0; a < n; a++) {
+                const double mu = (double)traj_mu(T, ti + t1, x, a);
+                const double2 l = L[a];
+                L[a] = make_double2(l.x + mu * g.x, l.y + mu * g.y);
+            }
+        }
+    }
+    gscale[v] = gsc;
+}
+
 }  // namespace
 
 int launch_adj_prep(const DevTraj &T, const AdjPlan &P, cudaStream_t s) {
@@ -233,6 +488,23 @@ int launch_adj_bwd(const DevTraj &T, const AdjPlan &P, const AbsJob &J, const do
     return (int)cudaGetLastError();
 }
 
+int launch_adj_rk4(const DevTraj &T, const AdjPlan &P, const Rk4Adj &R, const AbsJob &J, const double2 *G,
+                   double2 *resp, double2 *ckpt, double *gshift_part, double *gscale_part, double *gshift,
+                   double *gscale, cudaStream_t s) {
+    const long tot = P.nf * P.n + P.nf * P.k;
+    if (!G) {
+        if (tot > 0)
+            k_adj_rk4_prep<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(T, P, R.fm, (double *)R.D, (double *)R.Jc,
+                                                                       (double *)R.jf);
+        k_adj_rk4_fwd<<<(R.nvec + 63) / 64, 64, 0, s>>>(T, R, J, resp, ckpt);
+        return (int)cudaGetLastError();
+    }
+    k_adj_rk4_bwd<<<(R.nvec + 63) / 64, 64, 0, s>>>(T, R, J, G, ckpt, gshift_part, gscale_part);
+    k_adj_reduce<<<(P.n + 127) / 128, 128, 0, s>>>(gshift_part, R.nvec, P.n, gshift);
+    k_adj_reduce<<<1, 1, 0, s>>>(gscale_part, R.nvec, 1, gscale);
+    return (int)cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ host
 #include <cmath>
 #include <cstring>
@@ -257,7 +529,7 @@ int adj_forward(nise_ctx *c, const double *shift, double scale, int K, AdjRun &R
                 DevBuf<double2> &ckpt, AdjPlan &P, AbsJob &J) {
     const nise_params &p = c->p;
     if (p.propagation != NISE_PROP_COUPLING)
-        return nise_fail(c, NISE_ERR_UNSUPPORTED, "the absorption adjoint differentiates Propagation Coupling");
+        return nise_fail(c, NISE_ERR_UNSUPPORTED, "the absorption adjoint differentiates Propagation Coupling and RK4");
     if (!c->loaded) return nise_fail(c, NISE_ERR_STATE, "no trajectory loaded");
     if (!shift || !(scale == scale)) return nise_fail(c, NISE_ERR_ARG, "null shifts or invalid scale");
     const int N = c->n, tmax = p.tmax1;
@@ -315,6 +587,95 @@ int adj_forward(nise_ctx *c, const double *shift, double scale, int K, AdjRun &R
     R.S.resize(tmax);
     cudaMemcpyAsync(R.S.data(), out.p, sizeof(double2) * tmax, cudaMemcpyDeviceToHost, c->stream);
     return nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "adjoint forward");
+}
+
+// The RK4 model (Propagation RK4): forward responses, tables and checkpoints
+// left in W for the backward sweep.
+struct Rk4Work {
+    DevBuf<double> dshift, D, Jc, jf;
+    DevBuf<int2> dpairs;
+    DevBuf<double2> scr, ckpt;
+    AdjPlan P;
+    Rk4Adj A;
+    AbsJob J;
+};
+
+int adj_rk4_forward(nise_ctx *c, const double *shift, double scale, int K, AdjRun &R, Rk4Work &W) {
+    const nise_params &p = c->p;
+    if (!c->loaded) return nise_fail(c, NISE_ERR_STATE, "no trajectory loaded");
+    if (!shift || !(scale == scale)) return nise_fail(c, NISE_ERR_ARG, "null shifts or invalid scale");
+    const int N = c->n, tmax = p.tmax1;
+    int n_samples = (p.length - p.tmax1 - 1) / p.sample + 1;
+    if (n_samples <= 0) return nise_fail(c, NISE_ERR_ARG, "Insufficient data to calculate spectrum.");
+    R.end = p.end == 0 ? n_samples : p.end;
+    R.begin = p.begin;
+    if (R.end > n_samples || R.begin < 0 || R.begin >= R.end) return nise_fail(c, NISE_ERR_ARG, "bad BeginPoint/EndPoint");
+    R.nsamp = R.end - R.begin;
+    R.f0 = (long)R.begin * p.sample;
+    long f1 = (long)(R.end - 1) * p.sample + tmax - 1;
+    int rc;
+    if ((rc = nise_check_frames(c, f1))) return rc;
+    R.nf = f1 - R.f0 > 0 ? f1 - R.f0 : 1;
+    std::vector<int2> pairs;
+    if ((rc = nise_pattern(c, R.f0, R.nf, pairs))) return rc;
+    const int nvec = 3 * R.nsamp, m = p.ts;
+    AdjPlan &P = W.P;
+    memset(&P, 0, sizeof(P));
+    P.n = N;
+    P.k = (int)pairs.size();
+    P.ts = m;
+    P.f0 = R.f0;
+    P.nf = R.nf;
+    P.scale = scale;
+    Rk4Adj &A = W.A;
+    memset(&A, 0, sizeof(A));
+    A.n = N;
+    A.k = P.k;
+    A.m = m;
+    A.K = K;
+    A.nck = (tmax - 1 + K - 1) / K;
+    A.nvec = nvec;
+    A.f0 = R.f0;
+    A.nf = R.nf;
+    A.fm = nise_f64(p, 1, m);
+    const size_t slots = 14 + (size_t)K + m;
+    if ((size_t)nvec * N * slots * sizeof(double2) > ((size_t)8 << 30))
+        return nise_fail(c, NISE_ERR_NOMEM, "RK4 adjoint: %zu bytes of scratch", (size_t)nvec * N * slots * 16);
+    std::vector<double> hs(shift, shift + N);
+    if ((rc = W.dshift.upload(c, hs)) || (rc = W.dpairs.upload(c, pairs.empty() ? std::vector<int2>(1) : pairs)) ||
+        (rc = W.D.alloc(c, (size_t)R.nf * N)) || (rc = W.Jc.alloc(c, (size_t)R.nf * (P.k ? P.k : 1))) ||
+        (rc = W.jf.alloc(c, (size_t)R.nf * (P.k ? P.k : 1))) || (rc = W.scr.alloc(c, slots * N * nvec)) ||
+        (rc = W.ckpt.alloc(c, (size_t)nvec * (A.nck ? A.nck : 1) * N)))
+        return rc;
+    P.shift = W.dshift.p;
+    P.pairs = W.dpairs.p;
+    A.pairs = W.dpairs.p;
+    A.D = W.D.p;
+    A.Jc = W.Jc.p;
+    A.jf = W.jf.p;
+    A.scr = W.scr.p;
+    AbsJob &J = W.J;
+    memset(&J, 0, sizeof(J));
+    J.begin = R.begin;
+    J.nsamp = R.nsamp;
+    J.sample = p.sample;
+    J.tmax = tmax;
+    J.ts = m;
+    DevTraj T = nise_devtraj(c);
+    DevBuf<double2> resp, out;
+    if ((rc = resp.alloc(c, (size_t)nvec * tmax)) || (rc = out.alloc(c, tmax))) return rc;
+    c->launches = 0;
+    cudaEventRecord(c->ev0, c->stream);
+    cudaEventRecord(c->evk0, c->stream);
+    if ((rc = nise_cuda(c, launch_adj_rk4(T, P, A, J, nullptr, resp.p, W.ckpt.p, nullptr, nullptr, nullptr, nullptr,
+                                          c->stream),
+                        "RK4 adjoint forward")) ||
+        (rc = nise_cuda(c, launch_reduce_resp(resp.p, nvec, tmax, out.p, c->stream), "response reduction")))
+        return rc;
+    c->launches += 3;
+    R.S.resize(tmax);
+    cudaMemcpyAsync(R.S.data(), out.p, sizeof(double2) * tmax, cudaMemcpyDeviceToHost, c->stream);
+    return nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "RK4 adjoint forward");
 }
 
 // The FP64 branch of the 1D transform input factors (1DFFT.c:170-200) for
@@ -386,7 +747,10 @@ extern "C" int nise_absorption_model(nise_ctx *c, const double *site_shift, doub
     DevBuf<double2> U, rot, ckpt;
     AdjPlan P;
     AbsJob J;
-    int rc = adj_forward(c, site_shift, coupling_scale, c->p.tmax1, R, dshift, dpairs, U, rot, jf, ckpt, P, J);
+    Rk4Work W;
+    int rc = c->p.propagation == NISE_PROP_RK4
+                 ? adj_rk4_forward(c, site_shift, coupling_scale, 32, R, W)
+                 : adj_forward(c, site_shift, coupling_scale, c->p.tmax1, R, dshift, dpairs, U, rot, jf, ckpt, P, J);
     if (rc) return rc;
     cudaEventRecord(c->evk1, c->stream);
     cudaEventRecord(c->ev1, c->stream);
@@ -428,7 +792,10 @@ extern "C" int nise_backward_absorption(nise_ctx *c, const double *site_shift, d
     AdjPlan P;
     AbsJob J;
     const int K = 32;  // checkpoint interval (steps)
-    int rc = adj_forward(c, site_shift, coupling_scale, K, R, dshift, dpairs, U, rot, jf, ckpt, P, J);
+    const bool rk4 = p.propagation == NISE_PROP_RK4;
+    Rk4Work W;
+    int rc = rk4 ? adj_rk4_forward(c, site_shift, coupling_scale, K, R, W)
+                 : adj_forward(c, site_shift, coupling_scale, K, R, dshift, dpairs, U, rot, jf, ckpt, P, J);
     if (rc) return rc;
     // adjoint of the transform: dL/dOut_k = (dL/dspec_im + i dL/dspec_re) * 2 dt c_v,
     // dL/din_j = sum_k exp(+2 pi i jk/fft) dL/dOut_k, then through the input factors
@@ -459,9 +826,13 @@ extern "C" int nise_backward_absorption(nise_ctx *c, const double *site_shift, d
         (rc = gs.alloc(c, N)) || (rc = gc.alloc(c, 1)))
         return rc;
     DevTraj T = nise_devtraj(c);
-    if ((rc = nise_cuda(c, launch_adj_bwd(T, P, J, dG.p, ckpt.p, gsp.p, gcp.p, gs.p, gc.p, c->stream),
-                        "adjoint backward")))
-        return rc;
+    if (rk4)
+        rc = nise_cuda(c, launch_adj_rk4(T, W.P, W.A, W.J, dG.p, nullptr, W.ckpt.p, gsp.p, gcp.p, gs.p, gc.p, c->stream),
+                       "RK4 adjoint backward");
+    else
+        rc = nise_cuda(c, launch_adj_bwd(T, P, J, dG.p, ckpt.p, gsp.p, gcp.p, gs.p, gc.p, c->stream),
+                       "adjoint backward");
+    if (rc) return rc;
     c->launches += 3;
     cudaEventRecord(c->evk1, c->stream);
     std::vector<double> hs(N);

@@ -149,8 +149,10 @@ def test_gradcheck_autograd_function(tmp_path):
 
 
 def test_adjoint_rejects_other_schemes(tmp_path):
+    """Coupling and RK4 have adjoints (RK4: tests/test_adjoint_rk4_gpu.py); the
+    exact propagators do not."""
     kw, files = make_case(tmp_path)
-    kw = dict(kw, Propagation="RK4")
+    kw = dict(kw, Propagation="Sparse", Threshold=0)
     p = nise.params_from_keywords(kw, files, precision=nise.FP64)
     with nise.Context(p) as c:
         c.load_files()
