@@ -307,10 +307,13 @@ int nise_last_work(const nise_ctx *ctx, double *flops, double *hbm_bytes);
 int nise_probe_fp32_peak(int device, double *tflops);
 
 /* No counterpart in the reference (it has no derivatives).  A differentiable
- * FP64 model of linear absorption with Propagation Coupling or RK4: the
- * Trotter scheme of propagate_vec_coupling_S (propagate.c:821-899) or the RK4
- * scheme of propagate_vec_RK4 (propagate.c:261-373, every nonzero coupling
- * of the pattern kept) on the loaded
+ * FP64 model of linear absorption with Propagation Coupling, RK4, Diagonal or
+ * Sparse with Threshold 0: the Trotter scheme of propagate_vec_coupling_S
+ * (propagate.c:821-899), the RK4 scheme of propagate_vec_RK4
+ * (propagate.c:261-373) or the exact propagator exp(-i H f) of
+ * propagate_vec_DIA (propagate.c:60-125; a degree-18 Taylor polynomial of
+ * exp(-i H f/m), m sub-steps per frame with ||H|| f/m <= 1, remainder below
+ * 2e-17), every nonzero coupling of the pattern kept, on the loaded
  * trajectory with site_shift[a] (cm^-1, N values) added to every shifted
  * diagonal energy (a SingleShift with a = 1), every coupling multiplied by
  * coupling_scale after the read cut, and the transform of do_1DFFT
@@ -321,9 +324,11 @@ int nise_absorption_model(nise_ctx *ctx, const double *site_shift, double coupli
 /* Gradient of a loss L of that spectrum: given dL/dspec_re and dL/dspec_im at
  * its `rows` rows, returns dL/dsite_shift (N values), dL/dcoupling_scale and
  * dL/dlifetime, by reverse-time propagation from checkpoints stored every 32
- * steps of a forward recomputation (RK4: the states of each checkpoint block
- * recomputed forward, then the sub-steps differentiated in reverse).  Other
- * propagation schemes return NISE_ERR_UNSUPPORTED. */
+ * steps of a forward recomputation (RK4 and the exact propagator: the states
+ * of each checkpoint block recomputed forward, then the sub-steps'
+ * polynomials differentiated in reverse).  The truncated propagator (Sparse
+ * with a Threshold in (0, 1], propagate_vec_DIA_S) returns
+ * NISE_ERR_UNSUPPORTED. */
 int nise_backward_absorption(nise_ctx *ctx, const double *site_shift, double coupling_scale, double lifetime,
                              const double *dL_dspec_re, const double *dL_dspec_im, int rows, double *g_shift,
                              double *g_scale, double *g_lifetime);

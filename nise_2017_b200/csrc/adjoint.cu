@@ -2,7 +2,8 @@
 // no derivatives).  The differentiable model is the Trotter "Coupling"
 // absorption of propagate_vec_coupling_S (propagate.c:821-899) and
 // absorption.c:119-145 in FP64 (and, further below, the RK4 scheme of
-// propagate_vec_RK4), with three parameters:
+// propagate_vec_RK4 and the exact propagator of propagate_vec_DIA), with
+// three parameters:
 //   b_a  per-site energy shifts added to the shifted diagonal (the b of a
 //        SingleShift with a = 1, hamshift.c:59-66),
 //   s    a global scale of every coupling (after the read cut),
@@ -199,28 +200,37 @@ int lanes_adj(size_t lane_bytes) {
     return B;
 }
 
-// ------------------------------------------------------------------ RK4
-// The RK4 scheme of propagate_vec_RK4 (propagate.c:261-373) as the model:
-// per frame m = Trotter sub-steps of y = P(A) x, P(A) = I + A + A^2/2 + A^3/6
-// + A^4/24 (RK4 for a constant H is its fourth-order Taylor polynomial),
-// A = -i H f/m, then x' = y |x| / |y| (re_normalize to the pre-step norm).
+// ------------------------------------------------- RK4 and the exact step
+// Models whose step is a Taylor polynomial of A = -i H f/m, applied m times
+// per frame: y = P(A) x, P(A) = sum_(j<=deg) A^j / j!.
+//  * RK4 (propagate_vec_RK4, propagate.c:261-373): deg 4 (RK4 for a
+//    constant H is its fourth-order Taylor polynomial), m = Trotter
+//    sub-steps, then x' = y |x| / |y| (re_normalize to the pre-step norm).
+//  * The exact propagator exp(-i H f) of propagate_vec_DIA
+//    (propagate.c:60-125; Propagation Sparse with Threshold 0, or Diagonal):
+//    deg 18 and m = ceil(f ||H||) over the job's frames (||H|| bounded by
+//    max |h_a + b_a| + |s| ||J||_F), so ||A|| <= 1 and the series' remainder
+//    is below 1/19! * e = 2e-17 relative; no renormalisation.
 // H = diag(h + b) + s J over every nonzero coupling of the pattern (as the
 // Trotter model, so that it is smooth in s).  Vectors live in global scratch,
 // slot q of vector v at base + (q n + a) nvec + v (a warp's lanes read
 // consecutive addresses).
 //
 // Adjoint of one sub-step, l the gradient with respect to x':
-//   c = Re(l . y), l_y = r l - c |x| y / |y|^3 (r = |x|/|y|), and the norm's
-//   own term c x / (|x| |y|) goes to l_x;
+//   renormalised: c = Re(l . y), l_y = r l - c |x| y / |y|^3 (r = |x|/|y|),
+//   and the norm's own term c x / (|x| |y|) goes to l_x; otherwise l_y = l;
 //   l_x += P(A)^+ l_y = sum_p w_p / p!, w_p = (A^+)^p l_y, A^+ = +i H f/m;
-//   dL = Re sum_{p+q<=3} w_p^+ dA u_q / (p+q+1)!, u_q = A^q x, dA = -i dH f/m:
-//   the shift b_a gets (f/m) sum Im(conj(v_q,a) u_q,a) and the scale s gets
-//   (f/m) sum_k J_k [Im(conj(v_q,a) u_q,b) + Im(conj(v_q,b) u_q,a)], with
-//   v_q = sum_{p<=3-q} w_p / (p+q+1)!.
+//   dL = Re sum_{p+q<=deg-1} w_p^+ dA u_q / (p+q+1)!, u_q = A^q x,
+//   dA = -i dH f/m: the shift b_a gets (f/m) sum Im(conj(v_q,a) u_q,a) and
+//   the scale s gets (f/m) sum_k J_k [Im(conj(v_q,a) u_q,b) +
+//   Im(conj(v_q,b) u_q,a)], with v_q = sum_{p<=deg-1-q} w_p / (p+q+1)!.
 // The backward sweep recomputes the frame states of each checkpoint block,
 // then each frame's sub-step inputs, from the forward checkpoints.
+constexpr int kPolyMaxDeg = 18;
+
 struct Rk4Adj {
     int n, k, m, K, nck, nvec;
+    int deg, renorm;  // polynomial degree; renormalise each sub-step (RK4)
     const int2 *pairs;
     long f0, nf;
     const double *D, *Jc, *jf;  // [nf][n] (h + b) f/m, [nf][k] s J f/m, [nf][k] J f/m
@@ -246,6 +256,27 @@ __global__ void k_adj_rk4_prep(DevTraj T, AdjPlan P, double fm, double *D, doubl
         jf[g] = J;
         Jc[g] = P.scale * J;
     }
+}
+
+// Per frame an upper bound of ||A|| for m = 1, from the tables built with
+// fm = f: max_a |D_a| + sqrt(2 sum_k Jc_k^2) (the Frobenius norm of the
+// couplings); bnd[0] gets the maximum over the frames.
+__global__ void k_adj_bound(const double *D, const double *Jc, int n, int k, long nf, double *bnd) {
+    __shared__ double red[256];
+    double mx = 0;
+    for (long t = threadIdx.x; t < nf; t += blockDim.x) {
+        double d = 0, j2 = 0;
+        for (int a = 0; a < n; a++) d = fmax(d, fabs(D[t * n + a]));
+        for (int q = 0; q < k; q++) j2 += Jc[t * k + q] * Jc[t * k + q];
+        mx = fmax(mx, d + sqrt(2 * j2));
+    }
+    red[threadIdx.x] = mx;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) bnd[0] = red[0];
 }
 
 struct Slot {
@@ -292,10 +323,10 @@ __device__ double rk4_norm2(const Rk4Adj &R, Slot x) {
     return s;
 }
 
-// y = P(A) x by Horner's rule (t <- x + A t / j, j = 4, 3, 2, 1); tmp is scratch.
+// y = P(A) x by Horner's rule (t <- x + A t / j, j = deg .. 1); tmp is scratch.
 __device__ void rk4_poly(const Rk4Adj &R, long fi, Slot x, Slot y, Slot tmp) {
     for (int a = 0; a < R.n; a++) y[a] = x[a];
-    for (int j = 4; j >= 1; j--) {
+    for (int j = R.deg; j >= 1; j--) {
         rk4_a(R, fi, y, tmp, false);
         const double c = 1.0 / j;
         for (int a = 0; a < R.n; a++) {
@@ -305,12 +336,13 @@ __device__ void rk4_poly(const Rk4Adj &R, long fi, Slot x, Slot y, Slot tmp) {
     }
 }
 
-// One frame: m sub-steps x <- P(A) x |x| / |P(A) x|, in place (y, tmp scratch).
+// One frame: m sub-steps x <- P(A) x (|x| / |P(A) x| when renormalised), in
+// place (y, tmp scratch).
 __device__ void rk4_frame(const Rk4Adj &R, long fi, Slot x, Slot y, Slot tmp) {
     for (int sub = 0; sub < R.m; sub++) {
-        const double n0 = rk4_norm2(R, x);
+        const double n0 = R.renorm ? rk4_norm2(R, x) : 1.0;
         rk4_poly(R, fi, x, y, tmp);
-        const double sc = sqrt(n0 / rk4_norm2(R, y));
+        const double sc = R.renorm ? sqrt(n0 / rk4_norm2(R, y)) : 1.0;
         for (int a = 0; a < R.n; a++) {
             const double2 z = y[a];
             x[a] = make_double2(z.x * sc, z.y * sc);
@@ -343,9 +375,9 @@ __global__ void k_adj_rk4_fwd(DevTraj T, Rk4Adj R, AbsJob J, double2 *resp, doub
     }
 }
 
-// slots of the backward kernel: 0 l, 1 y, 2 tmp, 3 l_new, 4 w, 5 w', 6..9 u_q,
-// 10..13 v_q, 14.. the block's frame states (K), then the frame's sub-step
-// inputs (m)
+// slots of the backward kernel: 0 l, 1 y, 2 tmp, 3 l_new, 4 w, 5 w',
+// 6 .. 6+deg-1 u_q, then deg slots v_q, then the block's frame states (K),
+// then the frame's sub-step inputs (m)
 __global__ void k_adj_rk4_bwd(DevTraj T, Rk4Adj R, AbsJob J, const double2 *G, const double2 *ckpt, double *gshift,
                               double *gscale) {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -364,72 +396,81 @@ __global__ void k_adj_rk4_bwd(DevTraj T, Rk4Adj R, AbsJob J, const double2 *G, c
             L[a] = make_double2(mu * g.x, mu * g.y);
         }
     }
-    const double c_pq[7] = {1.0, 1.0, 1.0 / 2, 1.0 / 6, 1.0 / 24, 1.0 / 120, 1.0 / 720};  // 1/j!
+    const int D = R.deg, su = 6, sv = 6 + D, ss = 6 + 2 * D, si = ss + R.K;  // slot bases
+    double c_pq[kPolyMaxDeg + 1];  // 1/j!
+    c_pq[0] = 1.0;
+    for (int j = 1; j <= D; j++) c_pq[j] = c_pq[j - 1] / j;
     for (int cb = R.nck - 1; cb >= 0; cb--) {
         const int tb0 = cb * R.K, tb1 = min(tb0 + R.K, J.tmax - 1);  // frames [tb0, tb1) propagate
         // the block's frame states from its checkpoint
-        Slot S0 = slot(R, 14, v);
+        Slot S0 = slot(R, ss, v);
         for (int a = 0; a < n; a++) S0[a] = ckpt[((size_t)v * R.nck + cb) * n + a];
         for (int j = 1; j < tb1 - tb0; j++) {
-            Slot Sp = slot(R, 14 + j - 1, v), Sj = slot(R, 14 + j, v);
+            Slot Sp = slot(R, ss + j - 1, v), Sj = slot(R, ss + j, v);
             for (int a = 0; a < n; a++) Sj[a] = Sp[a];
             rk4_frame(R, ti + tb0 + j - 1 - R.f0, Sj, Y, Tm);
         }
         for (int t1 = tb1 - 1; t1 >= tb0; t1--) {
             const long fi = ti + t1 - R.f0;
             // the frame's sub-step inputs
-            for (int a = 0; a < n; a++) slot(R, 14 + R.K, v)[a] = slot(R, 14 + t1 - tb0, v)[a];
+            for (int a = 0; a < n; a++) slot(R, si, v)[a] = slot(R, ss + t1 - tb0, v)[a];
             for (int s = 1; s < R.m; s++) {
-                Slot Ip = slot(R, 14 + R.K + s - 1, v), Is = slot(R, 14 + R.K + s, v);
+                Slot Ip = slot(R, si + s - 1, v), Is = slot(R, si + s, v);
                 for (int a = 0; a < n; a++) Is[a] = Ip[a];
-                const double n0 = rk4_norm2(R, Is);
+                const double n0 = R.renorm ? rk4_norm2(R, Is) : 1.0;
                 rk4_poly(R, fi, Is, Y, Tm);
-                const double sc = sqrt(n0 / rk4_norm2(R, Y));
+                const double sc = R.renorm ? sqrt(n0 / rk4_norm2(R, Y)) : 1.0;
                 for (int a = 0; a < n; a++) {
                     const double2 z = Y[a];
                     Is[a] = make_double2(z.x * sc, z.y * sc);
                 }
             }
             for (int s = R.m - 1; s >= 0; s--) {
-                Slot X = slot(R, 14 + R.K + s, v);
+                Slot X = slot(R, si + s, v);
                 // forward powers u_q = A^q x (u_0 = x)
-                for (int a = 0; a < n; a++) slot(R, 6, v)[a] = X[a];
-                for (int q = 1; q < 4; q++) rk4_a(R, fi, slot(R, 6 + q - 1, v), slot(R, 6 + q, v), false);
-                // y = P(A) x and the renormalisation
-                rk4_poly(R, fi, X, Y, Tm);
-                const double nx = sqrt(rk4_norm2(R, X)), ny = sqrt(rk4_norm2(R, Y)), r = nx / ny;
-                double c = 0;
-                for (int a = 0; a < n; a++) {
-                    const double2 l = L[a], y = Y[a];
-                    c += l.x * y.x + l.y * y.y;
+                for (int a = 0; a < n; a++) slot(R, su, v)[a] = X[a];
+                for (int q = 1; q < D; q++) rk4_a(R, fi, slot(R, su + q - 1, v), slot(R, su + q, v), false);
+                // the renormalisation: y = P(A) x
+                double r = 1.0, cy = 0.0, cx = 0.0;
+                if (R.renorm) {
+                    rk4_poly(R, fi, X, Y, Tm);
+                    const double nx = sqrt(rk4_norm2(R, X)), ny = sqrt(rk4_norm2(R, Y));
+                    double c = 0;
+                    for (int a = 0; a < n; a++) {
+                        const double2 l = L[a], y = Y[a];
+                        c += l.x * y.x + l.y * y.y;
+                    }
+                    r = nx / ny;
+                    cy = c * nx / (ny * ny * ny);
+                    cx = c / (nx * ny);
                 }
-                const double cy = c * nx / (ny * ny * ny), cx = c / (nx * ny);
                 // w_0 = l_y; l_new = norm term + w_0; v_q = w_0 / (q+1)!
                 for (int a = 0; a < n; a++) {
-                    const double2 l = L[a], y = Y[a], z = X[a];
+                    const double2 l = L[a], z = X[a];
+                    const double2 y = R.renorm ? Y[a] : make_double2(0.0, 0.0);
                     const double2 w = make_double2(r * l.x - cy * y.x, r * l.y - cy * y.y);
                     W[a] = w;
                     Ln[a] = make_double2(cx * z.x + w.x, cx * z.y + w.y);
-                    for (int q = 0; q < 4; q++) slot(R, 10 + q, v)[a] = make_double2(w.x * c_pq[q + 1], w.y * c_pq[q + 1]);
+                    for (int q = 0; q < D; q++) slot(R, sv + q, v)[a] = make_double2(w.x * c_pq[q + 1], w.y * c_pq[q + 1]);
                 }
-                for (int p = 1; p <= 4; p++) {  // w_p = A^+ w_(p-1)
+                for (int p = 1; p <= D; p++) {  // w_p = A^+ w_(p-1)
                     rk4_a(R, fi, p % 2 ? W : W2, p % 2 ? W2 : W, true);
                     Slot Wp = p % 2 ? W2 : W;
                     for (int a = 0; a < n; a++) {
                         const double2 w = Wp[a];
                         const double2 ln = Ln[a];
                         Ln[a] = make_double2(ln.x + c_pq[p] * w.x, ln.y + c_pq[p] * w.y);
-                        for (int q = 0; q + p <= 3; q++) {
-                            const double2 vq = slot(R, 10 + q, v)[a];
+                        for (int q = 0; q + p <= D - 1; q++) {
+                            const double2 vq = slot(R, sv + q, v)[a];
                             const double cf = c_pq[p + q + 1];
-                            slot(R, 10 + q, v)[a] = make_double2(vq.x + cf * w.x, vq.y + cf * w.y);
+                            slot(R, sv + q, v)[a] = make_double2(vq.x + cf * w.x, vq.y + cf * w.y);
                         }
                     }
                 }
                 // parameter gradients: Im(conj(v) u) = v.x u.y - v.y u.x
                 const double *jf = R.jf + fi * R.k;
-                for (int q = 0; q < 4; q++) {
-                    Slot Vq = slot(R, 10 + q, v), Uq = slot(R, 6 + q, v);
+                for (int q = 0; q < D; q++) {
+                    Slot Vq = slot(R, sv + q, v), Uq = slot(R, su + q, v);
                     for (int a = 0; a < n; a++) {
                         const double2 vv = Vq[a], uu = Uq[a];
                         gs[a] += R.fm * (vv.x * uu.y - vv.y * uu.x);
@@ -491,17 +532,23 @@ int launch_adj_bwd(const DevTraj &T, const AdjPlan &P, const AbsJob &J, const do
 int launch_adj_rk4(const DevTraj &T, const AdjPlan &P, const Rk4Adj &R, const AbsJob &J, const double2 *G,
                    double2 *resp, double2 *ckpt, double *gshift_part, double *gscale_part, double *gshift,
                    double *gscale, cudaStream_t s) {
-    const long tot = P.nf * P.n + P.nf * P.k;
     if (!G) {
-        if (tot > 0)
-            k_adj_rk4_prep<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(T, P, R.fm, (double *)R.D, (double *)R.Jc,
-                                                                       (double *)R.jf);
         k_adj_rk4_fwd<<<(R.nvec + 63) / 64, 64, 0, s>>>(T, R, J, resp, ckpt);
         return (int)cudaGetLastError();
     }
     k_adj_rk4_bwd<<<(R.nvec + 63) / 64, 64, 0, s>>>(T, R, J, G, ckpt, gshift_part, gscale_part);
     k_adj_reduce<<<(P.n + 127) / 128, 128, 0, s>>>(gshift_part, R.nvec, P.n, gshift);
     k_adj_reduce<<<1, 1, 0, s>>>(gscale_part, R.nvec, 1, gscale);
+    return (int)cudaGetLastError();
+}
+
+// Tables D, Jc, jf of the polynomial models for the step f/m (fm); with bnd,
+// also the bound of ||A|| over the frames (meaningful for fm = f).
+int launch_adj_poly_prep(const DevTraj &T, const AdjPlan &P, double fm, double *D, double *Jc, double *jf,
+                         double *bnd, cudaStream_t s) {
+    const long tot = P.nf * P.n + P.nf * P.k;
+    if (tot > 0) k_adj_rk4_prep<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(T, P, fm, D, Jc, jf);
+    if (bnd) k_adj_bound<<<1, 256, 0, s>>>(D, Jc, P.n, P.k, P.nf, bnd);
     return (int)cudaGetLastError();
 }
 
@@ -528,8 +575,6 @@ int adj_forward(nise_ctx *c, const double *shift, double scale, int K, AdjRun &R
                 DevBuf<int2> &dpairs, DevBuf<double2> &U, DevBuf<double2> &rot, DevBuf<double> &jf,
                 DevBuf<double2> &ckpt, AdjPlan &P, AbsJob &J) {
     const nise_params &p = c->p;
-    if (p.propagation != NISE_PROP_COUPLING)
-        return nise_fail(c, NISE_ERR_UNSUPPORTED, "the absorption adjoint differentiates Propagation Coupling and RK4");
     if (!c->loaded) return nise_fail(c, NISE_ERR_STATE, "no trajectory loaded");
     if (!shift || !(scale == scale)) return nise_fail(c, NISE_ERR_ARG, "null shifts or invalid scale");
     const int N = c->n, tmax = p.tmax1;
@@ -589,10 +634,10 @@ int adj_forward(nise_ctx *c, const double *shift, double scale, int K, AdjRun &R
     return nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "adjoint forward");
 }
 
-// The RK4 model (Propagation RK4): forward responses, tables and checkpoints
-// left in W for the backward sweep.
+// The polynomial models (Propagation RK4, or the exact propagator): forward
+// responses, tables and checkpoints left in W for the backward sweep.
 struct Rk4Work {
-    DevBuf<double> dshift, D, Jc, jf;
+    DevBuf<double> dshift, D, Jc, jf, bnd;
     DevBuf<int2> dpairs;
     DevBuf<double2> scr, ckpt;
     AdjPlan P;
@@ -600,7 +645,7 @@ struct Rk4Work {
     AbsJob J;
 };
 
-int adj_rk4_forward(nise_ctx *c, const double *shift, double scale, int K, AdjRun &R, Rk4Work &W) {
+int adj_rk4_forward(nise_ctx *c, const double *shift, double scale, int K, bool exact, AdjRun &R, Rk4Work &W) {
     const nise_params &p = c->p;
     if (!c->loaded) return nise_fail(c, NISE_ERR_STATE, "no trajectory loaded");
     if (!shift || !(scale == scale)) return nise_fail(c, NISE_ERR_ARG, "null shifts or invalid scale");
@@ -618,42 +663,70 @@ int adj_rk4_forward(nise_ctx *c, const double *shift, double scale, int K, AdjRu
     R.nf = f1 - R.f0 > 0 ? f1 - R.f0 : 1;
     std::vector<int2> pairs;
     if ((rc = nise_pattern(c, R.f0, R.nf, pairs))) return rc;
-    const int nvec = 3 * R.nsamp, m = p.ts;
+    const int nvec = 3 * R.nsamp;
     AdjPlan &P = W.P;
     memset(&P, 0, sizeof(P));
     P.n = N;
     P.k = (int)pairs.size();
-    P.ts = m;
     P.f0 = R.f0;
     P.nf = R.nf;
     P.scale = scale;
+    std::vector<double> hs(shift, shift + N);
+    if ((rc = W.dshift.upload(c, hs)) || (rc = W.dpairs.upload(c, pairs.empty() ? std::vector<int2>(1) : pairs)) ||
+        (rc = W.D.alloc(c, (size_t)R.nf * N)) || (rc = W.Jc.alloc(c, (size_t)R.nf * (P.k ? P.k : 1))) ||
+        (rc = W.jf.alloc(c, (size_t)R.nf * (P.k ? P.k : 1))) || (rc = W.bnd.alloc(c, 1)))
+        return rc;
+    P.shift = W.dshift.p;
+    P.pairs = W.dpairs.p;
+    DevTraj T = nise_devtraj(c);
+    c->launches = 0;
+    cudaEventRecord(c->ev0, c->stream);
+    cudaEventRecord(c->evk0, c->stream);
+    // RK4: degree 4, m = Trotter sub-steps, renormalised; the exact step:
+    // degree 18, m = ceil(f ||H||) so that every sub-step has ||A|| <= 1
+    int m = p.ts, deg = 4;
+    if (exact) {
+        deg = kPolyMaxDeg;
+        double hb = 0;
+        if ((rc = nise_cuda(c, launch_adj_poly_prep(T, P, nise_f64(p, 1, 1), W.D.p, W.Jc.p, W.jf.p, W.bnd.p, c->stream),
+                            "adjoint tables")))
+            return rc;
+        cudaMemcpyAsync(&hb, W.bnd.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+        if ((rc = nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "adjoint norm bound"))) return rc;
+        if (!(hb >= 0 && hb < 1e6)) return nise_fail(c, NISE_ERR_ARG, "exact-propagator adjoint: |H| f = %g", hb);
+        m = hb > 1 ? (int)ceil(hb) : 1;
+        c->launches += 2;
+    }
+    P.ts = m;
     Rk4Adj &A = W.A;
     memset(&A, 0, sizeof(A));
     A.n = N;
     A.k = P.k;
     A.m = m;
+    A.deg = deg;
+    A.renorm = exact ? 0 : 1;
     A.K = K;
     A.nck = (tmax - 1 + K - 1) / K;
     A.nvec = nvec;
     A.f0 = R.f0;
     A.nf = R.nf;
     A.fm = nise_f64(p, 1, m);
-    const size_t slots = 14 + (size_t)K + m;
+    const size_t slots = 6 + 2 * (size_t)deg + K + m;
     if ((size_t)nvec * N * slots * sizeof(double2) > ((size_t)8 << 30))
-        return nise_fail(c, NISE_ERR_NOMEM, "RK4 adjoint: %zu bytes of scratch", (size_t)nvec * N * slots * 16);
-    std::vector<double> hs(shift, shift + N);
-    if ((rc = W.dshift.upload(c, hs)) || (rc = W.dpairs.upload(c, pairs.empty() ? std::vector<int2>(1) : pairs)) ||
-        (rc = W.D.alloc(c, (size_t)R.nf * N)) || (rc = W.Jc.alloc(c, (size_t)R.nf * (P.k ? P.k : 1))) ||
-        (rc = W.jf.alloc(c, (size_t)R.nf * (P.k ? P.k : 1))) || (rc = W.scr.alloc(c, slots * N * nvec)) ||
-        (rc = W.ckpt.alloc(c, (size_t)nvec * (A.nck ? A.nck : 1) * N)))
+        return nise_fail(c, NISE_ERR_NOMEM, "adjoint: %zu bytes of scratch", (size_t)nvec * N * slots * 16);
+    if ((rc = W.scr.alloc(c, slots * N * nvec)) || (rc = W.ckpt.alloc(c, (size_t)nvec * (A.nck ? A.nck : 1) * N)))
         return rc;
-    P.shift = W.dshift.p;
-    P.pairs = W.dpairs.p;
     A.pairs = W.dpairs.p;
     A.D = W.D.p;
     A.Jc = W.Jc.p;
     A.jf = W.jf.p;
     A.scr = W.scr.p;
+    if (!exact || m > 1) {
+        if ((rc = nise_cuda(c, launch_adj_poly_prep(T, P, A.fm, W.D.p, W.Jc.p, W.jf.p, nullptr, c->stream),
+                            "adjoint tables")))
+            return rc;
+        c->launches++;
+    }
     AbsJob &J = W.J;
     memset(&J, 0, sizeof(J));
     J.begin = R.begin;
@@ -661,21 +734,36 @@ int adj_rk4_forward(nise_ctx *c, const double *shift, double scale, int K, AdjRu
     J.sample = p.sample;
     J.tmax = tmax;
     J.ts = m;
-    DevTraj T = nise_devtraj(c);
     DevBuf<double2> resp, out;
     if ((rc = resp.alloc(c, (size_t)nvec * tmax)) || (rc = out.alloc(c, tmax))) return rc;
-    c->launches = 0;
-    cudaEventRecord(c->ev0, c->stream);
-    cudaEventRecord(c->evk0, c->stream);
     if ((rc = nise_cuda(c, launch_adj_rk4(T, P, A, J, nullptr, resp.p, W.ckpt.p, nullptr, nullptr, nullptr, nullptr,
                                           c->stream),
-                        "RK4 adjoint forward")) ||
+                        "adjoint forward")) ||
         (rc = nise_cuda(c, launch_reduce_resp(resp.p, nvec, tmax, out.p, c->stream), "response reduction")))
         return rc;
-    c->launches += 3;
+    c->launches += 2;
     R.S.resize(tmax);
     cudaMemcpyAsync(R.S.data(), out.p, sizeof(double2) * tmax, cudaMemcpyDeviceToHost, c->stream);
-    return nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "RK4 adjoint forward");
+    return nise_cuda(c, (int)cudaStreamSynchronize(c->stream), "adjoint forward");
+}
+
+// Which model differentiates the context's propagation: 0 the Trotter
+// model, 1 RK4, 2 the exact propagator (Sparse with Threshold 0 or above 1,
+// Diagonal); -1 none (Sparse with a truncating Threshold, propagate_vec_DIA_S).
+int adj_model(const nise_ctx *c) {
+    switch (c->p.propagation) {
+    case NISE_PROP_COUPLING: return 0;
+    case NISE_PROP_RK4: return 1;
+    case NISE_PROP_SPARSE:
+    case NISE_PROP_DIAGONAL: return c->thres != 0 && !(c->thres > 1) ? -1 : 2;
+    default: return -1;
+    }
+}
+
+int adj_unsupported(nise_ctx *c) {
+    return nise_fail(c, NISE_ERR_UNSUPPORTED,
+                     "the absorption adjoint differentiates Propagation Coupling, RK4, Diagonal and Sparse with "
+                     "Threshold 0 (not the truncated propagator)");
 }
 
 // The FP64 branch of the 1D transform input factors (1DFFT.c:170-200) for
@@ -748,9 +836,10 @@ extern "C" int nise_absorption_model(nise_ctx *c, const double *site_shift, doub
     AdjPlan P;
     AbsJob J;
     Rk4Work W;
-    int rc = c->p.propagation == NISE_PROP_RK4
-                 ? adj_rk4_forward(c, site_shift, coupling_scale, 32, R, W)
-                 : adj_forward(c, site_shift, coupling_scale, c->p.tmax1, R, dshift, dpairs, U, rot, jf, ckpt, P, J);
+    const int model = adj_model(c);
+    if (model < 0) return adj_unsupported(c);
+    int rc = model ? adj_rk4_forward(c, site_shift, coupling_scale, 32, model == 2, R, W)
+                   : adj_forward(c, site_shift, coupling_scale, c->p.tmax1, R, dshift, dpairs, U, rot, jf, ckpt, P, J);
     if (rc) return rc;
     cudaEventRecord(c->evk1, c->stream);
     cudaEventRecord(c->ev1, c->stream);
@@ -792,9 +881,11 @@ extern "C" int nise_backward_absorption(nise_ctx *c, const double *site_shift, d
     AdjPlan P;
     AbsJob J;
     const int K = 32;  // checkpoint interval (steps)
-    const bool rk4 = p.propagation == NISE_PROP_RK4;
+    const int model = adj_model(c);
+    if (model < 0) return adj_unsupported(c);
+    const bool rk4 = model > 0;  // a polynomial model
     Rk4Work W;
-    int rc = rk4 ? adj_rk4_forward(c, site_shift, coupling_scale, K, R, W)
+    int rc = rk4 ? adj_rk4_forward(c, site_shift, coupling_scale, K, model == 2, R, W)
                  : adj_forward(c, site_shift, coupling_scale, K, R, dshift, dpairs, U, rot, jf, ckpt, P, J);
     if (rc) return rc;
     // adjoint of the transform: dL/dOut_k = (dL/dspec_im + i dL/dspec_re) * 2 dt c_v,
@@ -828,7 +919,7 @@ extern "C" int nise_backward_absorption(nise_ctx *c, const double *site_shift, d
     DevTraj T = nise_devtraj(c);
     if (rk4)
         rc = nise_cuda(c, launch_adj_rk4(T, W.P, W.A, W.J, dG.p, nullptr, W.ckpt.p, gsp.p, gcp.p, gs.p, gc.p, c->stream),
-                       "RK4 adjoint backward");
+                       "polynomial adjoint backward");
     else
         rc = nise_cuda(c, launch_adj_bwd(T, P, J, dG.p, ckpt.p, gsp.p, gcp.p, gs.p, gc.p, c->stream),
                        "adjoint backward");

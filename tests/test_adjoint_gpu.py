@@ -149,10 +149,11 @@ def test_gradcheck_autograd_function(tmp_path):
 
 
 def test_adjoint_rejects_other_schemes(tmp_path):
-    """Coupling and RK4 have adjoints (RK4: tests/test_adjoint_rk4_gpu.py); the
-    exact propagators do not."""
+    """Coupling, RK4 and the exact propagator have adjoints (tests/test_adjoint_rk4_gpu.py,
+    tests/test_adjoint_exact_gpu.py); the truncated propagator (Sparse with a
+    Threshold in (0, 1], propagate_vec_DIA_S) is not differentiable and is refused."""
     kw, files = make_case(tmp_path)
-    kw = dict(kw, Propagation="Sparse", Threshold=0)
+    kw = dict(kw, Propagation="Sparse", Threshold=0.001)
     p = nise.params_from_keywords(kw, files, precision=nise.FP64)
     with nise.Context(p) as c:
         c.load_files()
