@@ -338,11 +338,15 @@ int nise_backward_absorption(nise_ctx *ctx, const double *site_shift, double cou
  * lexicographic order, one after another).  ab holds k pairs (a, b), a < b,
  * in that order.  Rotation q gets level 1 + the highest level of the earlier
  * rotations sharing one of its sites; perm (k values) lists the rotations by
- * (level, list index), lvptr (nlev + 1 values, at most k + 1) bounds the
- * levels in perm, and chkptr (nchk + 1 values, at most k + 1) splits every
- * level into chunks of at most 32 rotations, one warp step each.  Touches no
- * GPU. */
-int nise_rotation_schedule(const int *ab, int k, int n, int *perm, int *lvptr, int *nlev, int *chkptr, int *nchk);
+ * level, lvptr (nlev + 1 values, at most k + 1) bounds the levels in perm,
+ * and chkptr (nchk + 1 values, at most k + 1) splits every level into chunks
+ * of at most 32 rotations, one warp step each.  Within a chunk the rotations
+ * are ordered, and flip[q] = 1 (k values; may be NULL) applies rotation
+ * perm[q] as (b, a), to spread the lanes' shared-memory loads over the banks;
+ * the rotations of a chunk are disjoint and the rotation is symmetric in its
+ * sites, so neither changes the float operations.  Touches no GPU. */
+int nise_rotation_schedule(const int *ab, int k, int n, int *perm, int *lvptr, int *nlev, int *chkptr, int *nchk,
+                           int *flip);
 
 /* No counterpart in the reference.  Linear absorption with the Trotter
  * "Coupling" scheme (HamiltonianType Full) for callers whose device memory is

@@ -127,7 +127,7 @@ def lib():
         L.nise_linear_file.restype = ctypes.c_char_p
         L.nise_write_td.argtypes = [ctypes.c_char_p, P, dp, dp, ctypes.c_int, ctypes.c_int]
         L.nise_translate.argtypes = [ctypes.c_char_p]
-        L.nise_rotation_schedule.argtypes = [ip, ctypes.c_int, ctypes.c_int, ip, ip, ip, ip, ip]
+        L.nise_rotation_schedule.argtypes = [ip, ctypes.c_int, ctypes.c_int, ip, ip, ip, ip, ip, ip]
         _lib = L
     return _lib
 
@@ -138,19 +138,22 @@ def _dp(a):
 
 def rotation_schedule(pairs, n):
     """The engine's Trotter rotation order for a lexicographic coupling list
-    (host only): (perm, level bounds, chunk bounds) as numpy int arrays."""
+    (host only): (perm, level bounds, chunk bounds, flip) as numpy int arrays;
+    flip[q] = 1 applies rotation perm[q] with its two sites swapped."""
     ab = np.ascontiguousarray(np.asarray(pairs, dtype=np.int32).reshape(-1, 2))
     k = len(ab)
     perm = np.zeros(max(k, 1), np.int32)
     lv = np.zeros(k + 1, np.int32)
     chk = np.zeros(k + 1, np.int32)
+    flip = np.zeros(max(k, 1), np.int32)
     nlev, nchk = ctypes.c_int(), ctypes.c_int()
     ip = ctypes.POINTER(ctypes.c_int)
     rc = lib().nise_rotation_schedule(ab.ctypes.data_as(ip), k, n, perm.ctypes.data_as(ip), lv.ctypes.data_as(ip),
-                                      ctypes.byref(nlev), chk.ctypes.data_as(ip), ctypes.byref(nchk))
+                                      ctypes.byref(nlev), chk.ctypes.data_as(ip), ctypes.byref(nchk),
+                                      flip.ctypes.data_as(ip))
     if rc != 0:
         raise NiseError(rc, lib().nise_global_error().decode())
-    return perm[:k], lv[:nlev.value + 1], chk[:nchk.value + 1]
+    return perm[:k], lv[:nlev.value + 1], chk[:nchk.value + 1], flip[:k]
 
 
 def translate(keyword_file):

@@ -108,10 +108,121 @@ void rotation_chunks(const std::vector<int> &lvptr, std::vector<int> &chk) {
         for (int q = lvptr[l]; q < lvptr[l + 1]; q += 32) chk.push_back(std::min(q + 32, lvptr[l + 1]));
 }
 
+// Bank order within each chunk.  The warp kernels give lane l of a chunk the
+// chunk's l-th rotation and load its two sites with one shared-memory load
+// each (idle lanes: the spare site n + ((start + l - K) & 31)).  A load is
+// served in groups of lanes (a site of 8 bytes: half-warps, the site's bank
+// pair given by site mod 16; of 16 bytes, the two-vector kernel: quarter-warps,
+// site mod 8), and sites of one group with the same residue conflict.  The
+// rotations of a chunk are disjoint and the 2x2 rotation is symmetric in its
+// two sites, so any order within the chunk and either site first give the same
+// float operations on every site; a local search (fixed seed) picks the order
+// and the orientation with the fewest conflicting wavefronts over both
+// layouts.  flip[q] = 1: rotation perm[q] is applied as (b, a).
+void bank_order(const std::vector<int2> &pairs, int n, const std::vector<int> &chk, std::vector<int> &perm,
+                std::vector<char> &flip) {
+    const int K = (int)pairs.size();
+    flip.assign(perm.size(), 0);
+    uint32_t st = 0x9e3779b9u;
+    auto rnd = [&]() {
+        st ^= st << 13;
+        st ^= st >> 17;
+        st ^= st << 5;
+        return st;
+    };
+    for (size_t c = 0; c + 1 < chk.size(); c++) {
+        const int c0 = chk[c], m = chk[c + 1] - c0;
+        if (m < 2) continue;
+        int sa[32], sb[32];
+        auto load = [&]() {
+            for (int l = 0; l < 32; l++) {
+                if (l < m) {
+                    const int2 p = pairs[perm[c0 + l]];
+                    sa[l] = flip[c0 + l] ? p.y : p.x;
+                    sb[l] = flip[c0 + l] ? p.x : p.y;
+                } else {
+                    sa[l] = sb[l] = n + ((c0 + l - K) & 31);
+                }
+            }
+        };
+        auto cost = [&]() {
+            int tot = 0;
+            for (int lay = 0; lay < 2; lay++) {
+                const int w = lay ? 8 : 16, g = lay ? 8 : 16;
+                for (int l0 = 0; l0 < 32; l0 += w)
+                    for (const int *s : {sa, sb}) {
+                        int cnt[16] = {0}, mx = 0;
+                        for (int l = l0; l < l0 + w; l++) mx = std::max(mx, ++cnt[s[l] % g]);
+                        tot += mx;
+                    }
+            }
+            return tot;
+        };
+        // greedy start: lane by lane the rotation and orientation whose sites
+        // collide least with the sites already in the lane's groups (the idle
+        // lanes' spare sites included)
+        {
+            int ca8[2][16] = {{0}}, cb8[2][16] = {{0}}, ca16[4][8] = {{0}}, cb16[4][8] = {{0}};
+            for (int l = m; l < 32; l++) {
+                const int s = n + ((c0 + l - K) & 31);
+                ca8[l >> 4][s % 16]++;
+                cb8[l >> 4][s % 16]++;
+                ca16[l >> 3][s % 8]++;
+                cb16[l >> 3][s % 8]++;
+            }
+            std::vector<int> rest(perm.begin() + c0, perm.begin() + c0 + m);
+            for (int l = 0; l < m; l++) {
+                int bi = 0, bo = 0, bc = 1 << 30;
+                for (int i = 0; i < (int)rest.size(); i++)
+                    for (int o = 0; o < 2; o++) {
+                        const int2 p = pairs[rest[i]];
+                        const int a = o ? p.y : p.x, b = o ? p.x : p.y;
+                        const int cc = ca8[l >> 4][a % 16] + cb8[l >> 4][b % 16] + ca16[l >> 3][a % 8] +
+                                       cb16[l >> 3][b % 8];
+                        if (cc < bc) bc = cc, bi = i, bo = o;
+                    }
+                const int2 p = pairs[rest[bi]];
+                const int a = bo ? p.y : p.x, b = bo ? p.x : p.y;
+                ca8[l >> 4][a % 16]++;
+                cb8[l >> 4][b % 16]++;
+                ca16[l >> 3][a % 8]++;
+                cb16[l >> 3][b % 8]++;
+                perm[c0 + l] = rest[bi];
+                flip[c0 + l] = (char)bo;
+                rest.erase(rest.begin() + bi);
+            }
+        }
+        load();
+        int best = cost();
+        for (int it = 0; it < 24 * m; it++) {
+            const int i = (int)(rnd() % m);
+            if (rnd() % 10 < 3) {
+                flip[c0 + i] ^= 1;
+                load();
+                const int t = cost();
+                if (t <= best) best = t;
+                else flip[c0 + i] ^= 1;
+            } else {
+                const int j = (int)(rnd() % m);
+                if (i == j) continue;
+                std::swap(perm[c0 + i], perm[c0 + j]);
+                std::swap(flip[c0 + i], flip[c0 + j]);
+                load();
+                const int t = cost();
+                if (t <= best) best = t;
+                else {
+                    std::swap(perm[c0 + i], perm[c0 + j]);
+                    std::swap(flip[c0 + i], flip[c0 + j]);
+                }
+            }
+        }
+    }
+}
+
 }  // namespace
 
 extern "C" int nise_rotation_schedule(const int *ab, int k, int n, int *perm, int *lvptr, int *nlev, int *chkptr,
-                                      int *nchk) {
+                                      int *nchk, int *flip) {
     if (k < 0 || n < 1 || (k && (!ab || !perm)) || !lvptr || !nlev || !chkptr || !nchk) {
         nise_set_global_error("bad rotation schedule arguments");
         return NISE_ERR_ARG;
@@ -127,7 +238,10 @@ extern "C" int nise_rotation_schedule(const int *ab, int k, int n, int *perm, in
     std::vector<int> hperm, hlv, hchk;
     rotation_levels(pairs, n, hperm, hlv);
     rotation_chunks(hlv, hchk);
+    std::vector<char> hflip;
+    bank_order(pairs, n, hchk, hperm, hflip);
     std::copy(hperm.begin(), hperm.end(), perm);
+    if (flip) std::copy(hflip.begin(), hflip.end(), flip);
     std::copy(hlv.begin(), hlv.end(), lvptr);
     std::copy(hchk.begin(), hchk.end(), chkptr);
     *nlev = (int)hlv.size() - 1;
@@ -287,16 +401,21 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
         std::vector<int> hperm, hlv;
         rotation_levels(pairs, N, hperm, hlv);
         nlev = (int)hlv.size() - 1;
+        std::vector<int> hchk;
+        rotation_chunks(hlv, hchk);
+        nchk = (int)hchk.size() - 1;
+        std::vector<char> hflip;
+        bank_order(pairs, N, hchk, hperm, hflip);
         std::vector<int2> lpairs(pairs.size());
-        for (size_t q = 0; q < pairs.size(); q++) lpairs[q] = pairs[hperm[q]];
+        for (size_t q = 0; q < pairs.size(); q++) {
+            const int2 ab = pairs[hperm[q]];
+            lpairs[q] = hflip[q] ? make_int2(ab.y, ab.x) : ab;
+        }
         if ((rc = dpairs.upload(c, lpairs.empty() ? std::vector<int2>(1) : lpairs)) ||
             (rc = U.alloc(c, r2 * (size_t)nf * N)) ||
             (rc = rot.alloc(c, r2 * (size_t)(TP.rot_static ? 1 : nf) * (TP.k ? TP.k : 1))) ||
             (rc = lvptr.upload(c, hlv)))
             return rc;
-        std::vector<int> hchk;
-        rotation_chunks(hlv, hchk);
-        nchk = (int)hchk.size() - 1;
         if ((rc = lvchk.upload(c, hchk))) return rc;
         TP.pairs = dpairs.p;
         TP.U = U.p;
