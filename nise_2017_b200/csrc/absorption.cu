@@ -1514,6 +1514,17 @@ int launch_abs_trotter_lv(int prec, const DevTraj &T, const TrotterPlan &P, cons
     return (int)cudaGetLastError();
 }
 
+// Warps per CTA for `units` warps of work when shared memory allows W: one CTA
+// runs per SM, so the job takes rounds = ceil(units / (W * nsm)) CTA times;
+// the fewest warps per CTA with that many rounds spread the work evenly (a
+// CTA's time grows with its warps).  On the 1024-site lattice with 5985
+// vectors (2993 warps of two): 9 warps give 333 CTAs, 2.25 rounds run as 3,
+// 7 warps give 428 CTAs in the same 3 rounds.
+static int even_width(int units, int W, int nsm) {
+    const long rounds = ((long)units + (long)W * nsm - 1) / ((long)W * nsm);
+    return (int)std::max(1L, ((long)units + rounds * nsm - 1) / (rounds * nsm));
+}
+
 // Shared memory of k_abs_trotter_wv: chunk table, rotation table (sm), W
 // vectors (and their phases with ustage).
 static size_t trotter_wv_smem(int prec, const TrotterPlan &P, int nchk, bool sm, bool ustage, int W) {
@@ -1548,6 +1559,7 @@ int launch_abs_trotter_wv(int prec, const DevTraj &T, const TrotterPlan &P, cons
     if (sm && P.rot_static) W = widest(true);
     if (!sm) W = widest(false);
     if (!fits(sm, false, W)) return (int)cudaErrorNotSupported;
+    if (sm ? P.rot_static : true) W = even_width(nvec, W, nsm);
     ustage = fits(sm, true, W);
     const size_t smem = trotter_wv_smem(prec, P, nchk, sm, ustage, W);
     const int grid = (nvec + W - 1) / W, us = ustage ? 1 : 0;
@@ -1591,6 +1603,7 @@ int launch_abs_trotter_wv2(int prec, const DevTraj &T, const TrotterPlan &P, con
         while (W > 1 && bytes(false, W) > kMaxSmem) W--;
     }
     if (bytes(sm, W) > kMaxSmem) return (int)cudaErrorNotSupported;
+    W = even_width(npair, W, nsm);
     const size_t smem = bytes(sm, W);
     const int grid = (npair + W - 1) / W;
     int e;
