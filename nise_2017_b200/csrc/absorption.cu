@@ -883,26 +883,30 @@ __global__ void __launch_bounds__(NT, 1) k_abs_taylor3(DevTraj T, TaylorPlan P, 
         for (int o = 1; o < G; o <<= 1) K = max(K, __shfl_xor_sync(0xffffffffu, K, o));
         R ir = 0, ir2 = 0;
         const float2 *cf = nullptr;
+        float cen = 0.f;  // Chebyshev: the diagonal relative to the frame's centre
         if constexpr (CHEB) {
             ir = (R)P.cheb_inv_r[fl];
             ir2 = 2 * ir;
             cf = P.cheb_coef + fl * KC;
+            cen = P.cheb_center[fl];
         }
 #pragma unroll
         for (int it = 0; it < IT; it++) {
             int i = rowof(slice(it));
-            const float d = i < n ? traj_diag(T, tj, i, P.singleshift != 0) : 0.0f;
+            float d = i < n ? traj_diag(T, tj, i, P.singleshift != 0) : 0.0f;
+            if constexpr (CHEB) d = i < n ? __fsub_rn(d, cen) : 0.0f;
             if (kDgShared) {
                 if (i < n) dgs[(size_t)i * G + g] = d;
             } else {
                 dg[it] = d;
             }
             if (i < n) cur[(size_t)i * RS + g] = psi[it];
-            if constexpr (CHEB) {  // psi becomes a_0 T_0; T_0 is kept
-                const R a0 = (R)cf[0].x;
-                prev[it] = psi[it];
-                psi[it].x *= a0;
-                psi[it].y *= a0;
+            if constexpr (CHEB) {  // psi becomes a_0 T_0 (a_0 complex: the centre's phase); T_0 is kept
+                const float2 a0 = cf[0];
+                const R2 z = psi[it];
+                prev[it] = z;
+                psi[it].x = (R)a0.x * z.x - (R)a0.y * z.y;
+                psi[it].y = (R)a0.x * z.y + (R)a0.y * z.x;
             }
         }
         for (int k = 1; k <= K; k++) {
@@ -1066,22 +1070,31 @@ __global__ void __launch_bounds__(512, 2) k_abs_taylor4(DevTraj T, TaylorPlan P,
 
 // Chebyshev expansion of the exact step (FP32, sliced ELL in shared memory).
 //
-// With R_t the Gershgorin radius of frame t (max |h_ii| + max row sum of
-// |J|) and x = f R_t, exp(-i f H) = sum_k a_k T_k(H / R_t) with a_0 = J_0(x),
-// a_k = 2 (-i)^k J_k(x) (the Jacobi-Anger expansion); the T_k(H/R) psi follow
-// the three-term recurrence T_k = 2 (H/R) T_(k-1) - T_(k-2).  For the small
+// With c_t the centre of frame t's diagonal range, R_t the Gershgorin radius
+// of H - c_t (half the diagonal range + max row sum of |J|) and x = f R_t,
+// exp(-i f H) = exp(-i f c_t) sum_k a_k T_k((H - c_t) / R_t) with
+// a_0 = J_0(x), a_k = 2 (-i)^k J_k(x) (the Jacobi-Anger expansion; the phase
+// exp(-i f c_t) is folded into the stored coefficients); the
+// T_k((H - c)/R) psi follow the three-term recurrence
+// T_k = 2 ((H - c)/R) T_(k-1) - T_(k-2).  Centring shrinks R_t, so the order
+// drops for frames whose diagonal range is off centre.  For the small
 // x of a time step the Bessel coefficients fall off like (x/2)^k / k!,
 // against x^k / k! for the Taylor terms, so fewer sparse products reach the
-// same tolerance.  Per frame the prep kernel stores 1/R_t, the coefficients
-// and the order K_t (2 * sum_(k>K) |J_k(x)| <= tol).
+// same tolerance.  Per frame the prep kernel stores 1/R_t, c_t, the
+// coefficients and the order K_t (2 * sum_(k>K) |J_k(x)| <= tol).
 __global__ void k_prep_cheb(DevTraj T, TaylorPlan P, double rowabs, double f, double tol, int *order,
-                            float *inv_r, float2 *coef) {
+                            float *inv_r, float *center, float2 *coef) {
     long fi = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (fi >= P.nf) return;
     long t = P.f0 + fi;
-    double dmax = 0;
-    for (int i = 0; i < P.n; i++) dmax = fmax(dmax, fabs((double)traj_diag(T, t, i, P.singleshift != 0)));
-    double R = dmax + rowabs;
+    double lo = 0, hi = 0;
+    for (int i = 0; i < P.n; i++) {
+        const double d = (double)traj_diag(T, t, i, P.singleshift != 0);
+        lo = i ? fmin(lo, d) : d;
+        hi = i ? fmax(hi, d) : d;
+    }
+    const float cen = (float)(0.5 * (lo + hi));
+    double R = fmax(hi - (double)cen, (double)cen - lo) + rowabs;
     if (!(R > 0)) R = 1;
     const double x = fabs(f) * R;
     // J_k(x), k = 0..KMAX+8, by Miller's downward recurrence normalised with
@@ -1122,16 +1135,21 @@ __global__ void k_prep_cheb(DevTraj T, TaylorPlan P, double rowabs, double f, do
     }
     order[fi] = K;
     inv_r[fi] = (float)(1.0 / R);
+    center[fi] = cen;
+    // a_k times the phase exp(-i f c) = (pc, -ps)
+    double ps, pc;
+    sincos(f * (double)cen, &ps, &pc);
     float2 *c = coef + fi * (NISE_CHEB_KMAX + 1);
-    c[0] = make_float2((float)jv[0], 0.f);
-    for (int k = 1; k <= NISE_CHEB_KMAX; k++) {
-        float a = (float)(2 * jv[k]);
+    for (int k = 0; k <= NISE_CHEB_KMAX; k++) {
+        const double a = k ? 2 * jv[k] : jv[0];
+        double ar = 0, ai = 0;
         switch (k & 3) {  // (-i)^k
-        case 0: c[k] = make_float2(a, 0.f); break;
-        case 1: c[k] = make_float2(0.f, -a); break;
-        case 2: c[k] = make_float2(-a, 0.f); break;
-        default: c[k] = make_float2(0.f, a); break;
+        case 0: ar = a; break;
+        case 1: ai = -a; break;
+        case 2: ar = -a; break;
+        default: ai = a; break;
         }
+        c[k] = make_float2((float)(ar * pc + ai * ps), (float)(ai * pc - ar * ps));
     }
 }
 
@@ -1203,17 +1221,19 @@ __global__ void __launch_bounds__(512) k_abs_cheb3(DevTraj T, TaylorPlan P, AbsJ
         for (int o = 1; o < G; o <<= 1) K = max(K, __shfl_xor_sync(0xffffffffu, K, o));
         const float ir = inv_r[fl], ir2 = 2.f * ir;
         const float2 *cf = coef + fl * KC;
-        const float a0 = cf[0].x;
+        const float2 a0 = cf[0];  // J_0 times the centre's phase
+        const float cen = P.cheb_center[fl];
 #pragma unroll
         for (int it = 0; it < IT; it++) {
             int i = rowof(warp + NW * it);
             if (i < n) {
-                dgs[(size_t)i * G + g] = traj_diag(T, tj, i, P.singleshift != 0);
+                dgs[(size_t)i * G + g] = __fsub_rn(traj_diag(T, tj, i, P.singleshift != 0), cen);
                 cur[(size_t)i * RS + g] = psi[it];
             }
             prev[it] = psi[it];
-            psi[it].x *= a0;
-            psi[it].y *= a0;
+            const float2 z = psi[it];
+            psi[it].x = a0.x * z.x - a0.y * z.y;
+            psi[it].y = a0.x * z.y + a0.y * z.x;
         }
         for (int k = 1; k <= K; k++) {
             __syncthreads();
@@ -1921,10 +1941,12 @@ int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const Abs
 }
 
 int launch_prep_cheb(const DevTraj &T, TaylorPlan &P, double rowabs_max, double f, int *order, float *inv_r,
-                     float2 *coef, cudaStream_t s) {
-    if (P.nf) k_prep_cheb<<<(P.nf + 127) / 128, 128, 0, s>>>(T, P, rowabs_max, f, kSeriesTolF32, order, inv_r, coef);
+                     float *center, float2 *coef, cudaStream_t s) {
+    if (P.nf)
+        k_prep_cheb<<<(P.nf + 127) / 128, 128, 0, s>>>(T, P, rowabs_max, f, kSeriesTolF32, order, inv_r, center, coef);
     P.order = order;
     P.cheb_inv_r = inv_r;
+    P.cheb_center = center;
     P.cheb_coef = coef;
     return (int)cudaGetLastError();
 }

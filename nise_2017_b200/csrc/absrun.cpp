@@ -277,7 +277,7 @@ struct AbsRun {
     DevBuf<int> dtptr8, drows8, dwsl8[2], derr;
     int ell8_nslices = 0, ell8_ntg = 0, ell8_it[2] = {0, 0};
     DevBuf<char> dval, dell;
-    DevBuf<float> dinvr;
+    DevBuf<float> dinvr, dcen;
     DevBuf<float2> dcoef;
     TaylorPlan XP;
     double rowabs = 0;
@@ -789,7 +789,7 @@ int AbsRun::plan(nise_ctx *ctx, bool autotune) {
             // Chebyshev kernel: FP32, its shared-memory footprint (state, diagonal, ELL)
             const size_t csm = (size_t)N * NISE_T3_ROW * 8 + (size_t)N * 32 + (size_t)nent * 8 + 4 * (5 * nsl + 1) + 4096;
             cheb = prec == NISE_FP32 && ((csm <= 227 * 1024 && (nsl + 15) / 16 <= 32) || dtri8.p);
-            if (cheb && ((rc = dcorder.alloc(c, (size_t)nf)) || (rc = dinvr.alloc(c, (size_t)nf)) ||
+            if (cheb && ((rc = dcorder.alloc(c, (size_t)nf)) || (rc = dinvr.alloc(c, (size_t)nf)) || (rc = dcen.alloc(c, (size_t)nf)) ||
                          (rc = dcoef.alloc(c, (size_t)nf * (NISE_CHEB_KMAX + 1)))))
                 return rc;
         }
@@ -843,12 +843,14 @@ int AbsRun::run_main(cudaStream_t s, int cfg, double2 *dst) {
             if (cfg == 10 || cfg == 15) {
                 P.order = dcorder.p;
                 P.cheb_inv_r = dinvr.p;
+                P.cheb_center = dcen.p;
                 P.cheb_coef = dcoef.p;
                 P.rv_cheb = cfg == 15;
                 P.order_taylor = dorder.p;
             } else {
                 P.order = dorder.p;
                 P.cheb_inv_r = nullptr;
+                P.cheb_center = nullptr;
                 P.cheb_coef = nullptr;
             }
             P.rv_shape = cfg == 14 ? 1 : 0;
@@ -913,7 +915,7 @@ int AbsRun::tune() {
         TaylorPlan P = XP;
         if ((rc = nise_cuda(c, launch_prep_taylor(prec, T, P, rowabs, J.f, dorder.p, c->stream), "Taylor prep")))
             return rc;
-        if (cheb && (rc = nise_cuda(c, launch_prep_cheb(T, P, rowabs, J.f, dcorder.p, dinvr.p, dcoef.p, c->stream),
+        if (cheb && (rc = nise_cuda(c, launch_prep_cheb(T, P, rowabs, J.f, dcorder.p, dinvr.p, dcen.p, dcoef.p, c->stream),
                                     "Chebyshev prep")))
             return rc;
     }
@@ -957,6 +959,7 @@ int AbsRun::enqueue_waves(cudaStream_t s) {
     if (config == 15) {
         P.order = dcorder.p;
         P.cheb_inv_r = dinvr.p;
+        P.cheb_center = dcen.p;
         P.cheb_coef = dcoef.p;
         P.rv_cheb = 1;
         P.order_taylor = dorder.p;
@@ -983,7 +986,7 @@ int AbsRun::enqueue_waves(cudaStream_t s) {
         const long o = prepped - f0;
         int e = 0;
         if (config == 15) {
-            e = nise_cuda(c, launch_prep_cheb(T, Q, rowabs, J.f, dcorder.p + o, dinvr.p + o,
+            e = nise_cuda(c, launch_prep_cheb(T, Q, rowabs, J.f, dcorder.p + o, dinvr.p + o, dcen.p + o,
                                               dcoef.p + o * (NISE_CHEB_KMAX + 1), s), "Chebyshev prep");
             c->launches++;
         }
@@ -1045,7 +1048,7 @@ int AbsRun::enqueue(cudaStream_t s, bool events) {
     case SCHEME_TAYLOR: {
         TaylorPlan P = XP;
         if (config == 10 || config == 15) {
-            rc = nise_cuda(c, launch_prep_cheb(T, P, rowabs, J.f, dcorder.p, dinvr.p, dcoef.p, s), "Chebyshev prep");
+            rc = nise_cuda(c, launch_prep_cheb(T, P, rowabs, J.f, dcorder.p, dinvr.p, dcen.p, dcoef.p, s), "Chebyshev prep");
             c->launches++;
         }
         if (!rc && config != 10 && config != 15) {

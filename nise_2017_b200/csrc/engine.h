@@ -61,6 +61,7 @@ struct TaylorPlan {
     // the FP32 Chebyshev kernel): 1/R per frame and [nf][NISE_CHEB_KMAX+1]
     // complex coefficients a_k
     const float *cheb_inv_r;
+    const float *cheb_center;  // c_t: the centre subtracted from the diagonal
     const float2 *cheb_coef;
     // 4-vector variant (k_abs_taylor4, FP32): 8-row slices, entries (column * 4,
     // weight bits) as int2 [slot][row], rows [nslices][8]
@@ -141,7 +142,7 @@ int launch_abs_taylor(int prec, const DevTraj &T, const TaylorPlan &P, const Abs
 // Chebyshev coefficients of the exact step per frame (FP32 kernel); sets
 // P.order, P.cheb_inv_r and P.cheb_coef.
 int launch_prep_cheb(const DevTraj &T, TaylorPlan &P, double rowabs_max, double f, int *order, float *inv_r,
-                     float2 *coef, cudaStream_t s);
+                     float *center, float2 *coef, cudaStream_t s);
 // flag[idx] = 1 for packed off-diagonals with |J| > cut in any frame of [f0, f0+nf).
 int launch_pattern_scan(const DevTraj &T, long f0, long nf, int *flag, cudaStream_t s);
 // Sum resp[v][t] over v in order (deterministic) into out[t].

@@ -139,11 +139,12 @@ __device__ __forceinline__ void rv_stage(const DevTraj &T, const AbsJob &J, int 
 }
 
 // CHEB: the Chebyshev expansion of exp(-i H f) instead of the Taylor series
-// (tables from k_prep_cheb: per frame 1/R, R >= ||H||_2 by Gershgorin, and the
-// coefficients c_0 = J_0(fR), c_k = 2 (-i)^k J_k(fR); order by the tail of the
-// Bessel coefficients).  T_0 = psi, T_1 = (H/R) psi, T_k = 2 (H/R) T_(k-1) -
-// T_(k-2); the result is sum_k c_k T_k.  Each vector uses its own frame's R
-// and coefficients.
+// (tables from k_prep_cheb: per frame the centre c of the diagonal range,
+// 1/R with R >= ||H - c||_2 by Gershgorin, and the coefficients
+// c_0 = J_0(fR), c_k = 2 (-i)^k J_k(fR), times the phase exp(-i f c); order by
+// the tail of the Bessel coefficients).  With H' = (H - c)/R: T_0 = psi,
+// T_1 = H' psi, T_k = 2 H' T_(k-1) - T_(k-2); the result is sum_k c_k T_k.
+// Each vector uses its own frame's c, R and coefficients.
 template <int IT, int NT, bool CHEB>
 __global__ void __launch_bounds__(NT, 1)
     k_abs_taylor_rv(DevTraj T, TaylorPlan P, AbsJob J, double2 *resp, int v0, int nvec, const int *__restrict__ wsl_g) {
@@ -256,6 +257,12 @@ __global__ void __launch_bounds__(NT, 1)
             rv_rec_word(T, (long)(J.begin + sfirst + s0) * J.sample + t1, &lead0);
             rv_rec_word(T, (long)(J.begin + sfirst + s1) * J.sample + t1, &lead1);
             const float *r0 = dg + (size_t)s0 * L.dgw + lead0, *r1 = dg + (size_t)s1 * L.dgw + lead1;
+            // Chebyshev: the diagonal relative to each frame's centre c_t
+            float c0 = 0.f, c1 = 0.f;
+            if constexpr (CHEB) {
+                c0 = __ldg(P.cheb_center + (long)(J.begin + sfirst + s0) * J.sample + t1 - P.f0);
+                c1 = __ldg(P.cheb_center + (long)(J.begin + sfirst + s1) * J.sample + t1 - P.f0);
+            }
 #pragma unroll
             for (int it = 0; it < IT; it++) {
                 const int i = site(it);
@@ -267,8 +274,8 @@ __global__ void __launch_bounds__(NT, 1)
                             h1 = __fadd_rn(__fmul_rn(h1, T.shift_ab[2 * e]), T.shift_ab[2 * e + 1]);
                         }
                     }
-                    d0[it] = h0;
-                    d1[it] = h1;
+                    d0[it] = CHEB ? __fsub_rn(h0, c0) : h0;
+                    d1[it] = CHEB ? __fsub_rn(h1, c1) : h1;
                     cur[(size_t)i * 4 + c] = psi[it];  // term 0 into buffer 0
                 }
             }

@@ -42,3 +42,23 @@ def test_pair_kernel_needs_static_couplings(tmp_path):
         c.load_files()
         with pytest.raises(nise.NiseError):
             c.absorption()
+
+
+def test_warp_kernels_over_several_cta_rounds(tmp_path):
+    """A job of 4740 vectors on a 300-site lattice: more vectors than one round
+    of the widest CTAs (16 warps on 148 SMs), so the launchers narrow the CTAs
+    to spread the vectors evenly over the rounds (the warp kernel 3 rounds of
+    11 warps, the two-vector kernel 2 rounds of 9).  Every configuration gives
+    the thread-per-vector kernel's responses bitwise."""
+    n, tmax, nsamp = 300, 8, 1580
+    frames = nsamp + tmax
+    s = synth.c1_spec(n_sites=n, frames=frames, seed=830)
+    files = synth.write(s, str(tmp_path))
+    kw = synth.c1_keywords(Singles=n, Length=frames, RunTimes="%d 0 0" % tmax, Samplerate=1, Propagation="Coupling")
+    r1, i1, n1 = absorb(kw, files, kernel_config=1)
+    assert n1 == nsamp
+    for cfg in (32, 34, 0):
+        r, i, nn = absorb(kw, files, kernel_config=cfg)
+        assert nn == n1
+        assert np.array_equal(r, r1) and np.array_equal(i, i1), cfg
+    assert np.abs(r1).max() > 0
